@@ -1,0 +1,52 @@
+#!/usr/bin/env bash
+# Builds the reference's own CPU gridrec into oracle/_ref/ (test infrastructure).
+#
+#   oracle/_ref/libgridrec_ref.so     GridRec class, FP32, NR FFT  (gridrec/GPU)
+#   oracle/_ref/libgridrec_ref64.so   the same sources with float -> double,
+#                                     made on temporary copies outside the repo
+#   oracle/_ref/libgridrec_refb.so    GridrecCPP 5.2 C API (centre, sampl, filter name)
+#
+# The sources are compiled where they lie under the reference tree; nothing of
+# the reference is copied into this repository.  gridrec.cu is plain host C++
+# when USE_GRIDREC_GPU is undefined, so an empty tomo_recon_config.h suffices.
+#
+# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+set -euo pipefail
+REF="${1:-/root/reference}"
+HERE="$(cd "$(dirname "$0")" && pwd)"
+OUT="$HERE/_ref"
+GPU="$REF/gridrec/GPU"
+CPP="$REF/gridrec/GridrecCPP/Gridrec5.2"
+if [ ! -f "$GPU/gridrec.cu" ]; then
+  echo "build_ref.sh: reference not found at $REF" >&2
+  exit 1
+fi
+mkdir -p "$OUT"
+TMP="$(mktemp -d)"
+trap 'rm -rf "$TMP"' EXIT
+: > "$TMP/tomo_recon_config.h"
+CXX="${CXX:-g++}"
+FLAGS="-O2 -fPIC -shared -w -Wl,-Bsymbolic"
+
+# Oracle A: reference GridRec, FP32.
+$CXX $FLAGS -I"$TMP" -I"$GPU" -x c++ "$GPU/gridrec.cu" -x c++ \
+  "$GPU/recon_algorithm.cpp" "$GPU/fft_nr.cpp" "$HERE/ref_driver.cpp" \
+  -o "$OUT/libgridrec_ref.so"
+
+# Oracle A64: the same algorithm in double (temporary copies, sed float->double).
+mkdir -p "$TMP/f64"
+for f in gridrec.h recon_algorithm.h recon_algorithm.cpp fft.h fft_nr.cpp; do
+  sed 's/\bfloat\b/double/g' "$GPU/$f" > "$TMP/f64/$f"
+done
+sed 's/\bfloat\b/double/g' "$GPU/gridrec.cu" > "$TMP/f64/gridrec.cpp"
+cp "$TMP/tomo_recon_config.h" "$TMP/f64/"
+$CXX $FLAGS -DREAL=double -I"$TMP/f64" "$TMP/f64/gridrec.cpp" \
+  "$TMP/f64/recon_algorithm.cpp" "$TMP/f64/fft_nr.cpp" "$HERE/ref_driver.cpp" \
+  -o "$OUT/libgridrec_ref64.so"
+
+# Oracle B: GridrecCPP 5.2 (grid_io.cpp needs netCDF and is left out).
+$CXX $FLAGS -fpermissive -I"$CPP" "$CPP/grid.cpp" "$CPP/fftgr.cpp" \
+  "$CPP/filters.cpp" "$CPP/pswf.cpp" "$CPP/grid_math.cpp" "$HERE/refb_driver.cpp" \
+  -o "$OUT/libgridrec_refb.so"
+
+echo "built: $(ls "$OUT")"

@@ -1,0 +1,37 @@
+/* gridrec_oracle.h -- TEST INFRASTRUCTURE ONLY: float64 CPU restatement of the
+ * reference gridrec (see gridrec_oracle.c).  Not part of the product. */
+#ifndef GRIDREC_ORACLE_H
+#define GRIDREC_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+  int n_det, n_ang;
+  double center1, center2; /* rotation centre of slice 1 / slice 2 (pixels) */
+  int filter;              /* ReconAlgorithm codes: 0 none, 1 shlo, 2 hann, 3 hamm, 4 ramp */
+  double C;                /* PSWF parameter: 4.0, 4.2, 5.0, 6.0 or 7.0 */
+  double sampl;            /* oversampling request (1.0 = GridRec class default) */
+  int ltbl;                /* convolvent table length (512) */
+} orc_params;
+
+typedef struct {
+  long pdim, M, M02, M0;
+  double sampl, L, scale, C, lmbda;
+} orc_sizes_t;
+
+int orc_sizes(const orc_params* p, orc_sizes_t* s);
+int orc_tables(const orc_params* p, double* wtbl, double* winv);
+void orc_fft1d(double* x, long n, int sign);
+int orc_spectra(const orc_params* p, const double* sino1, const double* sino2, double* spec);
+int orc_grid(const orc_params* p, const double* theta_deg, const double* spec, double* H);
+void orc_fft2d(double* H, long M);
+int orc_deapod(const orc_params* p, const double* H, double* out1, double* out2, long out_stride);
+int orc_gridrec_pair(const orc_params* p, const double* theta_deg, const double* sino1,
+                     const double* sino2, double* out1, double* out2, long out_stride);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,205 @@
+"""ctypes access to the gridrec oracles -- TEST INFRASTRUCTURE ONLY.
+
+* ``port_*``  -- the float64 C restatement in gridrec_oracle.c (always built).
+* ``ref_*``   -- the reference's own CPU GridRec compiled from its sources into
+  ``_ref/`` by build_ref.sh: FP32 (``libgridrec_ref.so``), the FP64 sed build
+  (``libgridrec_ref64.so``) and GridrecCPP 5.2 (``libgridrec_refb.so``).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg import
+this module; the product path never does.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_REF = os.path.join(_HERE, "_ref")
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+
+
+class OrcParams(C.Structure):
+    _fields_ = [("n_det", C.c_int), ("n_ang", C.c_int), ("center1", C.c_double),
+                ("center2", C.c_double), ("filter", C.c_int), ("C", C.c_double),
+                ("sampl", C.c_double), ("ltbl", C.c_int)]
+
+
+class OrcSizes(C.Structure):
+    _fields_ = [("pdim", C.c_long), ("M", C.c_long), ("M02", C.c_long), ("M0", C.c_long),
+                ("sampl", C.c_double), ("L", C.c_double), ("scale", C.c_double),
+                ("C", C.c_double), ("lmbda", C.c_double)]
+
+
+_port = None
+
+
+def port_lib():
+    global _port
+    if _port is None:
+        path = os.path.join(_HERE, "libgridrec_oracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"oracle not built: {path} (run make -C oracle)")
+        lib = C.CDLL(path)
+        P = C.POINTER(OrcParams)
+        lib.orc_sizes.argtypes = [P, C.POINTER(OrcSizes)]
+        lib.orc_tables.argtypes = [P, _dp, C.c_void_p]
+        lib.orc_spectra.argtypes = [P, _dp, _dp, _dp]
+        lib.orc_grid.argtypes = [P, _dp, _dp, _dp]
+        lib.orc_fft1d.argtypes = [_dp, C.c_long, C.c_int]
+        lib.orc_fft2d.argtypes = [_dp, C.c_long]
+        lib.orc_fft2d.restype = None
+        lib.orc_fft1d.restype = None
+        lib.orc_deapod.argtypes = [P, _dp, _dp, _dp, C.c_long]
+        lib.orc_gridrec_pair.argtypes = [P, _dp, _dp, _dp, _dp, _dp, C.c_long]
+        _port = lib
+    return _port
+
+
+def params(n_det, n_ang, center1=None, center2=None, filter=1, C_=6.0, sampl=1.0, ltbl=512):
+    c1 = n_det / 2.0 if center1 is None else float(center1)
+    c2 = c1 if center2 is None else float(center2)
+    return OrcParams(int(n_det), int(n_ang), c1, c2, int(filter), float(C_), float(sampl),
+                     int(ltbl))
+
+
+def port_sizes(p: OrcParams) -> OrcSizes:
+    s = OrcSizes()
+    rc = port_lib().orc_sizes(C.byref(p), C.byref(s))
+    if rc:
+        raise ValueError(f"orc_sizes failed ({rc})")
+    return s
+
+
+def port_tables(p: OrcParams):
+    s = port_sizes(p)
+    wtbl = np.zeros(p.ltbl + 1)
+    winv = np.zeros(s.M0)
+    port_lib().orc_tables(C.byref(p), wtbl, winv.ctypes.data)
+    return wtbl, winv
+
+
+def port_spectra(p, sino1, sino2):
+    s = port_sizes(p)
+    J = s.pdim // 2
+    spec = np.zeros((p.n_ang, 2, J, 2))
+    rc = port_lib().orc_spectra(C.byref(p), np.ascontiguousarray(sino1, np.float64),
+                                np.ascontiguousarray(sino2, np.float64), spec)
+    if rc:
+        raise ValueError(rc)
+    return spec[..., 0] + 1j * spec[..., 1]
+
+
+def port_grid(p, theta_deg, spec):
+    s = port_sizes(p)
+    sp = np.ascontiguousarray(np.stack([spec.real, spec.imag], -1), np.float64)
+    H = np.zeros((s.M, s.M, 2))
+    rc = port_lib().orc_grid(C.byref(p), np.ascontiguousarray(theta_deg, np.float64), sp, H)
+    if rc:
+        raise ValueError(rc)
+    return H[..., 0] + 1j * H[..., 1]
+
+
+def port_fft2d(H):
+    M = H.shape[0]
+    h = np.ascontiguousarray(np.stack([H.real, H.imag], -1), np.float64)
+    port_lib().orc_fft2d(h, M)
+    return h[..., 0] + 1j * h[..., 1]
+
+
+def port_gridrec_pair(sino1, sino2, theta_deg, center1=None, center2=None, filter=1,
+                      C_=6.0, sampl=1.0, ltbl=512, out_stride=None):
+    """float64 gridrec of one pair; returns (out1, out2) of shape (M0, stride)."""
+    n_ang, n_det = sino1.shape
+    p = params(n_det, n_ang, center1, center2, filter, C_, sampl, ltbl)
+    s = port_sizes(p)
+    stride = max(n_det, s.M0) if out_stride is None else out_stride
+    o1 = np.zeros((s.M0, stride))
+    o2 = np.zeros((s.M0, stride))
+    rc = port_lib().orc_gridrec_pair(C.byref(p), np.ascontiguousarray(theta_deg, np.float64),
+                                     np.ascontiguousarray(sino1, np.float64),
+                                     np.ascontiguousarray(sino2, np.float64), o1, o2, stride)
+    if rc:
+        raise ValueError(f"orc_gridrec_pair failed ({rc})")
+    return o1, o2
+
+
+# ---------------------------------------------------------------- reference builds
+
+def ref_available() -> bool:
+    return os.path.exists(os.path.join(_REF, "libgridrec_ref.so"))
+
+
+_refs: dict = {}
+
+
+def _ref_lib(name, real):
+    if name not in _refs:
+        path = os.path.join(_REF, name)
+        if not os.path.exists(path):
+            raise RuntimeError(f"reference oracle not built: {path}")
+        lib = C.CDLL(path)
+        rp = np.ctypeslib.ndpointer(dtype=real, flags="C_CONTIGUOUS")
+        if name == "libgridrec_refb.so":
+            lib.refb_gridrec_pair.argtypes = [C.c_int, C.c_int, rp, C.c_float, C.c_char_p,
+                                              C.c_float, C.c_float, C.c_int, rp, rp, rp, rp,
+                                              C.c_int]
+            lib.refb_gridrec_pair.restype = C.c_int
+        else:
+            lib.ref_gridrec_pair.argtypes = [C.c_int, C.c_int, rp, C.c_int, rp, rp, rp, rp,
+                                             C.POINTER(C.c_double), C.POINTER(C.c_double)]
+            lib.ref_gridrec_pair.restype = C.c_int
+            lib.ref_gridrec_pairs.argtypes = [C.c_int, C.c_int, rp, C.c_int, C.c_int, rp, rp]
+            lib.ref_gridrec_pairs.restype = C.c_double
+        _refs[name] = lib
+    return _refs[name]
+
+
+def ref_gridrec_pair(sino1, sino2, theta_deg, filter=1, fp64=False):
+    """The reference GridRec class (centre n_det/2).  Returns (out1, out2, M0, t_recon)."""
+    real = np.float64 if fp64 else np.float32
+    lib = _ref_lib("libgridrec_ref64.so" if fp64 else "libgridrec_ref.so", real)
+    n_ang, n_det = sino1.shape
+    o1 = np.zeros((n_det, n_det), real)
+    o2 = np.zeros((n_det, n_det), real)
+    tr, tt = C.c_double(), C.c_double()
+    m0 = lib.ref_gridrec_pair(n_det, n_ang, np.ascontiguousarray(theta_deg, real), int(filter),
+                              np.ascontiguousarray(sino1, real),
+                              np.ascontiguousarray(sino2, real), o1, o2, C.byref(tr),
+                              C.byref(tt))
+    return o1, o2, m0, tr.value
+
+
+def ref_gridrec_pairs(sinos, theta_deg, filter=1):
+    """Reference GridRec over consecutive pairs of an (2P, n_ang, n_det) float32 stack.
+
+    Returns (outs[2P, n_det, n_det], seconds spent in reconstruct())."""
+    lib = _ref_lib("libgridrec_ref.so", np.float32)
+    n2, n_ang, n_det = sinos.shape
+    outs = np.zeros((n2, n_det, n_det), np.float32)
+    t = lib.ref_gridrec_pairs(n_det, n_ang, np.ascontiguousarray(theta_deg, np.float32),
+                              int(filter), n2 // 2, np.ascontiguousarray(sinos, np.float32),
+                              outs)
+    return outs, t
+
+
+def refb_gridrec_pair(sino1, sino2, theta_deg, center, filter_name="shlo", C_=6.0, sampl=1.2,
+                      ltbl=512):
+    """GridrecCPP 5.2 (explicit centre/sampl/filter name).  Returns (out1, out2, M0)."""
+    lib = _ref_lib("libgridrec_refb.so", np.float32)
+    n_ang, n_det = sino1.shape
+    th = np.ascontiguousarray(theta_deg, np.float32)
+    s1 = np.ascontiguousarray(sino1, np.float32)
+    s2 = np.ascontiguousarray(sino2, np.float32)
+    dummy = np.zeros(1, np.float32)
+    m0 = lib.refb_gridrec_pair(n_det, n_ang, th, center, filter_name.encode(), C_, sampl, ltbl,
+                               s1, s2, dummy, dummy, 0)
+    stride = max(m0, n_det)
+    o1 = np.zeros((m0, stride), np.float32)
+    o2 = np.zeros((m0, stride), np.float32)
+    lib.refb_gridrec_pair(n_det, n_ang, th, center, filter_name.encode(), C_, sampl, ltbl,
+                          s1, s2, o1, o2, stride)
+    return o1, o2, m0
