@@ -1,0 +1,394 @@
+#!/usr/bin/env python
+"""Throughput benchmark of the B200 gridrec hot path.
+
+Workload (one "step"): plain full-width gridrec of 256 slices, 2048 detector
+pixels x 1500 angles on [0, pi), float32 sinograms of random-ellipse phantoms
+(seed = slice index, 1e4-photon Poisson noise), per-slice rotation centres
+1024 + U[-2, 2], Hann filter, PSWF C = 6 (L = 3.82), output 2047 x 2047 valid
+in 2048-stride float32 images.  Inputs (3.1 GB per step) are larger than L2.
+
+  value  slices/s with sinograms resident in HBM (gr_reconstruct_batch)
+  e2e    slices/s through the host-buffer entry point (gr_reconstruct_host)
+         with pinned host inputs/outputs, H2D and D2H inside the timed region
+  roofline  dominant kernel's algorithmic bytes / its CUDA-event time vs the
+         measured copy bandwidth
+  cpu_baseline  the reference's own CPU GridRec (compiled from its sources into
+         oracle/_ref) on the host cores, bounded sample
+
+python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+Under torchrun each rank reconstructs its own 256 slices (weak scaling, no
+collective on the data path); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import concurrent.futures as cf
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = ("slices/s 2048²@1500 angles, learned vs plain gridrec, 1 B200, "
+          "relL2≤1e-3; %HBM peak")
+UNIT = "slices/s"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=40)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--slices", type=int, default=256)
+    ap.add_argument("--n-det", type=int, default=2048)
+    ap.add_argument("--n-ang", type=int, default=1500)
+    ap.add_argument("--max-pairs", type=int, default=16)
+    ap.add_argument("--dtype", default="f32", choices=["f32", "f16", "bf16"])
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    return ap.parse_args()
+
+
+# ------------------------------------------------------------------ helpers
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            pk = json.load(f)
+        return float(pk["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during a region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = str(device)
+        try:  # nvidia-smi numbering can differ from CUDA's: select by UUID
+            import torch
+            u = str(torch.cuda.get_device_properties(device).uuid)
+            self.device = u if u.startswith("GPU-") else "GPU-" + u
+        except Exception:
+            pass
+        self.proc = None
+        self.f = None
+
+    def __enter__(self):
+        try:
+            self.f = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", self.device], stdout=self.f,
+                stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if self.proc is None or self.f is None:
+            return None
+        self.f.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.f.read().splitlines():
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() in ("active", "1"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        loaded = [x for x in sm if x > 0.5 * max(sm)] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "samples": len(sm),
+                "reasons": sorted(reasons)}
+
+
+def make_sinograms(n_slices, n_det, n_ang, first_seed, device):
+    """Random-ellipse sinograms (seed = slice index) on the device + centres."""
+    import torch
+
+    from projects_b200 import phantom as ph
+    th = ph.angles_deg(n_ang)
+    sinos = torch.empty((n_slices, n_ang, n_det), dtype=torch.float32, device=device)
+    centers = np.zeros(n_slices, np.float32)
+    for i in range(n_slices):
+        s, c = ph.random_ellipse_sinogram(first_seed + i, n_det, n_ang, device=device)
+        sinos[i].copy_(s)
+        centers[i] = c
+    return th, sinos, centers
+
+
+def algorithmic_bytes_per_pair(n_det, n_ang, pdim, M, M0, in_bytes=4):
+    """Bytes each stage must move per slice pair (read + write), staged design."""
+    J = pdim // 2
+    spec = 2 * n_ang * J * 8
+    return {
+        "phase": J * 16,
+        "spectra": 2 * n_ang * n_det * in_bytes + spec,
+        "grid": spec + M * M * 8,
+        "cols": 2 * M * M * 8,
+        "rows_deapod": M * M * 8 + 2 * M0 * M0 * 4,
+    }
+
+
+def traffic_from_profile(stage):
+    """DRAM bytes per launch from a committed ncu summary, if one exists."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    if not os.path.exists(path):
+        return None
+    with open(path) as f:
+        t = json.load(f)
+    return t.get(stage)
+
+
+def cpu_reference(n_det, n_ang, seconds, threads=None, steps=None):
+    """The reference CPU GridRec on the host cores: returns (slices/s, info).
+
+    Each thread reconstructs slice pairs with its own GridRec instance until
+    `seconds` elapse (or `steps` rounds of one pair per thread)."""
+    from oracle import oracle as O
+    from projects_b200 import phantom as ph
+    th = ph.angles_deg(n_ang)
+    s = [ph.random_ellipse_sinogram(k, n_det, n_ang)[0] for k in range(2)]
+    pair = np.stack(s)
+    threads = threads or os.cpu_count() or 1
+    if O.ref_available():
+        kind = "reference"
+
+        def one():
+            return O.ref_gridrec_pairs(pair, th, filter=2)[1]
+    else:
+        kind = "port"
+
+        def one():
+            t0 = time.perf_counter()
+            O.port_gridrec_pair(pair[0], pair[1], th, filter=2)
+            return time.perf_counter() - t0
+
+    def worker(deadline, rounds):
+        done = 0
+        while True:
+            one()
+            done += 1
+            if rounds is not None and done >= rounds:
+                return done
+            if rounds is None and time.perf_counter() >= deadline:
+                return done
+
+    t0 = time.perf_counter()
+    with cf.ThreadPoolExecutor(threads) as ex:
+        futs = [ex.submit(worker, t0 + seconds, steps) for _ in range(threads)]
+        pairs = sum(f.result() for f in futs)
+    wall = time.perf_counter() - t0
+    return 2.0 * pairs / wall, {"kind": kind, "cores": threads, "pairs": pairs, "wall_s": wall}
+
+
+# ------------------------------------------------------------------ arms
+
+def run_reference(args, rank):
+    if rank != 0:
+        return
+    per_step = []
+    for i in range(args.warmup + args.steps):
+        v, info = cpu_reference(args.n_det, args.n_ang, 0, steps=1)
+        if i >= args.warmup:
+            per_step.append((v, info))
+    pairs = sum(i["pairs"] for _, i in per_step)
+    wall = sum(i["wall_s"] for _, i in per_step)
+    value = 2.0 * pairs / wall
+    info = per_step[0][1]
+    out = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * wall / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": f"reference CPU GridRec (FP32, NR FFT), {args.n_det} det x "
+                   f"{args.n_ang} angles, Hann; each step = one slice pair per host thread",
+                   "n_det": args.n_det, "n_ang": args.n_ang},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"],
+                         "kind": info["kind"],
+                         "sample": f"{args.steps} steps x {info['cores']} threads x 1 pair"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(out), flush=True)
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+
+    from projects_b200 import gridrec as G
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    S, n, a = args.slices, args.n_det, args.n_ang
+    th, sinos, centers = make_sinograms(S, n, a, rank * S, dev)
+    tdt = {"f32": torch.float32, "f16": torch.float16, "bf16": torch.bfloat16}[args.dtype]
+    if tdt != torch.float32:
+        sinos = sinos.to(tdt)
+    in_bytes = sinos.element_size()
+    plan = G.Plan(n, a, th, filter=G.FILTER_HANN, max_pairs=args.max_pairs, device=local_rank)
+    outs = torch.empty((S, plan.M0, n), dtype=torch.float32, device=dev)
+    centers_d = torch.from_numpy(centers).to(dev)
+    stream = torch.cuda.current_stream()
+
+    def step():
+        plan.reconstruct_batch(sinos, outs, centers=centers_d, stream=stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    l0 = plan.launches()
+    with ClockSampler(local_rank) as clk:
+        plan.set_timing(True)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            step()
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        elapsed = ev0.elapsed_time(ev1) / 1000.0
+    stage_ms, chunks = plan.stage_times()
+    plan.set_timing(False)
+    launches = plan.launches() - l0
+    if world > 1:
+        dist.barrier()
+        t = torch.tensor([elapsed], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    value = S * args.steps * world / elapsed
+
+    # roofline of the dominant kernel
+    bpp = algorithmic_bytes_per_pair(n, a, plan.pdim, plan.M, plan.M0, in_bytes)
+    pairs_timed = args.steps * ((S + 1) // 2)
+    dominant = max(stage_ms, key=stage_ms.get)
+    n_launch = chunks
+    bytes_total = bpp[dominant] * pairs_timed
+    achieved = bytes_total / (stage_ms[dominant] / 1000.0) / 1e9
+    peak, peak_src = peaks()
+    traffic = traffic_from_profile(dominant)
+    per_launch_bytes = bytes_total / max(n_launch, 1)
+    stages = {k: {"ms_per_pair": v / pairs_timed,
+                  "gbs": bpp[k] * pairs_timed / max(v / 1000.0, 1e-12) / 1e9}
+              for k, v in stage_ms.items()}
+    model_bytes_slice = (bpp["spectra"] + bpp["grid"] + bpp["cols"] + bpp["rows_deapod"]) / 2
+
+    # end to end through the host-buffer entry point
+    e2e = None
+    if not args.no_e2e:
+        h_in = torch.empty(sinos.shape, dtype=sinos.dtype).pin_memory()
+        h_in.copy_(sinos.cpu())
+        h_out = torch.empty(outs.shape, dtype=torch.float32).pin_memory()
+        plan.reconstruct_host(h_in, h_out, centers=centers, stream=int(stream.cuda_stream))
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.e2e_steps):
+            plan.reconstruct_host(h_in, h_out, centers=centers, stream=int(stream.cuda_stream))
+            float(h_out[0, plan.M0 // 2, plan.M0 // 2])   # read the result on the host
+        te = time.perf_counter() - t0
+        if world > 1:
+            t = torch.tensor([te], device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            te = float(t.item())
+        e2e = {"value": S * args.e2e_steps * world / te, "unit": UNIT,
+               "h2d_bytes_per_step": int(h_in.numel() * h_in.element_size()),
+               "d2h_bytes_per_step": int(h_out.numel() * h_out.element_size()),
+               "steps": args.e2e_steps, "path": "gr_reconstruct_host, pinned host buffers"}
+        del h_in, h_out
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, info = cpu_reference(n, a, args.cpu_seconds)
+        cpu = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
+               "sample": f"{info['pairs']} slice pairs of {n}x{a} (Hann) over "
+                         f"{info['wall_s']:.1f} s on {info['cores']} host threads"}
+
+    if rank == 0:
+        out = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * elapsed / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": {"f32": "f32", "f16": "f16 storage, f32 compute",
+                      "bf16": "bf16 storage, f32 compute"}[args.dtype],
+            "data": "synthetic (seeded random-ellipse phantoms, Poisson 1e4 photons)",
+            "config": {"workload": f"plain full-width gridrec (C=6, L={plan.L:.3f}), {S} slices "
+                                   f"of {n} det x {a} angles per step, Hann, per-slice centres "
+                                   f"{n // 2}+U[-2,2], output {plan.M0}^2 in {n}-stride f32",
+                       "n_det": n, "n_ang": a, "slices_per_step": S,
+                       "pairs_per_launch": args.max_pairs, "parallelism": f"slices x{world}",
+                       "l2": f"inputs larger than L2 ({S * a * n * in_bytes / 1e9:.1f} GB/step)"},
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
+                         "traffic": traffic, "algorithmic_bytes_per_launch": per_launch_bytes},
+            "stages": stages,
+            "pipeline": {"staged_model_bytes_per_slice": model_bytes_slice,
+                         "frac_of_hbm": model_bytes_slice * value / world / 1e9 / peak},
+            "gpu_launches": launches,
+            "clocks": clk.summary(),
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(out), flush=True)
+    plan.close()
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank)
+        return
+    import datetime
+
+    import torch.distributed as dist
+    if world > 1:
+        import torch
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_b200(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

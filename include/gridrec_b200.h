@@ -1,0 +1,180 @@
+/*
+ * gridrec_b200.h -- C ABI of the B200 (sm_100a) gridrec reconstructor.
+ *
+ * Gridrec reconstructs parallel-beam tomography slices by Fourier gridding:
+ * per projection a zero-padded 1-D FFT times filter and centre phase ramp,
+ * PSWF convolution onto an oversampled Cartesian frequency grid, a 2-D FFT,
+ * and deapodisation with a crop.  Two real slices are reconstructed per pass,
+ * packed as the real and imaginary parts of one complex signal.
+ *
+ * Everything below is plain C: pointers, sizes and status codes.  Device
+ * pointers are CUDA device addresses on the plan's device; `stream` is a
+ * cudaStream_t (NULL = the legacy default stream).  Every call returns
+ * GR_OK (0) or a negative gr_status; no call exits the process or prints.
+ *
+ * Interfaces replaced (reference, decarlof/projects):
+ *   gr_plan_create       <- GridRec::init               gridrec/GPU/gridrec.cu:216-310
+ *                           recon_init                 gridrec/GridrecCPP/Gridrec5.2/grid.cpp:54-147
+ *   gr_reconstruct_pair  <- GridRec::setSinoAndReconBuffers + GridRec::reconstruct
+ *                                                      gridrec/GPU/gridrec.cu:174-212, 314-369
+ *                           do_recon                   gridrec/GridrecCPP/Gridrec5.2/grid.cpp:152-415
+ *   gr_plan_destroy      <- GridRec::destroy           gridrec/GPU/gridrec.cu:373-422
+ *                           recon_free                 gridrec/GridrecCPP/Gridrec5.2/grid.cpp:418-434
+ *   gr_filter_code       <- get_filter (by name)       gridrec/GridrecCPP/Gridrec5.2/filters.cpp:26-48
+ *   gr_reconstruct_batch <- the slice-pair loop of GridRecSlices
+ *                                                      gridrec/GPU/tomo_recon.cpp:3702-3852
+ *   gr_reconstruct_host  <- GridRec::reconstruct on host buffers (the reference keeps
+ *                           sinograms and images in host memory, gridrec.cu:174-212)
+ *   GR_DTYPE_U16_RAW     <- flat/dark normalisation and log of the slice pipeline
+ *                                                      gridrec/GPU/tomo_recon.cpp:1533-1541
+ */
+#ifndef GRIDREC_B200_H
+#define GRIDREC_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  GR_OK = 0,
+  GR_ERR_ARG = -1,      /* invalid argument (size, pointer, stride, dtype) */
+  GR_ERR_PSWF = -2,     /* PSWF parameter C not in the database (gridrec.cu:906-922) */
+  GR_ERR_CUDA = -3,     /* a CUDA runtime call failed; see gr_last_error() */
+  GR_ERR_NOMEM = -4,    /* device or pinned host allocation failed */
+  GR_ERR_UNSUPPORTED = -5, /* size outside what the kernels implement */
+  GR_ERR_TIMEOUT = -6   /* a bounded device wait expired */
+} gr_status;
+
+/* Filter codes of ReconAlgorithm (gridrec/GPU/recon_algorithm.h:18-23).
+ * Codes 0 and 5 (and any other value) leave |x| unfiltered, i.e. a ramp,
+ * exactly like Filter::filterData (gridrec/GPU/recon_algorithm.cpp:36-48). */
+enum {
+  GR_FILTER_NONE = 0,
+  GR_FILTER_SHEPP_LOGAN = 1,
+  GR_FILTER_HANN = 2,
+  GR_FILTER_HAMMING = 3,
+  GR_FILTER_RAMP = 4,
+  GR_FILTER_FBP = 5
+};
+
+/* Sinogram element types accepted by the batched entry points. */
+typedef enum {
+  GR_DTYPE_F32 = 0,
+  GR_DTYPE_F16 = 1,
+  GR_DTYPE_BF16 = 2,
+  GR_DTYPE_U16_RAW = 3 /* raw detector counts; needs flat/dark rows, see gr_batch_desc */
+} gr_dtype;
+
+typedef struct {
+  int n_det;               /* detector pixels per projection (sinogram row length) */
+  int n_ang;               /* projections (sinogram rows) */
+  const float* theta_deg;  /* n_ang projection angles in degrees, host memory;
+                              copied at plan creation (the reference keeps the
+                              pointer, gridrec/GPU/recon_algorithm.cpp:133-137) */
+  float center;            /* rotation centre in pixels; < 0 selects n_det/2,
+                              the GridRec class default (gridrec.cu:227) */
+  int filter;              /* GR_FILTER_* */
+  float pswf_c;            /* PSWF parameter C: 4.0, 4.2, 5.0, 6.0 (default) or 7.0 */
+  float sampl;             /* oversampling request; 1.0 = GridRec class default,
+                              1.2 = GridrecCPP CLI default (grid_io.cpp:47) */
+  int ltbl;                /* convolvent table length (512) */
+  int max_pairs;           /* slice pairs processed per launch (workspace size) */
+  int device;              /* CUDA device ordinal (GridRec::setGPUDeviceID) */
+} gr_params;
+
+typedef struct gr_plan gr_plan;
+
+/* Fills *p with the GridRec class defaults for an n_det x n_ang sinogram. */
+int gr_params_default(gr_params* p, int n_det, int n_ang, const float* theta_deg);
+
+/* Filter code for a GridrecCPP filter name ("shlo", "shepp", "hann", "hamm",
+ * "hamming", "ramp", "ramlak", plus "none"); unknown names map to Shepp-Logan,
+ * the GridrecCPP default. */
+int gr_filter_code(const char* name);
+
+/* Creates a plan: sizes, FP64-built tables, the gridding work list and the
+ * device workspaces for max_pairs pairs.  Allocates device memory. */
+int gr_plan_create(const gr_params* p, gr_plan** plan);
+int gr_plan_destroy(gr_plan* plan);
+
+/* Sizes derived exactly as GridRec::init (gridrec.cu:243-268):
+ * pdim = next pow2 >= n_det; M = next pow2 >= sampl*n_det;
+ * M0 = 2*floor(M/2/sampl - 0.5) + 1 = side of the reconstructed image. */
+int gr_plan_sizes(const gr_plan* plan, int* pdim, int* M, int* M0, float* L, float* scale);
+
+/* Device bytes held by the plan (tables, work list, workspaces). */
+int gr_plan_device_bytes(const gr_plan* plan, size_t* bytes);
+
+/* One slice pair, device pointers.  sino1/sino2: n_ang x n_det float32, row
+ * stride n_det.  out1/out2: M0 rows of out_stride floats (out_stride >= M0);
+ * element [j*out_stride + k] is the reference's S[j][k] (j along the first,
+ * cos-direction, frequency axis, gridrec.cu:691-719).  Both slices use the
+ * plan's centre. */
+int gr_reconstruct_pair(gr_plan* plan, const float* sino1, const float* sino2, float* out1,
+                        float* out2, long out_stride, void* stream);
+
+/* A batch of n_slices slices (n_slices even, or odd with the last slice
+ * paired with zeros), device pointers:
+ *   sinos      n_slices sinograms, each n_ang x n_det of `dtype`, contiguous
+ *   centers    optional device array of n_slices float centres (NULL = plan centre);
+ *              the two slices of a pair may have different centres
+ *   flat, dark device rows of n_det floats (GR_DTYPE_U16_RAW only): the load
+ *              computes v = raw - dark; r = (flat - dark)/v; value = log(r) when
+ *              v > 0 and r > 0, else 0 -- the normalisation of
+ *              gridrec/GPU/tomo_recon.cpp:1533-1541 -- fused into the first kernel
+ *   outs       n_slices images, each M0 rows of out_stride floats, contiguous
+ * Pairs are processed max_pairs at a time on `stream`. */
+typedef struct {
+  int n_slices;
+  gr_dtype dtype;
+  const void* sinos;
+  const float* centers;
+  const float* flat;
+  const float* dark;
+  float* outs;
+  long out_stride;
+} gr_batch_desc;
+
+int gr_reconstruct_batch(gr_plan* plan, const gr_batch_desc* batch, void* stream);
+
+/* As gr_reconstruct_batch, with sinos, centers, flat, dark and outs in HOST
+ * memory: the sinograms stream in double-buffered chunks of max_pairs pairs
+ * through pinned staging buffers owned by the plan (host->device copies of
+ * chunk i+1 overlap the kernels of chunk i; device->host copies of images
+ * overlap likewise).  Synchronises `stream` before returning. */
+int gr_reconstruct_host(gr_plan* plan, const gr_batch_desc* batch, void* stream);
+
+/* Per-stage timing with CUDA events recorded on the launching stream around
+ * each kernel of each chunk (stages: 0 phase ramps, 1 spectra, 2 gridding,
+ * 3 first-axis FFT, 4 second-axis FFT + deapodisation).  Enabling resets
+ * the record; gr_plan_stage_times synchronises on the last event and returns
+ * the summed milliseconds per stage and the number of chunks recorded. */
+int gr_plan_set_timing(gr_plan* plan, int enable);
+int gr_plan_stage_times(gr_plan* plan, double* ms5, long* chunks);
+
+/* Host-only export of the gridding work list a plan with these parameters
+ * would use (no GPU needed).  With items/runs/splits NULL, only the counts
+ * are returned.  Layouts: items = n_items x {tile, run_begin, run_end, slot};
+ * runs = n_runs x {direction (2*angle + half), jlo, jhi}; splits = one
+ * {counter, slot0, nsplit, 0} per tile (tile = tu * tiles_v + tv, 32 x 32 cells). */
+int gr_worklist_export(const gr_params* p, int* n_items, int* n_runs, int* tiles_v, int* items,
+                       int* runs, int* splits, int cap_items, int cap_runs);
+
+/* Text of the last error recorded on this thread (never NULL). */
+const char* gr_last_error(void);
+
+/* Number of kernel launches the plan has issued since creation. */
+int gr_plan_launch_count(const gr_plan* plan, long* launches);
+
+/* Shape of the gridding work list: work items (CTAs per pair), sample runs,
+ * scratch slots of split tiles, and samples visited per pair (with halo). */
+int gr_plan_work_stats(const gr_plan* plan, int* n_items, int* n_runs, int* n_slots,
+                       long* total_samples);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GRIDREC_B200_H */

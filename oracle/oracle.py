@@ -163,6 +163,11 @@ def ref_gridrec_pair(sino1, sino2, theta_deg, filter=1, fp64=False):
     real = np.float64 if fp64 else np.float32
     lib = _ref_lib("libgridrec_ref64.so" if fp64 else "libgridrec_ref.so", real)
     n_ang, n_det = sino1.shape
+    m0 = port_sizes(params(n_det, n_ang)).M0
+    if m0 > n_det:
+        # GridRec writes M0 columns with row stride n_det (gridrec.cu:196-197,
+        # 691-719): rows overlap and the caller's n_det x n_det buffer overflows.
+        raise ValueError(f"reference GridRec needs M0 <= n_det (M0={m0}, n_det={n_det})")
     o1 = np.zeros((n_det, n_det), real)
     o2 = np.zeros((n_det, n_det), real)
     tr, tt = C.c_double(), C.c_double()
@@ -179,6 +184,8 @@ def ref_gridrec_pairs(sinos, theta_deg, filter=1):
     Returns (outs[2P, n_det, n_det], seconds spent in reconstruct())."""
     lib = _ref_lib("libgridrec_ref.so", np.float32)
     n2, n_ang, n_det = sinos.shape
+    if port_sizes(params(n_det, n_ang)).M0 > n_det:
+        raise ValueError("reference GridRec needs M0 <= n_det")
     outs = np.zeros((n2, n_det, n_det), np.float32)
     t = lib.ref_gridrec_pairs(n_det, n_ang, np.ascontiguousarray(theta_deg, np.float32),
                               int(filter), n2 // 2, np.ascontiguousarray(sinos, np.float32),

@@ -1,0 +1,111 @@
+// Internal definitions shared by the gridrec kernels and the plan code.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <string>
+#include <vector>
+
+#include "gridrec_b200.h"
+
+namespace gr {
+
+// Gridding tile: T x T grid cells per work item.
+constexpr int kTile = 32;
+// Largest number of taps per dimension the gridding kernel handles
+// (floor(L) + 1 with L = 2*C*sampl/pi < 6).
+constexpr int kMaxTaps = 6;
+// Samples per gridding work item before a tile is split across CTAs.
+constexpr int kItemCap = 6144;
+
+// One run of samples: direction d (= 2*angle + half), samples j in [jlo, jhi].
+struct Run {
+  int dir;
+  int jlo;
+  int jhi;
+};
+
+// One gridding work item: runs [run_begin, run_end) of `tile`; slot >= 0 when
+// the tile is split over several items (partial tile written to scratch slot).
+struct Item {
+  int tile;
+  int run_begin;
+  int run_end;
+  int slot;
+};
+
+// Per split tile: counter index, first scratch slot, number of items.
+struct Split {
+  int counter;
+  int slot0;
+  int nsplit;
+  int pad;
+};
+
+struct SpectraArgs {
+  const void* s1;        // slice 1 of pair 0
+  const void* s2;        // slice 2 of pair 0
+  long pair_stride;      // elements between consecutive pairs' sinograms
+  int n_slices_valid;    // slices that exist (2*pairs or 2*pairs-1)
+  int slice_base;        // global index of slice 1 of pair 0 (for centres)
+  const float* flat;     // u16 raw only
+  const float* dark;
+  const float4* pq;      // [pair][J] (P.re, P.im, Q.re, Q.im)
+  float2* spec;          // [pair][n_ang][2][J]
+  const float2* tw;      // pdim twiddles exp(+2 pi i k/pdim)
+  int n_det, n_ang, pdim, J, pairs;
+};
+
+struct PhaseArgs {
+  const float* centers;  // device, per slice (may be null)
+  float center_default;
+  int slice_base;
+  int n_slices_valid;
+  const float* filt;     // [J] filter * pi/(pdim*n_ang)
+  float4* pq;
+  int J, pdim, pairs;
+};
+
+struct GridArgs {
+  const float2* spec;
+  float2* H;             // [pair][M][M]
+  float2* scratch;       // [pair][n_slots][T*T]
+  unsigned* counters;    // [pair][n_split]
+  const Item* items;
+  const Run* runs;
+  const Split* splits;   // per tile index (only meaningful when slot >= 0)
+  const float2* dir;     // per direction (scale*dx, scale*dy)
+  const float* wtbl;     // ltbl + 1
+  int n_items, pairs, n_ang, J, M, tiles_v, n_slots, n_split, ltbl;
+  float L2, tblspcg;
+};
+
+struct ColArgs {
+  float2* H;
+  const float2* tw;      // M twiddles exp(+2 pi i k/M)
+  int M, pairs;
+};
+
+struct RowArgs {
+  const float2* H;
+  const float2* tw;
+  const float* winv;     // M0
+  float* out1;           // slice 1 of pair 0
+  float* out2;
+  long pair_stride;      // floats between consecutive pairs' images
+  long out_stride;
+  int n_slices_valid;
+  int M, M0, M02, pairs;
+};
+
+// Kernel launchers (gridrec_kernels.cu).  Return cudaGetLastError().
+cudaError_t init_kernel_attributes();
+cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t s);
+cudaError_t launch_spectra(const SpectraArgs& a, gr_dtype dt, cudaStream_t s);
+cudaError_t launch_grid(const GridArgs& a, int ntaps, cudaStream_t s);
+int cols_group(int M);
+cudaError_t launch_cols(const ColArgs& a, cudaStream_t s);
+cudaError_t launch_rows(const RowArgs& a, cudaStream_t s);
+
+}  // namespace gr

@@ -1,0 +1,534 @@
+// sm_100a kernels of the gridrec pipeline.
+//
+//   phase_kernel    per pair: filter x centre phase ramps P_j, Q_j (FP64 -> FP32)
+//   spectra_kernel  per (pair, angle): load (f32/f16/bf16/u16 raw with fused
+//                   flat/dark + log), pack slice 1 + i*slice 2, zero-pad to
+//                   pdim, shared-memory Stockham FFT exp(+i), filter/phase
+//                   multiply -> filtered samples C1_j, C2_j
+//                   (gridrec/GPU/gridrec.cu:500-538)
+//   grid_kernel     per (tile work item, pair): binned gather of all samples
+//                   whose PSWF footprint meets a 32x32 tile of the M x M grid,
+//                   accumulated in shared memory, tile written once
+//                   (gridrec.cu:540-576; no global atomics)
+//   cols_kernel     per (column group, pair): Stockham FFT exp(-i) along the
+//                   first grid axis, in place (first half of gridrec.cu:641-646)
+//   rows_kernel     per (grid row, pair): Stockham FFT exp(-i) along the second
+//                   axis fused with deapodisation winv[j]*winv[k], the
+//                   four-corner crop and the split into two real images
+//                   (gridrec.cu:641-646 + 691-719)
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+
+#include "gr_internal.h"
+
+namespace gr {
+
+// ------------------------------------------------------------------ complex helpers
+
+__device__ __forceinline__ float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ float2 cmul(float2 a, float2 b) {
+  return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x));
+}
+// a * (S * i)
+template <int S>
+__device__ __forceinline__ float2 mul_si(float2 a) {
+  return S > 0 ? make_float2(-a.y, a.x) : make_float2(a.y, -a.x);
+}
+// a * exp(S * 2 pi i m / 16) for the compile-time constant m used by dft16/dft8
+template <int S, int m>
+__device__ __forceinline__ float2 tw16(float2 a) {
+  constexpr float c1 = 0.92387953251128676f, c2 = 0.70710678118654752f, c3 = 0.38268343236508977f;
+  constexpr float cs[10] = {1.f, c1, c2, c3, 0.f, -c3, -c2, -c1, -1.f, -c1};
+  constexpr float sn[10] = {0.f, c3, c2, c1, 1.f, c1, c2, c3, 0.f, -c3};
+  if constexpr (m == 0) {
+    return a;
+  } else if constexpr (m == 4) {
+    return mul_si<S>(a);
+  } else if constexpr (m == 8) {
+    return make_float2(-a.x, -a.y);
+  } else {
+    return cmul(a, make_float2(cs[m], S * sn[m]));
+  }
+}
+
+// Shared-memory index with one pad slot per 16 elements (bank-conflict-free
+// radix-16 Stockham stores).
+__device__ __forceinline__ int phys(int i) { return i + (i >> 4); }
+
+// ------------------------------------------------------------------ in-register DFTs
+// Natural order in and out: v[k] <- sum_n v[n] exp(S 2 pi i n k / R).
+
+template <int S>
+__device__ __forceinline__ void dft2(float2* v) {
+  float2 a = v[0], b = v[1];
+  v[0] = cadd(a, b);
+  v[1] = csub(a, b);
+}
+
+template <int S>
+__device__ __forceinline__ void dft4(float2& a0, float2& a1, float2& a2, float2& a3) {
+  float2 t0 = cadd(a0, a2), t1 = csub(a0, a2), t2 = cadd(a1, a3), t3 = mul_si<S>(csub(a1, a3));
+  a0 = cadd(t0, t2);
+  a2 = csub(t0, t2);
+  a1 = cadd(t1, t3);
+  a3 = csub(t1, t3);
+}
+
+template <int S>
+__device__ __forceinline__ void dft4(float2* v) { dft4<S>(v[0], v[1], v[2], v[3]); }
+
+// R = 8 as 2 x 4: n = 2 n2 + n1, k = k1 + 4 k2.
+template <int S>
+__device__ __forceinline__ void dft8(float2* v) {
+  dft4<S>(v[0], v[2], v[4], v[6]);  // n1 = 0 -> Y0[k1] at v[2 k1]
+  dft4<S>(v[1], v[3], v[5], v[7]);  // n1 = 1 -> Y1[k1] at v[2 k1 + 1]
+  float2 y1[4] = {v[1], tw16<S, 2>(v[3]), tw16<S, 4>(v[5]), tw16<S, 6>(v[7])};
+  float2 y0[4] = {v[0], v[2], v[4], v[6]};
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) {
+    v[k1] = cadd(y0[k1], y1[k1]);
+    v[k1 + 4] = csub(y0[k1], y1[k1]);
+  }
+}
+
+// R = 16 as 4 x 4: n = 4 n2 + n1, k = k1 + 4 k2.
+template <int S>
+__device__ __forceinline__ void dft16(float2* v) {
+#pragma unroll
+  for (int n1 = 0; n1 < 4; ++n1) dft4<S>(v[n1], v[4 + n1], v[8 + n1], v[12 + n1]);
+  // Y[n1][k1] sits at v[4 k1 + n1]; twiddle by W16^(n1 k1)
+  v[5] = tw16<S, 1>(v[5]);
+  v[6] = tw16<S, 2>(v[6]);
+  v[7] = tw16<S, 3>(v[7]);
+  v[9] = tw16<S, 2>(v[9]);
+  v[10] = tw16<S, 4>(v[10]);
+  v[11] = tw16<S, 6>(v[11]);
+  v[13] = tw16<S, 3>(v[13]);
+  v[14] = tw16<S, 6>(v[14]);
+  v[15] = tw16<S, 9>(v[15]);
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1) dft4<S>(v[4 * k1], v[4 * k1 + 1], v[4 * k1 + 2], v[4 * k1 + 3]);
+  // now v[4 k1 + k2] = X[k1 + 4 k2]: transpose the 4 x 4 register block
+  float2 t[16];
+#pragma unroll
+  for (int i = 0; i < 16; ++i) t[i] = v[i];
+#pragma unroll
+  for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) v[k1 + 4 * k2] = t[4 * k1 + k2];
+}
+
+template <int R, int S>
+__device__ __forceinline__ void dftR(float2* v) {
+  if constexpr (R == 16) dft16<S>(v);
+  else if constexpr (R == 8) dft8<S>(v);
+  else if constexpr (R == 4) dft4<S>(v);
+  else dft2<S>(v);
+}
+
+// ------------------------------------------------------------------ block Stockham FFT
+// One line of N = 2^m (m >= 4) complex values in shared memory (phys()
+// layout), transformed in place by nthr = N/16 threads, each holding 16
+// values per pass.  Pass with radix R and span Ns (Ns = product of earlier
+// radices): butterfly j reads x[j + r N/R], twiddles by exp(S 2 pi i r k /(Ns R)),
+// k = j mod Ns, and writes x[(j - k) R + k + r Ns].  tw[t] = exp(+2 pi i t/N).
+
+template <int R, int S>
+__device__ __forceinline__ void stockham_pass(float2* buf, int N, int Ns, int tid, int nthr,
+                                              const float2* __restrict__ tw) {
+  constexpr int B = 16 / R;
+  float2 v[16];
+  const int NR = N / R;
+#pragma unroll
+  for (int i = 0; i < B; ++i) {
+    const int j = tid + i * nthr;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[i * R + r] = buf[phys(j + r * NR)];
+  }
+  __syncthreads();
+  const int tstep = N / (Ns * R);
+#pragma unroll
+  for (int i = 0; i < B; ++i) {
+    const int j = tid + i * nthr;
+    const int k = j & (Ns - 1);
+    if (Ns > 1) {
+      // powers w^r of w = exp(S 2 pi i k/(Ns R)): w, w^2, w^4, w^8 from the
+      // table, the rest as products of at most two table entries
+      float2 w[16];
+      const int e = k * tstep;
+      w[1] = __ldg(&tw[e]);
+      if constexpr (R >= 4) w[2] = __ldg(&tw[2 * e]);
+      if constexpr (R >= 8) w[4] = __ldg(&tw[4 * e]);
+      if constexpr (R >= 16) w[8] = __ldg(&tw[8 * e]);
+      if constexpr (R >= 4) w[3] = cmul(w[1], w[2]);
+      if constexpr (R >= 8) {
+        w[5] = cmul(w[1], w[4]);
+        w[6] = cmul(w[2], w[4]);
+        w[7] = cmul(w[3], w[4]);
+      }
+      if constexpr (R >= 16) {
+#pragma unroll
+        for (int r = 9; r < 16; ++r) w[r] = cmul(w[r - 8], w[8]);
+      }
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        float2 ww = w[r];
+        if (S < 0) ww.y = -ww.y;
+        v[i * R + r] = cmul(v[i * R + r], ww);
+      }
+    }
+    dftR<R, S>(&v[i * R]);
+    const int base = (j - k) * R + k;
+#pragma unroll
+    for (int r = 0; r < R; ++r) buf[phys(base + r * Ns)] = v[i * R + r];
+  }
+  __syncthreads();
+}
+
+template <int S>
+__device__ __forceinline__ void block_fft(float2* buf, int N, int tid, int nthr,
+                                          const float2* __restrict__ tw) {
+  int m = 31 - __clz(N);
+  int Ns = 1;
+  for (; m >= 4; m -= 4) {
+    stockham_pass<16, S>(buf, N, Ns, tid, nthr, tw);
+    Ns <<= 4;
+  }
+  if (m == 3) stockham_pass<8, S>(buf, N, Ns, tid, nthr, tw);
+  else if (m == 2) stockham_pass<4, S>(buf, N, Ns, tid, nthr, tw);
+  else if (m == 1) stockham_pass<2, S>(buf, N, Ns, tid, nthr, tw);
+}
+
+// ------------------------------------------------------------------ phase ramps
+
+__global__ void phase_kernel(PhaseArgs a) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  const int pair = blockIdx.y;
+  if (j >= a.J) return;
+  const int s1 = a.slice_base + 2 * pair;
+  const int s2 = s1 + 1;
+  double c1 = a.centers ? (double)a.centers[s1] : (double)a.center_default;
+  double c2 = (a.centers && (2 * pair + 1) < a.n_slices_valid) ? (double)a.centers[s2] : c1;
+  // e_k = exp(-2 pi i j c_k / pdim) in FP64
+  double sn1, cs1, sn2, cs2;
+  sincospi(-2.0 * (double)j * c1 / (double)a.pdim, &sn1, &cs1);
+  sincospi(-2.0 * (double)j * c2 / (double)a.pdim, &sn2, &cs2);
+  const double f = 0.5 * (double)a.filt[j];
+  a.pq[(size_t)pair * a.J + j] =
+      make_float4((float)(f * (cs1 + cs2)), (float)(f * (sn1 + sn2)), (float)(f * (cs1 - cs2)),
+                  (float)(f * (sn1 - sn2)));
+}
+
+// ------------------------------------------------------------------ spectra (K1)
+
+template <typename T>
+__device__ __forceinline__ float load_sino(const T* row, int k, const float*, const float*);
+template <>
+__device__ __forceinline__ float load_sino<float>(const float* row, int k, const float*, const float*) {
+  return __ldg(&row[k]);
+}
+template <>
+__device__ __forceinline__ float load_sino<__half>(const __half* row, int k, const float*, const float*) {
+  return __half2float(row[k]);
+}
+template <>
+__device__ __forceinline__ float load_sino<__nv_bfloat16>(const __nv_bfloat16* row, int k,
+                                                          const float*, const float*) {
+  return __bfloat162float(row[k]);
+}
+// Raw uint16 counts with flat/dark: the normalisation of
+// gridrec/GPU/tomo_recon.cpp:1533-1541 (log((flat-dark)/(raw-dark)), 0 when
+// raw <= dark or the ratio is not positive).
+template <>
+__device__ __forceinline__ float load_sino<uint16_t>(const uint16_t* row, int k, const float* flat,
+                                                     const float* dark) {
+  const float d = __ldg(&dark[k]);
+  const float v = (float)row[k] - d;
+  if (v <= 0.f) return 0.f;
+  const float r = (__ldg(&flat[k]) - d) / v;
+  return r > 0.f ? logf(r) : 0.f;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(512) spectra_kernel(SpectraArgs a) {
+  extern __shared__ float2 sm[];
+  const int n = blockIdx.x, pair = blockIdx.y;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const T* r1 = static_cast<const T*>(a.s1) + pair * a.pair_stride + (long)n * a.n_det;
+  const T* r2 = (2 * pair + 1 < a.n_slices_valid)
+                    ? static_cast<const T*>(a.s2) + pair * a.pair_stride + (long)n * a.n_det
+                    : nullptr;
+  for (int k = tid; k < a.pdim; k += nthr) {
+    float x = 0.f, y = 0.f;
+    if (k < a.n_det) {
+      x = load_sino<T>(r1, k, a.flat, a.dark);
+      if (r2) y = load_sino<T>(r2, k, a.flat, a.dark);
+    }
+    sm[phys(k)] = make_float2(x, y);
+  }
+  __syncthreads();
+  block_fft<+1>(sm, a.pdim, tid, nthr, a.tw);
+  const float4* pq = a.pq + (size_t)pair * a.J;
+  float2* o1 = a.spec + ((size_t)pair * a.n_ang + n) * 2 * a.J;
+  float2* o2 = o1 + a.J;
+  for (int j = tid; j < a.J; j += nthr) {
+    float2 c1 = make_float2(0.f, 0.f), c2 = make_float2(0.f, 0.f);
+    if (j > 0) {
+      const float2 F = sm[phys(j)];
+      const float2 G = sm[phys(a.pdim - j)];
+      const float4 q = __ldg(&pq[j]);  // P = (x, y), Q = (z, w)
+      // C1 = P F + Q conj(G);  C2 = conj(P) G + conj(Q) conj(F)
+      c1.x = q.x * F.x - q.y * F.y + q.z * G.x + q.w * G.y;
+      c1.y = q.x * F.y + q.y * F.x - q.z * G.y + q.w * G.x;
+      c2.x = q.x * G.x + q.y * G.y + q.z * F.x - q.w * F.y;
+      c2.y = q.x * G.y - q.y * G.x - q.z * F.y - q.w * F.x;
+    }
+    o1[j] = c1;
+    o2[j] = c2;
+  }
+}
+
+// ------------------------------------------------------------------ gridding (K2)
+// Gather formulation: the CTA owns one kTile x kTile tile of H and visits the
+// samples of its work item (runs of consecutive j along one direction, built
+// on the host from the exact ray/tile geometry).  Each sample adds
+// w(|u - iu|) w(|v - iv|) C to every cell of the tile within L/2 in both
+// coordinates, the tap set and nearest-neighbour table index of
+// gridrec.cu:546-566.  The second half of the reference's scatter
+// (H[M-iu][M-iv] += w C2) is the direction d = 2n+1 at the mirrored position.
+// Cells in row 0 or column 0 stay zero (the reference clamps taps to [1, M-1]).
+
+template <int NT>
+__global__ void __launch_bounds__(256) grid_kernel(GridArgs a) {
+  __shared__ float acc_re[kTile * kTile];
+  __shared__ float acc_im[kTile * kTile];
+  __shared__ float s_wtbl[1025];
+  __shared__ int s_last;
+  const int item_idx = blockIdx.x / a.pairs;
+  const int pair = blockIdx.x - item_idx * a.pairs;
+  const Item it = a.items[item_idx];
+  const int tu = it.tile / a.tiles_v, tv = it.tile - (it.tile / a.tiles_v) * a.tiles_v;
+  const int p0 = tu * kTile, q0 = tv * kTile;
+  for (int i = threadIdx.x; i < kTile * kTile; i += blockDim.x) {
+    acc_re[i] = 0.f;
+    acc_im[i] = 0.f;
+  }
+  for (int i = threadIdx.x; i <= a.ltbl; i += blockDim.x) s_wtbl[i] = __ldg(&a.wtbl[i]);
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  const float half_m = (float)(a.M / 2);
+  const float offu = half_m - (float)p0, offv = half_m - (float)q0;
+  const float L2 = a.L2, ts = a.tblspcg;
+  const int ltbl = a.ltbl;
+  const float2* specp = a.spec + (size_t)pair * a.n_ang * 2 * a.J;
+  for (int r = it.run_begin + warp; r < it.run_end; r += nwarps) {
+    const Run run = a.runs[r];
+    const float2 d = __ldg(&a.dir[run.dir]);
+    const float2* sp = specp + (size_t)run.dir * a.J;
+    for (int j = run.jlo + lane; j <= run.jhi; j += 32) {
+      const float fj = (float)j;
+      const float u = fmaf(fj, d.x, offu);
+      const float v = fmaf(fj, d.y, offv);
+      const float fu0 = ceilf(u - L2), fv0 = ceilf(v - L2);
+      const int iu0 = (int)fu0, iv0 = (int)fv0;
+      if (iu0 >= kTile || iv0 >= kTile || iu0 + NT <= 0 || iv0 + NT <= 0) continue;
+      const float2 c = __ldg(&sp[j]);
+      float wu[NT], wv[NT];
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        const float du = fabsf(u - (fu0 + (float)t));
+        const int row = iu0 + t;
+        wu[t] = (du <= L2 && row >= 0 && row < kTile) ? s_wtbl[min((int)(du * ts + 0.5f), ltbl)] : 0.f;
+        const float dv = fabsf(v - (fv0 + (float)t));
+        const int col = iv0 + t;
+        wv[t] = (dv <= L2 && col >= 0 && col < kTile) ? s_wtbl[min((int)(dv * ts + 0.5f), ltbl)] : 0.f;
+      }
+#pragma unroll
+      for (int t = 0; t < NT; ++t) {
+        if (wu[t] != 0.f) {
+          const float cr = wu[t] * c.x, ci = wu[t] * c.y;
+          const int rowoff = (iu0 + t) * kTile + iv0;
+#pragma unroll
+          for (int s = 0; s < NT; ++s) {
+            if (wv[s] != 0.f) {
+              atomicAdd(&acc_re[rowoff + s], wv[s] * cr);
+              atomicAdd(&acc_im[rowoff + s], wv[s] * ci);
+            }
+          }
+        }
+      }
+    }
+  }
+  __syncthreads();
+  const int np = min(kTile, a.M - p0), nq = min(kTile, a.M - q0);
+  float2* Hp = a.H + (size_t)pair * a.M * a.M;
+  if (it.slot < 0) {
+    for (int i = threadIdx.x; i < kTile * kTile; i += blockDim.x) {
+      const int pr = i / kTile, qc = i - (i / kTile) * kTile;
+      if (pr < np && qc < nq) {
+        const int p = p0 + pr, q = q0 + qc;
+        const float2 val = (p == 0 || q == 0) ? make_float2(0.f, 0.f) : make_float2(acc_re[i], acc_im[i]);
+        Hp[(size_t)p * a.M + q] = val;
+      }
+    }
+    return;
+  }
+  // Split tile: publish this item's partial tile; the last item of the tile
+  // to finish sums all partials in slot order (deterministic) and writes H.
+  float2* part = a.scratch + ((size_t)pair * a.n_slots + it.slot) * (kTile * kTile);
+  for (int i = threadIdx.x; i < kTile * kTile; i += blockDim.x)
+    part[i] = make_float2(acc_re[i], acc_im[i]);
+  __threadfence();
+  __syncthreads();
+  const Split sp = a.splits[it.tile];
+  if (threadIdx.x == 0) {
+    const unsigned prev = atomicAdd(&a.counters[(size_t)pair * a.n_split + sp.counter], 1u);
+    s_last = (prev == (unsigned)(sp.nsplit - 1));
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  const float2* base = a.scratch + ((size_t)pair * a.n_slots + sp.slot0) * (kTile * kTile);
+  for (int i = threadIdx.x; i < kTile * kTile; i += blockDim.x) {
+    const int pr = i / kTile, qc = i - (i / kTile) * kTile;
+    if (pr < np && qc < nq) {
+      float sr = 0.f, si = 0.f;
+      for (int k = 0; k < sp.nsplit; ++k) {
+        const float2 t = __ldcg(&base[(size_t)k * (kTile * kTile) + i]);
+        sr += t.x;
+        si += t.y;
+      }
+      const int p = p0 + pr, q = q0 + qc;
+      Hp[(size_t)p * a.M + q] = (p == 0 || q == 0) ? make_float2(0.f, 0.f) : make_float2(sr, si);
+    }
+  }
+  if (threadIdx.x == 0) a.counters[(size_t)pair * a.n_split + sp.counter] = 0u;
+}
+
+// ------------------------------------------------------------------ 2-D FFT, first axis (K3)
+// G columns of H per CTA, each a contiguous shared-memory line of stride LP.
+
+__global__ void __launch_bounds__(512) cols_kernel(ColArgs a, int G) {
+  extern __shared__ float2 sm[];
+  const int M = a.M;
+  const int LP = M + (M >> 4) + 1;
+  const int q0 = blockIdx.x * G, pair = blockIdx.y;
+  const int per_line = M >> 4;
+  const int line = threadIdx.x / per_line, tl = threadIdx.x - line * per_line;
+  float2* Hp = a.H + (size_t)pair * M * M;
+  for (int i = threadIdx.x; i < G * M; i += blockDim.x) {
+    const int p = i / G, g = i - (i / G) * G;
+    sm[g * LP + phys(p)] = Hp[(size_t)p * M + q0 + g];
+  }
+  __syncthreads();
+  block_fft<-1>(sm + line * LP, M, tl, per_line, a.tw);
+  for (int i = threadIdx.x; i < G * M; i += blockDim.x) {
+    const int p = i / G, g = i - (i / G) * G;
+    Hp[(size_t)p * M + q0 + g] = sm[g * LP + phys(p)];
+  }
+}
+
+// ------------------------------------------------------------------ second axis + deapod (K4)
+
+__global__ void __launch_bounds__(512) rows_kernel(RowArgs a) {
+  extern __shared__ float2 sm[];
+  const int M = a.M;
+  const int iu = blockIdx.x, pair = blockIdx.y;
+  const float2* row = a.H + ((size_t)pair * M + iu) * M;
+  for (int q = threadIdx.x; q < M; q += blockDim.x) sm[phys(q)] = row[q];
+  __syncthreads();
+  block_fft<-1>(sm, M, threadIdx.x, blockDim.x, a.tw);
+  // iu = (j - M02) mod M  (gridrec.cu:694-719)
+  int j = iu + a.M02;
+  if (j >= M) j -= M;
+  if (j >= a.M0) return;
+  const float wj = __ldg(&a.winv[j]);
+  float* o1 = a.out1 + pair * a.pair_stride + (long)j * a.out_stride;
+  float* o2 = (2 * pair + 1 < a.n_slices_valid) ? a.out2 + pair * a.pair_stride + (long)j * a.out_stride
+                                                : nullptr;
+  for (int k = threadIdx.x; k < a.M0; k += blockDim.x) {
+    int iv = k - a.M02;
+    if (iv < 0) iv += M;
+    const float2 h = sm[phys(iv)];
+    const float c = wj * __ldg(&a.winv[k]);
+    o1[k] = c * h.x;
+    if (o2) o2[k] = c * h.y;
+  }
+}
+
+// ------------------------------------------------------------------ launchers
+
+static int fft_smem_bytes(int N) { return (N + (N >> 4)) * (int)sizeof(float2); }
+
+// Allows the dynamic-shared-memory kernels the device's opt-in maximum; called
+// once per device at plan creation so that launches need no attribute calls
+// (and can be captured in a CUDA graph).
+cudaError_t init_kernel_attributes() {
+  int dev = 0, optin = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const void* fns[] = {(const void*)spectra_kernel<float>, (const void*)spectra_kernel<__half>,
+                       (const void*)spectra_kernel<__nv_bfloat16>,
+                       (const void*)spectra_kernel<uint16_t>, (const void*)cols_kernel,
+                       (const void*)rows_kernel};
+  for (const void* f : fns) {
+    if (e != cudaSuccess) break;
+    e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  }
+  return e;
+}
+
+cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t s) {
+  dim3 grid((a.J + 255) / 256, a.pairs);
+  phase_kernel<<<grid, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+template <typename T>
+static cudaError_t launch_spectra_t(const SpectraArgs& a, cudaStream_t s) {
+  const int smem = fft_smem_bytes(a.pdim);
+  dim3 grid(a.n_ang, a.pairs);
+  spectra_kernel<T><<<grid, a.pdim / 16, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_spectra(const SpectraArgs& a, gr_dtype dt, cudaStream_t s) {
+  switch (dt) {
+    case GR_DTYPE_F32: return launch_spectra_t<float>(a, s);
+    case GR_DTYPE_F16: return launch_spectra_t<__half>(a, s);
+    case GR_DTYPE_BF16: return launch_spectra_t<__nv_bfloat16>(a, s);
+    case GR_DTYPE_U16_RAW: return launch_spectra_t<uint16_t>(a, s);
+  }
+  return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_grid(const GridArgs& a, int ntaps, cudaStream_t s) {
+  if (a.n_items == 0) return cudaSuccess;
+  dim3 grid((unsigned)a.n_items * (unsigned)a.pairs);
+  if (ntaps <= 4) grid_kernel<4><<<grid, 256, 0, s>>>(a);
+  else grid_kernel<kMaxTaps><<<grid, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+int cols_group(int M) {
+  int g = 8192 / M;
+  return g < 1 ? 1 : (g > 8 ? 8 : g);
+}
+
+cudaError_t launch_cols(const ColArgs& a, cudaStream_t s) {
+  const int G = cols_group(a.M);
+  const int smem = G * (a.M + (a.M >> 4) + 1) * (int)sizeof(float2);
+  dim3 grid(a.M / G, a.pairs);
+  cols_kernel<<<grid, G * (a.M / 16), smem, s>>>(a, G);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rows(const RowArgs& a, cudaStream_t s) {
+  const int smem = fft_smem_bytes(a.M);
+  dim3 grid(a.M, a.pairs);
+  rows_kernel<<<grid, a.M / 16, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+}  // namespace gr

@@ -1,0 +1,820 @@
+// Host side of the gridrec C ABI: plan creation (sizes, FP64 tables, the
+// gridding work list, device workspaces), the per-chunk launch sequence, and
+// the host-memory streaming entry point.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "gr_internal.h"
+
+namespace gr {
+
+namespace {
+
+thread_local std::string g_err = "no error";
+
+int fail(int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  g_err = buf;
+  return code;
+}
+
+#define GR_CUDA(call)                                                                   \
+  do {                                                                                  \
+    cudaError_t e_ = (call);                                                            \
+    if (e_ != cudaSuccess)                                                              \
+      return fail(GR_ERR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(e_), \
+                  __FILE__, __LINE__);                                                  \
+  } while (0)
+
+// PSWF database: the numerical table of gridrec/GPU/gridrec.cu:21-114 (C,
+// eigenvalue, Legendre degree, even-order Legendre coefficients).
+struct Pswf {
+  double C, lmbda;
+  int nt;
+  double coefs[11];
+};
+const Pswf kPswfDb[5] = {
+    {4.0, 0.99588549, 16,
+     {0.5239891E+01, -0.5308499E+01, 0.1184591E+01, -0.1230763E-00, 0.7371623E-02,
+      -0.2864074E-03, 0.7789983E-05, -0.1564700E-06, 0.2414647E-08, 0.0, 0.0}},
+    {4.2, 0.99657887, 16,
+     {0.6062942E+01, -0.6450252E+01, 0.1551875E+01, -0.1755960E-01, 0.1150712E-01,
+      -0.4903653E-03, 0.1464986E-04, -0.3235110E-06, 0.5492141E-08, 0.0, 0.0}},
+    {5.0, 0.99935241, 18,
+     {0.1115509E+02, -0.1384861E+02, 0.4289811E+01, -0.6514303E-00, 0.5844993E-01,
+      -0.3447736E-02, 0.1435066E-03, -0.4433680E-05, 0.1056040E-06, -0.1997173E-08, 0.0}},
+    {6.0, 0.9990188, 18,
+     {0.2495593E+02, -0.3531124E+02, 0.1383722E+02, -0.2799028E+01, 0.3437217E-00,
+      -0.2818024E-01, 0.1645842E-02, -0.7179160E-04, 0.2424510E-05, -0.6520875E-07, 0.0}},
+    {7.0, 0.99998546, 20,
+     {0.5767616E+02, -0.8931343E+02, 0.4167596E+02, -0.1053599E+02, 0.1662374E+01,
+      -0.1780527E-00, 0.1372983E-01, -0.7963169E-03, 0.3593372E-04, -0.1295941E-05,
+      0.3817796E-07}},
+};
+
+const Pswf* find_pswf(double C) {
+  for (const Pswf& p : kPswfDb)
+    if (std::fabs(C - p.C) <= 0.01) return &p;
+  return nullptr;
+}
+
+// Sum_k coefs[k] P_2k(x) via the Legendre three-term recurrence.
+double legendre_even(const Pswf& p, double x) {
+  double y = p.coefs[0], penult = 1.0, last = x;
+  int k = 1;
+  for (int j = 2; j <= p.nt; ++j) {
+    const double nw = (x * (2 * j - 1) * last - (j - 1) * penult) / j;
+    if ((j & 1) == 0) y += nw * p.coefs[k++];
+    penult = last;
+    last = nw;
+  }
+  return y;
+}
+
+// Filter::filterData semantics (gridrec/GPU/recon_algorithm.cpp:36-73).
+double filter_value(int code, double x) {
+  switch (code) {
+    case GR_FILTER_SHEPP_LOGAN: return std::fabs(std::sin(M_PI * x) / M_PI);
+    case GR_FILTER_HANN: return std::fabs(x) * 0.5 * (1.0 + std::cos(2 * M_PI * x));
+    case GR_FILTER_HAMMING: return std::fabs(x) * (0.54 + 0.46 * std::cos(2 * M_PI * x));
+    case GR_FILTER_RAMP: return std::fabs(x);
+    default: return x;
+  }
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ the plan
+
+struct Plan {
+  int device = 0;
+  int n_det = 0, n_ang = 0, pdim = 0, M = 0, M02 = 0, M0 = 0, J = 0, ltbl = 0, filter = 0;
+  int ntaps = 0, max_pairs = 1;
+  double sampl = 1, L = 0, scale = 0, C = 6, lmbda = 0;
+  float center = 0;
+  // device tables
+  float* d_wtbl = nullptr;
+  float* d_winv = nullptr;
+  float* d_filt = nullptr;
+  float2* d_tw_p = nullptr;
+  float2* d_tw_m = nullptr;
+  float2* d_dir = nullptr;
+  // gridding work list
+  int tiles_u = 0, tiles_v = 0, n_items = 0, n_runs = 0, n_slots = 0, n_split = 0;
+  long total_samples = 0;
+  Item* d_items = nullptr;
+  Run* d_runs = nullptr;
+  Split* d_splits = nullptr;
+  unsigned* d_counters = nullptr;
+  // workspaces (max_pairs pairs)
+  float2* d_spec = nullptr;
+  float2* d_H = nullptr;
+  float2* d_scratch = nullptr;
+  float4* d_pq = nullptr;
+  // host streaming (gr_reconstruct_host)
+  void* h_in[2] = {nullptr, nullptr};
+  float* h_out[2] = {nullptr, nullptr};
+  void* d_in[2] = {nullptr, nullptr};
+  float* d_out[2] = {nullptr, nullptr};
+  size_t in_bytes = 0, out_bytes = 0;  // per staging buffer
+  long out_stride_staged = 0;
+  cudaStream_t copy_stream = nullptr;
+  cudaEvent_t ev_h2d[2] = {}, ev_comp[2] = {}, ev_d2h[2] = {};
+  size_t device_bytes = 0;
+  long launches = 0;
+  // optional per-stage timing: 6 events per chunk (before phase, after each stage)
+  bool timing = false;
+  std::vector<cudaEvent_t> events;
+  size_t events_used = 0;
+  std::vector<void*> allocs;
+  std::vector<double> h_winv, h_wtbl;
+};
+
+namespace {
+
+template <typename T>
+int dev_alloc(Plan* p, T** ptr, size_t count) {
+  *ptr = nullptr;
+  if (count == 0) count = 1;
+  cudaError_t e = cudaMalloc((void**)ptr, count * sizeof(T));
+  if (e != cudaSuccess) {
+    *ptr = nullptr;
+    cudaGetLastError();
+    return fail(GR_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", count * sizeof(T),
+                cudaGetErrorString(e));
+  }
+  p->allocs.push_back(*ptr);
+  p->device_bytes += count * sizeof(T);
+  return GR_OK;
+}
+
+template <typename T>
+int upload(Plan* p, T** dptr, const std::vector<T>& h) {
+  int rc = dev_alloc(p, dptr, h.size());
+  if (rc) return rc;
+  GR_CUDA(cudaMemcpy(*dptr, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+  return GR_OK;
+}
+
+// The gridding work list: for each 32x32 tile, the runs of samples
+// (direction, j range) whose L x L footprint can reach the tile; tiles whose
+// runs exceed kItemCap samples are split into several items.
+struct WorkList {
+  std::vector<Item> items;
+  std::vector<Run> runs;
+  std::vector<Split> splits;
+  int tiles_u = 0, tiles_v = 0, n_slots = 0, n_split = 0;
+  long total = 0;
+};
+
+void build_work_list(int M, int J, double L, int n_ang, const std::vector<double>& dxy,
+                     WorkList* wl) {
+  const int T = kTile;
+  const double M2 = M / 2;
+  const double L2 = L / 2 + 1e-3;  // box margin covers FP32 position rounding
+  wl->tiles_u = (M + T - 1) / T;
+  wl->tiles_v = wl->tiles_u;
+  const int n_tiles = wl->tiles_u * wl->tiles_v;
+  const int n_dir = 2 * n_ang;
+  struct TRun { int tile, dir, jlo, jhi; };
+  std::vector<TRun> all;
+  all.reserve((size_t)n_dir * wl->tiles_u * 2);
+  auto slab = [](double o, double dd, double lo, double hi, double& tmin, double& tmax) {
+    if (std::fabs(dd) < 1e-12) return o >= lo && o <= hi;
+    double t1 = (lo - o) / dd, t2 = (hi - o) / dd;
+    if (t1 > t2) std::swap(t1, t2);
+    tmin = std::max(tmin, t1);
+    tmax = std::min(tmax, t2);
+    return tmin <= tmax;
+  };
+  for (int d = 0; d < n_dir; ++d) {
+    const double dx = dxy[2 * d], dy = dxy[2 * d + 1];
+    for (int tu = 0; tu < wl->tiles_u; ++tu) {
+      const double x0 = tu * T - L2, x1 = std::min(tu * T + T, M) - 1 + L2;
+      double ta = 1.0, tb = J - 1.0;
+      if (!slab(M2, dx, x0, x1, ta, tb)) continue;
+      // y extent of the samples in this x slab -> candidate tile columns
+      const double ya = M2 + ta * dy, yb = M2 + tb * dy;
+      const double ymin = std::min(ya, yb), ymax = std::max(ya, yb);
+      int tv0 = (int)std::floor((ymin - L2) / T) - 1;
+      int tv1 = (int)std::floor((ymax + L2) / T) + 1;
+      tv0 = std::max(tv0, 0);
+      tv1 = std::min(tv1, wl->tiles_v - 1);
+      for (int tv = tv0; tv <= tv1; ++tv) {
+        const double y0 = tv * T - L2, y1 = std::min(tv * T + T, M) - 1 + L2;
+        double sa = ta, sb = tb;
+        if (!slab(M2, dy, y0, y1, sa, sb)) continue;
+        const int jlo = std::max(1, (int)std::floor(sa) - 1);
+        const int jhi = std::min(J - 1, (int)std::ceil(sb) + 1);
+        if (jlo > jhi) continue;
+        all.push_back({tu * wl->tiles_v + tv, d, jlo, jhi});
+      }
+    }
+  }
+  std::stable_sort(all.begin(), all.end(),
+                   [](const TRun& a, const TRun& b) { return a.tile < b.tile; });
+  wl->runs.resize(all.size());
+  std::vector<int> first(n_tiles + 1, 0);
+  for (size_t i = 0; i < all.size(); ++i) {
+    wl->runs[i] = {all[i].dir, all[i].jlo, all[i].jhi};
+    first[all[i].tile + 1]++;
+  }
+  for (int t = 0; t < n_tiles; ++t) first[t + 1] += first[t];
+  struct CItem { Item it; long cost; };
+  std::vector<CItem> items;
+  wl->splits.assign(n_tiles, Split{0, 0, 1, 0});
+  int n_slots = 0, n_split = 0;
+  long total = 0;
+  for (int t = 0; t < n_tiles; ++t) {
+    const int b = first[t], e = first[t + 1];
+    long cost = 0;
+    for (int r = b; r < e; ++r) cost += wl->runs[r].jhi - wl->runs[r].jlo + 1;
+    total += cost;
+    if (cost <= kItemCap) {
+      items.push_back({{t, b, e, -1}, cost});
+      continue;
+    }
+    std::vector<std::pair<int, long>> cuts;  // (run_end, cost)
+    long c = 0;
+    for (int r = b; r < e; ++r) {
+      const long rc = wl->runs[r].jhi - wl->runs[r].jlo + 1;
+      if (c > 0 && c + rc > kItemCap) {
+        cuts.push_back({r, c});
+        c = 0;
+      }
+      c += rc;
+    }
+    cuts.push_back({e, c});
+    wl->splits[t] = Split{n_split++, n_slots, (int)cuts.size(), 0};
+    int start = b;
+    for (const auto& cut : cuts) {
+      items.push_back({{t, start, cut.first, n_slots++}, cut.second});
+      start = cut.first;
+    }
+  }
+  // heaviest items first so that the long ones start early
+  std::stable_sort(items.begin(), items.end(),
+                   [](const CItem& a, const CItem& b) { return a.cost > b.cost; });
+  wl->items.resize(items.size());
+  for (size_t i = 0; i < items.size(); ++i) wl->items[i] = items[i].it;
+  wl->n_slots = n_slots;
+  wl->n_split = n_split;
+  wl->total = total;
+}
+
+// Sizes exactly as GridRec::init (gridrec/GPU/gridrec.cu:243-268), in FP64.
+struct Geometry {
+  long pdim, M, M02, M0;
+  double sampl, L, scale;
+  int ntaps;
+};
+
+int geometry(const gr_params* prm, const Pswf* pw, Geometry* g) {
+  long pdim = 1, itmp = prm->n_det - 1;
+  while (itmp) { pdim <<= 1; itmp >>= 1; }
+  const double D0 = prm->n_det;
+  const double D1 = (double)prm->sampl * D0;
+  long M = 1;
+  itmp = (long)(D1 - 1);
+  while (itmp) { M <<= 1; itmp >>= 1; }
+  long M02 = (long)std::floor((double)(M / 2) / (double)prm->sampl - 0.5);
+  if (M02 < 0) M02 = 0;
+  g->pdim = pdim;
+  g->M = M;
+  g->M02 = M02;
+  g->M0 = 2 * M02 + 1;
+  g->sampl = (double)M / g->M0;
+  g->L = 2 * pw->C * g->sampl / M_PI;
+  g->scale = g->sampl * D0 / pdim;
+  g->ntaps = (int)std::floor(g->L) + 1;
+  if (pdim > 8192 || M > 8192 || M < 16 || g->ntaps > kMaxTaps)
+    return fail(GR_ERR_UNSUPPORTED, "sizes pdim=%ld M=%ld L=%.3f outside the kernels' range", pdim,
+                M, g->L);
+  return GR_OK;
+}
+
+int check_params(const gr_params* prm, const Pswf** pw) {
+  if (!prm) return fail(GR_ERR_ARG, "null argument");
+  if (prm->n_det < 9 || prm->n_ang < 1 || !prm->theta_deg)
+    return fail(GR_ERR_ARG, "need n_det >= 9, n_ang >= 1 and a theta list");
+  if (prm->ltbl < 1 || prm->ltbl > 1024) return fail(GR_ERR_ARG, "ltbl must be in [1, 1024]");
+  if (!(prm->sampl >= 1.0f) || prm->sampl > 4.0f)
+    return fail(GR_ERR_ARG, "sampl must be in [1, 4]");
+  if (prm->max_pairs < 1) return fail(GR_ERR_ARG, "max_pairs must be >= 1");
+  *pw = find_pswf(prm->pswf_c);
+  if (!*pw) return fail(GR_ERR_PSWF, "Prolate parameter C = %f not in data base", prm->pswf_c);
+  return GR_OK;
+}
+
+// Direction vectors in grid units: half 0 = scale*(cos, sin), half 1 = mirrored.
+std::vector<double> directions(const gr_params* prm, double scale) {
+  std::vector<double> dxy(4 * (size_t)prm->n_ang);
+  for (int n = 0; n < prm->n_ang; ++n) {
+    const double th = (double)prm->theta_deg[n] * (M_PI / 180.0);
+    const double cs = std::cos(th) * scale, sn = std::sin(th) * scale;
+    dxy[4 * n + 0] = cs;
+    dxy[4 * n + 1] = sn;
+    dxy[4 * n + 2] = -cs;
+    dxy[4 * n + 3] = -sn;
+  }
+  return dxy;
+}
+
+cudaEvent_t next_event(Plan* p) {
+  if (p->events_used == p->events.size()) {
+    cudaEvent_t e = nullptr;
+    if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+    p->events.push_back(e);
+  }
+  return p->events[p->events_used++];
+}
+
+#define GR_MARK()                                                  \
+  do {                                                             \
+    if (p->timing) {                                               \
+      cudaEvent_t ev_ = next_event(p);                             \
+      if (!ev_) return fail(GR_ERR_CUDA, "cudaEventCreate failed"); \
+      GR_CUDA(cudaEventRecord(ev_, st));                           \
+    }                                                              \
+  } while (0)
+
+int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1,
+                 const void* s2, long in_pair_stride, gr_dtype dt, const float* centers,
+                 const float* flat, const float* dark, float* o1, float* o2,
+                 long out_pair_stride, long out_stride, cudaStream_t st) {
+  GR_MARK();
+  PhaseArgs ph{centers, p->center, slice_base, n_valid, p->d_filt, p->d_pq, p->J, p->pdim, pairs};
+  GR_CUDA(launch_phase(ph, st));
+  GR_MARK();
+  SpectraArgs sa{s1, s2, in_pair_stride, n_valid, slice_base, flat, dark, p->d_pq, p->d_spec,
+                 p->d_tw_p, p->n_det, p->n_ang, p->pdim, p->J, pairs};
+  GR_CUDA(launch_spectra(sa, dt, st));
+  GR_MARK();
+  GridArgs ga{p->d_spec, p->d_H, p->d_scratch, p->d_counters, p->d_items, p->d_runs,
+              p->d_splits, p->d_dir, p->d_wtbl, p->n_items, pairs, p->n_ang, p->J, p->M,
+              p->tiles_v, p->n_slots, p->n_split, p->ltbl, (float)(p->L / 2),
+              (float)(2.0 * p->ltbl / p->L)};
+  GR_CUDA(launch_grid(ga, p->ntaps, st));
+  GR_MARK();
+  ColArgs ca{p->d_H, p->d_tw_m, p->M, pairs};
+  GR_CUDA(launch_cols(ca, st));
+  GR_MARK();
+  RowArgs ra{p->d_H, p->d_tw_m, p->d_winv, o1, o2, out_pair_stride, out_stride, n_valid,
+             p->M, p->M0, p->M02, pairs};
+  GR_CUDA(launch_rows(ra, st));
+  GR_MARK();
+  p->launches += 5;
+  return GR_OK;
+}
+
+size_t dtype_size(gr_dtype dt) {
+  switch (dt) {
+    case GR_DTYPE_F32: return 4;
+    case GR_DTYPE_F16:
+    case GR_DTYPE_BF16:
+    case GR_DTYPE_U16_RAW: return 2;
+  }
+  return 0;
+}
+
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+int validate_batch(const Plan* p, const gr_batch_desc* b) {
+  if (!b || b->n_slices < 1 || !b->sinos || !b->outs)
+    return fail(GR_ERR_ARG, "batch: n_slices >= 1, sinos and outs are required");
+  if (b->out_stride < p->M0)
+    return fail(GR_ERR_ARG, "out_stride %ld < M0 %d", b->out_stride, p->M0);
+  if (dtype_size(b->dtype) == 0) return fail(GR_ERR_ARG, "unknown dtype %d", (int)b->dtype);
+  if (b->dtype == GR_DTYPE_U16_RAW && (!b->flat || !b->dark))
+    return fail(GR_ERR_ARG, "GR_DTYPE_U16_RAW needs flat and dark rows");
+  return GR_OK;
+}
+
+}  // namespace
+}  // namespace gr
+
+using gr::Plan;
+struct gr_plan : public Plan {};
+
+extern "C" {
+
+const char* gr_last_error(void) { return gr::g_err.c_str(); }
+
+int gr_filter_code(const char* name) {
+  if (!name) return GR_FILTER_SHEPP_LOGAN;
+  struct { const char* n; int c; } tbl[] = {{"shlo", 1}, {"shepp", 1}, {"hann", 2}, {"hamm", 3},
+                                            {"hamming", 3}, {"ramp", 4}, {"ramlak", 4},
+                                            {"none", 0}};
+  for (auto& e : tbl)
+    if (!std::strcmp(name, e.n)) return e.c;
+  return GR_FILTER_SHEPP_LOGAN;
+}
+
+int gr_params_default(gr_params* p, int n_det, int n_ang, const float* theta_deg) {
+  if (!p) return gr::fail(GR_ERR_ARG, "null params");
+  std::memset(p, 0, sizeof(*p));
+  p->n_det = n_det;
+  p->n_ang = n_ang;
+  p->theta_deg = theta_deg;
+  p->center = -1.0f;
+  p->filter = GR_FILTER_SHEPP_LOGAN;
+  p->pswf_c = 6.0f;
+  p->sampl = 1.0f;
+  p->ltbl = 512;
+  p->max_pairs = 1;
+  p->device = 0;
+  return GR_OK;
+}
+
+int gr_plan_destroy(gr_plan* plan) {
+  if (!plan) return GR_OK;
+  gr::DeviceGuard g(plan->device);
+  for (void* ptr : plan->allocs) cudaFree(ptr);
+  for (int b = 0; b < 2; ++b) {
+    if (plan->h_in[b]) cudaFreeHost(plan->h_in[b]);
+    if (plan->h_out[b]) cudaFreeHost(plan->h_out[b]);
+    if (plan->d_in[b]) cudaFree(plan->d_in[b]);
+    if (plan->d_out[b]) cudaFree(plan->d_out[b]);
+    if (plan->ev_h2d[b]) cudaEventDestroy(plan->ev_h2d[b]);
+    if (plan->ev_comp[b]) cudaEventDestroy(plan->ev_comp[b]);
+    if (plan->ev_d2h[b]) cudaEventDestroy(plan->ev_d2h[b]);
+  }
+  if (plan->copy_stream) cudaStreamDestroy(plan->copy_stream);
+  for (cudaEvent_t e : plan->events) cudaEventDestroy(e);
+  delete plan;
+  return GR_OK;
+}
+
+int gr_plan_create(const gr_params* prm, gr_plan** out) {
+  using namespace gr;
+  if (!out) return fail(GR_ERR_ARG, "null argument");
+  *out = nullptr;
+  const Pswf* pw = nullptr;
+  int rc = check_params(prm, &pw);
+  if (rc) return rc;
+  Geometry geo;
+  if ((rc = geometry(prm, pw, &geo))) return rc;
+  int ndev = 0;
+  GR_CUDA(cudaGetDeviceCount(&ndev));
+  if (prm->device < 0 || prm->device >= ndev)
+    return fail(GR_ERR_ARG, "device %d out of range (%d devices)", prm->device, ndev);
+  DeviceGuard guard(prm->device);
+  GR_CUDA(init_kernel_attributes());
+
+  gr_plan* p = new gr_plan();
+  p->device = prm->device;
+  p->n_det = prm->n_det;
+  p->n_ang = prm->n_ang;
+  p->ltbl = prm->ltbl;
+  p->filter = prm->filter;
+  p->max_pairs = prm->max_pairs;
+  p->center = prm->center < 0 ? (float)(prm->n_det / 2) : prm->center;
+  const long pdim = geo.pdim, M = geo.M, M02 = geo.M02;
+  p->pdim = (int)pdim;
+  p->J = (int)(pdim / 2);
+  p->M = (int)M;
+  p->M02 = (int)M02;
+  p->M0 = (int)geo.M0;
+  p->sampl = geo.sampl;
+  p->C = pw->C;
+  p->lmbda = pw->lmbda;
+  p->L = geo.L;
+  p->scale = geo.scale;
+  p->ntaps = geo.ntaps;
+  // PSWF tables (pswf_su, gridrec.cu:807-857), FP64 then rounded once
+  std::vector<double> wtbl(p->ltbl + 1), winv(p->M0);
+  const double polyz = legendre_even(*pw, 0.0);
+  wtbl[0] = 1.0;
+  for (int i = 1; i <= p->ltbl; ++i) wtbl[i] = legendre_even(*pw, (double)i / p->ltbl) / polyz;
+  {
+    const double fac = (double)p->ltbl / (M02 + 0.5);
+    double norm = std::sqrt(M_PI / 2 / pw->C / pw->lmbda) / p->sampl;
+    winv[M02] = norm / wtbl[0];
+    for (long i = 1; i <= M02; ++i) {
+      norm = -norm;
+      winv[M02 + i] = winv[M02 - i] = norm / wtbl[(long)(i * fac + 0.5)];
+    }
+  }
+  p->h_wtbl = wtbl;
+  p->h_winv = winv;
+  std::vector<float> fw(wtbl.begin(), wtbl.end()), fi(winv.begin(), winv.end());
+  // filter x normalisation (filphase_su magnitude, gridrec.cu:789-797)
+  std::vector<float> filt(p->J);
+  const double norm = M_PI / pdim / prm->n_ang;
+  for (int j = 0; j < p->J; ++j) filt[j] = (float)(filter_value(prm->filter, (double)j / pdim) * norm);
+  // twiddles exp(+2 pi i k/N)
+  auto twiddles = [](int N) {
+    std::vector<float2> t(N);
+    for (int k = 0; k < N; ++k) {
+      const double a = 2.0 * M_PI * k / N;
+      t[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    return t;
+  };
+  const std::vector<double> dxy = directions(prm, p->scale);
+  std::vector<float2> dirs(2 * (size_t)prm->n_ang);
+  for (size_t d = 0; d < dirs.size(); ++d)
+    dirs[d] = make_float2((float)dxy[2 * d], (float)dxy[2 * d + 1]);
+  WorkList wl;
+  build_work_list(p->M, p->J, p->L, p->n_ang, dxy, &wl);
+  p->tiles_u = wl.tiles_u;
+  p->tiles_v = wl.tiles_v;
+  p->n_items = (int)wl.items.size();
+  p->n_runs = (int)wl.runs.size();
+  p->n_slots = wl.n_slots;
+  p->n_split = wl.n_split;
+  p->total_samples = wl.total;
+  if ((rc = upload(p, &p->d_wtbl, fw)) || (rc = upload(p, &p->d_winv, fi)) ||
+      (rc = upload(p, &p->d_filt, filt)) || (rc = upload(p, &p->d_tw_p, twiddles((int)pdim))) ||
+      (rc = upload(p, &p->d_tw_m, twiddles((int)M))) || (rc = upload(p, &p->d_dir, dirs)) ||
+      (rc = upload(p, &p->d_items, wl.items)) || (rc = upload(p, &p->d_runs, wl.runs)) ||
+      (rc = upload(p, &p->d_splits, wl.splits))) {
+    gr_plan_destroy(p);
+    return rc;
+  }
+  const size_t P = (size_t)p->max_pairs;
+  if ((rc = dev_alloc(p, &p->d_spec, P * p->n_ang * 2 * p->J)) ||
+      (rc = dev_alloc(p, &p->d_H, P * (size_t)M * M)) ||
+      (rc = dev_alloc(p, &p->d_scratch, P * (size_t)std::max(p->n_slots, 1) * kTile * kTile)) ||
+      (rc = dev_alloc(p, &p->d_pq, P * p->J)) ||
+      (rc = dev_alloc(p, &p->d_counters, P * (size_t)std::max(p->n_split, 1)))) {
+    gr_plan_destroy(p);
+    return rc;
+  }
+  cudaError_t e = cudaMemset(p->d_counters, 0, P * std::max(p->n_split, 1) * sizeof(unsigned));
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (e != cudaSuccess) {
+    gr_plan_destroy(p);
+    return fail(GR_ERR_CUDA, "plan init: %s", cudaGetErrorString(e));
+  }
+  *out = p;
+  return GR_OK;
+}
+
+int gr_worklist_export(const gr_params* prm, int* n_items, int* n_runs, int* tiles_v,
+                       int* items, int* runs, int* splits, int cap_items, int cap_runs) {
+  using namespace gr;
+  const Pswf* pw = nullptr;
+  int rc = check_params(prm, &pw);
+  if (rc) return rc;
+  Geometry geo;
+  if ((rc = geometry(prm, pw, &geo))) return rc;
+  WorkList wl;
+  build_work_list((int)geo.M, (int)(geo.pdim / 2), geo.L, prm->n_ang, directions(prm, geo.scale),
+                  &wl);
+  if (n_items) *n_items = (int)wl.items.size();
+  if (n_runs) *n_runs = (int)wl.runs.size();
+  if (tiles_v) *tiles_v = wl.tiles_v;
+  if (!items || !runs || !splits) return GR_OK;
+  if (cap_items < (int)wl.items.size() || cap_runs < (int)wl.runs.size())
+    return fail(GR_ERR_ARG, "work list needs %zu items / %zu runs", wl.items.size(), wl.runs.size());
+  std::memcpy(items, wl.items.data(), wl.items.size() * sizeof(Item));
+  std::memcpy(runs, wl.runs.data(), wl.runs.size() * sizeof(Run));
+  std::memcpy(splits, wl.splits.data(), wl.splits.size() * sizeof(Split));
+  return GR_OK;
+}
+
+int gr_plan_set_timing(gr_plan* p, int enable) {
+  if (!p) return gr::fail(GR_ERR_ARG, "null plan");
+  p->timing = enable != 0;
+  p->events_used = 0;
+  return GR_OK;
+}
+
+int gr_plan_stage_times(gr_plan* p, double* ms, long* chunks) {
+  using namespace gr;
+  if (!p || !ms) return gr::fail(GR_ERR_ARG, "null argument");
+  for (int k = 0; k < 5; ++k) ms[k] = 0.0;
+  const size_t n = p->events_used / 6;
+  if (chunks) *chunks = (long)n;
+  if (n == 0) return GR_OK;
+  gr::DeviceGuard g(p->device);
+  GR_CUDA(cudaEventSynchronize(p->events[6 * n - 1]));
+  for (size_t c = 0; c < n; ++c)
+    for (int k = 0; k < 5; ++k) {
+      float t = 0.f;
+      GR_CUDA(cudaEventElapsedTime(&t, p->events[6 * c + k], p->events[6 * c + k + 1]));
+      ms[k] += t;
+    }
+  return GR_OK;
+}
+
+int gr_plan_sizes(const gr_plan* p, int* pdim, int* M, int* M0, float* L, float* scale) {
+  if (!p) return gr::fail(GR_ERR_ARG, "null plan");
+  if (pdim) *pdim = p->pdim;
+  if (M) *M = p->M;
+  if (M0) *M0 = p->M0;
+  if (L) *L = (float)p->L;
+  if (scale) *scale = (float)p->scale;
+  return GR_OK;
+}
+
+int gr_plan_device_bytes(const gr_plan* p, size_t* bytes) {
+  if (!p || !bytes) return gr::fail(GR_ERR_ARG, "null argument");
+  *bytes = p->device_bytes;
+  return GR_OK;
+}
+
+int gr_plan_launch_count(const gr_plan* p, long* launches) {
+  if (!p || !launches) return gr::fail(GR_ERR_ARG, "null argument");
+  *launches = p->launches;
+  return GR_OK;
+}
+
+int gr_plan_work_stats(const gr_plan* p, int* n_items, int* n_runs, int* n_slots,
+                       long* total_samples) {
+  if (!p) return gr::fail(GR_ERR_ARG, "null plan");
+  if (n_items) *n_items = p->n_items;
+  if (n_runs) *n_runs = p->n_runs;
+  if (n_slots) *n_slots = p->n_slots;
+  if (total_samples) *total_samples = p->total_samples;
+  return GR_OK;
+}
+
+int gr_reconstruct_pair(gr_plan* p, const float* sino1, const float* sino2, float* out1,
+                        float* out2, long out_stride, void* stream) {
+  using namespace gr;
+  if (!p || !sino1 || !out1) return fail(GR_ERR_ARG, "null argument");
+  if (out_stride < p->M0) return fail(GR_ERR_ARG, "out_stride %ld < M0 %d", out_stride, p->M0);
+  DeviceGuard g(p->device);
+  const int n_valid = (sino2 && out2) ? 2 : 1;
+  return launch_chunk(p, 1, n_valid, 0, sino1, sino2 ? sino2 : sino1, 0, GR_DTYPE_F32, nullptr,
+                      nullptr, nullptr, out1, out2 ? out2 : out1, 0, out_stride,
+                      (cudaStream_t)stream);
+}
+
+int gr_reconstruct_batch(gr_plan* p, const gr_batch_desc* b, void* stream) {
+  using namespace gr;
+  if (!p) return fail(GR_ERR_ARG, "null plan");
+  int rc = validate_batch(p, b);
+  if (rc) return rc;
+  DeviceGuard g(p->device);
+  const size_t es = dtype_size(b->dtype);
+  const long slice_in = (long)p->n_ang * p->n_det;
+  const long slice_out = (long)p->M0 * b->out_stride;
+  const int n_pairs = (b->n_slices + 1) / 2;
+  for (int c0 = 0; c0 < n_pairs; c0 += p->max_pairs) {
+    const int pairs = std::min(p->max_pairs, n_pairs - c0);
+    const int s0 = 2 * c0;
+    const int n_valid = std::min(2 * pairs, b->n_slices - s0);
+    const char* base = static_cast<const char*>(b->sinos) + (size_t)s0 * slice_in * es;
+    float* ob = b->outs + (size_t)s0 * slice_out;
+    rc = launch_chunk(p, pairs, n_valid, s0, base, base + slice_in * es, 2 * slice_in,
+                      b->dtype, b->centers, b->flat, b->dark, ob, ob + slice_out, 2 * slice_out,
+                      b->out_stride, (cudaStream_t)stream);
+    if (rc) return rc;
+  }
+  return GR_OK;
+}
+
+int gr_reconstruct_host(gr_plan* p, const gr_batch_desc* b, void* stream) {
+  using namespace gr;
+  if (!p) return fail(GR_ERR_ARG, "null plan");
+  int rc = validate_batch(p, b);
+  if (rc) return rc;
+  DeviceGuard g(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t es = dtype_size(b->dtype);
+  const size_t slice_in = (size_t)p->n_ang * p->n_det * es;
+  const size_t slice_out = (size_t)p->M0 * b->out_stride * sizeof(float);
+  const size_t in_bytes = 2 * (size_t)p->max_pairs * slice_in;
+  const size_t out_bytes = 2 * (size_t)p->max_pairs * slice_out;
+  // pinned user buffers are copied directly; pageable ones go through staging
+  auto is_pinned = [](const void* ptr) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, ptr) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    return at.type == cudaMemoryTypeHost;
+  };
+  const bool in_pinned = is_pinned(b->sinos);
+  const bool out_pinned = is_pinned(b->outs);
+  if (!p->copy_stream) {
+    GR_CUDA(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+    for (int k = 0; k < 2; ++k) {
+      GR_CUDA(cudaEventCreateWithFlags(&p->ev_h2d[k], cudaEventDisableTiming));
+      GR_CUDA(cudaEventCreateWithFlags(&p->ev_comp[k], cudaEventDisableTiming));
+      GR_CUDA(cudaEventCreateWithFlags(&p->ev_d2h[k], cudaEventDisableTiming));
+    }
+  }
+  if (p->in_bytes < in_bytes || p->out_bytes < out_bytes) {
+    for (int k = 0; k < 2; ++k) {
+      if (p->h_in[k]) cudaFreeHost(p->h_in[k]);
+      if (p->h_out[k]) cudaFreeHost(p->h_out[k]);
+      if (p->d_in[k]) cudaFree(p->d_in[k]);
+      if (p->d_out[k]) cudaFree(p->d_out[k]);
+      p->h_in[k] = p->h_out[k] = nullptr;
+      p->d_in[k] = p->d_out[k] = nullptr;
+    }
+    for (int k = 0; k < 2; ++k) {
+      if (cudaMallocHost(&p->h_in[k], in_bytes) != cudaSuccess ||
+          cudaMallocHost((void**)&p->h_out[k], out_bytes) != cudaSuccess ||
+          cudaMalloc(&p->d_in[k], in_bytes) != cudaSuccess ||
+          cudaMalloc((void**)&p->d_out[k], out_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        p->in_bytes = p->out_bytes = 0;
+        return fail(GR_ERR_NOMEM, "staging buffers (%zu + %zu bytes x 2)", in_bytes, out_bytes);
+      }
+    }
+    p->in_bytes = in_bytes;
+    p->out_bytes = out_bytes;
+  }
+  // per-slice centres are small: upload once to the device
+  float* d_centers = nullptr;
+  float* d_flat = nullptr;
+  float* d_dark = nullptr;
+  auto cleanup = [&]() {
+    if (d_centers) cudaFree(d_centers);
+    if (d_flat) cudaFree(d_flat);
+    if (d_dark) cudaFree(d_dark);
+  };
+  if (b->centers) {
+    GR_CUDA(cudaMalloc(&d_centers, b->n_slices * sizeof(float)));
+    GR_CUDA(cudaMemcpy(d_centers, b->centers, b->n_slices * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  if (b->dtype == GR_DTYPE_U16_RAW) {
+    GR_CUDA(cudaMalloc(&d_flat, p->n_det * sizeof(float)));
+    GR_CUDA(cudaMalloc(&d_dark, p->n_det * sizeof(float)));
+    GR_CUDA(cudaMemcpy(d_flat, b->flat, p->n_det * sizeof(float), cudaMemcpyHostToDevice));
+    GR_CUDA(cudaMemcpy(d_dark, b->dark, p->n_det * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  const int n_pairs = (b->n_slices + 1) / 2;
+  const int n_chunks = (n_pairs + p->max_pairs - 1) / p->max_pairs;
+  struct Pending { int chunk = -1; size_t bytes = 0; size_t off = 0; };
+  Pending pend[2];
+  auto finish = [&](int k) -> int {  // copy a finished chunk's images to the user
+    if (pend[k].chunk < 0) return GR_OK;
+    GR_CUDA(cudaEventSynchronize(p->ev_d2h[k]));
+    if (!out_pinned)
+      std::memcpy(reinterpret_cast<char*>(b->outs) + pend[k].off, p->h_out[k], pend[k].bytes);
+    pend[k].chunk = -1;
+    return GR_OK;
+  };
+  for (int c = 0; c < n_chunks; ++c) {
+    const int k = c & 1;
+    const int c0 = c * p->max_pairs;
+    const int pairs = std::min(p->max_pairs, n_pairs - c0);
+    const int s0 = 2 * c0;
+    const int n_valid = std::min(2 * pairs, b->n_slices - s0);
+    const size_t ib = (size_t)n_valid * slice_in, ob = (size_t)n_valid * slice_out;
+    const char* src = static_cast<const char*>(b->sinos) + (size_t)s0 * slice_in;
+    if ((rc = finish(k))) { cleanup(); return rc; }
+    // the staging input k was last read by the H2D of chunk c-2 (finished:
+    // its D2H completed above); the device input k by the kernels of chunk c-2
+    GR_CUDA(cudaStreamWaitEvent(p->copy_stream, p->ev_comp[k], 0));
+    if (in_pinned) {
+      GR_CUDA(cudaMemcpyAsync(p->d_in[k], src, ib, cudaMemcpyHostToDevice, p->copy_stream));
+    } else {
+      std::memcpy(p->h_in[k], src, ib);
+      GR_CUDA(cudaMemcpyAsync(p->d_in[k], p->h_in[k], ib, cudaMemcpyHostToDevice, p->copy_stream));
+    }
+    GR_CUDA(cudaEventRecord(p->ev_h2d[k], p->copy_stream));
+    GR_CUDA(cudaStreamWaitEvent(st, p->ev_h2d[k], 0));
+    // the device output k was last read by the D2H of chunk c-2 (complete)
+    const char* dbase = static_cast<const char*>(p->d_in[k]);
+    const long slice_in_el = (long)p->n_ang * p->n_det;
+    const long slice_out_el = (long)p->M0 * b->out_stride;
+    rc = launch_chunk(p, pairs, n_valid, s0, dbase, dbase + slice_in, 2 * slice_in_el, b->dtype,
+                      d_centers, d_flat, d_dark, p->d_out[k], p->d_out[k] + slice_out_el,
+                      2 * slice_out_el, b->out_stride, st);
+    if (rc) { cleanup(); return rc; }
+    GR_CUDA(cudaEventRecord(p->ev_comp[k], st));
+    GR_CUDA(cudaStreamWaitEvent(p->copy_stream, p->ev_comp[k], 0));
+    char* dst = out_pinned ? reinterpret_cast<char*>(b->outs) + (size_t)s0 * slice_out
+                           : reinterpret_cast<char*>(p->h_out[k]);
+    GR_CUDA(cudaMemcpyAsync(dst, p->d_out[k], ob, cudaMemcpyDeviceToHost, p->copy_stream));
+    GR_CUDA(cudaEventRecord(p->ev_d2h[k], p->copy_stream));
+    pend[k].chunk = c;
+    pend[k].bytes = ob;
+    pend[k].off = (size_t)s0 * slice_out;
+  }
+  for (int k = 0; k < 2; ++k)
+    if ((rc = finish(k))) { cleanup(); return rc; }
+  GR_CUDA(cudaStreamSynchronize(st));
+  cleanup();
+  return GR_OK;
+}
+
+}  // extern "C"

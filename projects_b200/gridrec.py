@@ -1,0 +1,354 @@
+"""Python host side of the B200 gridrec: ctypes bindings of the C ABI
+(include/gridrec_b200.h) plus a ``GridRec`` class with the reference's
+setter API (gridrec/GPU/gridrec.h:72-143, recon_algorithm.h:56-95).
+
+The library ``libgridrec_b200.so`` is built in-tree (projects_b200/build.py).
+There is no CPU fallback: every compute call goes to the sm_100a kernels and
+raises if the library or a GPU is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libgridrec_b200.so")
+
+GR_OK = 0
+STATUS = {0: "GR_OK", -1: "GR_ERR_ARG", -2: "GR_ERR_PSWF", -3: "GR_ERR_CUDA",
+          -4: "GR_ERR_NOMEM", -5: "GR_ERR_UNSUPPORTED", -6: "GR_ERR_TIMEOUT"}
+
+FILTER_NONE, FILTER_SHEPP_LOGAN, FILTER_HANN, FILTER_HAMMING, FILTER_RAMP, FILTER_FBP = range(6)
+DTYPE_F32, DTYPE_F16, DTYPE_BF16, DTYPE_U16_RAW = range(4)
+
+# Functions declared in include/gridrec_b200.h (checked by the CPU tests).
+EXPORTS = ("gr_params_default", "gr_filter_code", "gr_plan_create", "gr_plan_destroy",
+           "gr_plan_sizes", "gr_plan_device_bytes", "gr_reconstruct_pair",
+           "gr_reconstruct_batch", "gr_reconstruct_host", "gr_last_error",
+           "gr_plan_launch_count", "gr_plan_work_stats", "gr_worklist_export",
+           "gr_plan_set_timing", "gr_plan_stage_times")
+STAGES = ("phase", "spectra", "grid", "cols", "rows_deapod")
+
+
+class GrError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        self.code = code
+        super().__init__(f"{where}: {STATUS.get(code, code)}: {last_error()}")
+
+
+class GrParams(C.Structure):
+    _fields_ = [("n_det", C.c_int), ("n_ang", C.c_int), ("theta_deg", C.POINTER(C.c_float)),
+                ("center", C.c_float), ("filter", C.c_int), ("pswf_c", C.c_float),
+                ("sampl", C.c_float), ("ltbl", C.c_int), ("max_pairs", C.c_int),
+                ("device", C.c_int)]
+
+
+class GrBatch(C.Structure):
+    _fields_ = [("n_slices", C.c_int), ("dtype", C.c_int), ("sinos", C.c_void_p),
+                ("centers", C.c_void_p), ("flat", C.c_void_p), ("dark", C.c_void_p),
+                ("outs", C.c_void_p), ("out_stride", C.c_long)]
+
+
+_lib = None
+
+
+def lib():
+    """Loads libgridrec_b200.so (raises if it was not built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} missing: run projects_b200/build.py (needs nvcc)")
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER(GrParams)
+        L.gr_params_default.argtypes = [P, C.c_int, C.c_int, C.POINTER(C.c_float)]
+        L.gr_filter_code.argtypes = [C.c_char_p]
+        L.gr_plan_create.argtypes = [P, C.POINTER(C.c_void_p)]
+        L.gr_plan_destroy.argtypes = [C.c_void_p]
+        L.gr_plan_sizes.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                    C.POINTER(C.c_int), C.POINTER(C.c_float),
+                                    C.POINTER(C.c_float)]
+        L.gr_plan_device_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_size_t)]
+        L.gr_reconstruct_pair.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                          C.c_void_p, C.c_long, C.c_void_p]
+        L.gr_reconstruct_batch.argtypes = [C.c_void_p, C.POINTER(GrBatch), C.c_void_p]
+        L.gr_reconstruct_host.argtypes = [C.c_void_p, C.POINTER(GrBatch), C.c_void_p]
+        L.gr_last_error.restype = C.c_char_p
+        L.gr_plan_launch_count.argtypes = [C.c_void_p, C.POINTER(C.c_long)]
+        L.gr_plan_work_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                         C.POINTER(C.c_int), C.POINTER(C.c_long)]
+        L.gr_plan_set_timing.argtypes = [C.c_void_p, C.c_int]
+        L.gr_plan_stage_times.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_long)]
+        ip = C.POINTER(C.c_int)
+        L.gr_worklist_export.argtypes = [P, ip, ip, ip, C.c_void_p, C.c_void_p, C.c_void_p,
+                                         C.c_int, C.c_int]
+        _lib = L
+    return _lib
+
+
+def last_error() -> str:
+    return lib().gr_last_error().decode()
+
+
+def _check(rc: int, where: str):
+    if rc != GR_OK:
+        raise GrError(rc, where)
+
+
+def filter_code(name: str) -> int:
+    """GridrecCPP filter name -> ReconAlgorithm code (filters.cpp:26-48)."""
+    return int(lib().gr_filter_code(name.encode()))
+
+
+def make_params(n_det: int, n_ang: int, theta_deg, center=None, filter=FILTER_SHEPP_LOGAN,
+                pswf_c=6.0, sampl=1.0, ltbl=512, max_pairs=1, device=0):
+    """GrParams plus the float32 theta array that must outlive plan creation."""
+    th = np.ascontiguousarray(theta_deg, dtype=np.float32)
+    if th.shape != (n_ang,):
+        raise ValueError(f"theta_deg must have {n_ang} entries")
+    if isinstance(filter, str):
+        filter = filter_code(filter)
+    p = GrParams()
+    lib().gr_params_default(C.byref(p), n_det, n_ang, th.ctypes.data_as(C.POINTER(C.c_float)))
+    p.center = -1.0 if center is None else float(center)
+    p.filter = int(filter)
+    p.pswf_c = float(pswf_c)
+    p.sampl = float(sampl)
+    p.ltbl = int(ltbl)
+    p.max_pairs = int(max_pairs)
+    p.device = int(device)
+    return p, th
+
+
+def worklist(n_det, n_ang, theta_deg, sampl=1.0, pswf_c=6.0):
+    """Host-only gridding work list: (items[n,4], runs[n,3], splits[tiles,4], tiles_v)."""
+    p, th = make_params(n_det, n_ang, theta_deg, sampl=sampl, pswf_c=pswf_c)
+    ni, nr, tv = C.c_int(), C.c_int(), C.c_int()
+    _check(lib().gr_worklist_export(C.byref(p), C.byref(ni), C.byref(nr), C.byref(tv), None,
+                                    None, None, 0, 0), "gr_worklist_export")
+    items = np.zeros((ni.value, 4), np.int32)
+    runs = np.zeros((nr.value, 3), np.int32)
+    splits = np.zeros((tv.value * tv.value, 4), np.int32)
+    _check(lib().gr_worklist_export(C.byref(p), C.byref(ni), C.byref(nr), C.byref(tv),
+                                    items.ctypes.data, runs.ctypes.data, splits.ctypes.data,
+                                    ni.value, nr.value), "gr_worklist_export")
+    return items, runs, splits, tv.value
+
+
+def _ptr(t) -> int:
+    """Device address of a torch tensor (or an int address)."""
+    if t is None:
+        return 0
+    if isinstance(t, int):
+        return t
+    return int(t.data_ptr())
+
+
+def _stream_ptr(stream) -> int:
+    if stream is None:
+        import torch
+        return int(torch.cuda.current_stream().cuda_stream)
+    if isinstance(stream, int):
+        return stream
+    return int(stream.cuda_stream)
+
+
+class Plan:
+    """A gridrec plan: sizes, tables, work list and workspaces on one GPU."""
+
+    def __init__(self, n_det: int, n_ang: int, theta_deg, center=None,
+                 filter=FILTER_SHEPP_LOGAN, pswf_c=6.0, sampl=1.0, ltbl=512, max_pairs=1,
+                 device=0):
+        self._params, self._theta = make_params(n_det, n_ang, theta_deg, center, filter,
+                                                pswf_c, sampl, ltbl, max_pairs, device)
+        h = C.c_void_p()
+        _check(lib().gr_plan_create(C.byref(self._params), C.byref(h)), "gr_plan_create")
+        self._h = h
+        self.n_det, self.n_ang, self.device = n_det, n_ang, device
+        self.max_pairs = max_pairs
+        pd, M, M0 = C.c_int(), C.c_int(), C.c_int()
+        L, sc = C.c_float(), C.c_float()
+        _check(lib().gr_plan_sizes(h, C.byref(pd), C.byref(M), C.byref(M0), C.byref(L),
+                                   C.byref(sc)), "gr_plan_sizes")
+        self.pdim, self.M, self.M0, self.L, self.scale = pd.value, M.value, M0.value, L.value, sc.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gr_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    def device_bytes(self) -> int:
+        b = C.c_size_t()
+        _check(lib().gr_plan_device_bytes(self._h, C.byref(b)), "gr_plan_device_bytes")
+        return b.value
+
+    def launches(self) -> int:
+        n = C.c_long()
+        _check(lib().gr_plan_launch_count(self._h, C.byref(n)), "gr_plan_launch_count")
+        return n.value
+
+    def set_timing(self, enable: bool):
+        _check(lib().gr_plan_set_timing(self._h, int(enable)), "gr_plan_set_timing")
+
+    def stage_times(self):
+        """({stage: summed ms}, chunks) since set_timing(True); synchronises."""
+        ms = (C.c_double * 5)()
+        n = C.c_long()
+        _check(lib().gr_plan_stage_times(self._h, ms, C.byref(n)), "gr_plan_stage_times")
+        return dict(zip(STAGES, list(ms))), n.value
+
+    def work_stats(self):
+        a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_long()
+        _check(lib().gr_plan_work_stats(self._h, C.byref(a), C.byref(b), C.byref(c),
+                                        C.byref(d)), "gr_plan_work_stats")
+        return {"items": a.value, "runs": b.value, "slots": c.value, "samples": d.value}
+
+    def reconstruct_pair(self, sino1, sino2, out1, out2, out_stride=None, stream=None):
+        """Device tensors: sino (n_ang, n_det) float32, out (M0, >= M0) float32."""
+        stride = out1.shape[-1] if out_stride is None else out_stride
+        _check(lib().gr_reconstruct_pair(self._h, _ptr(sino1), _ptr(sino2), _ptr(out1),
+                                         _ptr(out2), stride, _stream_ptr(stream)),
+               "gr_reconstruct_pair")
+
+    def _batch(self, n_slices, dtype, sinos, centers, flat, dark, outs, out_stride):
+        b = GrBatch()
+        b.n_slices, b.dtype = int(n_slices), int(dtype)
+        b.sinos, b.centers, b.flat, b.dark, b.outs = sinos, centers, flat, dark, outs
+        b.out_stride = int(out_stride)
+        return b
+
+    def reconstruct_batch(self, sinos, outs, centers=None, flat=None, dark=None, dtype=None,
+                          stream=None):
+        """Device tensors: sinos (S, n_ang, n_det) f32/f16/bf16/uint16, outs (S, M0, stride)."""
+        import torch
+        if dtype is None:
+            dtype = {torch.float32: DTYPE_F32, torch.float16: DTYPE_F16,
+                     torch.bfloat16: DTYPE_BF16, torch.uint16: DTYPE_U16_RAW,
+                     torch.int16: DTYPE_U16_RAW}[sinos.dtype]
+        b = self._batch(sinos.shape[0], dtype, _ptr(sinos), _ptr(centers), _ptr(flat),
+                        _ptr(dark), _ptr(outs), outs.shape[-1])
+        _check(lib().gr_reconstruct_batch(self._h, C.byref(b), _stream_ptr(stream)),
+               "gr_reconstruct_batch")
+
+    def reconstruct_host(self, sinos: np.ndarray, outs: np.ndarray, centers=None, flat=None,
+                         dark=None, dtype=None, stream=0):
+        """Host arrays (numpy or pinned torch CPU tensors); blocks until done."""
+        def addr(x):
+            if x is None:
+                return None
+            if isinstance(x, np.ndarray):
+                return x.ctypes.data
+            return int(x.data_ptr())
+        if dtype is None:
+            dt = str(sinos.dtype)
+            dtype = DTYPE_F32 if "float32" in dt else DTYPE_F16 if "float16" in dt and "b" not in dt \
+                else DTYPE_BF16 if "bfloat16" in dt else DTYPE_U16_RAW
+        keep = []
+        if centers is not None and isinstance(centers, np.ndarray):
+            centers = np.ascontiguousarray(centers, np.float32)
+            keep.append(centers)
+        b = self._batch(sinos.shape[0], dtype, addr(sinos), addr(centers), addr(flat), addr(dark),
+                        addr(outs), outs.shape[-1])
+        _check(lib().gr_reconstruct_host(self._h, C.byref(b), stream), "gr_reconstruct_host")
+
+
+class GridRec:
+    """The reference's GridRec call surface on the B200 library.
+
+    Mirrors gridrec/GPU/gridrec.h:72-143 and recon_algorithm.h:56-95: set the
+    sinogram dimensions, theta list (degrees), filter code and device, call
+    init(), hand over the two slices' host buffers with setSinoAndReconBuffers
+    (sinogram n_ang x n_det float32; reconstruction n_det x n_det float32, the
+    leading M0 x M0 block written with row stride n_det as in gridrec.cu:196-197),
+    then reconstruct().  setCenter() adds the rotation centre that GridRec::init
+    fixes at n_det/2 (gridrec.cu:227) and find_shift's copy exposes.
+    """
+
+    def __init__(self):
+        self._dims = None
+        self._theta = None
+        self._filter = FILTER_NONE
+        self._device = 0
+        self._center = None
+        self._bufs = {}
+        self._plan = None
+
+    def numberOfSinogramsNeeded(self) -> int:
+        return 2
+
+    def numberOfReconstructions(self) -> int:
+        return 2
+
+    def setSinogramDimensions(self, x_dim: int, y_dim: int):
+        self._dims = (int(x_dim), int(y_dim))
+
+    def getSinogramXDimension(self):
+        return self._dims[0]
+
+    def getSinogramYDimension(self):
+        return self._dims[1]
+
+    def setThetaList(self, theta_list, theta_list_size: int):
+        self._theta = np.asarray(theta_list, np.float32)[:theta_list_size]
+
+    def getThetaListSize(self):
+        return len(self._theta)
+
+    def setFilter(self, filter_name: int):
+        self._filter = int(filter_name)
+
+    def getFilter(self) -> int:
+        return self._filter
+
+    def setGPUDeviceID(self, device: int):
+        self._device = int(device)
+
+    def getGPUDeviceID(self) -> int:
+        return self._device
+
+    def setCenter(self, center: float):
+        self._center = float(center)
+
+    def init(self):
+        n_det, n_ang = self._dims
+        self._plan = Plan(n_det, n_ang, self._theta, center=self._center, filter=self._filter,
+                          device=self._device, max_pairs=1)
+        self.M0 = self._plan.M0
+
+    def setSinoAndReconBuffers(self, number: int, sinogram, reconstruction):
+        if number in (1, 2):
+            self._bufs[number] = (sinogram, reconstruction)
+
+    def reconstruct(self):
+        n_det, n_ang = self._dims
+        s1, r1 = self._bufs[1]
+        s2, r2 = self._bufs.get(2, (np.zeros_like(s1), np.zeros_like(r1)))
+        sinos = np.stack([np.asarray(s1, np.float32).reshape(n_ang, n_det),
+                          np.asarray(s2, np.float32).reshape(n_ang, n_det)])
+        outs = np.zeros((2, self.M0, n_det), np.float32)
+        self._plan.reconstruct_host(sinos, outs)
+        for r, o in ((r1, outs[0]), (r2, outs[1])):
+            rv = np.asarray(r).reshape(-1, n_det)
+            rv[:self.M0, :self.M0] = o[:, :self.M0]
+
+    def destroy(self):
+        if self._plan is not None:
+            self._plan.close()
+            self._plan = None

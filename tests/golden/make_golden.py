@@ -1,0 +1,79 @@
+"""Generates the golden fixtures in this directory from the reference itself.
+
+Run from the repository root after ``oracle/build_ref.sh`` (needs the
+reference tree, so it runs in the build container, not on the GPU box):
+
+    python tests/golden/make_golden.py
+
+Each case_*.npz holds the inputs (two float32 sinograms, float32 angles,
+parameters) and the reference's outputs for them:
+  * ``ref32`` -- the reference GridRec class (FP32, NR FFT), gridrec/GPU/gridrec.cu
+  * ``ref64`` -- the same sources built with float -> double
+  * ``refb``  -- GridrecCPP 5.2 (explicit centre / sampl / C / filter name)
+Inputs are seeded synthetic sinograms (analytic ellipses + Poisson noise) or
+uniform random rows, so the files are reproducible from this script.
+"""
+from __future__ import annotations
+
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
+
+from oracle import oracle as O  # noqa: E402
+from projects_b200 import phantom as ph  # noqa: E402
+
+
+def _pair_phantom(n, a, center, seed, theta=None):
+    th = ph.angles_deg(a) if theta is None else theta
+    p = ph.line_integrals(ph.shepp_logan_ellipses(), n, th, center)
+    p *= 2.0 / p.max()
+    s1 = ph.poisson_log(p, 1e4, seed)
+    q = ph.line_integrals(ph.random_ellipses(seed), n, th, center) / (n / 2.0)
+    s2 = ph.poisson_log(q, 1e4, seed + 1)
+    return s1, s2, th.astype(np.float32)
+
+
+def case_gridrec_class(name, n, a, filt, seed, theta=None):
+    """Reference GridRec class (centre n/2, sampl 1, C 6)."""
+    s1, s2, th = _pair_phantom(n, a, n // 2, seed, theta)
+    r1, r2, m0, _ = O.ref_gridrec_pair(s1, s2, th, filter=filt)
+    q1, q2, _, _ = O.ref_gridrec_pair(s1, s2, th, filter=filt, fp64=True)
+    np.savez_compressed(os.path.join(HERE, f"case_{name}.npz"), kind="gridrec", sino1=s1,
+                        sino2=s2, theta=th, n_det=n, n_ang=a, filter=filt, center=n // 2,
+                        sampl=1.0, C=6.0, M0=m0, ref32_1=r1[:m0, :m0], ref32_2=r2[:m0, :m0],
+                        ref64_1=q1[:m0, :m0], ref64_2=q2[:m0, :m0])
+
+
+def case_gridrec_cpp(name, n, a, center, fname, C_, sampl, seed):
+    """GridrecCPP 5.2 with explicit centre, oversampling, PSWF C and filter name."""
+    s1, s2, th = _pair_phantom(n, a, center, seed)
+    b1, b2, m0 = O.refb_gridrec_pair(s1, s2, th, center=center, filter_name=fname, C_=C_,
+                                     sampl=sampl)
+    np.savez_compressed(os.path.join(HERE, f"case_{name}.npz"), kind="gridrec_cpp", sino1=s1,
+                        sino2=s2, theta=th, n_det=n, n_ang=a, filter_name=fname, center=center,
+                        sampl=sampl, C=C_, M0=m0, refb_1=b1[:m0, :m0], refb_2=b2[:m0, :m0])
+
+
+def main():
+    if not O.ref_available():
+        raise SystemExit("build the reference first: oracle/build_ref.sh")
+    rng = np.random.default_rng(7)
+    case_gridrec_class("a64x48_shlo", 64, 48, 1, 11)
+    case_gridrec_cpp("b100x37_c50_hann", 100, 37, 50.0, "hann", 6.0, 1.0, 12)
+    uneven = np.sort(rng.uniform(0.0, 180.0, 90)).astype(np.float32)
+    case_gridrec_class("a128x90_hamm_uneven", 128, 90, 3, 13, theta=uneven)
+    case_gridrec_class("a128x64_ramp", 128, 64, 4, 14)
+    case_gridrec_class("a32x50_none", 32, 50, 0, 15)
+    case_gridrec_cpp("b96x60_c47.3_s1.2_ramlak", 96, 60, 47.3, "ramlak", 6.0, 1.2, 21)
+    case_gridrec_cpp("b64x40_c31.7_C4_hann", 64, 40, 31.7, "hann", 4.0, 1.0, 22)
+    case_gridrec_cpp("b120x72_c61.2_C7_s1.2_shepp", 120, 72, 61.2, "shepp", 7.0, 1.2, 23)
+    case_gridrec_cpp("b72x45_c36.5_C5_hamming", 72, 45, 36.5, "hamming", 5.0, 1.0, 24)
+    print("\n".join(sorted(f for f in os.listdir(HERE) if f.endswith(".npz"))))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,221 @@
+"""GPU parity tests: the sm_100a path through the C ABI against the oracle.
+
+Tolerance (floating point): relative L2 <= 1e-3 against float64 gridrec,
+the bound the reconstructor is specified to; the reference's own FP32 build
+sits at ~5e-4 from float64.
+"""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from projects_b200 import gridrec as G
+from projects_b200 import phantom as ph
+from tests.golden_cases import cases
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-3
+CASES = cases()
+
+
+def _dev(a):
+    return torch.as_tensor(np.ascontiguousarray(a)).cuda()
+
+
+def _gpu_pair(s1, s2, theta, **kw):
+    n_ang, n_det = s1.shape
+    with G.Plan(n_det, n_ang, theta, **kw) as plan:
+        o1 = torch.zeros((plan.M0, max(plan.M0, n_det)), device="cuda")
+        o2 = torch.zeros_like(o1)
+        plan.reconstruct_pair(_dev(s1), _dev(s2), o1, o2)
+        torch.cuda.synchronize()
+        assert plan.launches() == 5
+        return o1.cpu().numpy()[:, :plan.M0], o2.cpu().numpy()[:, :plan.M0]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_pair_against_goldens(case):
+    g1, g2 = _gpu_pair(case["sino1"], case["sino2"], case["theta"], center=case["center"],
+                       filter=case["filter"], pswf_c=case["C"], sampl=case["sampl"])
+    m = case["M0"]
+    assert g1.shape == (m, m)
+    o1, o2 = O.port_gridrec_pair(case["sino1"], case["sino2"], case["theta"],
+                                 center1=case["center"], filter=case["filter"], C_=case["C"],
+                                 sampl=case["sampl"])
+    assert ph.rel_l2(g1, o1[:, :m]) < TOL
+    assert ph.rel_l2(g2, o2[:, :m]) < TOL
+    # and against the reference's own FP32 output
+    assert ph.rel_l2(g1, case["ref32"][0]) < 2 * TOL
+    assert ph.rel_l2(g2, case["ref32"][1]) < 2 * TOL
+
+
+def test_shepp_logan_512x360():
+    """512 detectors x 360 angles on [0, pi), centre 256.3, Shepp-Logan filter."""
+    th = ph.angles_deg(360)
+    s1 = ph.shepp_logan_sinogram(512, 360, center=256.3, noise_seed=1)
+    s2 = ph.shepp_logan_sinogram(512, 360, center=256.3, noise_seed=2)
+    g1, g2 = _gpu_pair(s1, s2, th, center=256.3, filter=G.FILTER_SHEPP_LOGAN)
+    o1, o2 = O.port_gridrec_pair(s1, s2, th, center1=256.3, filter=1)
+    assert g1.shape == (511, 511)
+    e1, e2 = ph.rel_l2(g1, o1[:, :511]), ph.rel_l2(g2, o2[:, :511])
+    assert e1 < TOL and e2 < TOL, (e1, e2)
+
+
+def test_reference_gridrec_class_live():
+    """Against the reference GridRec class run here (centre n/2)."""
+    if not O.ref_available():
+        pytest.skip("reference not built")
+    th = ph.angles_deg(180)
+    s1 = ph.shepp_logan_sinogram(256, 180, center=128.0, noise_seed=3)
+    s2 = ph.shepp_logan_sinogram(256, 180, center=128.0, noise_seed=4)
+    r1, r2, m0, _ = O.ref_gridrec_pair(s1, s2, th, filter=2)
+    g1, g2 = _gpu_pair(s1, s2, th, filter=2)
+    assert ph.rel_l2(g1, r1[:m0, :m0]) < 2 * TOL
+    assert ph.rel_l2(g2, r2[:m0, :m0]) < 2 * TOL
+
+
+def test_batch_per_slice_centres_odd_count():
+    n, a = 128, 96
+    th = ph.angles_deg(a)
+    centers = np.array([63.7, 64.9, 62.2, 65.5, 64.0], np.float32)
+    sinos = np.stack([ph.random_ellipse_sinogram(s, n, a, center=float(c))[0]
+                      for s, c in enumerate(centers)])
+    with G.Plan(n, a, th, filter=G.FILTER_HANN, max_pairs=2) as plan:
+        outs = torch.zeros((5, plan.M0, 136), device="cuda")
+        plan.reconstruct_batch(_dev(sinos), outs, centers=_dev(centers))
+        torch.cuda.synchronize()
+        got = outs.cpu().numpy()[:, :, :plan.M0]
+        assert plan.launches() == 5 * 2       # 3 pairs in chunks of 2
+    zero = np.zeros_like(sinos[0])
+    for i in range(5):
+        if i % 2 == 0:
+            other = sinos[i + 1] if i + 1 < 5 else zero
+            c2 = float(centers[i + 1]) if i + 1 < 5 else float(centers[i])
+            ref, _ = O.port_gridrec_pair(sinos[i], other, th, center1=float(centers[i]),
+                                         center2=c2, filter=2)
+        else:
+            _, ref = O.port_gridrec_pair(sinos[i - 1], sinos[i], th,
+                                         center1=float(centers[i - 1]),
+                                         center2=float(centers[i]), filter=2)
+        assert ph.rel_l2(got[i], ref[:, :got.shape[-1]]) < TOL, i
+
+
+@pytest.mark.parametrize("dtype,tol", [("float16", 2e-3), ("bfloat16", 1.5e-2)])
+def test_reduced_precision_storage(dtype, tol):
+    n, a = 256, 128
+    th = ph.angles_deg(a)
+    sinos = np.stack([ph.random_ellipse_sinogram(s, n, a, center=128.0)[0] for s in range(2)])
+    o1, o2 = O.port_gridrec_pair(sinos[0], sinos[1], th, center1=128.0, filter=2)
+    with G.Plan(n, a, th, filter=G.FILTER_HANN, center=128.0) as plan:
+        outs = torch.zeros((2, plan.M0, plan.M0), device="cuda")
+        plan.reconstruct_batch(_dev(sinos).to(getattr(torch, dtype)), outs)
+        got = outs.cpu().numpy()
+    e = max(ph.rel_l2(got[0], o1[:, :plan.M0]), ph.rel_l2(got[1], o2[:, :plan.M0]))
+    print(f"{dtype} storage: relL2 vs float64 = {e:.2e}")
+    assert e < tol
+
+
+def test_raw_uint16_fused_normalisation():
+    n, a = 256, 120
+    th = ph.angles_deg(a)
+    p = [ph.line_integrals(ph.random_ellipses(s), n, th, 128.0) / (n / 2) for s in range(2)]
+    raws, flat, dark = [], None, None
+    for s in range(2):
+        r, flat, dark = ph.raw_counts(p[s], seed=9)  # same flat/dark rows for both
+        raws.append(r)
+    raws = np.stack(raws)
+    # host-side normalisation, as gridrec/GPU/tomo_recon.cpp:1533-1541
+    v = raws.astype(np.float32) - dark
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = (flat - dark) / v
+        norm = np.where((v > 0) & (r > 0), np.log(r), 0.0).astype(np.float32)
+    o1, o2 = O.port_gridrec_pair(norm[0], norm[1], th, center1=128.0, filter=1)
+    with G.Plan(n, a, th, center=128.0) as plan:
+        outs = torch.zeros((2, plan.M0, plan.M0), device="cuda")
+        plan.reconstruct_batch(_dev(raws.view(np.int16)), outs, flat=_dev(flat), dark=_dev(dark),
+                               dtype=G.DTYPE_U16_RAW)
+        got = outs.cpu().numpy()
+    assert ph.rel_l2(got[0], o1[:, :plan.M0]) < TOL
+    assert ph.rel_l2(got[1], o2[:, :plan.M0]) < TOL
+
+
+def test_host_streaming_matches_device_batch():
+    n, a = 128, 64
+    th = ph.angles_deg(a)
+    sinos = np.stack([ph.random_ellipse_sinogram(s, n, a, center=64.0)[0] for s in range(7)])
+    with G.Plan(n, a, th, center=64.0, max_pairs=2) as plan:
+        host_out = np.zeros((7, plan.M0, 130), np.float32)
+        plan.reconstruct_host(sinos, host_out)            # pageable: staged
+        pinned_in = torch.from_numpy(sinos).pin_memory()
+        pinned_out = torch.zeros((7, plan.M0, 130)).pin_memory()
+        plan.reconstruct_host(pinned_in, pinned_out)      # pinned: direct copies
+        dev_out = torch.zeros((7, plan.M0, 130), device="cuda")
+        plan.reconstruct_batch(_dev(sinos), dev_out)
+        torch.cuda.synchronize()
+    d = dev_out.cpu().numpy()
+    assert ph.rel_l2(host_out[:, :, :plan.M0], d[:, :, :plan.M0]) < 1e-6
+    assert ph.rel_l2(pinned_out.numpy()[:, :, :plan.M0], d[:, :, :plan.M0]) < 1e-6
+
+
+def test_gridrec_class_call_surface():
+    """The reference's setter sequence (tomo_recon.cpp:1701-1706, 3846-3852)."""
+    n, a = 128, 100
+    th = ph.angles_deg(a)
+    s1 = ph.shepp_logan_sinogram(n, a, center=64.0, noise_seed=1)
+    s2 = ph.shepp_logan_sinogram(n, a, center=64.0, noise_seed=2)
+    g = G.GridRec()
+    assert g.numberOfSinogramsNeeded() == 2
+    g.setSinogramDimensions(n, a)
+    g.setThetaList(th, a)
+    g.setFilter(G.FILTER_HAMMING)
+    g.setGPUDeviceID(0)
+    g.init()
+    r1 = np.zeros((n, n), np.float32)
+    r2 = np.zeros((n, n), np.float32)
+    g.setSinoAndReconBuffers(1, s1, r1)
+    g.setSinoAndReconBuffers(2, s2, r2)
+    g.reconstruct()
+    g.destroy()
+    o1, o2 = O.port_gridrec_pair(s1, s2, th, filter=3)
+    m = o1.shape[0]
+    assert ph.rel_l2(r1[:m, :m], o1[:, :m]) < TOL
+    assert ph.rel_l2(r2[:m, :m], o2[:, :m]) < TOL
+    assert np.all(r1[m:, :] == 0) and np.all(r1[:, m:] == 0)
+
+
+@pytest.mark.parametrize("n,a,theta", [
+    (9, 1, None),                                   # smallest supported width, one angle
+    (33, 7, np.array([-40, 0, 10, 95, 180, 250, 359], np.float32)),  # angles outside [0, 180)
+    (300, 3, None),
+])
+def test_edge_shapes(n, a, theta):
+    th = ph.angles_deg(a) if theta is None else theta
+    rng = np.random.default_rng(n)
+    s1, s2 = rng.random((a, n)).astype(np.float32), rng.random((a, n)).astype(np.float32)
+    g1, g2 = _gpu_pair(s1, s2, th, filter=4)
+    o1, o2 = O.port_gridrec_pair(s1, s2, th, filter=4)
+    m = g1.shape[0]
+    assert ph.rel_l2(g1, o1[:, :m]) < TOL
+    assert ph.rel_l2(g2, o2[:, :m]) < TOL
+
+
+def test_full_size_2048x1500_and_linearity():
+    """One pair at the benchmark shape against float64, plus linearity in the input."""
+    n, a = 2048, 1500
+    th = ph.angles_deg(a)
+    s1, c1 = ph.random_ellipse_sinogram(0, n, a, center=1024.0)
+    s2, _ = ph.random_ellipse_sinogram(1, n, a, center=1024.0)
+    with G.Plan(n, a, th, filter=G.FILTER_HANN, max_pairs=1) as plan:
+        o = torch.zeros((2, plan.M0, n), device="cuda")
+        plan.reconstruct_pair(_dev(s1), _dev(s2), o[0], o[1])
+        o_lin = torch.zeros_like(o)
+        plan.reconstruct_pair(_dev(2.0 * s1 - s2), _dev(s2), o_lin[0], o_lin[1])
+        torch.cuda.synchronize()
+        g = o.cpu().numpy()[:, :, :plan.M0]
+        gl = o_lin.cpu().numpy()[:, :, :plan.M0]
+    r1, r2 = O.port_gridrec_pair(s1, s2, th, filter=2)
+    e1, e2 = ph.rel_l2(g[0], r1[:, :2047]), ph.rel_l2(g[1], r2[:, :2047])
+    print(f"2048x1500 relL2 vs float64: {e1:.2e} {e2:.2e}")
+    assert e1 < TOL and e2 < TOL
+    assert ph.rel_l2(gl[0], 2 * g[0] - g[1]) < TOL

@@ -1,0 +1,151 @@
+"""CPU tests: the C-ABI library, its host-side logic and the phantom generator."""
+import ctypes as C
+import os
+import re
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from projects_b200 import gridrec as G
+from projects_b200 import phantom as ph
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_functions():
+    names = set()
+    inc = os.path.join(ROOT, "include")
+    for f in os.listdir(inc):
+        if f.endswith(".h"):
+            src = open(os.path.join(inc, f)).read()
+            src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+            names |= set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(gr_\w+)\s*\(", src, re.M))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = G.lib()
+    declared = _declared_functions()
+    assert declared, "no declarations parsed"
+    for name in declared:
+        assert hasattr(lib, name), f"{name} declared in include/ but not exported"
+    assert set(G.EXPORTS) <= declared
+
+
+def test_filter_codes():
+    codes = {n: G.filter_code(n) for n in
+             ["shlo", "shepp", "hann", "hamm", "hamming", "ramp", "ramlak", "none", "bogus"]}
+    assert codes == {"shlo": 1, "shepp": 1, "hann": 2, "hamm": 3, "hamming": 3, "ramp": 4,
+                     "ramlak": 4, "none": 0, "bogus": 1}
+
+
+def test_params_default():
+    th = np.zeros(10, np.float32)
+    p, _ = G.make_params(64, 10, th)
+    assert (p.n_det, p.n_ang, p.filter, p.ltbl, p.max_pairs) == (64, 10, 1, 512, 1)
+    assert p.center < 0 and abs(p.pswf_c - 6.0) < 1e-6 and abs(p.sampl - 1.0) < 1e-6
+
+
+@pytest.mark.parametrize("bad,code", [
+    (dict(pswf_c=5.5), -2),       # not in the PSWF database
+    (dict(n_det=8), -1),          # below the smallest FFT
+    (dict(ltbl=0), -1),
+    (dict(sampl=0.5), -1),
+])
+def test_parameter_errors(bad, code):
+    kw = dict(n_det=64, n_ang=10, pswf_c=6.0, sampl=1.0, ltbl=512)
+    kw.update(bad)
+    p, th = G.make_params(kw["n_det"], kw["n_ang"], np.zeros(kw["n_ang"], np.float32),
+                          pswf_c=kw["pswf_c"], sampl=kw["sampl"], ltbl=kw["ltbl"])
+    ni = C.c_int()
+    rc = G.lib().gr_worklist_export(C.byref(p), C.byref(ni), None, None, None, None, None, 0, 0)
+    assert rc == code
+    assert G.last_error()
+
+
+def _emulate_gather(n, a, theta, sampl=1.0, pswf_c=6.0):
+    """Numpy float64 execution of the gridding kernel's gather over the
+    exported work list, compared with the oracle's scatter (gridrec.cu:540-576)."""
+    p = O.params(n, a, None, None, 1, pswf_c, sampl)
+    sz = O.port_sizes(p)
+    rng = np.random.default_rng(n + a)
+    spec = O.port_spectra(p, rng.random((a, n)), rng.random((a, n)))
+    href = O.port_grid(p, theta, spec)
+    items, runs, splits, tiles_v = G.worklist(n, a, theta, sampl=sampl, pswf_c=pswf_c)
+    M, L2 = sz.M, sz.L / 2
+    ts = 2 * 512 / sz.L
+    wtbl, _ = O.port_tables(p)
+    H = np.zeros((M, M), complex)
+    T = 32
+    seen = np.zeros(len(runs), int)
+    for tile, rb, re_, slot in items:
+        tu, tv = divmod(tile, tiles_v)
+        p0, q0 = tu * T, tv * T
+        seen[rb:re_] += 1
+        for d, jlo, jhi in runs[rb:re_]:
+            nn, h = divmod(d, 2)
+            t = np.deg2rad(float(theta[nn]))
+            sg = -1.0 if h else 1.0
+            js = np.arange(jlo, jhi + 1)
+            U = M / 2 + sg * sz.scale * js * np.cos(t)
+            V = M / 2 + sg * sz.scale * js * np.sin(t)
+            for k, j in enumerate(js):
+                for iu in range(max(int(np.ceil(U[k] - L2)), p0, 1),
+                                min(int(np.floor(U[k] + L2)), p0 + T - 1, M - 1) + 1):
+                    wu = wtbl[int(abs(U[k] - iu) * ts + 0.5)]
+                    for iv in range(max(int(np.ceil(V[k] - L2)), q0, 1),
+                                    min(int(np.floor(V[k] + L2)), q0 + T - 1, M - 1) + 1):
+                        H[iu, iv] += wu * wtbl[int(abs(V[k] - iv) * ts + 0.5)] * spec[nn, h, j]
+    assert np.all(seen == 1), "every run belongs to exactly one item"
+    # split tiles: slots of a tile are consecutive and counted
+    for tile, rb, re_, slot in items:
+        if slot >= 0:
+            sp = splits[tile]
+            assert sp[1] <= slot < sp[1] + sp[2]
+    return np.linalg.norm(H - href) / np.linalg.norm(href)
+
+
+@pytest.mark.parametrize("n,a,sampl,C_", [(64, 48, 1.0, 6.0), (100, 37, 1.2, 6.0),
+                                          (72, 30, 1.0, 4.0), (90, 25, 1.2, 7.0)])
+def test_worklist_gather_equals_scatter(n, a, sampl, C_):
+    th = ph.angles_deg(a)
+    assert _emulate_gather(n, a, th, sampl, C_) < 1e-14
+
+
+def test_worklist_gather_arbitrary_angles():
+    th = np.array([-30.0, 0.0, 12.5, 90.0, 179.9, 200.0, 359.0, 45.0], np.float32)
+    assert _emulate_gather(48, len(th), th) < 1e-14
+
+
+def test_worklist_splits_heavy_tiles():
+    items, runs, splits, tiles_v = G.worklist(2048, 1500, ph.angles_deg(1500))
+    cost = np.array([(runs[b:e, 2] - runs[b:e, 1] + 1).sum() for _, b, e, _ in items])
+    assert cost.max() <= 6144 + 2048       # kItemCap (+ one run)
+    assert (items[:, 3] >= 0).sum() > 0     # the centre tiles are split
+    assert np.all(np.diff(cost) <= 0)       # heaviest first
+    # samples visited ~ 2 * n_ang * (pdim/2 - 1) plus the tile halo
+    assert 1.0 < cost.sum() / (2 * 1500 * 1023) < 1.6
+
+
+def test_phantom_line_integrals():
+    # a centred disk of radius r: p(t) = 2 sqrt(r^2 - t^2) (in units of n/2)
+    e = np.array([[1.0, 0.5, 0.5, 0.0, 0.0, 0.0]])
+    n = 64
+    p = ph.line_integrals(e, n, np.array([0.0, 33.0]), n / 2)
+    t = (np.arange(n) - n / 2) / (n / 2)
+    expect = np.where(np.abs(t) < 0.5, 2 * np.sqrt(np.clip(0.25 - t * t, 0, None)), 0) * (n / 2)
+    np.testing.assert_allclose(p[0], expect, atol=1e-9)
+    np.testing.assert_allclose(p[1], expect, atol=1e-9)
+    s = ph.shepp_logan_sinogram(128, 90, center=64.3, noise_seed=1)
+    assert s.shape == (90, 128) and s.dtype == np.float32
+    assert 1.5 < s.max() < 3.0
+
+
+def test_raw_counts_roundtrip():
+    p = ph.line_integrals(ph.random_ellipses(4), 64, ph.angles_deg(20), 32.0) / 32.0
+    raw, flat, dark = ph.raw_counts(p, seed=1)
+    assert raw.dtype == np.uint16
+    v = raw.astype(np.float64) - dark
+    est = np.log((flat - dark) / v)
+    assert np.abs(est - p).mean() < 0.05

@@ -1,0 +1,80 @@
+"""CPU tests: the float64 oracle against the reference's own outputs."""
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from projects_b200 import phantom as ph
+from tests.golden_cases import cases
+
+CASES = cases()
+
+
+@pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
+def test_port_against_reference_goldens(case):
+    o1, o2 = O.port_gridrec_pair(case["sino1"], case["sino2"], case["theta"],
+                                 center1=case["center"], filter=case["filter"], C_=case["C"],
+                                 sampl=case["sampl"])
+    m = case["M0"]
+    assert o1.shape[0] == m
+    if case["ref64"] is not None:
+        # same algorithm, same float64 arithmetic: agreement to rounding
+        assert ph.rel_l2(o1[:, :m], case["ref64"][0]) < 1e-12
+        assert ph.rel_l2(o2[:, :m], case["ref64"][1]) < 1e-12
+    # the FP32 reference is ~5e-4 away from float64 gridrec
+    assert ph.rel_l2(o1[:, :m], case["ref32"][0]) < 2e-3
+    assert ph.rel_l2(o2[:, :m], case["ref32"][1]) < 2e-3
+
+
+def test_sizes_follow_gridrec_init():
+    # gridrec.cu:243-268 at the benchmark shapes
+    for n, pdim, M, M0 in [(512, 512, 512, 511), (2048, 2048, 2048, 2047), (100, 128, 128, 127),
+                           (1024, 1024, 1024, 1023)]:
+        s = O.port_sizes(O.params(n, 10))
+        assert (s.pdim, s.M, s.M0) == (pdim, M, M0)
+    s = O.port_sizes(O.params(2048, 10, sampl=1.2))
+    assert (s.M, s.M0) == (4096, 3413)
+    assert abs(s.L - 2 * 6.0 * s.sampl / np.pi) < 1e-12
+
+
+def test_tables():
+    p = O.params(512, 360)
+    wtbl, winv = O.port_tables(p)
+    assert wtbl[0] == 1.0
+    assert np.all(np.diff(wtbl) < 0)          # PSWF decreasing on [0, 1]
+    m02 = len(winv) // 2
+    np.testing.assert_allclose(winv[m02 - 5:m02], winv[m02 + 5:m02:-1])
+    assert np.all(np.sign(winv[m02:m02 + 6]) == [1, -1, 1, -1, 1, -1])  # checkerboard
+
+
+def test_fft_conventions():
+    x = np.random.default_rng(0).standard_normal(64) + 0j
+    y = np.ascontiguousarray(np.stack([x.real, x.imag], -1).ravel())
+    O.port_lib().orc_fft1d(y, 64, +1)
+    np.testing.assert_allclose(y[0::2] + 1j * y[1::2], np.fft.ifft(x) * 64, atol=1e-12)
+    H = np.random.default_rng(1).standard_normal((32, 32)) + 0j
+    np.testing.assert_allclose(O.port_fft2d(H), np.fft.fft2(H), atol=1e-10)
+
+
+def test_two_centres_decouple_the_slices():
+    """Per-slice centres: slice 1 of (s1, s2; c1, c2) equals slice 1 of (s1, 0; c1)."""
+    n, a = 64, 40
+    th = ph.angles_deg(a)
+    rng = np.random.default_rng(3)
+    s1, s2 = rng.random((a, n)), rng.random((a, n))
+    o1, o2 = O.port_gridrec_pair(s1, s2, th, center1=31.3, center2=33.1)
+    r1, _ = O.port_gridrec_pair(s1, np.zeros_like(s2), th, center1=31.3)
+    r2, _ = O.port_gridrec_pair(s2, np.zeros_like(s1), th, center1=33.1)
+    assert ph.rel_l2(o1, r1) < 1e-12
+    assert ph.rel_l2(o2, r2) < 1e-12
+
+
+@pytest.mark.skipif(not O.ref_available(), reason="reference not built (oracle/build_ref.sh)")
+def test_port_against_live_reference():
+    n, a = 256, 120
+    th = ph.angles_deg(a)
+    s1 = ph.shepp_logan_sinogram(n, a, center=128.0, noise_seed=5)
+    s2 = ph.shepp_logan_sinogram(n, a, center=128.0, noise_seed=6)
+    r1, r2, m0, _ = O.ref_gridrec_pair(s1, s2, th, filter=2, fp64=True)
+    o1, o2 = O.port_gridrec_pair(s1, s2, th, filter=2)
+    assert ph.rel_l2(o1[:, :m0], r1[:m0, :m0]) < 1e-12
+    assert ph.rel_l2(o2[:, :m0], r2[:m0, :m0]) < 1e-12
