@@ -158,7 +158,7 @@ int gr_plan_stage_times(gr_plan* plan, double* ms5, long* chunks);
 /* Host-only export of the gridding work list a plan with these parameters
  * would use (no GPU needed).  With items/runs/splits NULL, only the counts
  * are returned.  Layouts: items = n_items x {tile, run_begin, run_end, slot};
- * runs = n_runs x {direction (2*angle + half), jlo, jhi}; splits = one
+ * runs = n_runs x {direction (2*angle + half), jlo, jhi, step spacing P}; splits = one
  * {counter, slot0, nsplit, 0} per tile (tile = tu * tiles_v + tv, 32 x 32 cells). */
 int gr_worklist_export(const gr_params* p, int* n_items, int* n_runs, int* tiles_v, int* items,
                        int* runs, int* splits, int cap_items, int cap_runs);

@@ -60,7 +60,8 @@ def port_lib():
 
 
 def params(n_det, n_ang, center1=None, center2=None, filter=1, C_=6.0, sampl=1.0, ltbl=512):
-    c1 = n_det / 2.0 if center1 is None else float(center1)
+    # GridRec::init: center = sinogram_x_dim / 2 in integer arithmetic (gridrec.cu:227)
+    c1 = float(n_det // 2) if center1 is None else float(center1)
     c2 = c1 if center2 is None else float(center2)
     return OrcParams(int(n_det), int(n_ang), c1, c2, int(filter), float(C_), float(sampl),
                      int(ltbl))

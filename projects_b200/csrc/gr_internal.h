@@ -16,14 +16,17 @@ constexpr int kTile = 32;
 // Largest number of taps per dimension the gridding kernel handles
 // (floor(L) + 1 with L = 2*C*sampl/pi < 6).
 constexpr int kMaxTaps = 6;
-// Samples per gridding work item before a tile is split across CTAs.
-constexpr int kItemCap = 6144;
+// Work per gridding item before a tile is split over several items, in
+// sample slots (steps x samples per step).
+constexpr int kItemCap = 2048;
 
-// One run of samples: direction d (= 2*angle + half), samples j in [jlo, jhi].
+// One run of samples: direction d (= 2*angle + half), samples j in [jlo, jhi],
+// gridded in steps of samples P apart (footprints of one step disjoint).
 struct Run {
   int dir;
   int jlo;
   int jhi;
+  int P;
 };
 
 // One gridding work item: runs [run_begin, run_end) of `tile`; slot >= 0 when
@@ -70,14 +73,15 @@ struct PhaseArgs {
 struct GridArgs {
   const float2* spec;
   float2* H;             // [pair][M][M]
-  float2* scratch;       // [pair][n_slots][T*T]
-  unsigned* counters;    // [pair][n_split]
+  float4* scratch;       // [pair group][n_slots][T*T] partial tiles of split tiles
+  unsigned* queue;       // work-queue head (zeroed before each launch)
   const Item* items;
   const Run* runs;
-  const Split* splits;   // per tile index (only meaningful when slot >= 0)
+  const int4* split_list;  // per split tile: (tile, slot0, nsplit, 0)
+  int n_split_tiles;
   const float2* dir;     // per direction (scale*dx, scale*dy)
   const float* wtbl;     // ltbl + 1
-  int n_items, pairs, n_ang, J, M, tiles_v, n_slots, n_split, ltbl;
+  int n_items, pairs, n_ang, J, M, tiles_v, n_slots, ltbl;
   float L2, tblspcg;
 };
 

@@ -19,6 +19,8 @@
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
+
 #include "gr_internal.h"
 
 namespace gr {
@@ -290,120 +292,205 @@ __global__ void __launch_bounds__(512) spectra_kernel(SpectraArgs a) {
 }
 
 // ------------------------------------------------------------------ gridding (K2)
-// Gather formulation: the CTA owns one kTile x kTile tile of H and visits the
-// samples of its work item (runs of consecutive j along one direction, built
-// on the host from the exact ray/tile geometry).  Each sample adds
-// w(|u - iu|) w(|v - iv|) C to every cell of the tile within L/2 in both
-// coordinates, the tap set and nearest-neighbour table index of
+// Gather over binned work items: each work item is one kTile x kTile tile of
+// H plus the runs of samples (consecutive j along one direction, built on the
+// host from the exact ray/tile geometry) whose footprint can reach the tile.
+// Each sample adds w(|u - iu|) w(|v - iv|) C to every cell within L/2 in both
+// coordinates -- the tap set and nearest-neighbour table index of
 // gridrec.cu:546-566.  The second half of the reference's scatter
 // (H[M-iu][M-iv] += w C2) is the direction d = 2n+1 at the mirrored position.
 // Cells in row 0 or column 0 stay zero (the reference clamps taps to [1, M-1]).
+//
+// Execution: a persistent grid of warps pulls (work item, pair group) entries
+// from a queue.  A warp accumulates the tile of kGridPairs slice pairs (their
+// cells interleaved as float4) in a private shared-memory tile, NT lanes per
+// sample (lane t owns footprint row t; column weights are exchanged by
+// shuffles), so the geometry -- positions, table lookups -- is computed once
+// for both pairs.  The samples of one step are taken P apart along the run
+// with P * max(|du|,|dv|) >= NT, so their NT x NT footprints are disjoint:
+// (P per run from the host, which uses the same criterion)
+// plain read-modify-write needs no atomics, and the summation order is fixed,
+// so the result is bitwise reproducible.  Float/int conversions use exact
+// magic-number rounding on the FP32 pipe.  Tiles split over several items
+// leave partial tiles in scratch, summed in slot order by split_reduce_kernel.
+
+constexpr int kTileStride = kTile + 1;
+constexpr int kGridWarps = 4;
+constexpr int kGridPairs = 2;   // slice pairs gridded together from one set of weights
+constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: x + kMagic rounds x to an integer
+constexpr int kMagicBits = 0x4B400000;
+
+// ceil(x) as float and int, exact for |x| < 2^22.
+__device__ __forceinline__ float ceil_exact(float x, int& xi) {
+  const float y = x + kMagic;
+  float r = y - kMagic;
+  int i = __float_as_int(y) - kMagicBits;
+  if (r < x) {
+    r += 1.f;
+    i += 1;
+  }
+  xi = i;
+  return r;
+}
+
+// (int)(d * ts + 0.5) for d >= 0 -- the nearest-neighbour table index of
+// gridrec.h:53 -- exact for arguments below 2^22.
+__device__ __forceinline__ int table_index(float d, float ts) {
+  const float y = fmaf(d, ts, 0.5f);
+  const float r = (y + kMagic) - kMagic;
+  int i = __float_as_int(y + kMagic) - kMagicBits;
+  if (r > y) i -= 1;
+  return i;
+}
 
 template <int NT>
-__global__ void __launch_bounds__(256) grid_kernel(GridArgs a) {
-  __shared__ float acc_re[kTile * kTile];
-  __shared__ float acc_im[kTile * kTile];
-  __shared__ float s_wtbl[1025];
-  __shared__ int s_last;
-  const int item_idx = blockIdx.x / a.pairs;
-  const int pair = blockIdx.x - item_idx * a.pairs;
-  const Item it = a.items[item_idx];
-  const int tu = it.tile / a.tiles_v, tv = it.tile - (it.tile / a.tiles_v) * a.tiles_v;
-  const int p0 = tu * kTile, q0 = tv * kTile;
-  for (int i = threadIdx.x; i < kTile * kTile; i += blockDim.x) {
-    acc_re[i] = 0.f;
-    acc_im[i] = 0.f;
-  }
+__global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
+  constexpr int SPW = 32 / NT;  // samples per step
+  extern __shared__ float4 smem4[];
+  float* s_wtbl = reinterpret_cast<float*>(smem4);
+  float4* tiles = smem4 + 257;  // table: up to 1028 floats
   for (int i = threadIdx.x; i <= a.ltbl; i += blockDim.x) s_wtbl[i] = __ldg(&a.wtbl[i]);
   __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  const float half_m = (float)(a.M / 2);
-  const float offu = half_m - (float)p0, offv = half_m - (float)q0;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float4* tile = tiles + warp * (kTile * kTileStride);
+  const int slot_k = lane / NT;          // sample slot of this lane
+  const int t = lane - slot_k * NT;      // footprint row of this lane
+  const int lane0 = slot_k * NT;         // first lane of this sample
+  const bool lane_used = slot_k < SPW;
+  const float ft = (float)t, fslot = (float)slot_k;
   const float L2 = a.L2, ts = a.tblspcg;
   const int ltbl = a.ltbl;
-  const float2* specp = a.spec + (size_t)pair * a.n_ang * 2 * a.J;
-  for (int r = it.run_begin + warp; r < it.run_end; r += nwarps) {
-    const Run run = a.runs[r];
-    const float2 d = __ldg(&a.dir[run.dir]);
-    const float2* sp = specp + (size_t)run.dir * a.J;
-    for (int j = run.jlo + lane; j <= run.jhi; j += 32) {
-      const float fj = (float)j;
-      const float u = fmaf(fj, d.x, offu);
-      const float v = fmaf(fj, d.y, offv);
-      const float fu0 = ceilf(u - L2), fv0 = ceilf(v - L2);
-      const int iu0 = (int)fu0, iv0 = (int)fv0;
-      if (iu0 >= kTile || iv0 >= kTile || iu0 + NT <= 0 || iv0 + NT <= 0) continue;
-      const float2 c = __ldg(&sp[j]);
-      float wu[NT], wv[NT];
-#pragma unroll
-      for (int t = 0; t < NT; ++t) {
-        const float du = fabsf(u - (fu0 + (float)t));
-        const int row = iu0 + t;
-        wu[t] = (du <= L2 && row >= 0 && row < kTile) ? s_wtbl[min((int)(du * ts + 0.5f), ltbl)] : 0.f;
-        const float dv = fabsf(v - (fv0 + (float)t));
-        const int col = iv0 + t;
-        wv[t] = (dv <= L2 && col >= 0 && col < kTile) ? s_wtbl[min((int)(dv * ts + 0.5f), ltbl)] : 0.f;
-      }
-#pragma unroll
-      for (int t = 0; t < NT; ++t) {
-        if (wu[t] != 0.f) {
-          const float cr = wu[t] * c.x, ci = wu[t] * c.y;
-          const int rowoff = (iu0 + t) * kTile + iv0;
-#pragma unroll
-          for (int s = 0; s < NT; ++s) {
-            if (wv[s] != 0.f) {
-              atomicAdd(&acc_re[rowoff + s], wv[s] * cr);
-              atomicAdd(&acc_im[rowoff + s], wv[s] * ci);
-            }
+  const float half_m = (float)(a.M / 2);
+  const int groups = (a.pairs + kGridPairs - 1) / kGridPairs;
+  const unsigned total = (unsigned)a.n_items * (unsigned)groups;
+  const size_t spec_pair = (size_t)a.n_ang * 2 * a.J;
+  for (;;) {
+    unsigned w = 0;
+    if (lane == 0) w = atomicAdd(a.queue, 1u);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    if (w >= total) break;
+    const int grp = (int)(w / (unsigned)a.n_items);
+    const Item it = a.items[w - (unsigned)grp * (unsigned)a.n_items];
+    const int pA = grp * kGridPairs;
+    const bool hasB = pA + 1 < a.pairs;
+    const int tu = it.tile / a.tiles_v;
+    const int tv = it.tile - tu * a.tiles_v;
+    const int p0 = tu * kTile, q0 = tv * kTile;
+    for (int i = lane; i < kTile * kTileStride; i += 32) tile[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    __syncwarp();
+    const float offu = half_m - (float)p0, offv = half_m - (float)q0;
+    const float2* specA = a.spec + (size_t)pA * spec_pair;
+    const float2* specB = hasB ? specA + spec_pair : specA;
+    for (int r = it.run_begin; r < it.run_end; ++r) {
+      const Run run = a.runs[r];
+      const float2 d = __ldg(&a.dir[run.dir]);
+      const float2* spA = specA + (size_t)run.dir * a.J;
+      const float2* spB = specB + (size_t)run.dir * a.J;
+      // run.P: samples P apart have disjoint footprints (P * max(|du|,|dv|)
+      // >= NT with margin), chosen on the host to minimise the steps
+      const int P = run.P;
+      const float fP = (float)P;
+      for (int blk = run.jlo; blk <= run.jhi; blk += SPW * P) {
+        const float fblk = (float)blk;
+        for (int ph = 0; ph < P && blk + ph <= run.jhi; ++ph) {
+          const int j = blk + ph + P * slot_k;
+          const bool active = lane_used && j <= run.jhi;
+          const float fj = fmaf(fP, fslot, fblk + (float)ph);
+          const float u = fmaf(fj, d.x, offu);
+          const float v = fmaf(fj, d.y, offv);
+          int iu0, iv0;
+          const float fu0 = ceil_exact(u - L2, iu0);
+          const float fv0 = ceil_exact(v - L2, iv0);
+          const int row = iu0 + t;
+          const int col = iv0 + t;
+          const float du = fabsf(u - (fu0 + ft));
+          const float dv = fabsf(v - (fv0 + ft));
+          const float wtu = s_wtbl[min(table_index(du, ts), ltbl)];
+          const float wtv = s_wtbl[min(table_index(dv, ts), ltbl)];
+          const float wu = (active && du <= L2 && (unsigned)row < (unsigned)kTile) ? wtu : 0.f;
+          const float wvt = (active && dv <= L2 && (unsigned)col < (unsigned)kTile) ? wtv : 0.f;
+          float2 cA = make_float2(0.f, 0.f), cB = make_float2(0.f, 0.f);
+          if (wu != 0.f) {
+            cA = __ldg(&spA[j]);
+            cB = __ldg(&spB[j]);
           }
+          const float4 c4 = make_float4(wu * cA.x, wu * cA.y, wu * cB.x, wu * cB.y);
+          float wv[NT];
+#pragma unroll
+          for (int s2 = 0; s2 < NT; ++s2) wv[s2] = __shfl_sync(0xffffffffu, wvt, lane0 + s2);
+          float4* cell = tile + row * kTileStride + iv0;
+          float4 h[NT];
+#pragma unroll
+          for (int s2 = 0; s2 < NT; ++s2)
+            if (wu != 0.f && wv[s2] != 0.f) h[s2] = cell[s2];
+#pragma unroll
+          for (int s2 = 0; s2 < NT; ++s2) {
+            h[s2].x = fmaf(wv[s2], c4.x, h[s2].x);
+            h[s2].y = fmaf(wv[s2], c4.y, h[s2].y);
+            h[s2].z = fmaf(wv[s2], c4.z, h[s2].z);
+            h[s2].w = fmaf(wv[s2], c4.w, h[s2].w);
+          }
+#pragma unroll
+          for (int s2 = 0; s2 < NT; ++s2)
+            if (wu != 0.f && wv[s2] != 0.f) cell[s2] = h[s2];
+          __syncwarp();
         }
       }
     }
-  }
-  __syncthreads();
-  const int np = min(kTile, a.M - p0), nq = min(kTile, a.M - q0);
-  float2* Hp = a.H + (size_t)pair * a.M * a.M;
-  if (it.slot < 0) {
-    for (int i = threadIdx.x; i < kTile * kTile; i += blockDim.x) {
-      const int pr = i / kTile, qc = i - (i / kTile) * kTile;
-      if (pr < np && qc < nq) {
-        const int p = p0 + pr, q = q0 + qc;
-        const float2 val = (p == 0 || q == 0) ? make_float2(0.f, 0.f) : make_float2(acc_re[i], acc_im[i]);
-        Hp[(size_t)p * a.M + q] = val;
+    const int np = min(kTile, a.M - p0), nq = min(kTile, a.M - q0);
+    if (it.slot < 0) {
+      const size_t MM = (size_t)a.M * a.M;
+      float2* HA = a.H + (size_t)pA * MM;
+      float2* HB = HA + MM;
+      if (lane < nq) {
+        const int q = q0 + lane;
+        for (int pr = 0; pr < np; ++pr) {
+          const int p = p0 + pr;
+          float4 val = tile[pr * kTileStride + lane];
+          if (p == 0 || q == 0) val = make_float4(0.f, 0.f, 0.f, 0.f);
+          HA[(size_t)p * a.M + q] = make_float2(val.x, val.y);
+          if (hasB) HB[(size_t)p * a.M + q] = make_float2(val.z, val.w);
+        }
       }
+    } else {
+      // partial tile of a split tile: summed later by split_reduce_kernel
+      float4* part = a.scratch + ((size_t)grp * a.n_slots + it.slot) * (kTile * kTile);
+      for (int pr = 0; pr < kTile; ++pr) part[pr * kTile + lane] = tile[pr * kTileStride + lane];
     }
-    return;
+    __syncwarp();
   }
-  // Split tile: publish this item's partial tile; the last item of the tile
-  // to finish sums all partials in slot order (deterministic) and writes H.
-  float2* part = a.scratch + ((size_t)pair * a.n_slots + it.slot) * (kTile * kTile);
-  for (int i = threadIdx.x; i < kTile * kTile; i += blockDim.x)
-    part[i] = make_float2(acc_re[i], acc_im[i]);
-  __threadfence();
-  __syncthreads();
-  const Split sp = a.splits[it.tile];
-  if (threadIdx.x == 0) {
-    const unsigned prev = atomicAdd(&a.counters[(size_t)pair * a.n_split + sp.counter], 1u);
-    s_last = (prev == (unsigned)(sp.nsplit - 1));
-  }
-  __syncthreads();
-  if (!s_last) return;
-  __threadfence();
-  const float2* base = a.scratch + ((size_t)pair * a.n_slots + sp.slot0) * (kTile * kTile);
+}
+
+// Sums the partial tiles of every split tile in slot order and writes H.
+// Grid: (split tiles, pair groups); 256 threads over the tile's cells.
+__global__ void __launch_bounds__(256) split_reduce_kernel(GridArgs a) {
+  const int4 sp = a.split_list[blockIdx.x];  // (tile, slot0, nsplit, -)
+  const int grp = blockIdx.y;
+  const int pA = grp * kGridPairs;
+  const bool hasB = pA + 1 < a.pairs;
+  const int tu = sp.x / a.tiles_v, tv = sp.x - (sp.x / a.tiles_v) * a.tiles_v;
+  const int p0 = tu * kTile, q0 = tv * kTile;
+  const int np = min(kTile, a.M - p0), nq = min(kTile, a.M - q0);
+  const float4* base = a.scratch + ((size_t)grp * a.n_slots + sp.y) * (kTile * kTile);
+  const size_t MM = (size_t)a.M * a.M;
+  float2* HA = a.H + (size_t)pA * MM;
+  float2* HB = HA + MM;
   for (int i = threadIdx.x; i < kTile * kTile; i += blockDim.x) {
     const int pr = i / kTile, qc = i - (i / kTile) * kTile;
-    if (pr < np && qc < nq) {
-      float sr = 0.f, si = 0.f;
-      for (int k = 0; k < sp.nsplit; ++k) {
-        const float2 t = __ldcg(&base[(size_t)k * (kTile * kTile) + i]);
-        sr += t.x;
-        si += t.y;
-      }
-      const int p = p0 + pr, q = q0 + qc;
-      Hp[(size_t)p * a.M + q] = (p == 0 || q == 0) ? make_float2(0.f, 0.f) : make_float2(sr, si);
+    if (pr >= np || qc >= nq) continue;
+    float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int k = 0; k < sp.z; ++k) {
+      const float4 v4 = __ldg(&base[(size_t)k * (kTile * kTile) + i]);
+      sum.x += v4.x;
+      sum.y += v4.y;
+      sum.z += v4.z;
+      sum.w += v4.w;
     }
+    const int p = p0 + pr, q = q0 + qc;
+    if (p == 0 || q == 0) sum = make_float4(0.f, 0.f, 0.f, 0.f);
+    HA[(size_t)p * a.M + q] = make_float2(sum.x, sum.y);
+    if (hasB) HB[(size_t)p * a.M + q] = make_float2(sum.z, sum.w);
   }
-  if (threadIdx.x == 0) a.counters[(size_t)pair * a.n_split + sp.counter] = 0u;
 }
 
 // ------------------------------------------------------------------ 2-D FFT, first axis (K3)
@@ -471,7 +558,8 @@ cudaError_t init_kernel_attributes() {
   const void* fns[] = {(const void*)spectra_kernel<float>, (const void*)spectra_kernel<__half>,
                        (const void*)spectra_kernel<__nv_bfloat16>,
                        (const void*)spectra_kernel<uint16_t>, (const void*)cols_kernel,
-                       (const void*)rows_kernel};
+                       (const void*)rows_kernel, (const void*)grid_kernel<4>,
+                       (const void*)grid_kernel<kMaxTaps>};
   for (const void* f : fns) {
     if (e != cudaSuccess) break;
     e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
@@ -503,11 +591,33 @@ cudaError_t launch_spectra(const SpectraArgs& a, gr_dtype dt, cudaStream_t s) {
   return cudaErrorInvalidValue;
 }
 
+static int grid_smem_bytes() {
+  return 257 * (int)sizeof(float4) + kGridWarps * kTile * kTileStride * (int)sizeof(float4);
+}
+
 cudaError_t launch_grid(const GridArgs& a, int ntaps, cudaStream_t s) {
   if (a.n_items == 0) return cudaSuccess;
-  dim3 grid((unsigned)a.n_items * (unsigned)a.pairs);
-  if (ntaps <= 4) grid_kernel<4><<<grid, 256, 0, s>>>(a);
-  else grid_kernel<kMaxTaps><<<grid, 256, 0, s>>>(a);
+  cudaError_t e = cudaMemsetAsync(a.queue, 0, sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int smem = grid_smem_bytes();
+  int per_sm = 0;
+  if (ntaps <= 4) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_kernel<4>, kGridWarps * 32, smem);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_kernel<kMaxTaps>, kGridWarps * 32, smem);
+  }
+  const long groups = (a.pairs + kGridPairs - 1) / kGridPairs;
+  const long want = ((long)a.n_items * groups + kGridWarps - 1) / kGridWarps;
+  const int blocks = (int)std::min<long>(want, (long)std::max(per_sm, 1) * sms);
+  if (ntaps <= 4) grid_kernel<4><<<blocks, kGridWarps * 32, smem, s>>>(a);
+  else grid_kernel<kMaxTaps><<<blocks, kGridWarps * 32, smem, s>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess || a.n_split_tiles == 0) return e;
+  dim3 rgrid(a.n_split_tiles, (unsigned)groups);
+  split_reduce_kernel<<<rgrid, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -116,11 +116,13 @@ struct Plan {
   Item* d_items = nullptr;
   Run* d_runs = nullptr;
   Split* d_splits = nullptr;
-  unsigned* d_counters = nullptr;
+  int4* d_split_list = nullptr;
+  int n_split_tiles = 0;
+  unsigned* d_queue = nullptr;
   // workspaces (max_pairs pairs)
   float2* d_spec = nullptr;
   float2* d_H = nullptr;
-  float2* d_scratch = nullptr;
+  float4* d_scratch = nullptr;
   float4* d_pq = nullptr;
   // host streaming (gr_reconstruct_host)
   void* h_in[2] = {nullptr, nullptr};
@@ -178,11 +180,34 @@ struct WorkList {
   long total = 0;
 };
 
+// Step spacing P of a run (see grid_kernel): the smallest P with
+// P * max(|du|,|dv|) >= NT (with the kernel's margin) and, above it, the P
+// needing the fewest steps of spw samples; returns the step count in *steps.
+int run_spacing(double du, double dv, int n, int nt, int spw, int* steps) {
+  const float step = (float)std::max(std::fabs(du), std::fabs(dv));
+  const int pmin = std::max(1, (int)((float)nt * 1.0002f / step) + 1);
+  auto count = [&](int P) {
+    int st = 0;
+    for (int b = 0; b < n; b += spw * P) st += std::min(P, n - b);
+    return st;
+  };
+  int best = count(pmin), P = pmin;
+  for (int q = pmin + 1; q <= pmin + spw; ++q) {
+    const int c = count(q);
+    if (c < best) {
+      best = c;
+      P = q;
+    }
+  }
+  *steps = best;
+  return P;
+}
+
 void build_work_list(int M, int J, double L, int n_ang, const std::vector<double>& dxy,
                      WorkList* wl) {
   const int T = kTile;
   const double M2 = M / 2;
-  const double L2 = L / 2 + 1e-3;  // box margin covers FP32 position rounding
+  const double L2 = L / 2 + 2e-3;  // box margin covers FP32 position rounding
   wl->tiles_u = (M + T - 1) / T;
   wl->tiles_v = wl->tiles_u;
   const int n_tiles = wl->tiles_u * wl->tiles_v;
@@ -215,8 +240,8 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
         const double y0 = tv * T - L2, y1 = std::min(tv * T + T, M) - 1 + L2;
         double sa = ta, sb = tb;
         if (!slab(M2, dy, y0, y1, sa, sb)) continue;
-        const int jlo = std::max(1, (int)std::floor(sa) - 1);
-        const int jhi = std::min(J - 1, (int)std::ceil(sb) + 1);
+        const int jlo = std::max(1, (int)std::ceil(sa - 1e-6));
+        const int jhi = std::min(J - 1, (int)std::floor(sb + 1e-6));
         if (jlo > jhi) continue;
         all.push_back({tu * wl->tiles_v + tv, d, jlo, jhi});
       }
@@ -225,9 +250,16 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
   std::stable_sort(all.begin(), all.end(),
                    [](const TRun& a, const TRun& b) { return a.tile < b.tile; });
   wl->runs.resize(all.size());
+  std::vector<long> run_cost(all.size());
+  const int nt = (int)std::floor(L) + 1 <= 4 ? 4 : kMaxTaps;  // the kernel's NT
+  const int spw = 32 / nt;
   std::vector<int> first(n_tiles + 1, 0);
   for (size_t i = 0; i < all.size(); ++i) {
-    wl->runs[i] = {all[i].dir, all[i].jlo, all[i].jhi};
+    int steps = 0;
+    const int P = run_spacing(dxy[2 * all[i].dir], dxy[2 * all[i].dir + 1],
+                              all[i].jhi - all[i].jlo + 1, nt, spw, &steps);
+    wl->runs[i] = {all[i].dir, all[i].jlo, all[i].jhi, P};
+    run_cost[i] = (long)steps * spw + 4;  // sample slots + per-run overhead
     first[all[i].tile + 1]++;
   }
   for (int t = 0; t < n_tiles; ++t) first[t + 1] += first[t];
@@ -239,8 +271,10 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
   for (int t = 0; t < n_tiles; ++t) {
     const int b = first[t], e = first[t + 1];
     long cost = 0;
-    for (int r = b; r < e; ++r) cost += wl->runs[r].jhi - wl->runs[r].jlo + 1;
-    total += cost;
+    for (int r = b; r < e; ++r) {
+      cost += run_cost[r];
+      total += wl->runs[r].jhi - wl->runs[r].jlo + 1;
+    }
     if (cost <= kItemCap) {
       items.push_back({{t, b, e, -1}, cost});
       continue;
@@ -248,7 +282,7 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
     std::vector<std::pair<int, long>> cuts;  // (run_end, cost)
     long c = 0;
     for (int r = b; r < e; ++r) {
-      const long rc = wl->runs[r].jhi - wl->runs[r].jlo + 1;
+      const long rc = run_cost[r];
       if (c > 0 && c + rc > kItemCap) {
         cuts.push_back({r, c});
         c = 0;
@@ -361,9 +395,9 @@ int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1
                  p->d_tw_p, p->n_det, p->n_ang, p->pdim, p->J, pairs};
   GR_CUDA(launch_spectra(sa, dt, st));
   GR_MARK();
-  GridArgs ga{p->d_spec, p->d_H, p->d_scratch, p->d_counters, p->d_items, p->d_runs,
-              p->d_splits, p->d_dir, p->d_wtbl, p->n_items, pairs, p->n_ang, p->J, p->M,
-              p->tiles_v, p->n_slots, p->n_split, p->ltbl, (float)(p->L / 2),
+  GridArgs ga{p->d_spec, p->d_H, p->d_scratch, p->d_queue, p->d_items, p->d_runs,
+              p->d_split_list, p->n_split_tiles, p->d_dir, p->d_wtbl, p->n_items, pairs,
+              p->n_ang, p->J, p->M, p->tiles_v, p->n_slots, p->ltbl, (float)(p->L / 2),
               (float)(2.0 * p->ltbl / p->L)};
   GR_CUDA(launch_grid(ga, p->ntaps, st));
   GR_MARK();
@@ -545,25 +579,29 @@ int gr_plan_create(const gr_params* prm, gr_plan** out) {
   p->n_slots = wl.n_slots;
   p->n_split = wl.n_split;
   p->total_samples = wl.total;
+  std::vector<int4> split_list;
+  for (size_t t = 0; t < wl.splits.size(); ++t)
+    if (wl.splits[t].nsplit > 1)
+      split_list.push_back(make_int4((int)t, wl.splits[t].slot0, wl.splits[t].nsplit, 0));
+  p->n_split_tiles = (int)split_list.size();
   if ((rc = upload(p, &p->d_wtbl, fw)) || (rc = upload(p, &p->d_winv, fi)) ||
       (rc = upload(p, &p->d_filt, filt)) || (rc = upload(p, &p->d_tw_p, twiddles((int)pdim))) ||
       (rc = upload(p, &p->d_tw_m, twiddles((int)M))) || (rc = upload(p, &p->d_dir, dirs)) ||
       (rc = upload(p, &p->d_items, wl.items)) || (rc = upload(p, &p->d_runs, wl.runs)) ||
-      (rc = upload(p, &p->d_splits, wl.splits))) {
+      (rc = upload(p, &p->d_splits, wl.splits)) || (rc = upload(p, &p->d_split_list, split_list))) {
     gr_plan_destroy(p);
     return rc;
   }
   const size_t P = (size_t)p->max_pairs;
   if ((rc = dev_alloc(p, &p->d_spec, P * p->n_ang * 2 * p->J)) ||
       (rc = dev_alloc(p, &p->d_H, P * (size_t)M * M)) ||
-      (rc = dev_alloc(p, &p->d_scratch, P * (size_t)std::max(p->n_slots, 1) * kTile * kTile)) ||
+      (rc = dev_alloc(p, &p->d_scratch, ((P + 1) / 2) * (size_t)std::max(p->n_slots, 1) * kTile * kTile)) ||
       (rc = dev_alloc(p, &p->d_pq, P * p->J)) ||
-      (rc = dev_alloc(p, &p->d_counters, P * (size_t)std::max(p->n_split, 1)))) {
+      (rc = dev_alloc(p, &p->d_queue, 1))) {
     gr_plan_destroy(p);
     return rc;
   }
-  cudaError_t e = cudaMemset(p->d_counters, 0, P * std::max(p->n_split, 1) * sizeof(unsigned));
-  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  cudaError_t e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     gr_plan_destroy(p);
     return fail(GR_ERR_CUDA, "plan init: %s", cudaGetErrorString(e));

@@ -122,13 +122,16 @@ def make_params(n_det: int, n_ang: int, theta_deg, center=None, filter=FILTER_SH
 
 
 def worklist(n_det, n_ang, theta_deg, sampl=1.0, pswf_c=6.0):
-    """Host-only gridding work list: (items[n,4], runs[n,3], splits[tiles,4], tiles_v)."""
+    """Host-only gridding work list: (items[n,4], runs[n,4], splits[tiles,4], tiles_v).
+
+    runs rows are (direction, jlo, jhi, P): direction = 2*angle + half, samples
+    jlo..jhi, processed in steps of samples P apart."""
     p, th = make_params(n_det, n_ang, theta_deg, sampl=sampl, pswf_c=pswf_c)
     ni, nr, tv = C.c_int(), C.c_int(), C.c_int()
     _check(lib().gr_worklist_export(C.byref(p), C.byref(ni), C.byref(nr), C.byref(tv), None,
                                     None, None, 0, 0), "gr_worklist_export")
     items = np.zeros((ni.value, 4), np.int32)
-    runs = np.zeros((nr.value, 3), np.int32)
+    runs = np.zeros((nr.value, 4), np.int32)
     splits = np.zeros((tv.value * tv.value, 4), np.int32)
     _check(lib().gr_worklist_export(C.byref(p), C.byref(ni), C.byref(nr), C.byref(tv),
                                     items.ctypes.data, runs.ctypes.data, splits.ctypes.data,

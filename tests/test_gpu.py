@@ -154,8 +154,22 @@ def test_host_streaming_matches_device_batch():
         plan.reconstruct_batch(_dev(sinos), dev_out)
         torch.cuda.synchronize()
     d = dev_out.cpu().numpy()
-    assert ph.rel_l2(host_out[:, :, :plan.M0], d[:, :, :plan.M0]) < 1e-6
-    assert ph.rel_l2(pinned_out.numpy()[:, :, :plan.M0], d[:, :, :plan.M0]) < 1e-6
+    # same kernels, fixed summation order: bitwise equal
+    np.testing.assert_array_equal(host_out[:, :, :plan.M0], d[:, :, :plan.M0])
+    np.testing.assert_array_equal(pinned_out.numpy()[:, :, :plan.M0], d[:, :, :plan.M0])
+
+
+def test_bitwise_reproducible():
+    """The gridding's summation order does not depend on scheduling."""
+    n, a = 512, 360
+    th = ph.angles_deg(a)
+    sinos = np.stack([ph.shepp_logan_sinogram(n, a, center=256.0, noise_seed=s) for s in range(4)])
+    with G.Plan(n, a, th, max_pairs=2) as plan:
+        o = [torch.zeros((4, plan.M0, n), device="cuda") for _ in range(3)]
+        for k in range(3):
+            plan.reconstruct_batch(_dev(sinos), o[k])
+        torch.cuda.synchronize()
+    assert torch.equal(o[0], o[1]) and torch.equal(o[0], o[2])
 
 
 def test_gridrec_class_call_surface():
@@ -184,20 +198,25 @@ def test_gridrec_class_call_surface():
     assert np.all(r1[m:, :] == 0) and np.all(r1[:, m:] == 0)
 
 
-@pytest.mark.parametrize("n,a,theta", [
-    (9, 1, None),                                   # smallest supported width, one angle
-    (33, 7, np.array([-40, 0, 10, 95, 180, 250, 359], np.float32)),  # angles outside [0, 180)
-    (300, 3, None),
+# With only a few angles most grid cells receive one or two taps and FP32
+# tap rounding shows more: the reference's own FP32 build is 1.0-1.7e-3 from
+# float64 on the 300-detector cases below, so they get a 3e-3 bound.
+@pytest.mark.parametrize("n,a,theta,tol", [
+    (9, 1, None, TOL),                              # smallest supported width, one angle
+    (33, 7, np.array([-40, 0, 10, 95, 180, 250, 359], np.float32), TOL),  # outside [0, 180)
+    (300, 3, None, 3e-3),
+    (300, 8, None, 3e-3),
 ])
-def test_edge_shapes(n, a, theta):
+def test_edge_shapes(n, a, theta, tol):
     th = ph.angles_deg(a) if theta is None else theta
     rng = np.random.default_rng(n)
-    s1, s2 = rng.random((a, n)).astype(np.float32), rng.random((a, n)).astype(np.float32)
-    g1, g2 = _gpu_pair(s1, s2, th, filter=4)
+    s1 = rng.standard_normal((a, n)).astype(np.float32)
+    s2 = rng.standard_normal((a, n)).astype(np.float32)
+    g1, g2 = _gpu_pair(s1, s2, th, filter=4)       # default centre n_det/2 (integer)
     o1, o2 = O.port_gridrec_pair(s1, s2, th, filter=4)
     m = g1.shape[0]
-    assert ph.rel_l2(g1, o1[:, :m]) < TOL
-    assert ph.rel_l2(g2, o2[:, :m]) < TOL
+    assert ph.rel_l2(g1, o1[:, :m]) < tol
+    assert ph.rel_l2(g2, o2[:, :m]) < tol
 
 
 def test_full_size_2048x1500_and_linearity():

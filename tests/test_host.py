@@ -83,7 +83,7 @@ def _emulate_gather(n, a, theta, sampl=1.0, pswf_c=6.0):
         tu, tv = divmod(tile, tiles_v)
         p0, q0 = tu * T, tv * T
         seen[rb:re_] += 1
-        for d, jlo, jhi in runs[rb:re_]:
+        for d, jlo, jhi, _ in runs[rb:re_]:
             nn, h = divmod(d, 2)
             t = np.deg2rad(float(theta[nn]))
             sg = -1.0 if h else 1.0
@@ -118,14 +118,24 @@ def test_worklist_gather_arbitrary_angles():
     assert _emulate_gather(48, len(th), th) < 1e-14
 
 
+def _steps(n, P, spw=8):
+    return sum(min(P, n - b) for b in range(0, n, spw * P))
+
+
 def test_worklist_splits_heavy_tiles():
     items, runs, splits, tiles_v = G.worklist(2048, 1500, ph.angles_deg(1500))
-    cost = np.array([(runs[b:e, 2] - runs[b:e, 1] + 1).sum() for _, b, e, _ in items])
-    assert cost.max() <= 6144 + 2048       # kItemCap (+ one run)
+    n = runs[:, 2] - runs[:, 1] + 1
+    slots = np.array([_steps(int(k), int(P)) * 8 + 4 for k, P in zip(n, runs[:, 3])])
+    cost = np.array([slots[b:e].sum() for _, b, e, _ in items])
+    assert cost.max() <= 2048 + 1024       # kItemCap (+ one run)
     assert (items[:, 3] >= 0).sum() > 0     # the centre tiles are split
     assert np.all(np.diff(cost) <= 0)       # heaviest first
     # samples visited ~ 2 * n_ang * (pdim/2 - 1) plus the tile halo
-    assert 1.0 < cost.sum() / (2 * 1500 * 1023) < 1.6
+    assert 1.0 < n.sum() / (2 * 1500 * 1023) < 1.6
+    # footprints of one step are disjoint: P * max(|du|,|dv|) >= 4
+    th = np.deg2rad(ph.angles_deg(1500).astype(np.float64))[runs[:, 0] // 2]
+    step = np.maximum(np.abs(np.cos(th)), np.abs(np.sin(th))) * 2048 / 2047
+    assert np.all(runs[:, 3] * step >= 4.0)
 
 
 def test_phantom_line_integrals():
