@@ -56,7 +56,7 @@ struct SpectraArgs {
   const float* dark;
   const float4* pq;      // [pair][J] (P.re, P.im, Q.re, Q.im)
   float2* spec;          // [pair][n_ang][2][J]
-  const float2* tw;      // pdim twiddles exp(+2 pi i k/pdim)
+  const float2* tw;      // two-level twiddle table for pdim (see gridrec_kernels.cu)
   int n_det, n_ang, pdim, J, pairs;
 };
 
@@ -87,7 +87,7 @@ struct GridArgs {
 
 struct ColArgs {
   float2* H;
-  const float2* tw;      // M twiddles exp(+2 pi i k/M)
+  const float2* tw;      // two-level twiddle table for M
   int M, pairs;
 };
 

@@ -54,9 +54,6 @@ __device__ __forceinline__ float2 tw16(float2 a) {
   }
 }
 
-// Shared-memory index with one pad slot per 16 elements (bank-conflict-free
-// radix-16 Stockham stores).
-__device__ __forceinline__ int phys(int i) { return i + (i >> 4); }
 
 // ------------------------------------------------------------------ in-register DFTs
 // Natural order in and out: v[k] <- sum_n v[n] exp(S 2 pi i n k / R).
@@ -129,78 +126,118 @@ __device__ __forceinline__ void dftR(float2* v) {
   else dft2<S>(v);
 }
 
-// ------------------------------------------------------------------ block Stockham FFT
-// One line of N = 2^m (m >= 4) complex values in shared memory (phys()
-// layout), transformed in place by nthr = N/16 threads, each holding 16
-// values per pass.  Pass with radix R and span Ns (Ns = product of earlier
-// radices): butterfly j reads x[j + r N/R], twiddles by exp(S 2 pi i r k /(Ns R)),
-// k = j mod Ns, and writes x[(j - k) R + k + r Ns].  tw[t] = exp(+2 pi i t/N).
+// ------------------------------------------------------------------ register/shared Stockham FFT
+// One line of N = 2^m (m >= 4) complex values, transformed by nthr = N/16
+// threads holding 16 values each.  On entry thread tid holds
+// x[tid + r N/16] (r = 0..15) -- exactly the inputs of its first radix-16
+// butterfly -- so the caller loads straight from global memory into
+// registers.  Pass with radix R and span Ns (product of earlier radices):
+// butterfly j reads x[j + r N/R], twiddles by exp(S 2 pi i r k /(Ns R)) with
+// k = j mod Ns, and writes x[(j - k) R + k + r Ns].  Intermediate passes
+// exchange through shared memory (XOR-swizzled, bank-conflict-free for
+// these access patterns); the last pass leaves X[tid + nthr (i + r 16/R)] in
+// v[i R + r], natural order across threads, for the caller to store.
+// Twiddles exp(S 2 pi i e/N) = lo[e & 63] * hi[e >> 6] from a two-level table
+// of exp(+2 pi i e/N) in shared memory.
+
+__device__ __forceinline__ int swz(int i) { return i ^ ((i >> 4) & 15); }
+
+template <int S>
+__device__ __forceinline__ float2 twiddle(const float2* lo, const float2* hi, int e) {
+  float2 w = cmul(lo[e & 63], hi[e >> 6]);
+  if (S < 0) w.y = -w.y;
+  return w;
+}
 
 template <int R, int S>
-__device__ __forceinline__ void stockham_pass(float2* buf, int N, int Ns, int tid, int nthr,
-                                              const float2* __restrict__ tw) {
+__device__ __forceinline__ void fft_pass(float2 (&v)[16], float2* buf, int N, int Ns, int tid,
+                                         int nthr, const float2* lo, const float2* hi, bool last) {
   constexpr int B = 16 / R;
-  float2 v[16];
   const int NR = N / R;
 #pragma unroll
   for (int i = 0; i < B; ++i) {
     const int j = tid + i * nthr;
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[i * R + r] = buf[phys(j + r * NR)];
+    for (int r = 0; r < R; ++r) v[i * R + r] = buf[swz(j + r * NR)];
   }
-  __syncthreads();
   const int tstep = N / (Ns * R);
 #pragma unroll
   for (int i = 0; i < B; ++i) {
     const int j = tid + i * nthr;
     const int k = j & (Ns - 1);
-    if (Ns > 1) {
-      // powers w^r of w = exp(S 2 pi i k/(Ns R)): w, w^2, w^4, w^8 from the
-      // table, the rest as products of at most two table entries
-      float2 w[16];
-      const int e = k * tstep;
-      w[1] = __ldg(&tw[e]);
-      if constexpr (R >= 4) w[2] = __ldg(&tw[2 * e]);
-      if constexpr (R >= 8) w[4] = __ldg(&tw[4 * e]);
-      if constexpr (R >= 16) w[8] = __ldg(&tw[8 * e]);
-      if constexpr (R >= 4) w[3] = cmul(w[1], w[2]);
-      if constexpr (R >= 8) {
-        w[5] = cmul(w[1], w[4]);
-        w[6] = cmul(w[2], w[4]);
-        w[7] = cmul(w[3], w[4]);
-      }
-      if constexpr (R >= 16) {
-#pragma unroll
-        for (int r = 9; r < 16; ++r) w[r] = cmul(w[r - 8], w[8]);
-      }
-#pragma unroll
-      for (int r = 1; r < R; ++r) {
-        float2 ww = w[r];
-        if (S < 0) ww.y = -ww.y;
-        v[i * R + r] = cmul(v[i * R + r], ww);
-      }
+    const int e = k * tstep;
+    float2 w[16];
+    w[1] = twiddle<S>(lo, hi, e);
+    if constexpr (R >= 4) w[2] = twiddle<S>(lo, hi, 2 * e);
+    if constexpr (R >= 8) w[4] = twiddle<S>(lo, hi, 4 * e);
+    if constexpr (R >= 16) w[8] = twiddle<S>(lo, hi, 8 * e);
+    if constexpr (R >= 4) w[3] = cmul(w[1], w[2]);
+    if constexpr (R >= 8) {
+      w[5] = cmul(w[1], w[4]);
+      w[6] = cmul(w[2], w[4]);
+      w[7] = cmul(w[3], w[4]);
     }
+    if constexpr (R >= 16) {
+#pragma unroll
+      for (int r = 9; r < 16; ++r) w[r] = cmul(w[r - 8], w[8]);
+    }
+#pragma unroll
+    for (int r = 1; r < R; ++r) v[i * R + r] = cmul(v[i * R + r], w[r]);
     dftR<R, S>(&v[i * R]);
+  }
+  if (last) return;
+  __syncthreads();  // every thread has read buf
+#pragma unroll
+  for (int i = 0; i < B; ++i) {
+    const int j = tid + i * nthr;
+    const int k = j & (Ns - 1);
     const int base = (j - k) * R + k;
 #pragma unroll
-    for (int r = 0; r < R; ++r) buf[phys(base + r * Ns)] = v[i * R + r];
+    for (int r = 0; r < R; ++r) buf[swz(base + r * Ns)] = v[i * R + r];
   }
   __syncthreads();
 }
 
-template <int S>
-__device__ __forceinline__ void block_fft(float2* buf, int N, int tid, int nthr,
-                                          const float2* __restrict__ tw) {
-  int m = 31 - __clz(N);
-  int Ns = 1;
-  for (; m >= 4; m -= 4) {
-    stockham_pass<16, S>(buf, N, Ns, tid, nthr, tw);
-    Ns <<= 4;
-  }
-  if (m == 3) stockham_pass<8, S>(buf, N, Ns, tid, nthr, tw);
-  else if (m == 2) stockham_pass<4, S>(buf, N, Ns, tid, nthr, tw);
-  else if (m == 1) stockham_pass<2, S>(buf, N, Ns, tid, nthr, tw);
+// Radix of the last pass for N = 2^m.
+__device__ __forceinline__ int last_radix(int N) {
+  const int m = (31 - __clz(N)) & 3;
+  return m == 0 ? 16 : (1 << m);
 }
+
+// Index m of X[tid + nthr * m] held in v[idx] after fft_reg.
+__device__ __forceinline__ int out_index(int idx, int Rl) {
+  return idx / Rl + (idx % Rl) * (16 / Rl);
+}
+
+template <int S>
+__device__ __forceinline__ void fft_reg(float2 (&v)[16], float2* buf, int N, int tid, int nthr,
+                                        const float2* lo, const float2* hi) {
+  dft16<S>(v);  // first pass: R = 16, Ns = 1 (no twiddles)
+  int m = (31 - __clz(N)) - 4;
+  if (m == 0) return;
+#pragma unroll
+  for (int r = 0; r < 16; ++r) buf[swz(tid * 16 + r)] = v[r];
+  __syncthreads();
+  int Ns = 16;
+  while (m > 0) {
+    const int R = m >= 4 ? 16 : (1 << m);
+    m -= (R == 16 ? 4 : (R == 8 ? 3 : (R == 4 ? 2 : 1)));
+    const bool last = (m == 0);
+    if (R == 16) fft_pass<16, S>(v, buf, N, Ns, tid, nthr, lo, hi, last);
+    else if (R == 8) fft_pass<8, S>(v, buf, N, Ns, tid, nthr, lo, hi, last);
+    else if (R == 4) fft_pass<4, S>(v, buf, N, Ns, tid, nthr, lo, hi, last);
+    else fft_pass<2, S>(v, buf, N, Ns, tid, nthr, lo, hi, last);
+    Ns *= R;
+  }
+}
+
+// Copies the two-level twiddle table (64 + max(1, N/64) entries) to shared memory.
+__device__ __forceinline__ void load_twiddles(float2* dst, const float2* src, int N) {
+  const int n = 64 + max(1, N >> 6);
+  for (int i = threadIdx.x; i < n; i += blockDim.x) dst[i] = __ldg(&src[i]);
+}
+
+constexpr int kTwSlots = 64 + 128;  // table slots reserved in shared memory (N <= 8192)
 
 // ------------------------------------------------------------------ phase ramps
 
@@ -255,30 +292,42 @@ __device__ __forceinline__ float load_sino<uint16_t>(const uint16_t* row, int k,
 template <typename T>
 __global__ void __launch_bounds__(512) spectra_kernel(SpectraArgs a) {
   extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* buf = sm + kTwSlots;
   const int n = blockIdx.x, pair = blockIdx.y;
   const int tid = threadIdx.x, nthr = blockDim.x;
+  load_twiddles(tw, a.tw, a.pdim);
   const T* r1 = static_cast<const T*>(a.s1) + pair * a.pair_stride + (long)n * a.n_det;
   const T* r2 = (2 * pair + 1 < a.n_slices_valid)
                     ? static_cast<const T*>(a.s2) + pair * a.pair_stride + (long)n * a.n_det
                     : nullptr;
-  for (int k = tid; k < a.pdim; k += nthr) {
+  float2 v[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) {
+    const int k = tid + r * nthr;
     float x = 0.f, y = 0.f;
     if (k < a.n_det) {
       x = load_sino<T>(r1, k, a.flat, a.dark);
       if (r2) y = load_sino<T>(r2, k, a.flat, a.dark);
     }
-    sm[phys(k)] = make_float2(x, y);
+    v[r] = make_float2(x, y);
   }
+  __syncthreads();  // twiddle table ready
+  fft_reg<+1>(v, buf, a.pdim, tid, nthr, tw, tw + 64);
+  // F[j] and F[pdim - j] meet through shared memory
+  const int Rl = last_radix(a.pdim);
   __syncthreads();
-  block_fft<+1>(sm, a.pdim, tid, nthr, a.tw);
+#pragma unroll
+  for (int idx = 0; idx < 16; ++idx) buf[swz(tid + nthr * out_index(idx, Rl))] = v[idx];
+  __syncthreads();
   const float4* pq = a.pq + (size_t)pair * a.J;
   float2* o1 = a.spec + ((size_t)pair * a.n_ang + n) * 2 * a.J;
   float2* o2 = o1 + a.J;
   for (int j = tid; j < a.J; j += nthr) {
     float2 c1 = make_float2(0.f, 0.f), c2 = make_float2(0.f, 0.f);
     if (j > 0) {
-      const float2 F = sm[phys(j)];
-      const float2 G = sm[phys(a.pdim - j)];
+      const float2 F = buf[swz(j)];
+      const float2 G = buf[swz(a.pdim - j)];
       const float4 q = __ldg(&pq[j]);  // P = (x, y), Q = (z, w)
       // C1 = P F + Q conj(G);  C2 = conj(P) G + conj(Q) conj(F)
       c1.x = q.x * F.x - q.y * F.y + q.z * G.x + q.w * G.y;
@@ -494,38 +543,47 @@ __global__ void __launch_bounds__(256) split_reduce_kernel(GridArgs a) {
 }
 
 // ------------------------------------------------------------------ 2-D FFT, first axis (K3)
-// G columns of H per CTA, each a contiguous shared-memory line of stride LP.
+// G columns of H per CTA: thread t works on column g = t % G (so a warp's
+// loads cover G adjacent columns of several rows) and line position t / G.
+// Each column's exchange buffer has stride M + 16/G, which keeps the G lines
+// on distinct banks.
 
 __global__ void __launch_bounds__(512) cols_kernel(ColArgs a, int G) {
   extern __shared__ float2 sm[];
+  float2* tw = sm;
   const int M = a.M;
-  const int LP = M + (M >> 4) + 1;
+  const int nthr = M >> 4;
+  const int g = threadIdx.x % G, tid = threadIdx.x / G;
+  float2* buf = sm + kTwSlots + g * (M + 16 / G);
   const int q0 = blockIdx.x * G, pair = blockIdx.y;
-  const int per_line = M >> 4;
-  const int line = threadIdx.x / per_line, tl = threadIdx.x - line * per_line;
-  float2* Hp = a.H + (size_t)pair * M * M;
-  for (int i = threadIdx.x; i < G * M; i += blockDim.x) {
-    const int p = i / G, g = i - (i / G) * G;
-    sm[g * LP + phys(p)] = Hp[(size_t)p * M + q0 + g];
-  }
+  load_twiddles(tw, a.tw, M);
+  float2* Hp = a.H + (size_t)pair * M * M + q0 + g;
+  float2 v[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) v[r] = Hp[(size_t)(tid + r * nthr) * M];
   __syncthreads();
-  block_fft<-1>(sm + line * LP, M, tl, per_line, a.tw);
-  for (int i = threadIdx.x; i < G * M; i += blockDim.x) {
-    const int p = i / G, g = i - (i / G) * G;
-    Hp[(size_t)p * M + q0 + g] = sm[g * LP + phys(p)];
-  }
+  fft_reg<-1>(v, buf, M, tid, nthr, tw, tw + 64);
+  const int Rl = last_radix(M);
+#pragma unroll
+  for (int idx = 0; idx < 16; ++idx) Hp[(size_t)(tid + nthr * out_index(idx, Rl)) * M] = v[idx];
 }
 
 // ------------------------------------------------------------------ second axis + deapod (K4)
 
 __global__ void __launch_bounds__(512) rows_kernel(RowArgs a) {
   extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* buf = sm + kTwSlots;
   const int M = a.M;
   const int iu = blockIdx.x, pair = blockIdx.y;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  load_twiddles(tw, a.tw, M);
   const float2* row = a.H + ((size_t)pair * M + iu) * M;
-  for (int q = threadIdx.x; q < M; q += blockDim.x) sm[phys(q)] = row[q];
+  float2 v[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) v[r] = row[tid + r * nthr];
   __syncthreads();
-  block_fft<-1>(sm, M, threadIdx.x, blockDim.x, a.tw);
+  fft_reg<-1>(v, buf, M, tid, nthr, tw, tw + 64);
   // iu = (j - M02) mod M  (gridrec.cu:694-719)
   int j = iu + a.M02;
   if (j >= M) j -= M;
@@ -534,19 +592,23 @@ __global__ void __launch_bounds__(512) rows_kernel(RowArgs a) {
   float* o1 = a.out1 + pair * a.pair_stride + (long)j * a.out_stride;
   float* o2 = (2 * pair + 1 < a.n_slices_valid) ? a.out2 + pair * a.pair_stride + (long)j * a.out_stride
                                                 : nullptr;
-  for (int k = threadIdx.x; k < a.M0; k += blockDim.x) {
-    int iv = k - a.M02;
-    if (iv < 0) iv += M;
-    const float2 h = sm[phys(iv)];
-    const float c = wj * __ldg(&a.winv[k]);
-    o1[k] = c * h.x;
-    if (o2) o2[k] = c * h.y;
+  const int Rl = last_radix(M);
+#pragma unroll
+  for (int idx = 0; idx < 16; ++idx) {
+    const int iv = tid + nthr * out_index(idx, Rl);
+    int k = iv + a.M02;
+    if (k >= M) k -= M;
+    if (k < a.M0) {
+      const float c = wj * __ldg(&a.winv[k]);
+      o1[k] = c * v[idx].x;
+      if (o2) o2[k] = c * v[idx].y;
+    }
   }
 }
 
 // ------------------------------------------------------------------ launchers
 
-static int fft_smem_bytes(int N) { return (N + (N >> 4)) * (int)sizeof(float2); }
+static int fft_smem_bytes(int N) { return (kTwSlots + N) * (int)sizeof(float2); }
 
 // Allows the dynamic-shared-memory kernels the device's opt-in maximum; called
 // once per device at plan creation so that launches need no attribute calls
@@ -622,13 +684,13 @@ cudaError_t launch_grid(const GridArgs& a, int ntaps, cudaStream_t s) {
 }
 
 int cols_group(int M) {
-  int g = 8192 / M;
+  int g = 8192 / M;  // G * M / 16 <= 512 threads
   return g < 1 ? 1 : (g > 8 ? 8 : g);
 }
 
 cudaError_t launch_cols(const ColArgs& a, cudaStream_t s) {
   const int G = cols_group(a.M);
-  const int smem = G * (a.M + (a.M >> 4) + 1) * (int)sizeof(float2);
+  const int smem = (kTwSlots + G * (a.M + 16 / G)) * (int)sizeof(float2);
   dim3 grid(a.M / G, a.pairs);
   cols_kernel<<<grid, G * (a.M / 16), smem, s>>>(a, G);
   return cudaGetLastError();

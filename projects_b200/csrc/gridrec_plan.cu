@@ -557,12 +557,18 @@ int gr_plan_create(const gr_params* prm, gr_plan** out) {
   std::vector<float> filt(p->J);
   const double norm = M_PI / pdim / prm->n_ang;
   for (int j = 0; j < p->J; ++j) filt[j] = (float)(filter_value(prm->filter, (double)j / pdim) * norm);
-  // twiddles exp(+2 pi i k/N)
+  // two-level twiddle table of exp(+2 pi i e/N): lo[e] for e < 64, then
+  // hi[f] = exp(+2 pi i 64 f/N) for f < max(1, N/64); FP64, rounded once
   auto twiddles = [](int N) {
-    std::vector<float2> t(N);
-    for (int k = 0; k < N; ++k) {
-      const double a = 2.0 * M_PI * k / N;
-      t[k] = make_float2((float)std::cos(a), (float)std::sin(a));
+    const int nhi = std::max(1, N / 64);
+    std::vector<float2> t(64 + nhi);
+    for (int e = 0; e < 64; ++e) {
+      const double a = 2.0 * M_PI * e / N;
+      t[e] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    for (int f = 0; f < nhi; ++f) {
+      const double a = 2.0 * M_PI * 64.0 * f / N;
+      t[64 + f] = make_float2((float)std::cos(a), (float)std::sin(a));
     }
     return t;
   };
