@@ -16,6 +16,9 @@ constexpr int kTile = 32;
 // Largest number of taps per dimension the gridding kernel handles
 // (floor(L) + 1 with L = 2*C*sampl/pi < 6).
 constexpr int kMaxTaps = 6;
+// Longest run of samples the gridding kernel stages at once (longer runs
+// are split on the host).
+constexpr int kRunMax = 64;
 // Work per gridding item before a tile is split over several items, in
 // sample slots (steps x samples per step).
 constexpr int kItemCap = 2048;

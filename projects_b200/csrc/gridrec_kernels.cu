@@ -166,23 +166,35 @@ __device__ __forceinline__ void fft_pass(float2 (&v)[16], float2* buf, int N, in
     const int j = tid + i * nthr;
     const int k = j & (Ns - 1);
     const int e = k * tstep;
-    float2 w[16];
-    w[1] = twiddle<S>(lo, hi, e);
-    if constexpr (R >= 4) w[2] = twiddle<S>(lo, hi, 2 * e);
-    if constexpr (R >= 8) w[4] = twiddle<S>(lo, hi, 4 * e);
-    if constexpr (R >= 16) w[8] = twiddle<S>(lo, hi, 8 * e);
-    if constexpr (R >= 4) w[3] = cmul(w[1], w[2]);
-    if constexpr (R >= 8) {
-      w[5] = cmul(w[1], w[4]);
-      w[6] = cmul(w[2], w[4]);
-      w[7] = cmul(w[3], w[4]);
+    // w^r from the bases w, w^2, w^4, w^8, multiplied in just in time so
+    // that few twiddles are live at once
+    const float2 w1 = twiddle<S>(lo, hi, e);
+    v[i * R + 1] = cmul(v[i * R + 1], w1);
+    if constexpr (R >= 4) {
+      const float2 w2 = twiddle<S>(lo, hi, 2 * e);
+      const float2 w3 = cmul(w1, w2);
+      v[i * R + 2] = cmul(v[i * R + 2], w2);
+      v[i * R + 3] = cmul(v[i * R + 3], w3);
+      if constexpr (R >= 8) {
+        const float2 w4 = twiddle<S>(lo, hi, 4 * e);
+        v[i * R + 4] = cmul(v[i * R + 4], w4);
+        v[i * R + 5] = cmul(v[i * R + 5], cmul(w1, w4));
+        v[i * R + 6] = cmul(v[i * R + 6], cmul(w2, w4));
+        v[i * R + 7] = cmul(v[i * R + 7], cmul(w3, w4));
+        if constexpr (R >= 16) {
+          const float2 w8 = twiddle<S>(lo, hi, 8 * e);
+          const float2 w12 = cmul(w4, w8);
+          v[i * R + 8] = cmul(v[i * R + 8], w8);
+          v[i * R + 9] = cmul(v[i * R + 9], cmul(w1, w8));
+          v[i * R + 10] = cmul(v[i * R + 10], cmul(w2, w8));
+          v[i * R + 11] = cmul(v[i * R + 11], cmul(w3, w8));
+          v[i * R + 12] = cmul(v[i * R + 12], w12);
+          v[i * R + 13] = cmul(v[i * R + 13], cmul(w1, w12));
+          v[i * R + 14] = cmul(v[i * R + 14], cmul(w2, w12));
+          v[i * R + 15] = cmul(v[i * R + 15], cmul(w3, w12));
+        }
+      }
     }
-    if constexpr (R >= 16) {
-#pragma unroll
-      for (int r = 9; r < 16; ++r) w[r] = cmul(w[r - 8], w[8]);
-    }
-#pragma unroll
-    for (int r = 1; r < R; ++r) v[i * R + r] = cmul(v[i * R + r], w[r]);
     dftR<R, S>(&v[i * R]);
   }
   if (last) return;
@@ -289,8 +301,10 @@ __device__ __forceinline__ float load_sino<uint16_t>(const uint16_t* row, int k,
   return r > 0.f ? logf(r) : 0.f;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(512) spectra_kernel(SpectraArgs a) {
+// Lines of up to 4096 points run 64-register variants (several CTAs per SM);
+// 8192-point lines need 512 threads and use the MAXT = 512 variants.
+template <typename T, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs a) {
   extern __shared__ float2 sm[];
   float2* tw = sm;
   float2* buf = sm + kTwSlots;
@@ -402,6 +416,8 @@ __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float4* tile = tiles + warp * (kTile * kTileStride);
+  // the current run's samples of both pairs: stage[j - jlo] = (C_A, C_B)
+  float4* stage = tiles + kGridWarps * (kTile * kTileStride) + warp * kRunMax;
   const int slot_k = lane / NT;          // sample slot of this lane
   const int t = lane - slot_k * NT;      // footprint row of this lane
   const int lane0 = slot_k * NT;         // first lane of this sample
@@ -430,11 +446,32 @@ __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
     const float offu = half_m - (float)p0, offv = half_m - (float)q0;
     const float2* specA = a.spec + (size_t)pA * spec_pair;
     const float2* specB = hasB ? specA + spec_pair : specA;
+    // Software pipeline over runs: the samples of run r+1 are loaded into
+    // registers (lane l holds j = jlo + l and jlo + l + 32) while run r is
+    // gridded from the shared staging buffer.
+    float2 nA0 = make_float2(0.f, 0.f), nA1 = nA0, nB0 = nA0, nB1 = nA0;
+    auto prefetch = [&](int rr) {
+      if (rr >= it.run_end) return;
+      const Run nr = a.runs[rr];
+      const float2* pa = specA + (size_t)nr.dir * a.J;
+      const float2* pb = specB + (size_t)nr.dir * a.J;
+      if (nr.jlo + lane <= nr.jhi) {
+        nA0 = __ldg(&pa[nr.jlo + lane]);
+        nB0 = __ldg(&pb[nr.jlo + lane]);
+      }
+      if (nr.jlo + 32 + lane <= nr.jhi) {
+        nA1 = __ldg(&pa[nr.jlo + 32 + lane]);
+        nB1 = __ldg(&pb[nr.jlo + 32 + lane]);
+      }
+    };
+    prefetch(it.run_begin);
     for (int r = it.run_begin; r < it.run_end; ++r) {
       const Run run = a.runs[r];
       const float2 d = __ldg(&a.dir[run.dir]);
-      const float2* spA = specA + (size_t)run.dir * a.J;
-      const float2* spB = specB + (size_t)run.dir * a.J;
+      stage[lane] = make_float4(nA0.x, nA0.y, nB0.x, nB0.y);
+      stage[32 + lane] = make_float4(nA1.x, nA1.y, nB1.x, nB1.y);
+      __syncwarp();
+      prefetch(r + 1);
       // run.P: samples P apart have disjoint footprints (P * max(|du|,|dv|)
       // >= NT with margin), chosen on the host to minimise the steps
       const int P = run.P;
@@ -458,12 +495,9 @@ __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
           const float wtv = s_wtbl[min(table_index(dv, ts), ltbl)];
           const float wu = (active && du <= L2 && (unsigned)row < (unsigned)kTile) ? wtu : 0.f;
           const float wvt = (active && dv <= L2 && (unsigned)col < (unsigned)kTile) ? wtv : 0.f;
-          float2 cA = make_float2(0.f, 0.f), cB = make_float2(0.f, 0.f);
-          if (wu != 0.f) {
-            cA = __ldg(&spA[j]);
-            cB = __ldg(&spB[j]);
-          }
-          const float4 c4 = make_float4(wu * cA.x, wu * cA.y, wu * cB.x, wu * cB.y);
+          float4 cc = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (wu != 0.f) cc = stage[j - run.jlo];
+          const float4 c4 = make_float4(wu * cc.x, wu * cc.y, wu * cc.z, wu * cc.w);
           float wv[NT];
 #pragma unroll
           for (int s2 = 0; s2 < NT; ++s2) wv[s2] = __shfl_sync(0xffffffffu, wvt, lane0 + s2);
@@ -548,7 +582,8 @@ __global__ void __launch_bounds__(256) split_reduce_kernel(GridArgs a) {
 // Each column's exchange buffer has stride M + 16/G, which keeps the G lines
 // on distinct banks.
 
-__global__ void __launch_bounds__(512) cols_kernel(ColArgs a, int G) {
+template <int MAXT>
+__global__ void __launch_bounds__(MAXT, 1024 / MAXT) cols_kernel(ColArgs a, int G) {
   extern __shared__ float2 sm[];
   float2* tw = sm;
   const int M = a.M;
@@ -570,7 +605,8 @@ __global__ void __launch_bounds__(512) cols_kernel(ColArgs a, int G) {
 
 // ------------------------------------------------------------------ second axis + deapod (K4)
 
-__global__ void __launch_bounds__(512) rows_kernel(RowArgs a) {
+template <int MAXT>
+__global__ void __launch_bounds__(MAXT, 1024 / MAXT) rows_kernel(RowArgs a) {
   extern __shared__ float2 sm[];
   float2* tw = sm;
   float2* buf = sm + kTwSlots;
@@ -617,11 +653,17 @@ cudaError_t init_kernel_attributes() {
   int dev = 0, optin = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  const void* fns[] = {(const void*)spectra_kernel<float>, (const void*)spectra_kernel<__half>,
-                       (const void*)spectra_kernel<__nv_bfloat16>,
-                       (const void*)spectra_kernel<uint16_t>, (const void*)cols_kernel,
-                       (const void*)rows_kernel, (const void*)grid_kernel<4>,
-                       (const void*)grid_kernel<kMaxTaps>};
+  const void* fns[] = {(const void*)spectra_kernel<float, 256>,
+                       (const void*)spectra_kernel<__half, 256>,
+                       (const void*)spectra_kernel<__nv_bfloat16, 256>,
+                       (const void*)spectra_kernel<uint16_t, 256>,
+                       (const void*)spectra_kernel<float, 512>,
+                       (const void*)spectra_kernel<__half, 512>,
+                       (const void*)spectra_kernel<__nv_bfloat16, 512>,
+                       (const void*)spectra_kernel<uint16_t, 512>,
+                       (const void*)cols_kernel<256>, (const void*)cols_kernel<512>,
+                       (const void*)rows_kernel<256>, (const void*)rows_kernel<512>,
+                       (const void*)grid_kernel<4>, (const void*)grid_kernel<kMaxTaps>};
   for (const void* f : fns) {
     if (e != cudaSuccess) break;
     e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
@@ -639,7 +681,8 @@ template <typename T>
 static cudaError_t launch_spectra_t(const SpectraArgs& a, cudaStream_t s) {
   const int smem = fft_smem_bytes(a.pdim);
   dim3 grid(a.n_ang, a.pairs);
-  spectra_kernel<T><<<grid, a.pdim / 16, smem, s>>>(a);
+  if (a.pdim <= 4096) spectra_kernel<T, 256><<<grid, a.pdim / 16, smem, s>>>(a);
+  else spectra_kernel<T, 512><<<grid, a.pdim / 16, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -654,7 +697,7 @@ cudaError_t launch_spectra(const SpectraArgs& a, gr_dtype dt, cudaStream_t s) {
 }
 
 static int grid_smem_bytes() {
-  return 257 * (int)sizeof(float4) + kGridWarps * kTile * kTileStride * (int)sizeof(float4);
+  return (257 + kGridWarps * (kTile * kTileStride + kRunMax)) * (int)sizeof(float4);
 }
 
 cudaError_t launch_grid(const GridArgs& a, int ntaps, cudaStream_t s) {
@@ -684,7 +727,7 @@ cudaError_t launch_grid(const GridArgs& a, int ntaps, cudaStream_t s) {
 }
 
 int cols_group(int M) {
-  int g = 8192 / M;  // G * M / 16 <= 512 threads
+  int g = 8192 / M;  // G * M / 16 <= 512 threads; G = 4 (32-byte rows) at M = 2048
   return g < 1 ? 1 : (g > 8 ? 8 : g);
 }
 
@@ -692,14 +735,16 @@ cudaError_t launch_cols(const ColArgs& a, cudaStream_t s) {
   const int G = cols_group(a.M);
   const int smem = (kTwSlots + G * (a.M + 16 / G)) * (int)sizeof(float2);
   dim3 grid(a.M / G, a.pairs);
-  cols_kernel<<<grid, G * (a.M / 16), smem, s>>>(a, G);
+  if (G * (a.M / 16) <= 256) cols_kernel<256><<<grid, G * (a.M / 16), smem, s>>>(a, G);
+  else cols_kernel<512><<<grid, G * (a.M / 16), smem, s>>>(a, G);
   return cudaGetLastError();
 }
 
 cudaError_t launch_rows(const RowArgs& a, cudaStream_t s) {
   const int smem = fft_smem_bytes(a.M);
   dim3 grid(a.M, a.pairs);
-  rows_kernel<<<grid, a.M / 16, smem, s>>>(a);
+  if (a.M <= 4096) rows_kernel<256><<<grid, a.M / 16, smem, s>>>(a);
+  else rows_kernel<512><<<grid, a.M / 16, smem, s>>>(a);
   return cudaGetLastError();
 }
 

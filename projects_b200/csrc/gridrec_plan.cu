@@ -242,8 +242,8 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
         if (!slab(M2, dy, y0, y1, sa, sb)) continue;
         const int jlo = std::max(1, (int)std::ceil(sa - 1e-6));
         const int jhi = std::min(J - 1, (int)std::floor(sb + 1e-6));
-        if (jlo > jhi) continue;
-        all.push_back({tu * wl->tiles_v + tv, d, jlo, jhi});
+        for (int j0 = jlo; j0 <= jhi; j0 += kRunMax)  // runs of at most kRunMax samples
+          all.push_back({tu * wl->tiles_v + tv, d, j0, std::min(jhi, j0 + kRunMax - 1)});
       }
     }
   }
