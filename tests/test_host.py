@@ -159,3 +159,21 @@ def test_raw_counts_roundtrip():
     v = raw.astype(np.float64) - dark
     est = np.log((flat - dark) / v)
     assert np.abs(est - p).mean() < 0.05
+
+
+def _build_shim(tmp_path):
+    import shutil
+    import subprocess
+    if shutil.which("g++") is None:
+        pytest.skip("g++ not available")
+    exe = str(tmp_path / "shim_demo")
+    lib_dir = os.path.join(ROOT, "projects_b200")
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", os.path.join(ROOT, "include"),
+                    os.path.join(ROOT, "tests", "cxx", "shim_demo.cpp"), "-L", lib_dir,
+                    "-lgridrec_b200", f"-Wl,-rpath,{lib_dir}", "-o", exe], check=True)
+    return exe
+
+
+def test_cxx_shim_compiles_against_the_c_abi(tmp_path):
+    """include/gridrec_b200.hpp (the GridRec-compatible class) builds and links."""
+    assert os.path.exists(_build_shim(tmp_path))
