@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -862,3 +863,102 @@ int gr_reconstruct_host(gr_plan* p, const gr_batch_desc* b, void* stream) {
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ allocation-free pair entry
+// gr_reconstruct_pair_noalloc keeps every per-call intermediate (phase
+// ramps, filtered spectra, frequency grid, partial tiles of split tiles,
+// work-queue head) in one file-scope device array instead of the plan's
+// cudaMalloc'd workspaces.  Every GPU that loads the library holds the array
+// until the process exits; all calls on a device share it.
+
+namespace gr {
+namespace {
+
+constexpr size_t kNoallocBytes = size_t(32) << 20;  // 32 MiB per device
+constexpr int kNoallocMaxDevices = 64;
+
+}  // namespace
+}  // namespace gr
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[gr::kNoallocBytes];
+
+namespace gr {
+namespace {
+
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[kNoallocMaxDevices] = {};
+
+// Device address of g_noalloc_scratch on the current device (the array's
+// name in host code is only a stand-in).  Looked up once per device.
+int noalloc_scratch(int dev, unsigned char** ptr) {
+  if (dev < 0 || dev >= kNoallocMaxDevices)
+    return fail(GR_ERR_UNSUPPORTED, "device %d: static scratch covers devices 0..%d", dev,
+                kNoallocMaxDevices - 1);
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_addr[dev]) {
+    void* a = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&a, g_noalloc_scratch);
+    if (e != cudaSuccess)
+      return fail(GR_ERR_CUDA, "cudaGetSymbolAddress(static scratch) failed: %s",
+                  cudaGetErrorString(e));
+    g_noalloc_addr[dev] = a;
+  }
+  *ptr = static_cast<unsigned char*>(g_noalloc_addr[dev]);
+  return GR_OK;
+}
+
+size_t align256(size_t x) { return (x + 255) & ~size_t(255); }
+
+}  // namespace
+}  // namespace gr
+
+extern "C" int gr_reconstruct_pair_noalloc(gr_plan* p, const float* sino1, const float* sino2,
+                                           float* out1, float* out2, long out_stride,
+                                           void* stream) {
+  using namespace gr;
+  if (!p || !sino1 || !out1) return fail(GR_ERR_ARG, "null argument");
+  if (out_stride < p->M0) return fail(GR_ERR_ARG, "out_stride %ld < M0 %d", out_stride, p->M0);
+  // carve the static array: ramps | spectra | grid | partial tiles | queue head
+  const size_t off_pq = 0;
+  const size_t off_spec = align256(off_pq + (size_t)p->J * sizeof(float4));
+  const size_t off_H = align256(off_spec + (size_t)p->n_ang * 2 * p->J * sizeof(float2));
+  const size_t off_part = align256(off_H + (size_t)p->M * p->M * sizeof(float2));
+  const size_t off_queue =
+      align256(off_part + (size_t)std::max(p->n_slots, 1) * kTile * kTile * sizeof(float4));
+  const size_t need = off_queue + 256;
+  if (need > kNoallocBytes)
+    return fail(GR_ERR_UNSUPPORTED,
+                "gr_reconstruct_pair_noalloc: %d x %d needs %zu bytes of scratch, the static "
+                "array holds %zu; use gr_reconstruct_pair",
+                p->n_det, p->n_ang, need, kNoallocBytes);
+  DeviceGuard g(p->device);
+  unsigned char* base = nullptr;
+  int rc = noalloc_scratch(p->device, &base);
+  if (rc) return rc;
+  float4* pq = reinterpret_cast<float4*>(base + off_pq);
+  float2* spec = reinterpret_cast<float2*>(base + off_spec);
+  float2* H = reinterpret_cast<float2*>(base + off_H);
+  float4* part = reinterpret_cast<float4*>(base + off_part);
+  unsigned* queue = reinterpret_cast<unsigned*>(base + off_queue);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int n_valid = (sino2 && out2) ? 2 : 1;
+  const void* s2 = sino2 ? sino2 : sino1;
+  float* o2 = out2 ? out2 : out1;
+  // the same five kernels as gr_reconstruct_pair, one pair, workspaces above;
+  // launch_grid zeroes the queue head in-stream before the gridding kernel
+  PhaseArgs ph{nullptr, p->center, 0, n_valid, p->d_filt, pq, p->J, p->pdim, 1};
+  GR_CUDA(launch_phase(ph, st));
+  SpectraArgs sa{sino1, s2, 0, n_valid, 0, nullptr, nullptr, pq, spec, p->d_tw_p, p->n_det,
+                 p->n_ang, p->pdim, p->J, 1};
+  GR_CUDA(launch_spectra(sa, GR_DTYPE_F32, st));
+  GridArgs ga{spec, H, part, queue, p->d_items, p->d_runs, p->d_split_list, p->n_split_tiles,
+              p->d_dir, p->d_wtbl, p->n_items, 1, p->n_ang, p->J, p->M, p->tiles_v, p->n_slots,
+              p->ltbl, (float)(p->L / 2), (float)(2.0 * p->ltbl / p->L)};
+  GR_CUDA(launch_grid(ga, p->ntaps, st));
+  ColArgs ca{H, p->d_tw_m, p->M, 1};
+  GR_CUDA(launch_cols(ca, st));
+  RowArgs ra{H, p->d_tw_m, p->d_winv, out1, o2, 0, out_stride, n_valid, p->M, p->M0, p->M02, 1};
+  GR_CUDA(launch_rows(ra, st));
+  p->launches += 5;
+  return GR_OK;
+}

@@ -28,7 +28,7 @@ EXPORTS = ("gr_params_default", "gr_filter_code", "gr_plan_create", "gr_plan_des
            "gr_plan_sizes", "gr_plan_device_bytes", "gr_reconstruct_pair",
            "gr_reconstruct_batch", "gr_reconstruct_host", "gr_last_error",
            "gr_plan_launch_count", "gr_plan_work_stats", "gr_worklist_export",
-           "gr_plan_set_timing", "gr_plan_stage_times")
+           "gr_plan_set_timing", "gr_plan_stage_times", "gr_reconstruct_pair_noalloc")
 STAGES = ("phase", "spectra", "grid", "cols", "rows_deapod")
 
 
@@ -72,6 +72,8 @@ def lib():
         L.gr_plan_device_bytes.argtypes = [C.c_void_p, C.POINTER(C.c_size_t)]
         L.gr_reconstruct_pair.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                           C.c_void_p, C.c_long, C.c_void_p]
+        L.gr_reconstruct_pair_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p,
+                                                  C.c_void_p, C.c_void_p, C.c_long, C.c_void_p]
         L.gr_reconstruct_batch.argtypes = [C.c_void_p, C.POINTER(GrBatch), C.c_void_p]
         L.gr_reconstruct_host.argtypes = [C.c_void_p, C.POINTER(GrBatch), C.c_void_p]
         L.gr_last_error.restype = C.c_char_p
