@@ -162,14 +162,18 @@ def algorithmic_bytes_per_pair(n_det, n_ang, pdim, M, M0, in_bytes=4):
     }
 
 
-def traffic_from_profile(stage):
-    """DRAM bytes per launch from a committed ncu summary, if one exists."""
-    path = os.path.join(ROOT, "profiles", "traffic.json")
+def traffic_from_profile(stage, pairs_per_launch, n_det, n_ang):
+    """DRAM bytes per launch (ncu read + write per pair, scaled by the pairs of
+    one launch) from the committed profile summary of this workload."""
+    path = os.path.join(ROOT, "profiles", f"traffic_{n_det}x{n_ang}.txt")
     if not os.path.exists(path):
         return None
     with open(path) as f:
-        t = json.load(f)
-    return t.get(stage)
+        for line in f:
+            parts = line.split()
+            if len(parts) == 2 and parts[0] == stage:
+                return float(parts[1]) * pairs_per_launch
+    return None
 
 
 def cpu_reference(n_det, n_ang, seconds, threads=None, steps=None):
@@ -299,12 +303,16 @@ def run_b200(args, rank, world, local_rank):
     bytes_total = bpp[dominant] * pairs_timed
     achieved = bytes_total / (stage_ms[dominant] / 1000.0) / 1e9
     peak, peak_src = peaks()
-    traffic = traffic_from_profile(dominant)
+    traffic = traffic_from_profile(dominant, min(args.max_pairs, (S + 1) // 2), n, a)
     per_launch_bytes = bytes_total / max(n_launch, 1)
     stages = {k: {"ms_per_pair": v / pairs_timed,
                   "gbs": bpp[k] * pairs_timed / max(v / 1000.0, 1e-12) / 1e9}
               for k, v in stage_ms.items()}
     model_bytes_slice = (bpp["spectra"] + bpp["grid"] + bpp["cols"] + bpp["rows_deapod"]) / 2
+    # the staged byte model of the task description: sinogram in, spectrum out/in,
+    # H out, 2-D IFFT as 4 passes over H, H in, images out (per slice)
+    survey_model = (2 * a * n * in_bytes + 2 * a * (plan.pdim // 2) * 8 * 2 + plan.M ** 2 * 8
+                    + 4 * plan.M ** 2 * 8 + plan.M ** 2 * 8 + 2 * plan.M0 ** 2 * 4) / 2
 
     # end to end through the host-buffer entry point
     e2e = None
@@ -357,8 +365,10 @@ def run_b200(args, rank, world, local_rank):
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
                          "traffic": traffic, "algorithmic_bytes_per_launch": per_launch_bytes},
             "stages": stages,
-            "pipeline": {"staged_model_bytes_per_slice": model_bytes_slice,
-                         "frac_of_hbm": model_bytes_slice * value / world / 1e9 / peak},
+            "pipeline": {"algorithmic_bytes_per_slice": model_bytes_slice,
+                         "frac_of_hbm": model_bytes_slice * value / world / 1e9 / peak,
+                         "survey_staged_model_bytes_per_slice": survey_model,
+                         "survey_model_frac_of_hbm": survey_model * value / world / 1e9 / peak},
             "gpu_launches": launches,
             "clocks": clk.summary(),
             "e2e": e2e,
