@@ -168,6 +168,17 @@ int gr_reconstruct_host(gr_plan* plan, const gr_batch_desc* batch, void* stream)
 int gr_reconstruct_pair_noalloc(gr_plan* plan, const float* sino1, const float* sino2, float* out1,
                                 float* out2, long out_stride, void* stream);
 
+/* Synchronises `stream`, then reports whether a kernel of this plan stopped
+ * early because one of its bounded device waits (mbarrier polls on bulk
+ * copies) ran out: GR_ERR_TIMEOUT, and the flag is cleared; GR_OK otherwise.
+ * gr_reconstruct_host performs this check itself. */
+int gr_plan_device_status(gr_plan* plan, void* stream);
+
+/* Exercises the timeout path on `device`: a one-thread kernel polls an
+ * mbarrier that nothing ever completes, a few thousand times, and records the
+ * timeout.  Returns GR_ERR_TIMEOUT when the detection works. */
+int gr_selftest_wait_timeout(int device);
+
 /* Per-stage timing with CUDA events recorded on the launching stream around
  * each kernel of each chunk (stages: 0 phase ramps, 1 spectra, 2 gridding,
  * 3 first-axis FFT, 4 second-axis FFT + deapodisation).  Enabling resets

@@ -92,6 +92,7 @@ struct ColArgs {
   float2* H;
   const float2* tw;      // two-level twiddle table for M
   int M, pairs;
+  int* err;              // device error word for bounded-wait timeouts (null: plain loads)
 };
 
 struct RowArgs {
@@ -114,5 +115,6 @@ cudaError_t launch_grid(const GridArgs& a, int ntaps, cudaStream_t s);
 int cols_group(int M);
 cudaError_t launch_cols(const ColArgs& a, cudaStream_t s);
 cudaError_t launch_rows(const RowArgs& a, cudaStream_t s);
+cudaError_t launch_wait_probe(int* err, int limit, cudaStream_t s);
 
 }  // namespace gr

@@ -16,10 +16,13 @@
 //                   axis fused with deapodisation winv[j]*winv[k], the
 //                   four-corner crop and the split into two real images
 //                   (gridrec.cu:641-646 + 691-719)
+#include <cuda.h>
+#include <cudaTypedefs.h>
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <mutex>
 
 #include "gr_internal.h"
 
@@ -250,6 +253,69 @@ __device__ __forceinline__ void load_twiddles(float2* dst, const float2* src, in
 }
 
 constexpr int kTwSlots = 64 + 128;  // table slots reserved in shared memory (N <= 8192)
+
+// ------------------------------------------------------------------ bulk copies + mbarriers
+// One-dimensional TMA bulk copies (global -> shared) completed on an
+// mbarrier.  Every wait is bounded: after kWaitLimit polls the kernel records
+// a timeout in the plan's device error word and stops.
+
+constexpr int kWaitLimit = 1 << 22;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+// makes an mbarrier initialisation visible to the async proxy (bulk copies)
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+// orders this thread's generic-proxy shared accesses before later async-proxy ones
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
+                                         uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+// Tiled 2-D TMA load of one box at (x, y) (x: innermost, in elements) into
+// shared memory, completed on `bar`.  x * element size must be a multiple of 16.
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+      " [%0], [%1, {%2, %3}], [%4];" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
+      : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Bounded wait for phase `parity` of `bar`; false when the limit ran out.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
+  for (int it = 0; it < kWaitLimit; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  return false;
+}
 
 // ------------------------------------------------------------------ phase ramps
 
@@ -603,6 +669,54 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) cols_kernel(ColArgs a, int 
   for (int idx = 0; idx < 16; ++idx) Hp[(size_t)(tid + nthr * out_index(idx, Rl)) * M] = v[idx];
 }
 
+// TMA-fed variant: one thread loads the CTA's G columns x M rows with
+// M / box_rows tiled tensor copies (boxes of G complex x box_rows rows, rows
+// of the box contiguous in shared memory), the other threads fetch the
+// twiddle table meanwhile.  The landing buffer then serves as the FFT
+// exchange buffers.  The wait is bounded; a timeout sets *err and the CTA
+// returns after giving the copies a second bounded wait.
+template <int MAXT>
+__global__ void __launch_bounds__(MAXT, 1024 / MAXT)
+    cols_tma_kernel(const __grid_constant__ CUtensorMap tmap, ColArgs a, int G, int box_rows) {
+  extern __shared__ __align__(128) float2 sm[];
+  const int M = a.M;
+  const int nthr = M >> 4;
+  float2* tw = sm;
+  float2* land = sm + kTwSlots;  // [row][g], G * M values (+ 16 for exchange stride)
+  uint64_t* bar = reinterpret_cast<uint64_t*>(land + G * M + 16);
+  const int g = threadIdx.x % G, tid = threadIdx.x / G;
+  const int q0 = blockIdx.x * G, pair = blockIdx.y;
+  if (threadIdx.x == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  __syncthreads();  // the barrier is initialised before any thread polls it
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(bar, (unsigned)(G * M) * (unsigned)sizeof(float2));
+    for (int b = 0; b < M; b += box_rows)
+      tma_load_2d(land + (size_t)b * G, &tmap, 2 * q0, pair * M + b, bar);
+  }
+  load_twiddles(tw, a.tw, M);
+  const bool ok = mbar_wait(bar, 0u);
+  if (__syncthreads_or(!ok)) {
+    if (threadIdx.x == 0) {
+      atomicExch(a.err, 1);
+      mbar_wait(bar, 0u);
+    }
+    __syncthreads();
+    return;
+  }
+  float2 v[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) v[r] = land[(tid + r * nthr) * G + g];
+  __syncthreads();  // inputs read before the landing buffer becomes the exchange buffer
+  fft_reg<-1>(v, land + g * (M + 16 / G), M, tid, nthr, tw, tw + 64);
+  float2* Hp = a.H + (size_t)pair * M * M + q0 + g;
+  const int Rl = last_radix(M);
+#pragma unroll
+  for (int idx = 0; idx < 16; ++idx) Hp[(size_t)(tid + nthr * out_index(idx, Rl)) * M] = v[idx];
+}
+
 // ------------------------------------------------------------------ second axis + deapod (K4)
 
 template <int MAXT>
@@ -642,6 +756,24 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) rows_kernel(RowArgs a) {
   }
 }
 
+// Self-test of the bounded-wait path: one thread arms an mbarrier that no
+// copy or thread ever completes, polls it `limit` times, and records the
+// timeout in *err.  No fault, trap or hang is involved.
+__global__ void wait_timeout_probe(int* err, int limit) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x != 0) return;
+  mbar_init(&bar, 1);
+  fence_mbar_init();
+  bool done = false;
+  for (int it = 0; it < limit && !done; ++it) done = mbar_try_wait(&bar, 0u);
+  *err = done ? 0 : 1;
+}
+
+cudaError_t launch_wait_probe(int* err, int limit, cudaStream_t s) {
+  wait_timeout_probe<<<1, 32, 0, s>>>(err, limit);
+  return cudaGetLastError();
+}
+
 // ------------------------------------------------------------------ launchers
 
 static int fft_smem_bytes(int N) { return (kTwSlots + N) * (int)sizeof(float2); }
@@ -662,6 +794,7 @@ cudaError_t init_kernel_attributes() {
                        (const void*)spectra_kernel<__nv_bfloat16, 512>,
                        (const void*)spectra_kernel<uint16_t, 512>,
                        (const void*)cols_kernel<256>, (const void*)cols_kernel<512>,
+                       (const void*)cols_tma_kernel<256>, (const void*)cols_tma_kernel<512>,
                        (const void*)rows_kernel<256>, (const void*)rows_kernel<512>,
                        (const void*)grid_kernel<4>, (const void*)grid_kernel<kMaxTaps>};
   for (const void* f : fns) {
@@ -731,8 +864,45 @@ int cols_group(int M) {
   return g < 1 ? 1 : (g > 8 ? 8 : g);
 }
 
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
 cudaError_t launch_cols(const ColArgs& a, cudaStream_t s) {
   const int G = cols_group(a.M);
+  const int threads = G * (a.M / 16);
+  PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
+  if (a.err && encode && G >= 2 && a.M >= 16 && ((uintptr_t)a.H % 16) == 0) {
+    // H as a 2-D float array: 2*M floats per row, pairs*M rows
+    CUtensorMap map;
+    const int box_rows = a.M < 256 ? a.M : 256;
+    cuuint64_t dims[2] = {(cuuint64_t)2 * a.M, (cuuint64_t)a.pairs * a.M};
+    cuuint64_t strides[1] = {(cuuint64_t)2 * a.M * sizeof(float)};
+    cuuint32_t box[2] = {(cuuint32_t)(2 * G), (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)a.H, dims, strides, box,
+                        estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r == CUDA_SUCCESS) {
+      const int smem = (kTwSlots + G * a.M + 16) * (int)sizeof(float2) + (int)sizeof(uint64_t);
+      dim3 grid(a.M / G, a.pairs);
+      if (threads <= 256) cols_tma_kernel<256><<<grid, threads, smem, s>>>(map, a, G, box_rows);
+      else cols_tma_kernel<512><<<grid, threads, smem, s>>>(map, a, G, box_rows);
+      return cudaGetLastError();
+    }
+  }
   const int smem = (kTwSlots + G * (a.M + 16 / G)) * (int)sizeof(float2);
   dim3 grid(a.M / G, a.pairs);
   if (G * (a.M / 16) <= 256) cols_kernel<256><<<grid, G * (a.M / 16), smem, s>>>(a, G);

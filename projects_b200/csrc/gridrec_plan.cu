@@ -120,6 +120,7 @@ struct Plan {
   int4* d_split_list = nullptr;
   int n_split_tiles = 0;
   unsigned* d_queue = nullptr;
+  int* d_err = nullptr;  // device error word: nonzero after a bounded wait ran out
   // workspaces (max_pairs pairs)
   float2* d_spec = nullptr;
   float2* d_H = nullptr;
@@ -132,7 +133,8 @@ struct Plan {
   float* d_out[2] = {nullptr, nullptr};
   size_t in_bytes = 0, out_bytes = 0;  // per staging buffer
   long out_stride_staged = 0;
-  cudaStream_t copy_stream = nullptr;
+  cudaStream_t copy_stream = nullptr;   // host->device copies
+  cudaStream_t d2h_stream = nullptr;    // device->host copies (runs beside the H2D ones)
   cudaEvent_t ev_h2d[2] = {}, ev_comp[2] = {}, ev_d2h[2] = {};
   size_t device_bytes = 0;
   long launches = 0;
@@ -402,7 +404,7 @@ int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1
               (float)(2.0 * p->ltbl / p->L)};
   GR_CUDA(launch_grid(ga, p->ntaps, st));
   GR_MARK();
-  ColArgs ca{p->d_H, p->d_tw_m, p->M, pairs};
+  ColArgs ca{p->d_H, p->d_tw_m, p->M, pairs, p->d_err};
   GR_CUDA(launch_cols(ca, st));
   GR_MARK();
   RowArgs ra{p->d_H, p->d_tw_m, p->d_winv, o1, o2, out_pair_stride, out_stride, n_valid,
@@ -496,6 +498,7 @@ int gr_plan_destroy(gr_plan* plan) {
     if (plan->ev_d2h[b]) cudaEventDestroy(plan->ev_d2h[b]);
   }
   if (plan->copy_stream) cudaStreamDestroy(plan->copy_stream);
+  if (plan->d2h_stream) cudaStreamDestroy(plan->d2h_stream);
   for (cudaEvent_t e : plan->events) cudaEventDestroy(e);
   delete plan;
   return GR_OK;
@@ -604,11 +607,12 @@ int gr_plan_create(const gr_params* prm, gr_plan** out) {
       (rc = dev_alloc(p, &p->d_H, P * (size_t)M * M)) ||
       (rc = dev_alloc(p, &p->d_scratch, ((P + 1) / 2) * (size_t)std::max(p->n_slots, 1) * kTile * kTile)) ||
       (rc = dev_alloc(p, &p->d_pq, P * p->J)) ||
-      (rc = dev_alloc(p, &p->d_queue, 1))) {
+      (rc = dev_alloc(p, &p->d_queue, 1)) || (rc = dev_alloc(p, &p->d_err, 1))) {
     gr_plan_destroy(p);
     return rc;
   }
-  cudaError_t e = cudaDeviceSynchronize();
+  cudaError_t e = cudaMemset(p->d_err, 0, sizeof(int));
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
   if (e != cudaSuccess) {
     gr_plan_destroy(p);
     return fail(GR_ERR_CUDA, "plan init: %s", cudaGetErrorString(e));
@@ -638,6 +642,34 @@ int gr_worklist_export(const gr_params* prm, int* n_items, int* n_runs, int* til
   std::memcpy(runs, wl.runs.data(), wl.runs.size() * sizeof(Run));
   std::memcpy(splits, wl.splits.data(), wl.splits.size() * sizeof(Split));
   return GR_OK;
+}
+
+int gr_plan_device_status(gr_plan* p, void* stream) {
+  using namespace gr;
+  if (!p) return fail(GR_ERR_ARG, "null plan");
+  DeviceGuard g(p->device);
+  GR_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+  int flag = 0;
+  GR_CUDA(cudaMemcpy(&flag, p->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag) {
+    GR_CUDA(cudaMemset(p->d_err, 0, sizeof(int)));
+    return fail(GR_ERR_TIMEOUT, "a bounded device wait ran out (kernel stopped early)");
+  }
+  return GR_OK;
+}
+
+int gr_selftest_wait_timeout(int device) {
+  using namespace gr;
+  DeviceGuard g(device);
+  int* d = nullptr;
+  GR_CUDA(cudaMalloc(&d, sizeof(int)));
+  int flag = 0;
+  cudaError_t e = cudaMemset(d, 0, sizeof(int));
+  if (e == cudaSuccess) e = launch_wait_probe(d, 1 << 12, nullptr);
+  if (e == cudaSuccess) e = cudaMemcpy(&flag, d, sizeof(int), cudaMemcpyDeviceToHost);
+  cudaFree(d);
+  if (e != cudaSuccess) return fail(GR_ERR_CUDA, "wait self-test: %s", cudaGetErrorString(e));
+  return flag ? fail(GR_ERR_TIMEOUT, "mbarrier wait ran out as intended (self-test)") : GR_OK;
 }
 
 int gr_plan_set_timing(gr_plan* p, int enable) {
@@ -758,6 +790,7 @@ int gr_reconstruct_host(gr_plan* p, const gr_batch_desc* b, void* stream) {
   const bool out_pinned = is_pinned(b->outs);
   if (!p->copy_stream) {
     GR_CUDA(cudaStreamCreateWithFlags(&p->copy_stream, cudaStreamNonBlocking));
+    GR_CUDA(cudaStreamCreateWithFlags(&p->d2h_stream, cudaStreamNonBlocking));
     for (int k = 0; k < 2; ++k) {
       GR_CUDA(cudaEventCreateWithFlags(&p->ev_h2d[k], cudaEventDisableTiming));
       GR_CUDA(cudaEventCreateWithFlags(&p->ev_comp[k], cudaEventDisableTiming));
@@ -846,11 +879,11 @@ int gr_reconstruct_host(gr_plan* p, const gr_batch_desc* b, void* stream) {
                       2 * slice_out_el, b->out_stride, st);
     if (rc) { cleanup(); return rc; }
     GR_CUDA(cudaEventRecord(p->ev_comp[k], st));
-    GR_CUDA(cudaStreamWaitEvent(p->copy_stream, p->ev_comp[k], 0));
+    GR_CUDA(cudaStreamWaitEvent(p->d2h_stream, p->ev_comp[k], 0));
     char* dst = out_pinned ? reinterpret_cast<char*>(b->outs) + (size_t)s0 * slice_out
                            : reinterpret_cast<char*>(p->h_out[k]);
-    GR_CUDA(cudaMemcpyAsync(dst, p->d_out[k], ob, cudaMemcpyDeviceToHost, p->copy_stream));
-    GR_CUDA(cudaEventRecord(p->ev_d2h[k], p->copy_stream));
+    GR_CUDA(cudaMemcpyAsync(dst, p->d_out[k], ob, cudaMemcpyDeviceToHost, p->d2h_stream));
+    GR_CUDA(cudaEventRecord(p->ev_d2h[k], p->d2h_stream));
     pend[k].chunk = c;
     pend[k].bytes = ob;
     pend[k].off = (size_t)s0 * slice_out;
@@ -859,7 +892,7 @@ int gr_reconstruct_host(gr_plan* p, const gr_batch_desc* b, void* stream) {
     if ((rc = finish(k))) { cleanup(); return rc; }
   GR_CUDA(cudaStreamSynchronize(st));
   cleanup();
-  return GR_OK;
+  return gr_plan_device_status(p, stream);
 }
 
 }  // extern "C"
@@ -955,7 +988,9 @@ extern "C" int gr_reconstruct_pair_noalloc(gr_plan* p, const float* sino1, const
               p->d_dir, p->d_wtbl, p->n_items, 1, p->n_ang, p->J, p->M, p->tiles_v, p->n_slots,
               p->ltbl, (float)(p->L / 2), (float)(2.0 * p->ltbl / p->L)};
   GR_CUDA(launch_grid(ga, p->ntaps, st));
-  ColArgs ca{H, p->d_tw_m, p->M, 1};
+  int* err = reinterpret_cast<int*>(base + off_queue + 64);
+  GR_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
+  ColArgs ca{H, p->d_tw_m, p->M, 1, err};
   GR_CUDA(launch_cols(ca, st));
   RowArgs ra{H, p->d_tw_m, p->d_winv, out1, o2, 0, out_stride, n_valid, p->M, p->M0, p->M02, 1};
   GR_CUDA(launch_rows(ra, st));

@@ -28,7 +28,8 @@ EXPORTS = ("gr_params_default", "gr_filter_code", "gr_plan_create", "gr_plan_des
            "gr_plan_sizes", "gr_plan_device_bytes", "gr_reconstruct_pair",
            "gr_reconstruct_batch", "gr_reconstruct_host", "gr_last_error",
            "gr_plan_launch_count", "gr_plan_work_stats", "gr_worklist_export",
-           "gr_plan_set_timing", "gr_plan_stage_times", "gr_reconstruct_pair_noalloc")
+           "gr_plan_set_timing", "gr_plan_stage_times", "gr_reconstruct_pair_noalloc",
+           "gr_plan_device_status", "gr_selftest_wait_timeout")
 STAGES = ("phase", "spectra", "grid", "cols", "rows_deapod")
 
 
@@ -81,6 +82,8 @@ def lib():
         L.gr_plan_work_stats.argtypes = [C.c_void_p, C.POINTER(C.c_int), C.POINTER(C.c_int),
                                          C.POINTER(C.c_int), C.POINTER(C.c_long)]
         L.gr_plan_set_timing.argtypes = [C.c_void_p, C.c_int]
+        L.gr_plan_device_status.argtypes = [C.c_void_p, C.c_void_p]
+        L.gr_selftest_wait_timeout.argtypes = [C.c_int]
         L.gr_plan_stage_times.argtypes = [C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_long)]
         ip = C.POINTER(C.c_int)
         L.gr_worklist_export.argtypes = [P, ip, ip, ip, C.c_void_p, C.c_void_p, C.c_void_p,
@@ -208,6 +211,10 @@ class Plan:
         n = C.c_long()
         _check(lib().gr_plan_launch_count(self._h, C.byref(n)), "gr_plan_launch_count")
         return n.value
+
+    def device_status(self, stream=None):
+        """Raises GrError(GR_ERR_TIMEOUT) if a bounded device wait ran out."""
+        _check(lib().gr_plan_device_status(self._h, _stream_ptr(stream)), "gr_plan_device_status")
 
     def set_timing(self, enable: bool):
         _check(lib().gr_plan_set_timing(self._h, int(enable)), "gr_plan_set_timing")

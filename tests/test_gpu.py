@@ -30,6 +30,7 @@ def _gpu_pair(s1, s2, theta, **kw):
         o2 = torch.zeros_like(o1)
         plan.reconstruct_pair(_dev(s1), _dev(s2), o1, o2)
         torch.cuda.synchronize()
+        plan.device_status()
         assert plan.launches() == 5
         return o1.cpu().numpy()[:, :plan.M0], o2.cpu().numpy()[:, :plan.M0]
 
@@ -238,3 +239,11 @@ def test_full_size_2048x1500_and_linearity():
     print(f"2048x1500 relL2 vs float64: {e1:.2e} {e2:.2e}")
     assert e1 < TOL and e2 < TOL
     assert ph.rel_l2(gl[0], 2 * g[0] - g[1]) < TOL
+
+
+def test_bounded_wait_timeout_is_reported():
+    """Failure detection without a fault: a wait that nothing completes runs
+    out, the kernel returns, and the host reads GR_ERR_TIMEOUT."""
+    assert G.lib().gr_selftest_wait_timeout(0) == -6
+    x = torch.ones(4, device="cuda")          # the context is still usable
+    assert float(x.sum()) == 4.0
