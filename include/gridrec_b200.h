@@ -206,6 +206,64 @@ int gr_plan_launch_count(const gr_plan* plan, long* launches);
 int gr_plan_work_stats(const gr_plan* plan, int* n_items, int* n_runs, int* n_slots,
                        long* total_samples);
 
+/* ---- Slice pipeline around gridrec (the reference's tomo_recon and find_shift
+ * drivers).  Sinograms are n_ang rows of n_det float32, slices contiguous, in
+ * device memory; calls are asynchronous on `stream` unless stated. */
+
+/* Ring suppression <- RingCorrectionSinogram   gridrec/GPU/tomo_recon.cpp:3905-3972
+ * (the reference runs 20 rounds with RING_COEFF 1.0, tomo_recon.h:63).  In place on
+ * n_slices sinograms; workspace: gr_ring_workspace_bytes() bytes of device memory. */
+size_t gr_ring_workspace_bytes(int n_slices, int n_det, int n_ang);
+int gr_ring_removal(float* sinos, int n_slices, int n_det, int n_ang, float ring_coeff,
+                    int iterations, void* workspace, void* stream);
+
+/* Sub-pixel shift and half padding <- GridRecSlices  gridrec/GPU/tomo_recon.cpp:3708-3807
+ * (also find_shift/src/main/find_shift.cpp:1729-1808).  Slice s is shifted by
+ * xoffsets[s] (device array) with linear interpolation (neighbours clamped to the
+ * row), placed at column n_det/2 of rows of out_width floats, with the n_det/2
+ * columns on each side repeating the edge values.  Equal to the reference's float
+ * arithmetic bit for bit. */
+int gr_shift_pad(const float* in, float* out, int n_slices, int n_det, int n_ang,
+                 const float* xoffsets, int out_width, void* stream);
+
+/* Centre crop <- GridRecSlices  tomo_recon.cpp:3855-3862: out[j][k] =
+ * recon[j + offset][k + offset] for j, k < n; with radius > 0 also the circular
+ * crop of tomo_recon.cpp:2150-2165 (pixels with (k-n/2)^2 + (j-n/2)^2 >= radius^2
+ * set to 0).  Strides and per-slice sizes in floats. */
+int gr_crop_center(const float* recon, long recon_stride, long recon_slice_elems, float* out,
+                   long out_stride, long out_slice_elems, int n_slices, int n, int offset,
+                   int radius, void* stream);
+
+/* Histogram entropy <- entropy()  find_shift/src/main/find_shift.cpp:2078-2115.
+ * For each of n_groups groups of `group` image windows (rows x cols, row_stride;
+ * images image_stride apart, groups group_stride apart, all in floats): nbins + 1
+ * bins of width (vmax - vmin) / nbins, bin = (int)((x - vmin) / width) in float,
+ * entropies[g] = -sum p log2 p (device array of n_groups floats).  Workspace:
+ * gr_entropy_workspace_bytes() bytes.  nbins <= 50000. */
+size_t gr_entropy_workspace_bytes(int n_groups, int nbins);
+int gr_entropy(const float* images, int n_groups, int group, int rows, int cols, long row_stride,
+               long image_stride, long group_stride, float vmin, float vmax, int nbins,
+               float* entropies, void* workspace, void* stream);
+
+/* Half-padded slice reconstruction <- GridRecSlices  tomo_recon.cpp:3679-3862:
+ * every slice shifted by xoffset and half padded to the plan's width (the plan is
+ * made for 2 n_det detector pixels and n_ang angles), reconstructed in pairs, and
+ * cropped to n_det x n_det (rows of out_stride floats, slices n_det * out_stride
+ * apart).  Allocates its intermediates (stream-ordered). */
+int gr_reconstruct_padded(gr_plan* plan, const float* sinos, int n_slices, int n_det, int n_ang,
+                          float xoffset, float* outs, long out_stride, void* stream);
+
+/* Rotation-centre refinement by entropy <- find_shift  find_shift/src/main/find_shift.cpp:1653-1900.
+ * For each of n_cand shifts (host array) the slice pair (sino1, sino2; device) is
+ * shifted, half padded and reconstructed with `plan` (2 n_det wide, n_ang angles),
+ * both n_det x n_det crops are scored together with the histogram entropy
+ * [hist_lo, hist_hi] in nbins bins, and scores[c] (host) receives the score.
+ * *best = first index of the minimum score.  best_images (optional, device,
+ * 2 x n_det x n_det) receives the pair at the best shift.  Synchronises `stream`. */
+int gr_center_search(gr_plan* plan, const float* sino1, const float* sino2, int n_det, int n_ang,
+                     const float* shifts, int n_cand, float hist_lo, float hist_hi, int nbins,
+                     float* scores, int* best, float* best_images, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

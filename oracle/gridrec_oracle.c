@@ -335,3 +335,108 @@ int orc_gridrec_pair(const orc_params* p, const double* theta_deg,
   free(spec); free(H);
   return rc;
 }
+
+/* ---------------------------------------------------------------- slice pipeline
+ * Restatements of the steps around gridrec in the reference's drivers. */
+
+/* RingCorrectionSinogram (gridrec/GPU/tomo_recon.cpp:3905-3965): `iterations`
+ * rounds of (renormalise every projection to the global mean; column mean;
+ * 3-tap low-pass; subtract ring_coeff * (mean - low-pass), clamped at 0). */
+void orc_ring_removal(double* data, int n_det, int n_ang, double ring_coeff, int iterations) {
+  double* mv = (double*)malloc(n_ang * sizeof(double));
+  double* ms = (double*)malloc(n_det * sizeof(double));
+  double* lp = (double*)malloc(n_det * sizeof(double));
+  for (int m = 0; m < iterations; ++m) {
+    double total = 0.0;
+    for (int i = 0; i < n_ang; ++i) {
+      double s = 0.0;
+      for (int j = 0; j < n_det; ++j) s += data[(long)i * n_det + j];
+      mv[i] = s / n_det;
+      total += mv[i];
+    }
+    total /= n_ang;
+    for (int i = 0; i < n_ang; ++i)
+      if (mv[i] != 0.0)
+        for (int j = 0; j < n_det; ++j) data[(long)i * n_det + j] *= total / mv[i];
+    for (int j = 0; j < n_det; ++j) ms[j] = 0.0;
+    for (int i = 0; i < n_ang; ++i)
+      for (int j = 0; j < n_det; ++j) ms[j] += data[(long)i * n_det + j];
+    for (int j = 0; j < n_det; ++j) ms[j] /= n_ang;
+    for (int j = 1; j < n_det - 1; ++j) lp[j] = (ms[j - 1] + ms[j] + ms[j + 1]) / 3.0;
+    lp[0] = ms[0];
+    lp[n_det - 1] = ms[n_det - 1];
+    for (int i = 0; i < n_ang; ++i)
+      for (int j = 0; j < n_det; ++j) {
+        const double tmp = ms[j] - lp[j];
+        double* x = &data[(long)i * n_det + j];
+        *x = (*x - tmp * ring_coeff > 0.0) ? *x - tmp * ring_coeff : 0.0;
+      }
+  }
+  free(mv); free(ms); free(lp);
+}
+
+/* Sub-pixel shift by xoffset and half padding (GridRecSlices,
+ * gridrec/GPU/tomo_recon.cpp:3708-3810; find_shift/src/main/find_shift.cpp:1729-1808),
+ * in float like the reference: kk = k - xoffset, nkk = floor(kk), neighbours
+ * clamped to the row, value = in[nkk] (nkk + 1 - kk) + in[nkk + 1] (kk - nkk) at
+ * column k + n_det/2; the n_det/2 columns on each side repeat the edge value and
+ * any column past them (odd n_det) stays zero. */
+void orc_shift_pad(const float* in, float* out, int n_det, int n_ang, float xoffset,
+                   int out_width) {
+  const int pad = n_det / 2;
+  for (int i = 0; i < n_ang; ++i) {
+    const float* r = in + (long)i * n_det;
+    float* o = out + (long)i * out_width;
+    for (int k = 0; k < out_width; ++k) o[k] = 0.0f;
+    for (int k = 0; k < n_det; ++k) {
+      const float kk = (float)k - xoffset;
+      const int nk = (int)floorf(kk);
+      const int a = nk < 0 ? 0 : (nk >= n_det ? n_det - 1 : nk);
+      const int b = nk + 1 < 0 ? 0 : (nk + 1 >= n_det ? n_det - 1 : nk + 1);
+      float v = 0.0f;
+      v += r[a] * ((float)(nk + 1) - kk);
+      v += r[b] * (kk - (float)nk);
+      o[k + pad] = v;
+    }
+    for (int k = 0; k < pad; ++k) o[k] = o[pad];
+    for (int k = 0; k < pad && pad + n_det + k < out_width; ++k)
+      o[pad + n_det + k] = o[pad + n_det - 1];
+  }
+}
+
+/* Centre crop of GridRecSlices (tomo_recon.cpp:3855-3862) and the circular crop
+ * of the output stage (tomo_recon.cpp:2150-2165): out[j][k] = rec[j + offset][k + offset],
+ * and with radius > 0 pixels with (k - n/2)^2 + (j - n/2)^2 >= radius^2 are zero. */
+void orc_crop(const float* rec, long rec_stride, float* out, int n, int offset, int radius) {
+  for (int j = 0; j < n; ++j)
+    for (int k = 0; k < n; ++k) {
+      const long dk = k - n / 2, dj = j - n / 2;
+      float v = rec[(long)(j + offset) * rec_stride + k + offset];
+      if (radius > 0 && dk * dk + dj * dj >= (long)radius * radius) v = 0.0f;
+      out[(long)j * n + k] = v;
+    }
+}
+
+/* Histogram entropy of find_shift (find_shift/src/main/find_shift.cpp:2078-2115):
+ * num_hist_bin + 1 bins, bin = (int)((x - min) / inv) computed in float with
+ * inv = (max - min) / num_hist_bin (truncation toward zero; bins outside
+ * [0, num_hist_bin] and NaN ignored), entropy = -sum p log2 p with p = count / n,
+ * accumulated in double. */
+double orc_entropy(const float* data, long n, float vmin, float vmax, int num_hist_bin) {
+  long* hist = (long*)calloc(num_hist_bin + 1, sizeof(long));
+  const float inv = (vmax - vmin) / (float)num_hist_bin;
+  for (long i = 0; i < n; ++i) {
+    const float f = (data[i] - vmin) / inv;
+    if (!(f == f) || f >= 2147483648.0f || f <= -2147483649.0f) continue;
+    const int ind = (int)f;
+    if (ind >= 0 && ind <= num_hist_bin) hist[ind]++;
+  }
+  double e = 0.0;
+  for (int b = 0; b <= num_hist_bin; ++b)
+    if (hist[b] > 0) {
+      const double p = (double)hist[b] / n;
+      e += -p * log(p) / log(2.0);
+    }
+  free(hist);
+  return e;
+}

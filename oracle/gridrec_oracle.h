@@ -31,7 +31,14 @@ int orc_deapod(const orc_params* p, const double* H, double* out1, double* out2,
 int orc_gridrec_pair(const orc_params* p, const double* theta_deg, const double* sino1,
                      const double* sino2, double* out1, double* out2, long out_stride);
 
+/* Slice-pipeline steps around gridrec (see gridrec_oracle.c). */
+void orc_ring_removal(double* data, int n_det, int n_ang, double ring_coeff, int iterations);
+void orc_shift_pad(const float* in, float* out, int n_det, int n_ang, float xoffset, int out_width);
+void orc_crop(const float* rec, long rec_stride, float* out, int n, int offset, int radius);
+double orc_entropy(const float* data, long n, float vmin, float vmax, int num_hist_bin);
+
 #ifdef __cplusplus
 }
 #endif
 #endif
+

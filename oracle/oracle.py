@@ -55,6 +55,14 @@ def port_lib():
         lib.orc_fft1d.restype = None
         lib.orc_deapod.argtypes = [P, _dp, _dp, _dp, C.c_long]
         lib.orc_gridrec_pair.argtypes = [P, _dp, _dp, _dp, _dp, _dp, C.c_long]
+        lib.orc_ring_removal.argtypes = [_dp, C.c_int, C.c_int, C.c_double, C.c_int]
+        lib.orc_ring_removal.restype = None
+        lib.orc_shift_pad.argtypes = [_fp, _fp, C.c_int, C.c_int, C.c_float, C.c_int]
+        lib.orc_shift_pad.restype = None
+        lib.orc_crop.argtypes = [_fp, C.c_long, _fp, C.c_int, C.c_int, C.c_int]
+        lib.orc_crop.restype = None
+        lib.orc_entropy.argtypes = [_fp, C.c_long, C.c_float, C.c_float, C.c_int]
+        lib.orc_entropy.restype = C.c_double
         _port = lib
     return _port
 
@@ -128,6 +136,35 @@ def port_gridrec_pair(sino1, sino2, theta_deg, center1=None, center2=None, filte
     return o1, o2
 
 
+def port_ring_removal(sino, ring_coeff=1.0, iterations=20):
+    x = np.ascontiguousarray(sino, np.float64).copy()
+    port_lib().orc_ring_removal(x, x.shape[1], x.shape[0], float(ring_coeff), int(iterations))
+    return x
+
+
+def port_shift_pad(sino, xoffset, out_width=None):
+    """float32 sinogram (n_ang, n_det) -> (n_ang, out_width) shifted, half-padded rows."""
+    n_ang, n_det = sino.shape
+    w = 2 * n_det if out_width is None else int(out_width)
+    out = np.zeros((n_ang, w), np.float32)
+    port_lib().orc_shift_pad(np.ascontiguousarray(sino, np.float32), out, n_det, n_ang,
+                             float(xoffset), w)
+    return out
+
+
+def port_crop(rec, n, offset, radius=0):
+    """Centre crop rec[offset:offset+n, offset:offset+n] with optional circular mask."""
+    r = np.ascontiguousarray(rec, np.float32)
+    out = np.zeros((n, n), np.float32)
+    port_lib().orc_crop(r, r.shape[1], out, int(n), int(offset), int(radius))
+    return out
+
+
+def port_entropy(img, vmin, vmax, nbins):
+    x = np.ascontiguousarray(img, np.float32).ravel()
+    return port_lib().orc_entropy(x, x.size, float(vmin), float(vmax), int(nbins))
+
+
 # ---------------------------------------------------------------- reference builds
 
 def ref_available() -> bool:
@@ -144,7 +181,14 @@ def _ref_lib(name, real):
             raise RuntimeError(f"reference oracle not built: {path}")
         lib = C.CDLL(path)
         rp = np.ctypeslib.ndpointer(dtype=real, flags="C_CONTIGUOUS")
-        if name == "libgridrec_refb.so":
+        if name == "libprep_ref.so":
+            lib.ref_ring_removal.argtypes = [rp, C.c_int, C.c_int, C.c_float]
+            lib.ref_ring_removal.restype = None
+            lib.ref_entropy.argtypes = [rp, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int]
+            lib.ref_entropy.restype = C.c_float
+            lib.ref_shift_pad.argtypes = [rp, rp, C.c_int, C.c_int, C.c_float, rp]
+            lib.ref_shift_pad.restype = None
+        elif name == "libgridrec_refb.so":
             lib.refb_gridrec_pair.argtypes = [C.c_int, C.c_int, rp, C.c_float, C.c_char_p,
                                               C.c_float, C.c_float, C.c_int, rp, rp, rp, rp,
                                               C.c_int]
@@ -211,3 +255,33 @@ def refb_gridrec_pair(sino1, sino2, theta_deg, center, filter_name="shlo", C_=6.
     lib.refb_gridrec_pair(n_det, n_ang, th, center, filter_name.encode(), C_, sampl, ltbl,
                           s1, s2, o1, o2, stride)
     return o1, o2, m0
+
+
+def prep_ref_available() -> bool:
+    return os.path.exists(os.path.join(_REF, "libprep_ref.so"))
+
+
+def ref_ring_removal(sino, ring_coeff=1.0):
+    """RingCorrectionSinogram of the reference (20 rounds, float32, in place on a copy)."""
+    lib = _ref_lib("libprep_ref.so", np.float32)
+    x = np.ascontiguousarray(sino, np.float32).copy()
+    lib.ref_ring_removal(x, x.shape[1], x.shape[0], float(ring_coeff))
+    return x
+
+
+def ref_entropy(img, vmin, vmax, nbins):
+    """find_shift's entropy() over a (ym, xm) float32 image."""
+    lib = _ref_lib("libprep_ref.so", np.float32)
+    x = np.ascontiguousarray(img, np.float32)
+    ym, xm = x.shape
+    return float(lib.ref_entropy(x, float(vmin), float(vmax), int(nbins), xm, ym))
+
+
+def ref_shift_pad(sino1, sino2, xoffset):
+    """GridRecSlices' shift and half padding of a slice pair -> (2, n_ang, 2 n_det)."""
+    lib = _ref_lib("libprep_ref.so", np.float32)
+    n_ang, n_det = sino1.shape
+    out = np.zeros((2, n_ang, 2 * n_det), np.float32)
+    lib.ref_shift_pad(np.ascontiguousarray(sino1, np.float32),
+                      np.ascontiguousarray(sino2, np.float32), n_det, n_ang, float(xoffset), out)
+    return out

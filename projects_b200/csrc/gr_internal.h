@@ -107,6 +107,12 @@ struct RowArgs {
   int M, M0, M02, pairs;
 };
 
+// Records a formatted message for gr_last_error() and returns code (gridrec_plan.cu).
+int fail(int code, const char* fmt, ...);
+
+// Shape of a plan, for the pre/post-processing entry points (gridrec_plan.cu).
+int plan_shape(const gr_plan* p, int* n_det, int* n_ang, int* M0, int* max_pairs, int* device);
+
 // Kernel launchers (gridrec_kernels.cu).  Return cudaGetLastError().
 cudaError_t init_kernel_attributes();
 cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t s);

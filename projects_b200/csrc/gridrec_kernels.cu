@@ -436,8 +436,8 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
 // sample (lane t owns footprint row t; column weights are exchanged by
 // shuffles), so the geometry -- positions, table lookups -- is computed once
 // for both pairs.  The samples of one step are taken P apart along the run
-// with P * max(|du|,|dv|) >= NT, so their NT x NT footprints are disjoint:
-// (P per run from the host, which uses the same criterion)
+// with P * max(|du|,|dv|) > L, so no two of them share a valid tap (taps lie
+// within L/2 of their sample); P per run comes from the host
 // plain read-modify-write needs no atomics, and the summation order is fixed,
 // so the result is bitwise reproducible.  Float/int conversions use exact
 // magic-number rounding on the FP32 pipe.  Tiles split over several items
@@ -538,8 +538,8 @@ __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
       stage[32 + lane] = make_float4(nA1.x, nA1.y, nB1.x, nB1.y);
       __syncwarp();
       prefetch(r + 1);
-      // run.P: samples P apart have disjoint footprints (P * max(|du|,|dv|)
-      // >= NT with margin), chosen on the host to minimise the steps
+      // run.P: samples P apart never share a valid tap (P * max(|du|,|dv|)
+      // > L with margin), chosen on the host to minimise the steps
       const int P = run.P;
       const float fP = (float)P;
       for (int blk = run.jlo; blk <= run.jhi; blk += SPW * P) {

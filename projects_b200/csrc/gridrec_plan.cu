@@ -16,8 +16,6 @@
 
 namespace gr {
 
-namespace {
-
 thread_local std::string g_err = "no error";
 
 int fail(int code, const char* fmt, ...) {
@@ -29,6 +27,8 @@ int fail(int code, const char* fmt, ...) {
   g_err = buf;
   return code;
 }
+
+namespace {
 
 #define GR_CUDA(call)                                                                   \
   do {                                                                                  \
@@ -186,9 +186,11 @@ struct WorkList {
 // Step spacing P of a run (see grid_kernel): the smallest P with
 // P * max(|du|,|dv|) >= NT (with the kernel's margin) and, above it, the P
 // needing the fewest steps of spw samples; returns the step count in *steps.
-int run_spacing(double du, double dv, int n, int nt, int spw, int* steps) {
-  const float step = (float)std::max(std::fabs(du), std::fabs(dv));
-  const int pmin = std::max(1, (int)((float)nt * 1.0002f / step) + 1);
+int run_spacing(double du, double dv, int n, double L, int spw, int* steps) {
+  // valid taps lie within L/2 of a sample, so samples more than L apart in
+  // one coordinate never share a cell (margin above FP32 position error)
+  const double step = std::max(std::fabs(du), std::fabs(dv));
+  const int pmin = std::max(1, (int)((L + 2e-3) / step) + 1);
   auto count = [&](int P) {
     int st = 0;
     for (int b = 0; b < n; b += spw * P) st += std::min(P, n - b);
@@ -260,7 +262,7 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
   for (size_t i = 0; i < all.size(); ++i) {
     int steps = 0;
     const int P = run_spacing(dxy[2 * all[i].dir], dxy[2 * all[i].dir + 1],
-                              all[i].jhi - all[i].jlo + 1, nt, spw, &steps);
+                              all[i].jhi - all[i].jlo + 1, L, spw, &steps);
     wl->runs[i] = {all[i].dir, all[i].jlo, all[i].jhi, P};
     run_cost[i] = (long)steps * spw + 4;  // sample slots + per-run overhead
     first[all[i].tile + 1]++;
@@ -453,6 +455,18 @@ int validate_batch(const Plan* p, const gr_batch_desc* b) {
 
 using gr::Plan;
 struct gr_plan : public Plan {};
+
+namespace gr {
+int plan_shape(const gr_plan* p, int* n_det, int* n_ang, int* M0, int* max_pairs, int* device) {
+  if (!p) return fail(GR_ERR_ARG, "null plan");
+  *n_det = p->n_det;
+  *n_ang = p->n_ang;
+  *M0 = p->M0;
+  *max_pairs = p->max_pairs;
+  *device = p->device;
+  return GR_OK;
+}
+}  // namespace gr
 
 extern "C" {
 

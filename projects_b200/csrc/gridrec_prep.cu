@@ -1,0 +1,492 @@
+// Slice-pipeline steps around gridrec, on the device (decarlof/projects):
+//   ring suppression        RingCorrectionSinogram  gridrec/GPU/tomo_recon.cpp:3905-3968
+//   sub-pixel shift + pad   GridRecSlices           gridrec/GPU/tomo_recon.cpp:3708-3810
+//                           (same code in find_shift/src/main/find_shift.cpp:1729-1808)
+//   centre crop             GridRecSlices           gridrec/GPU/tomo_recon.cpp:3855-3862
+//   circular crop           output stage            gridrec/GPU/tomo_recon.cpp:2150-2165
+//   histogram entropy       entropy()               find_shift/src/main/find_shift.cpp:2078-2115
+//   centre search           entropy refinement      find_shift/src/main/find_shift.cpp:1653-1900
+// Sinograms are n_ang rows of n_det floats, slices contiguous.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "gr_internal.h"
+
+namespace gr {
+namespace {
+
+constexpr int kPrepThreads = 256;
+constexpr int kMaxBins = 50000;
+
+__device__ __forceinline__ float block_sum(float v, float* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  float s = 0.f;
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (int)(blockDim.x >> 5) ? red[threadIdx.x] : 0.f;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  }
+  return s;  // valid in thread 0
+}
+
+__device__ __forceinline__ double block_sum_d(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double s = 0.0;
+  if (threadIdx.x < 32) {
+    s = threadIdx.x < (int)(blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  }
+  return s;
+}
+
+// ---------------------------------------------------------------------------
+// Ring suppression.  Each of `iterations` rounds, per slice:
+//   r_i = mean_j x_ij,  g = mean_i r_i,  v_ij = x_ij g / r_i   (rows with r_i = 0 kept)
+//   c_j = mean_i v_ij,  t_j = c_j - (c_{j-1} + c_j + c_{j+1}) / 3   (t_0 = t_{n-1} = 0)
+//   x_ij <- v_ij - coeff t_j  where positive, else 0
+// Three launches per round: column partial sums over row chunks (v recomputed
+// on the fly), t_j, and the row update fused with the next round's row means.
+// The renormalised value is formed as (x g) / r in float, the reference's
+// expression, in both the column pass and the update, so both see equal v.
+
+int ring_chunks(int n_det, int n_ang, int n_slices) {
+  const int bx = (n_det + kPrepThreads - 1) / kPrepThreads;
+  const int want = (2 * 148 + bx * n_slices - 1) / (bx * n_slices);
+  return std::max(1, std::min({want, 32, n_ang}));
+}
+
+__global__ void ring_rowmean_kernel(const float* data, float* rowmean, int n_det, int n_ang) {
+  __shared__ float red[32];
+  const int i = blockIdx.x, s = blockIdx.y;
+  const float* row = data + ((size_t)s * n_ang + i) * n_det;
+  float acc = 0.f;
+  for (int j = threadIdx.x; j < n_det; j += blockDim.x) acc += row[j];
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) rowmean[(size_t)s * n_ang + i] = acc / n_det;
+}
+
+__device__ __forceinline__ float slice_gmean(const float* rm, int n_ang, float* red) {
+  __shared__ float g_s;
+  float acc = 0.f;
+  for (int i = threadIdx.x; i < n_ang; i += blockDim.x) acc += rm[i];
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) g_s = acc / n_ang;
+  __syncthreads();
+  return g_s;
+}
+
+__global__ void ring_colpart_kernel(const float* data, const float* rowmean, float* part,
+                                    float* gmean, int n_det, int n_ang, int rows_per_chunk) {
+  __shared__ float red[32];
+  const int r = blockIdx.y, s = blockIdx.z, R = gridDim.y;
+  const float* rm = rowmean + (size_t)s * n_ang;
+  const float g = slice_gmean(rm, n_ang, red);
+  if (threadIdx.x == 0 && blockIdx.x == 0 && r == 0) gmean[s] = g;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n_det) return;
+  const int i0 = r * rows_per_chunk, i1 = min(n_ang, i0 + rows_per_chunk);
+  const float* x = data + (size_t)s * n_ang * n_det + j;
+  float acc = 0.f;
+  for (int i = i0; i < i1; ++i) {
+    const float ri = rm[i];
+    const float v = x[(size_t)i * n_det];
+    acc += ri != 0.f ? __fdiv_rn(__fmul_rn(v, g), ri) : v;
+  }
+  part[((size_t)s * R + r) * n_det + j] = acc;
+}
+
+__global__ void ring_tilt_kernel(const float* part, float* tilt, int n_det, int n_ang, int R) {
+  const int s = blockIdx.y;
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n_det) return;
+  const float* p = part + (size_t)s * R * n_det;
+  float t = 0.f;
+  if (j > 0 && j < n_det - 1) {
+    float c[3] = {0.f, 0.f, 0.f};
+    for (int q = 0; q < R; ++q)
+      for (int d = 0; d < 3; ++d) c[d] += p[(size_t)q * n_det + j - 1 + d];
+    for (int d = 0; d < 3; ++d) c[d] /= n_ang;
+    t = c[1] - (c[0] + c[1] + c[2]) / 3.f;
+  }
+  tilt[(size_t)s * n_det + j] = t;
+}
+
+__global__ void ring_update_kernel(float* data, float* rowmean, const float* tilt,
+                                   const float* gmean, int n_det, int n_ang, float coeff) {
+  __shared__ float red[32];
+  const int i = blockIdx.x, s = blockIdx.y;
+  float* row = data + ((size_t)s * n_ang + i) * n_det;
+  const float* t = tilt + (size_t)s * n_det;
+  const float ri = rowmean[(size_t)s * n_ang + i];
+  const float g = gmean[s];
+  float acc = 0.f;
+  for (int j = threadIdx.x; j < n_det; j += blockDim.x) {
+    const float x = row[j];
+    const float v = ri != 0.f ? __fdiv_rn(__fmul_rn(x, g), ri) : x;
+    const float d = __fmul_rn(t[j], coeff);
+    const float y = __fsub_rn(v, d) > 0.f ? __fsub_rn(v, d) : 0.f;
+    row[j] = y;
+    acc += y;
+  }
+  acc = block_sum(acc, red);
+  if (threadIdx.x == 0) rowmean[(size_t)s * n_ang + i] = acc / n_det;
+}
+
+// ---------------------------------------------------------------------------
+// Sub-pixel shift and half padding.  Output slice s reads input slice
+// (s % in_mod) and shift xoff[s / off_div] (x_const when xoff is null).  Column k of the input row maps to
+// kp = k + pad (pad = n_det / 2) and takes
+//   kk = k - x0,  n = floor(kk),  in[clamp(n)] (n + 1 - kk) + in[clamp(n + 1)] (kk - n)
+// with indices clamped to [0, n_det); columns left of pad repeat column pad,
+// the pad columns right of pad + n_det repeat column pad + n_det - 1, and any
+// remaining column (odd n_det) is zero.  Float operations in the reference's
+// order without contraction, so the result equals its float arithmetic.
+__global__ void shift_pad_kernel(const float* in, long in_slice, int in_mod, const float* xoff,
+                                 int off_div, float x_const, float* out, int n_det, int n_ang,
+                                 int out_width) {
+  const int i = blockIdx.x, s = blockIdx.y;
+  const float* r = in + (size_t)(s % in_mod) * in_slice + (size_t)i * n_det;
+  float* o = out + ((size_t)s * n_ang + i) * out_width;
+  const float x0 = xoff ? xoff[s / off_div] : x_const;
+  const int pad = n_det / 2;
+  for (int kp = threadIdx.x; kp < out_width; kp += blockDim.x) {
+    if (kp >= 2 * pad + n_det) {
+      o[kp] = 0.f;
+      continue;
+    }
+    const int k = min(max(kp - pad, 0), n_det - 1);
+    const float kk = __fsub_rn((float)k, x0);
+    const int nk = (int)floorf(kk);
+    const int a = min(max(nk, 0), n_det - 1);
+    const int b = min(max(nk + 1, 0), n_det - 1);
+    const float wa = __fsub_rn((float)(nk + 1), kk);
+    const float wb = __fsub_rn(kk, (float)nk);
+    o[kp] = __fadd_rn(__fmul_rn(__ldg(&r[a]), wa), __fmul_rn(__ldg(&r[b]), wb));
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Window copy rows [offset, offset + n) x cols [offset, offset + n); with
+// radius > 0, pixels with (k - n/2)^2 + (j - n/2)^2 >= radius^2 become 0.
+__global__ void crop_kernel(const float* rec, long rec_stride, long rec_slice, float* out,
+                            long out_stride, long out_slice, int n, int offset, int radius) {
+  const int j = blockIdx.x, s = blockIdx.y;
+  const float* src = rec + (size_t)s * rec_slice + (size_t)(j + offset) * rec_stride + offset;
+  float* dst = out + (size_t)s * out_slice + (size_t)j * out_stride;
+  const long long r2 = (long long)radius * radius;
+  const int h = n / 2;
+  const long long dj = (long long)(j - h) * (j - h);
+  for (int k = threadIdx.x; k < n; k += blockDim.x) {
+    float v = src[k];
+    if (radius > 0 && (long long)(k - h) * (k - h) + dj >= r2) v = 0.f;
+    dst[k] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Histogram entropy of a group of image windows: nbins + 1 bins of width
+// inv = (vmax - vmin) / nbins, bin = (int)((x - vmin) / inv) in float
+// (truncation toward zero, values outside [0, nbins] ignored), entropy =
+// -sum p log2 p with p = count / (pixels in the group).
+struct Window {
+  const float* base;
+  long row_stride, image_stride, group_stride;
+  int rows, cols, group;
+};
+
+__global__ void hist_kernel(Window w, float vmin, float inv, int nbins, unsigned* ghist) {
+  extern __shared__ unsigned hist[];
+  for (int b = threadIdx.x; b <= nbins; b += blockDim.x) hist[b] = 0u;
+  __syncthreads();
+  const int g = blockIdx.y;
+  const int total_rows = w.rows * w.group;
+  for (int q = blockIdx.x; q < total_rows; q += gridDim.x) {
+    const int im = q / w.rows, r = q - im * w.rows;
+    const float* row = w.base + (size_t)g * w.group_stride + (size_t)im * w.image_stride +
+                       (size_t)r * w.row_stride;
+    for (int k = threadIdx.x; k < w.cols; k += blockDim.x) {
+      const float f = __fdiv_rn(__fsub_rn(row[k], vmin), inv);
+      const int ind = (int)f;  // NaN is skipped (a host cast gives INT_MIN for it)
+      if (f == f && ind >= 0 && ind <= nbins) atomicAdd(&hist[ind], 1u);
+    }
+  }
+  __syncthreads();
+  unsigned* gh = ghist + (size_t)g * (nbins + 1);
+  for (int b = threadIdx.x; b <= nbins; b += blockDim.x)
+    if (hist[b]) atomicAdd(&gh[b], hist[b]);
+}
+
+__global__ void entropy_final_kernel(const unsigned* ghist, int nbins, double n, float* out) {
+  __shared__ double red[32];
+  const unsigned* gh = ghist + (size_t)blockIdx.x * (nbins + 1);
+  double acc = 0.0;
+  for (int b = threadIdx.x; b <= nbins; b += blockDim.x)
+    if (gh[b]) {
+      const double p = (double)gh[b] / n;
+      acc += -p * log(p) / log(2.0);
+    }
+  acc = block_sum_d(acc, red);
+  if (threadIdx.x == 0) out[blockIdx.x] = (float)acc;
+}
+
+int launch_entropy(const Window& w, int n_groups, float vmin, float vmax, int nbins,
+                   unsigned* ghist, float* out, cudaStream_t st) {
+  const float inv = (vmax - vmin) / (float)nbins;
+  const int smem = (nbins + 1) * (int)sizeof(unsigned);
+  if (smem > 48 * 1024) {
+    cudaError_t e = cudaFuncSetAttribute(hist_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         smem);
+    if (e != cudaSuccess) return fail(GR_ERR_CUDA, "hist smem: %s", cudaGetErrorString(e));
+  }
+  cudaError_t e =
+      cudaMemsetAsync(ghist, 0, (size_t)n_groups * (nbins + 1) * sizeof(unsigned), st);
+  if (e != cudaSuccess) return fail(GR_ERR_CUDA, "hist memset: %s", cudaGetErrorString(e));
+  const int total_rows = w.rows * w.group;
+  const int bx = std::max(1, std::min(total_rows, (4 * 148 + n_groups - 1) / n_groups));
+  hist_kernel<<<dim3(bx, n_groups), 512, smem, st>>>(w, vmin, inv, nbins, ghist);
+  entropy_final_kernel<<<n_groups, 256, 0, st>>>(ghist, nbins,
+                                                 (double)w.rows * w.cols * w.group, out);
+  e = cudaGetLastError();
+  return e == cudaSuccess ? GR_OK : fail(GR_ERR_CUDA, "entropy: %s", cudaGetErrorString(e));
+}
+
+int cuda_fail(cudaError_t e, const char* what) {
+  return fail(GR_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+int check_launch(const char* what) {
+  cudaError_t e = cudaGetLastError();
+  return e == cudaSuccess ? GR_OK : fail(GR_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+// Device buffers freed on scope exit (stream-ordered).
+struct AsyncBuf {
+  void* p = nullptr;
+  cudaStream_t st;
+  explicit AsyncBuf(cudaStream_t s) : st(s) {}
+  ~AsyncBuf() {
+    if (p) cudaFreeAsync(p, st);
+  }
+  int alloc(size_t bytes) {
+    cudaError_t e = cudaMallocAsync(&p, bytes, st);
+    if (e != cudaSuccess) {
+      p = nullptr;
+      return fail(GR_ERR_NOMEM, "cudaMallocAsync(%zu bytes): %s", bytes, cudaGetErrorString(e));
+    }
+    return GR_OK;
+  }
+  template <class T> T* as() const { return static_cast<T*>(p); }
+};
+
+}  // namespace
+}  // namespace gr
+
+using namespace gr;
+
+extern "C" {
+
+size_t gr_ring_workspace_bytes(int n_slices, int n_det, int n_ang) {
+  if (n_slices < 1 || n_det < 1 || n_ang < 1) return 0;
+  const int R = ring_chunks(n_det, n_ang, n_slices);
+  const size_t floats = (size_t)n_slices * ((size_t)n_ang + (size_t)R * n_det + n_det + 1);
+  return floats * sizeof(float);
+}
+
+int gr_ring_removal(float* sinos, int n_slices, int n_det, int n_ang, float ring_coeff,
+                    int iterations, void* workspace, void* stream) {
+  if (!sinos || !workspace) return fail(GR_ERR_ARG, "ring removal: null pointer");
+  if (n_slices < 1 || n_det < 3 || n_ang < 1 || iterations < 0)
+    return fail(GR_ERR_ARG, "ring removal: need n_slices >= 1, n_det >= 3, n_ang >= 1, "
+                            "iterations >= 0");
+  if (iterations == 0) return GR_OK;
+  cudaStream_t st = (cudaStream_t)stream;
+  const int R = ring_chunks(n_det, n_ang, n_slices);
+  const int rows_per = (n_ang + R - 1) / R;
+  float* rowmean = static_cast<float*>(workspace);
+  float* part = rowmean + (size_t)n_slices * n_ang;
+  float* tilt = part + (size_t)n_slices * R * n_det;
+  float* gmean = tilt + (size_t)n_slices * n_det;
+  const int bx = (n_det + kPrepThreads - 1) / kPrepThreads;
+  ring_rowmean_kernel<<<dim3(n_ang, n_slices), kPrepThreads, 0, st>>>(sinos, rowmean, n_det,
+                                                                       n_ang);
+  for (int m = 0; m < iterations; ++m) {
+    ring_colpart_kernel<<<dim3(bx, R, n_slices), kPrepThreads, 0, st>>>(
+        sinos, rowmean, part, gmean, n_det, n_ang, rows_per);
+    ring_tilt_kernel<<<dim3(bx, n_slices), kPrepThreads, 0, st>>>(part, tilt, n_det, n_ang, R);
+    ring_update_kernel<<<dim3(n_ang, n_slices), kPrepThreads, 0, st>>>(
+        sinos, rowmean, tilt, gmean, n_det, n_ang, ring_coeff);
+  }
+  return check_launch("ring removal");
+}
+
+int gr_shift_pad(const float* in, float* out, int n_slices, int n_det, int n_ang,
+                 const float* xoffsets, int out_width, void* stream) {
+  if (!in || !out || !xoffsets) return fail(GR_ERR_ARG, "shift/pad: null pointer");
+  if (n_slices < 1 || n_det < 1 || n_ang < 1 || out_width < n_det)
+    return fail(GR_ERR_ARG, "shift/pad: need n_slices, n_det, n_ang >= 1 and out_width >= n_det");
+  shift_pad_kernel<<<dim3(n_ang, n_slices), kPrepThreads, 0, (cudaStream_t)stream>>>(
+      in, (long)n_ang * n_det, n_slices, xoffsets, 1, 0.f, out, n_det, n_ang, out_width);
+  return check_launch("shift/pad");
+}
+
+int gr_crop_center(const float* recon, long recon_stride, long recon_slice_elems, float* out,
+                   long out_stride, long out_slice_elems, int n_slices, int n, int offset,
+                   int radius, void* stream) {
+  if (!recon || !out) return fail(GR_ERR_ARG, "crop: null pointer");
+  if (n_slices < 1 || n < 1 || offset < 0 || out_stride < n || recon_stride < n + offset ||
+      radius < 0)
+    return fail(GR_ERR_ARG, "crop: bad sizes (n=%d offset=%d recon_stride=%ld out_stride=%ld)", n,
+                offset, recon_stride, out_stride);
+  crop_kernel<<<dim3(n, n_slices), kPrepThreads, 0, (cudaStream_t)stream>>>(
+      recon, recon_stride, recon_slice_elems, out, out_stride, out_slice_elems, n, offset, radius);
+  return check_launch("crop");
+}
+
+size_t gr_entropy_workspace_bytes(int n_groups, int nbins) {
+  if (n_groups < 1 || nbins < 1) return 0;
+  return (size_t)n_groups * (nbins + 1) * sizeof(unsigned);
+}
+
+int gr_entropy(const float* images, int n_groups, int group, int rows, int cols, long row_stride,
+               long image_stride, long group_stride, float vmin, float vmax, int nbins,
+               float* entropies, void* workspace, void* stream) {
+  if (!images || !entropies || !workspace) return fail(GR_ERR_ARG, "entropy: null pointer");
+  if (n_groups < 1 || group < 1 || rows < 1 || cols < 1 || row_stride < cols || nbins < 1 ||
+      nbins > kMaxBins || !(vmax > vmin))
+    return fail(GR_ERR_ARG, "entropy: bad sizes or range (nbins in [1, %d], vmax > vmin)",
+                kMaxBins);
+  Window w{images, row_stride, image_stride, group_stride, rows, cols, group};
+  return launch_entropy(w, n_groups, vmin, vmax, nbins, static_cast<unsigned*>(workspace),
+                        entropies, (cudaStream_t)stream);
+}
+
+int gr_reconstruct_padded(gr_plan* plan, const float* sinos, int n_slices, int n_det, int n_ang,
+                          float xoffset, float* outs, long out_stride, void* stream) {
+  int pn, pa, M0, max_pairs, dev;
+  int rc = plan_shape(plan, &pn, &pa, &M0, &max_pairs, &dev);
+  if (rc) return rc;
+  if (!sinos || !outs) return fail(GR_ERR_ARG, "padded: null pointer");
+  if (n_slices < 1 || pa != n_ang || pn < n_det + 2 * (n_det / 2) || out_stride < n_det)
+    return fail(GR_ERR_ARG, "padded: plan must be %d angles and >= %d wide (is %d x %d)", n_ang,
+                n_det + 2 * (n_det / 2), pa, pn);
+  const int off = n_det / 2;
+  if (off + n_det > M0)
+    return fail(GR_ERR_ARG, "padded: crop window [%d, %d) exceeds the image size %d", off,
+                off + n_det, M0);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int chunk = std::min(n_slices, 2 * max_pairs);
+  AsyncBuf sp(st), rec(st);
+  if ((rc = sp.alloc((size_t)chunk * n_ang * pn * sizeof(float)))) return rc;
+  if ((rc = rec.alloc((size_t)chunk * M0 * M0 * sizeof(float)))) return rc;
+  for (int s0 = 0; s0 < n_slices; s0 += chunk) {
+    const int ns = std::min(chunk, n_slices - s0);
+    shift_pad_kernel<<<dim3(n_ang, ns), kPrepThreads, 0, st>>>(
+        sinos + (size_t)s0 * n_ang * n_det, (long)n_ang * n_det, ns, nullptr, 1, xoffset,
+        sp.as<float>(), n_det, n_ang, pn);
+    if ((rc = check_launch("padded: shift/pad"))) return rc;
+    gr_batch_desc b{};
+    b.n_slices = ns;
+    b.dtype = GR_DTYPE_F32;
+    b.sinos = sp.p;
+    b.outs = rec.as<float>();
+    b.out_stride = M0;
+    if ((rc = gr_reconstruct_batch(plan, &b, st))) return rc;
+    crop_kernel<<<dim3(n_det, ns), kPrepThreads, 0, st>>>(
+        rec.as<float>(), M0, (long)M0 * M0, outs + (size_t)s0 * n_det * out_stride, out_stride,
+        (long)n_det * out_stride, n_det, off, 0);
+    if ((rc = check_launch("padded: crop"))) return rc;
+  }
+  return GR_OK;
+}
+
+int gr_center_search(gr_plan* plan, const float* sino1, const float* sino2, int n_det, int n_ang,
+                     const float* shifts, int n_cand, float hist_lo, float hist_hi, int nbins,
+                     float* scores, int* best, float* best_images, void* stream) {
+  int pn, pa, M0, max_pairs, dev;
+  int rc = plan_shape(plan, &pn, &pa, &M0, &max_pairs, &dev);
+  if (rc) return rc;
+  if (!sino1 || !sino2 || !shifts || !scores) return fail(GR_ERR_ARG, "centre search: null pointer");
+  if (n_cand < 1 || pa != n_ang || pn < n_det + 2 * (n_det / 2))
+    return fail(GR_ERR_ARG, "centre search: plan must be %d angles and >= %d wide (is %d x %d)",
+                n_ang, n_det + 2 * (n_det / 2), pa, pn);
+  if (nbins < 1 || nbins > kMaxBins || !(hist_hi > hist_lo))
+    return fail(GR_ERR_ARG, "centre search: nbins in [1, %d] and hist_hi > hist_lo", kMaxBins);
+  const int off = n_det / 2;
+  if (off + n_det > M0)
+    return fail(GR_ERR_ARG, "centre search: crop window [%d, %d) exceeds the image size %d", off,
+                off + n_det, M0);
+  cudaStream_t st = (cudaStream_t)stream;
+  const int chunk = std::min(n_cand, max_pairs);  // candidates per batch (one pair each)
+  const long slice_in = (long)n_ang * n_det;
+  const long slice_rec = (long)M0 * M0;
+  AsyncBuf pair(st), sp(st), rec(st), xo(st), gh(st), sc(st);
+  if ((rc = pair.alloc(2 * slice_in * sizeof(float)))) return rc;
+  if ((rc = sp.alloc((size_t)2 * chunk * n_ang * pn * sizeof(float)))) return rc;
+  if ((rc = rec.alloc((size_t)2 * chunk * slice_rec * sizeof(float)))) return rc;
+  if ((rc = xo.alloc((size_t)n_cand * sizeof(float)))) return rc;
+  if ((rc = gh.alloc((size_t)chunk * (nbins + 1) * sizeof(unsigned)))) return rc;
+  if ((rc = sc.alloc((size_t)n_cand * sizeof(float)))) return rc;
+  float* pr = pair.as<float>();
+  cudaError_t e = cudaMemcpyAsync(pr, sino1, slice_in * sizeof(float), cudaMemcpyDeviceToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(pr + slice_in, sino2, slice_in * sizeof(float), cudaMemcpyDeviceToDevice,
+                        st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(xo.p, shifts, n_cand * sizeof(float), cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) return cuda_fail(e, "centre search: copies");
+  for (int c0 = 0; c0 < n_cand; c0 += chunk) {
+    const int nc = std::min(chunk, n_cand - c0);
+    shift_pad_kernel<<<dim3(n_ang, 2 * nc), kPrepThreads, 0, st>>>(
+        pr, slice_in, 2, xo.as<float>() + c0, 2, 0.f, sp.as<float>(), n_det, n_ang, pn);
+    if ((rc = check_launch("centre search: shift/pad"))) return rc;
+    gr_batch_desc b{};
+    b.n_slices = 2 * nc;
+    b.dtype = GR_DTYPE_F32;
+    b.sinos = sp.p;
+    b.outs = rec.as<float>();
+    b.out_stride = M0;
+    if ((rc = gr_reconstruct_batch(plan, &b, st))) return rc;
+    Window w{rec.as<float>() + (size_t)off * M0 + off, M0, slice_rec, 2 * slice_rec, n_det,
+             n_det, 2};
+    if ((rc = launch_entropy(w, nc, hist_lo, hist_hi, nbins, gh.as<unsigned>(),
+                             sc.as<float>() + c0, st)))
+      return rc;
+  }
+  e = cudaMemcpyAsync(scores, sc.p, n_cand * sizeof(float), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return cuda_fail(e, "centre search: scores");
+  // First strict minimum, as the reference's `entropy_cur < entropy_optim` scan.
+  int bi = 0;
+  for (int c = 1; c < n_cand; ++c)
+    if (scores[c] < scores[bi]) bi = c;
+  if (best) *best = bi;
+  if (best_images) {
+    shift_pad_kernel<<<dim3(n_ang, 2), kPrepThreads, 0, st>>>(
+        pr, slice_in, 2, xo.as<float>() + bi, 2, 0.f, sp.as<float>(), n_det, n_ang, pn);
+    if ((rc = check_launch("centre search: shift/pad"))) return rc;
+    gr_batch_desc b{};
+    b.n_slices = 2;
+    b.dtype = GR_DTYPE_F32;
+    b.sinos = sp.p;
+    b.outs = rec.as<float>();
+    b.out_stride = M0;
+    if ((rc = gr_reconstruct_batch(plan, &b, st))) return rc;
+    crop_kernel<<<dim3(n_det, 2), kPrepThreads, 0, st>>>(rec.as<float>(), M0, slice_rec,
+                                                         best_images, n_det, (long)n_det * n_det,
+                                                         n_det, off, 0);
+    if ((rc = check_launch("centre search: crop"))) return rc;
+  }
+  return GR_OK;
+}
+
+}  // extern "C"

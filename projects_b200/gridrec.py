@@ -29,7 +29,9 @@ EXPORTS = ("gr_params_default", "gr_filter_code", "gr_plan_create", "gr_plan_des
            "gr_reconstruct_batch", "gr_reconstruct_host", "gr_last_error",
            "gr_plan_launch_count", "gr_plan_work_stats", "gr_worklist_export",
            "gr_plan_set_timing", "gr_plan_stage_times", "gr_reconstruct_pair_noalloc",
-           "gr_plan_device_status", "gr_selftest_wait_timeout")
+           "gr_plan_device_status", "gr_selftest_wait_timeout", "gr_ring_workspace_bytes",
+           "gr_ring_removal", "gr_shift_pad", "gr_crop_center", "gr_entropy_workspace_bytes",
+           "gr_entropy", "gr_reconstruct_padded", "gr_center_search")
 STAGES = ("phase", "spectra", "grid", "cols", "rows_deapod")
 
 
@@ -88,6 +90,18 @@ def lib():
         ip = C.POINTER(C.c_int)
         L.gr_worklist_export.argtypes = [P, ip, ip, ip, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_int, C.c_int]
+        vp, i_, l_, f_ = C.c_void_p, C.c_int, C.c_long, C.c_float
+        L.gr_ring_workspace_bytes.argtypes = [i_, i_, i_]
+        L.gr_ring_workspace_bytes.restype = C.c_size_t
+        L.gr_ring_removal.argtypes = [vp, i_, i_, i_, f_, i_, vp, vp]
+        L.gr_shift_pad.argtypes = [vp, vp, i_, i_, i_, vp, i_, vp]
+        L.gr_crop_center.argtypes = [vp, l_, l_, vp, l_, l_, i_, i_, i_, i_, vp]
+        L.gr_entropy_workspace_bytes.argtypes = [i_, i_]
+        L.gr_entropy_workspace_bytes.restype = C.c_size_t
+        L.gr_entropy.argtypes = [vp, i_, i_, i_, i_, l_, l_, l_, f_, f_, i_, vp, vp, vp]
+        L.gr_reconstruct_padded.argtypes = [vp, vp, i_, i_, i_, f_, vp, l_, vp]
+        L.gr_center_search.argtypes = [vp, vp, vp, i_, i_, C.POINTER(f_), i_, f_, f_, i_,
+                                       C.POINTER(f_), C.POINTER(i_), vp, vp]
         _lib = L
     return _lib
 
@@ -364,3 +378,97 @@ class GridRec:
         if self._plan is not None:
             self._plan.close()
             self._plan = None
+
+
+# ---------------------------------------------------------------- slice pipeline
+# Steps of the reference's drivers around gridrec (gridrec/GPU/tomo_recon.cpp,
+# find_shift/src/main/find_shift.cpp), on device tensors.
+
+def ring_removal(sinos, ring_coeff=1.0, iterations=20, stream=None):
+    """In place on a (S, n_ang, n_det) float32 CUDA tensor: RingCorrectionSinogram
+    (tomo_recon.cpp:3905-3972; the reference runs 20 rounds, RING_COEFF 1.0)."""
+    import torch
+    S, a, n = sinos.shape
+    ws = torch.empty(lib().gr_ring_workspace_bytes(S, n, a), dtype=torch.uint8,
+                     device=sinos.device)
+    _check(lib().gr_ring_removal(_ptr(sinos), S, n, a, float(ring_coeff), int(iterations),
+                                 _ptr(ws), _stream_ptr(stream)), "gr_ring_removal")
+    return sinos
+
+
+def shift_pad(sinos, xoffsets, out_width=None, stream=None):
+    """(S, n_ang, n_det) float32 -> (S, n_ang, out_width): sub-pixel shift by
+    xoffsets[s] and half padding (tomo_recon.cpp:3708-3807)."""
+    import torch
+    S, a, n = sinos.shape
+    w = 2 * n if out_width is None else int(out_width)
+    xo = torch.as_tensor(xoffsets, dtype=torch.float32).reshape(-1).to(sinos.device)
+    if xo.numel() == 1:
+        xo = xo.expand(S).contiguous()
+    out = torch.empty((S, a, w), dtype=torch.float32, device=sinos.device)
+    _check(lib().gr_shift_pad(_ptr(sinos), _ptr(out), S, n, a, _ptr(xo), w, _stream_ptr(stream)),
+           "gr_shift_pad")
+    return out
+
+
+def crop_center(recs, n, offset, radius=0, stream=None):
+    """(S, rows, stride) float32 -> (S, n, n) window at (offset, offset); radius > 0
+    zeroes pixels outside the circle of tomo_recon.cpp:2150-2165."""
+    import torch
+    S, rows, stride = recs.shape
+    out = torch.empty((S, n, n), dtype=torch.float32, device=recs.device)
+    if offset + n > rows:
+        raise ValueError("crop window exceeds the image rows")
+    _check(lib().gr_crop_center(_ptr(recs), stride, rows * stride, _ptr(out), n, n * n, S, n,
+                                offset, int(radius), _stream_ptr(stream)), "gr_crop_center")
+    return out
+
+
+def entropy(images, vmin, vmax, nbins, group=1, stream=None):
+    """Histogram entropy (find_shift.cpp:2078-2115) of each group of `group`
+    consecutive (rows, cols) images of a (G*group, rows, cols) float32 tensor."""
+    import torch
+    N, rows, cols = images.shape
+    if N % group:
+        raise ValueError("image count must be a multiple of group")
+    G = N // group
+    ws = torch.empty(lib().gr_entropy_workspace_bytes(G, nbins), dtype=torch.uint8,
+                     device=images.device)
+    out = torch.empty(G, dtype=torch.float32, device=images.device)
+    st = images.stride()
+    _check(lib().gr_entropy(_ptr(images), G, group, rows, cols, st[1], st[0], st[0] * group,
+                            float(vmin), float(vmax), int(nbins), _ptr(out), _ptr(ws),
+                            _stream_ptr(stream)), "gr_entropy")
+    return out
+
+
+def reconstruct_padded(plan: "Plan", sinos, xoffset=0.0, stream=None):
+    """GridRecSlices (tomo_recon.cpp:3679-3862): shift by xoffset, half-pad to the
+    plan's width (2 n_det), reconstruct, crop n_det x n_det.  sinos (S, n_ang, n_det)."""
+    import torch
+    S, a, n = sinos.shape
+    out = torch.empty((S, n, n), dtype=torch.float32, device=sinos.device)
+    _check(lib().gr_reconstruct_padded(plan.handle, _ptr(sinos), S, n, a, float(xoffset),
+                                       _ptr(out), n, _stream_ptr(stream)),
+           "gr_reconstruct_padded")
+    return out
+
+
+def center_search(plan: "Plan", sino1, sino2, shifts, hist_lo, hist_hi, nbins,
+                  want_images=False, stream=None):
+    """find_shift's entropy refinement (find_shift.cpp:1653-1900).
+
+    Returns (scores[n_cand] numpy, best index, best pair images (2, n, n) or None)."""
+    import torch
+    a, n = sino1.shape
+    sh = np.ascontiguousarray(shifts, np.float32)
+    scores = np.zeros(sh.size, np.float32)
+    best = C.c_int(-1)
+    imgs = torch.empty((2, n, n), dtype=torch.float32, device=sino1.device) if want_images \
+        else None
+    fp = C.POINTER(C.c_float)
+    _check(lib().gr_center_search(plan.handle, _ptr(sino1), _ptr(sino2), n, a,
+                                  sh.ctypes.data_as(fp), sh.size, float(hist_lo), float(hist_hi),
+                                  int(nbins), scores.ctypes.data_as(fp), C.byref(best),
+                                  _ptr(imgs), _stream_ptr(stream)), "gr_center_search")
+    return scores, best.value, imgs

@@ -10,6 +10,9 @@ parameters) and the reference's outputs for them:
   * ``ref32`` -- the reference GridRec class (FP32, NR FFT), gridrec/GPU/gridrec.cu
   * ``ref64`` -- the same sources built with float -> double
   * ``refb``  -- GridrecCPP 5.2 (explicit centre / sampl / C / filter name)
+Each prep_*.npz holds inputs and outputs of the reference's slice-pipeline
+code (oracle/_ref/libprep_ref.so): ring suppression, shift + half padding,
+and find_shift's histogram entropy.
 Inputs are seeded synthetic sinograms (analytic ellipses + Poisson noise) or
 uniform random rows, so the files are reproducible from this script.
 """
@@ -58,6 +61,37 @@ def case_gridrec_cpp(name, n, a, center, fname, C_, sampl, seed):
                         sampl=sampl, C=C_, M0=m0, refb_1=b1[:m0, :m0], refb_2=b2[:m0, :m0])
 
 
+def prep_cases(rng):
+    """Reference ring suppression, shift/half-padding and entropy."""
+    # shift + half padding: odd and even widths, shifts of both signs and beyond the row
+    for n, a in ((63, 20), (64, 24)):
+        s1 = rng.standard_normal((a, n)).astype(np.float32)
+        s2 = (rng.random((a, n)) * 3).astype(np.float32)
+        shifts = np.array([-3.7, 0.0, 0.25, 12.5, -70.2], np.float32)
+        outs = np.stack([O.ref_shift_pad(s1, s2, x) for x in shifts])
+        np.savez_compressed(os.path.join(HERE, f"prep_shift_pad_{n}x{a}.npz"), sino1=s1,
+                            sino2=s2, shifts=shifts, outs=outs)
+    # ring suppression: positive sinogram with detector stripes and a zero-mean row
+    n, a = 96, 40
+    th = ph.angles_deg(a)
+    p = ph.line_integrals(ph.shepp_logan_ellipses(), n, th, n // 2).astype(np.float32)
+    p = p / p.max() + 0.05
+    p[:, 17] *= 1.2
+    p[:, 60] += 0.1
+    p[:, 61] -= 0.05
+    p[5, :] = 0.0
+    ring = O.ref_ring_removal(p, 1.0)
+    np.savez_compressed(os.path.join(HERE, "prep_ring_96x40.npz"), sino=p, ring_coeff=1.0,
+                        out=ring)
+    # entropy: two images side by side as find_shift scores them (xm = 2 um, ym = um)
+    img = (rng.standard_normal((48, 96)) * 0.01).astype(np.float32)
+    img[10:20, 30:50] += 0.02
+    cfg = np.array([[-0.05, 0.05, 100], [-0.02, 0.03, 1000], [-0.1, 0.1, 10000]], np.float64)
+    ent = np.array([O.ref_entropy(img, lo, hi, int(nb)) for lo, hi, nb in cfg], np.float64)
+    np.savez_compressed(os.path.join(HERE, "prep_entropy_48x96.npz"), image=img, cfg=cfg,
+                        entropy=ent)
+
+
 def main():
     if not O.ref_available():
         raise SystemExit("build the reference first: oracle/build_ref.sh")
@@ -72,6 +106,8 @@ def main():
     case_gridrec_cpp("b64x40_c31.7_C4_hann", 64, 40, 31.7, "hann", 4.0, 1.0, 22)
     case_gridrec_cpp("b120x72_c61.2_C7_s1.2_shepp", 120, 72, 61.2, "shepp", 7.0, 1.2, 23)
     case_gridrec_cpp("b72x45_c36.5_C5_hamming", 72, 45, 36.5, "hamming", 5.0, 1.0, 24)
+    if O.prep_ref_available():
+        prep_cases(np.random.default_rng(8))
     print("\n".join(sorted(f for f in os.listdir(HERE) if f.endswith(".npz"))))
 
 

@@ -1,0 +1,149 @@
+"""GPU parity tests of the slice-pipeline kernels (ring suppression, shift + half
+padding, crop, entropy, padded reconstruction, centre search) through the C ABI,
+against the reference fixtures (prep_*.npz) and the oracle.
+
+Tolerances: shift/pad and crop are bit-exact (the kernels repeat the
+reference's float operations); entropy histograms are exact, entropies within
+1e-5 of the oracle's double sum; ring suppression sums in a different order
+than the reference, relative L2 <= 2e-5; padded reconstructions relative
+L2 <= 1e-3 against float64 gridrec.
+"""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from projects_b200 import gridrec as G
+from projects_b200 import phantom as ph
+
+torch = pytest.importorskip("torch")
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
+
+
+def _load(pattern):
+    return [dict(np.load(f)) for f in sorted(glob.glob(os.path.join(GOLDEN, pattern)))]
+
+
+def _dev(a):
+    return torch.as_tensor(np.ascontiguousarray(a)).cuda()
+
+
+@pytest.mark.parametrize("z", _load("prep_shift_pad_*.npz"))
+def test_shift_pad_bit_exact_against_reference(z):
+    k = len(z["shifts"])
+    sinos = _dev(np.stack([z["sino1"], z["sino2"]] * k))  # slice 2c+t, shift c
+    offs = np.repeat(z["shifts"], 2)
+    out = G.shift_pad(sinos, offs).cpu().numpy()
+    ref = z["outs"].reshape(2 * k, *z["outs"].shape[2:])
+    assert np.array_equal(out, ref)
+
+
+def test_shift_pad_wide_rows_and_port():
+    rng = np.random.default_rng(5)
+    s = rng.standard_normal((3, 50, 300)).astype(np.float32)
+    offs = np.array([-7.25, 0.5, 151.0], np.float32)
+    out = G.shift_pad(_dev(s), offs, out_width=700).cpu().numpy()
+    for i in range(3):
+        assert np.array_equal(out[i], O.port_shift_pad(s[i], offs[i], 700))
+
+
+def test_ring_removal_against_reference():
+    z = _load("prep_ring_*.npz")[0]
+    x = _dev(z["sino"][None])
+    G.ring_removal(x, float(z["ring_coeff"]), 20)
+    out = x.cpu().numpy()[0]
+    ref = z["out"]
+    assert ph.rel_l2(out, ref) < 2e-5
+    assert np.abs(out - ref).max() < 2e-4
+
+
+def test_ring_removal_batch_against_oracle():
+    rng = np.random.default_rng(6)
+    S, a, n = 3, 180, 256
+    s = (rng.random((S, a, n)) + 0.3).astype(np.float32)
+    s[:, :, 40] *= 1.3
+    s[1, 7, :] = 0.0
+    x = _dev(s)
+    G.ring_removal(x, 0.8, 20)
+    out = x.cpu().numpy()
+    for i in range(S):
+        assert ph.rel_l2(out[i], O.port_ring_removal(s[i], 0.8, 20)) < 2e-5
+    y = _dev(s)
+    G.ring_removal(y, 0.8, 0)  # zero rounds leave the data untouched
+    assert np.array_equal(y.cpu().numpy(), s)
+
+
+def test_crop_and_circle_mask():
+    rng = np.random.default_rng(7)
+    rec = rng.standard_normal((2, 70, 75)).astype(np.float32)
+    d = _dev(rec)
+    for radius in (0, 15):
+        out = G.crop_center(d, 40, 12, radius).cpu().numpy()
+        for i in range(2):
+            assert np.array_equal(out[i], O.port_crop(rec[i], 40, 12, radius))
+
+
+def test_entropy_against_reference_and_port():
+    z = _load("prep_entropy_*.npz")[0]
+    img = z["image"]
+    for (lo, hi, nb), ref in zip(z["cfg"], z["entropy"]):
+        e = float(G.entropy(_dev(img[None]), lo, hi, int(nb)).cpu()[0])
+        assert abs(e - O.port_entropy(img, lo, hi, int(nb))) < 1e-5
+        assert abs(e - ref) < 3e-5 * max(1.0, abs(ref))
+    # groups of two images score as one (find_shift scores the slice pair together)
+    rng = np.random.default_rng(8)
+    ims = rng.standard_normal((6, 64, 64)).astype(np.float32)
+    got = G.entropy(_dev(ims), -2.0, 2.0, 1000, group=2).cpu().numpy()
+    for g in range(3):
+        assert abs(got[g] - O.port_entropy(ims[2 * g:2 * g + 2], -2.0, 2.0, 1000)) < 1e-5
+
+
+def _padded_oracle(s, th, xoffset):
+    n = s.shape[1]
+    p = O.port_shift_pad(s, xoffset)
+    o, _ = O.port_gridrec_pair(p, p, th, filter=2)
+    return o[n // 2:n // 2 + n, n // 2:n // 2 + n]
+
+
+def test_reconstruct_padded_against_oracle():
+    n, a = 128, 90
+    th = ph.angles_deg(a)
+    s = np.stack([ph.shepp_logan_sinogram(n, a, center=63.0, noise_seed=k) for k in range(3)])
+    with G.Plan(2 * n, a, th, filter=G.FILTER_HANN, max_pairs=1) as plan:
+        out = G.reconstruct_padded(plan, _dev(s.astype(np.float32)), xoffset=1.0).cpu().numpy()
+        plan.device_status()
+    for i in range(3):
+        assert ph.rel_l2(out[i], _padded_oracle(s[i].astype(np.float32), th, 1.0)) < 1e-3
+
+
+def test_center_search_finds_axis_and_matches_oracle():
+    n, a = 128, 120
+    th = ph.angles_deg(a)
+    c_true = 62.0  # best shift = n/2 - c_true = 2.0 (plan centre n of the 2n-wide rows)
+    s1 = ph.shepp_logan_sinogram(n, a, center=c_true, noise_seed=3).astype(np.float32)
+    s2 = ph.shepp_logan_sinogram(n, a, center=c_true, noise_seed=4).astype(np.float32)
+    shifts = np.arange(-1.0, 5.01, 0.5).astype(np.float32)
+    lo, hi, nb = -0.01, 0.03, 1000
+    with G.Plan(2 * n, a, th, filter=G.FILTER_HANN, max_pairs=4) as plan:
+        scores, best, imgs = G.center_search(plan, _dev(s1), _dev(s2), shifts, lo, hi, nb,
+                                             want_images=True)
+        plan.device_status()
+    assert abs(shifts[best] - 2.0) <= 0.5
+    assert best == int(np.argmin(scores))
+    im = imgs.cpu().numpy()
+    # the score of the returned images, recomputed on the CPU from the same pixels
+    assert abs(scores[best] - O.port_entropy(im, lo, hi, nb)) < 1e-5
+    # the images equal the oracle pipeline at that shift
+    x = float(shifts[best])
+    assert ph.rel_l2(im[0], _padded_oracle(s1, th, x)) < 1e-3
+    assert ph.rel_l2(im[1], _padded_oracle(s2, th, x)) < 1e-3
+    # scores follow the oracle pipeline's (pixels near bin edges may move one bin)
+    ref = np.array([O.port_entropy(np.stack([_padded_oracle(s1, th, float(v)),
+                                             _padded_oracle(s2, th, float(v))]).astype(np.float32),
+                                   lo, hi, nb) for v in shifts])
+    assert np.abs(scores - ref).max() < 2e-2
+    assert int(np.argmin(ref)) == best

@@ -132,10 +132,10 @@ def test_worklist_splits_heavy_tiles():
     assert np.all(np.diff(cost) <= 0)       # heaviest first
     # samples visited ~ 2 * n_ang * (pdim/2 - 1) plus the tile halo
     assert 1.0 < n.sum() / (2 * 1500 * 1023) < 1.6
-    # footprints of one step are disjoint: P * max(|du|,|dv|) >= 4
+    # footprints of one step are disjoint: P * max(|du|,|dv|) > L
     th = np.deg2rad(ph.angles_deg(1500).astype(np.float64))[runs[:, 0] // 2]
     step = np.maximum(np.abs(np.cos(th)), np.abs(np.sin(th))) * 2048 / 2047
-    assert np.all(runs[:, 3] * step >= 4.0)
+    assert np.all(runs[:, 3] * step > 2 * 6.0 * (2048 / 2047) / np.pi)
 
 
 def test_phantom_line_integrals():
