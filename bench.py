@@ -56,6 +56,9 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-pipeline", action="store_true",
+                    help="skip the slice-pipeline step timings (ring, shift/pad, padded "
+                         "reconstruction, centre search)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     return ap.parse_args()
 
@@ -218,6 +221,58 @@ def cpu_reference(n_det, n_ang, seconds, threads=None, steps=None):
     return 2.0 * pairs / wall, {"kind": kind, "cores": threads, "pairs": pairs, "wall_s": wall}
 
 
+def measure_slice_pipeline(G, sinos, th, n, a, dev, stream, peak):
+    """CUDA-event timings of the steps around gridrec on 16 resident slices:
+    ring suppression (20 rounds), shift + half padding, the half-padded
+    reconstruction (2n-wide plan) and the entropy centre search (21 shifts)."""
+    import torch
+    S = min(16, sinos.shape[0])
+    src = sinos[:S].float().contiguous()
+    sl_bytes = a * n * 4
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1000.0 / reps
+
+    out = {"slices": S}
+    x = src.clone()
+    t = timed(lambda: G.ring_removal(x, 1.0, 20, stream=stream), 3)
+    per_round = 2 * sl_bytes * S * 20
+    out["ring_removal"] = {
+        "ms_per_slice": 1000.0 * t / S, "rounds": 20,
+        "round_bytes_gbs": per_round / t / 1e9,
+        "round_bytes_frac_of_hbm": per_round / t / 1e9 / peak,
+        "note": "round bytes = one read + write of the sinogram per round (each round "
+                "depends on every row of the previous one)"}
+    t = timed(lambda: G.shift_pad(src, 1.5, stream=stream), 10)
+    b = S * (sl_bytes + 2 * sl_bytes)
+    out["shift_pad"] = {"ms_per_slice": 1000.0 * t / S, "gbs": b / t / 1e9,
+                        "frac_of_hbm": b / t / 1e9 / peak}
+    with G.Plan(2 * n, a, th, filter=G.FILTER_HANN, max_pairs=8,
+                device=dev.index or 0) as p2:
+        t = timed(lambda: G.reconstruct_padded(p2, src, 1.5, stream=stream), 3)
+        out["reconstruct_padded"] = {"slices_per_s": S / t, "plan_width": 2 * n,
+                                     "image": f"{n}x{n} crop of {p2.M0}^2"}
+        shifts = np.arange(-5.0, 5.01, 0.5)
+        G.center_search(p2, src[0], src[1], shifts, 0.0, 1.0, 10000, stream=stream)
+        t0 = time.perf_counter()
+        G.center_search(p2, src[0], src[1], shifts, 0.0, 1.0, 10000, stream=stream)
+        tc = time.perf_counter() - t0
+        out["center_search"] = {"ms": 1000.0 * tc, "candidates": len(shifts),
+                                "ms_per_candidate": 1000.0 * tc / len(shifts),
+                                "timing": "host wall clock (the call synchronises)"}
+        p2.device_status()
+    del x, src
+    return out
+
+
 # ------------------------------------------------------------------ arms
 
 def run_reference(args, rank):
@@ -339,6 +394,10 @@ def run_b200(args, rank, world, local_rank):
                "steps": args.e2e_steps, "path": "gr_reconstruct_host, pinned host buffers"}
         del h_in, h_out
 
+    pipe = None
+    if rank == 0 and not args.no_pipeline:
+        pipe = measure_slice_pipeline(G, sinos, th, n, a, dev, stream, peaks()[0])
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, info = cpu_reference(n, a, args.cpu_seconds)
@@ -373,6 +432,7 @@ def run_b200(args, rank, world, local_rank):
             "clocks": clk.summary(),
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "slice_pipeline": pipe,
         }
         print(json.dumps(out), flush=True)
     plan.close()

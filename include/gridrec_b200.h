@@ -27,6 +27,8 @@
  *                           sinograms and images in host memory, gridrec.cu:174-212)
  *   GR_DTYPE_U16_RAW     <- flat/dark normalisation and log of the slice pipeline
  *                                                      gridrec/GPU/tomo_recon.cpp:1533-1541
+ *   GR_DTYPE_U16_LINEAR  <- 1 - (raw - dark)/(white - dark) of the HDF5 slice path
+ *                                                      gridrec/GPU/tomo_recon.cpp:1871-1877, 2019
  */
 #ifndef GRIDREC_B200_H
 #define GRIDREC_B200_H
@@ -65,7 +67,8 @@ typedef enum {
   GR_DTYPE_F32 = 0,
   GR_DTYPE_F16 = 1,
   GR_DTYPE_BF16 = 2,
-  GR_DTYPE_U16_RAW = 3 /* raw detector counts; needs flat/dark rows, see gr_batch_desc */
+  GR_DTYPE_U16_RAW = 3,   /* raw detector counts, log normalisation; needs flat/dark rows */
+  GR_DTYPE_U16_LINEAR = 4 /* raw detector counts, 1 - (raw-dark)/(flat-dark); needs flat/dark */
 } gr_dtype;
 
 typedef struct {
@@ -121,10 +124,12 @@ int gr_reconstruct_pair(gr_plan* plan, const float* sino1, const float* sino2, f
  *   sinos      n_slices sinograms, each n_ang x n_det of `dtype`, contiguous
  *   centers    optional device array of n_slices float centres (NULL = plan centre);
  *              the two slices of a pair may have different centres
- *   flat, dark device rows of n_det floats (GR_DTYPE_U16_RAW only): the load
- *              computes v = raw - dark; r = (flat - dark)/v; value = log(r) when
- *              v > 0 and r > 0, else 0 -- the normalisation of
- *              gridrec/GPU/tomo_recon.cpp:1533-1541 -- fused into the first kernel
+ *   flat, dark device rows of n_det floats (raw uint16 dtypes only), applied in
+ *              the first kernel as the sinogram is loaded:
+ *              GR_DTYPE_U16_RAW: v = raw - dark; r = (flat - dark)/v; value = log(r)
+ *              when v > 0 and r > 0, else 0 (gridrec/GPU/tomo_recon.cpp:1533-1541);
+ *              GR_DTYPE_U16_LINEAR: value = 1 - (raw - dark)/(flat - dark)
+ *              (tomo_recon.cpp:1871-1877, where flat = 0.5 white1 + 0.5 white2)
  *   outs       n_slices images, each M0 rows of out_stride floats, contiguous
  * Pairs are processed max_pairs at a time on `stream`. */
 typedef struct {

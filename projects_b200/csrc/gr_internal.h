@@ -112,6 +112,21 @@ int fail(int code, const char* fmt, ...);
 
 // Shape of a plan, for the pre/post-processing entry points (gridrec_plan.cu).
 int plan_shape(const gr_plan* p, int* n_det, int* n_ang, int* M0, int* max_pairs, int* device);
+// Grow-only device scratch owned by the plan (the slice-pipeline entry points).
+int plan_scratch(gr_plan* p, size_t bytes, void** out);
+
+// Makes `dev` current for the scope and restores the caller's device after.
+struct DeviceGuard {
+  int prev = -1;
+  explicit DeviceGuard(int dev) {
+    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+    if (prev != dev) cudaSetDevice(dev);
+  }
+  ~DeviceGuard() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
 
 // Kernel launchers (gridrec_kernels.cu).  Return cudaGetLastError().
 cudaError_t init_kernel_attributes();

@@ -366,6 +366,19 @@ __device__ __forceinline__ float load_sino<uint16_t>(const uint16_t* row, int k,
   const float r = (__ldg(&flat[k]) - d) / v;
   return r > 0.f ? logf(r) : 0.f;
 }
+// Raw uint16 counts, linear normalisation of the HDF5 path of
+// gridrec/GPU/tomo_recon.cpp:1871-1877 and :2019: 1 - (raw - dark) / (flat - dark)
+// in float, in that order (flat = 0.5 white1 + 0.5 white2 gives the reference's
+// denominator bit for bit; no guard, as there).
+struct U16Linear {
+  uint16_t v;
+};
+template <>
+__device__ __forceinline__ float load_sino<U16Linear>(const U16Linear* row, int k,
+                                                      const float* flat, const float* dark) {
+  const float d = __ldg(&dark[k]);
+  return __fsub_rn(1.f, __fdiv_rn(__fsub_rn((float)row[k].v, d), __fsub_rn(__ldg(&flat[k]), d)));
+}
 
 // Lines of up to 4096 points run 64-register variants (several CTAs per SM);
 // 8192-point lines need 512 threads and use the MAXT = 512 variants.
@@ -789,10 +802,12 @@ cudaError_t init_kernel_attributes() {
                        (const void*)spectra_kernel<__half, 256>,
                        (const void*)spectra_kernel<__nv_bfloat16, 256>,
                        (const void*)spectra_kernel<uint16_t, 256>,
+                       (const void*)spectra_kernel<U16Linear, 256>,
                        (const void*)spectra_kernel<float, 512>,
                        (const void*)spectra_kernel<__half, 512>,
                        (const void*)spectra_kernel<__nv_bfloat16, 512>,
                        (const void*)spectra_kernel<uint16_t, 512>,
+                       (const void*)spectra_kernel<U16Linear, 512>,
                        (const void*)cols_kernel<256>, (const void*)cols_kernel<512>,
                        (const void*)cols_tma_kernel<256>, (const void*)cols_tma_kernel<512>,
                        (const void*)rows_kernel<256>, (const void*)rows_kernel<512>,
@@ -825,6 +840,7 @@ cudaError_t launch_spectra(const SpectraArgs& a, gr_dtype dt, cudaStream_t s) {
     case GR_DTYPE_F16: return launch_spectra_t<__half>(a, s);
     case GR_DTYPE_BF16: return launch_spectra_t<__nv_bfloat16>(a, s);
     case GR_DTYPE_U16_RAW: return launch_spectra_t<uint16_t>(a, s);
+    case GR_DTYPE_U16_LINEAR: return launch_spectra_t<U16Linear>(a, s);
   }
   return cudaErrorInvalidValue;
 }

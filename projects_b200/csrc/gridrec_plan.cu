@@ -138,6 +138,9 @@ struct Plan {
   cudaEvent_t ev_h2d[2] = {}, ev_comp[2] = {}, ev_d2h[2] = {};
   size_t device_bytes = 0;
   long launches = 0;
+  // scratch of the slice-pipeline entry points (grow-only, freed with the plan)
+  void* d_prep = nullptr;
+  size_t prep_bytes = 0;
   // optional per-stage timing: 6 events per chunk (before phase, after each stage)
   bool timing = false;
   std::vector<cudaEvent_t> events;
@@ -423,21 +426,10 @@ size_t dtype_size(gr_dtype dt) {
     case GR_DTYPE_F16:
     case GR_DTYPE_BF16:
     case GR_DTYPE_U16_RAW: return 2;
+    case GR_DTYPE_U16_LINEAR: return 2;
   }
   return 0;
 }
-
-struct DeviceGuard {
-  int prev = -1;
-  explicit DeviceGuard(int dev) {
-    if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
-    if (prev != dev) cudaSetDevice(dev);
-  }
-  ~DeviceGuard() {
-    int cur = -1;
-    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
-  }
-};
 
 int validate_batch(const Plan* p, const gr_batch_desc* b) {
   if (!b || b->n_slices < 1 || !b->sinos || !b->outs)
@@ -445,8 +437,8 @@ int validate_batch(const Plan* p, const gr_batch_desc* b) {
   if (b->out_stride < p->M0)
     return fail(GR_ERR_ARG, "out_stride %ld < M0 %d", b->out_stride, p->M0);
   if (dtype_size(b->dtype) == 0) return fail(GR_ERR_ARG, "unknown dtype %d", (int)b->dtype);
-  if (b->dtype == GR_DTYPE_U16_RAW && (!b->flat || !b->dark))
-    return fail(GR_ERR_ARG, "GR_DTYPE_U16_RAW needs flat and dark rows");
+  if ((b->dtype == GR_DTYPE_U16_RAW || b->dtype == GR_DTYPE_U16_LINEAR) && (!b->flat || !b->dark))
+    return fail(GR_ERR_ARG, "raw uint16 dtypes need flat and dark rows");
   return GR_OK;
 }
 
@@ -464,6 +456,23 @@ int plan_shape(const gr_plan* p, int* n_det, int* n_ang, int* M0, int* max_pairs
   *M0 = p->M0;
   *max_pairs = p->max_pairs;
   *device = p->device;
+  return GR_OK;
+}
+
+int plan_scratch(gr_plan* p, size_t bytes, void** out) {
+  if (bytes > p->prep_bytes) {
+    if (p->d_prep) cudaFree(p->d_prep);  // synchronises with work still using it
+    p->d_prep = nullptr;
+    p->prep_bytes = 0;
+    cudaError_t e = cudaMalloc(&p->d_prep, bytes);
+    if (e != cudaSuccess) {
+      p->d_prep = nullptr;
+      return fail(GR_ERR_NOMEM, "cudaMalloc(%zu bytes) for pipeline scratch: %s", bytes,
+                  cudaGetErrorString(e));
+    }
+    p->prep_bytes = bytes;
+  }
+  *out = p->d_prep;
   return GR_OK;
 }
 }  // namespace gr
@@ -514,6 +523,7 @@ int gr_plan_destroy(gr_plan* plan) {
   if (plan->copy_stream) cudaStreamDestroy(plan->copy_stream);
   if (plan->d2h_stream) cudaStreamDestroy(plan->d2h_stream);
   for (cudaEvent_t e : plan->events) cudaEventDestroy(e);
+  if (plan->d_prep) cudaFree(plan->d_prep);
   delete plan;
   return GR_OK;
 }
@@ -846,7 +856,7 @@ int gr_reconstruct_host(gr_plan* p, const gr_batch_desc* b, void* stream) {
     GR_CUDA(cudaMalloc(&d_centers, b->n_slices * sizeof(float)));
     GR_CUDA(cudaMemcpy(d_centers, b->centers, b->n_slices * sizeof(float), cudaMemcpyHostToDevice));
   }
-  if (b->dtype == GR_DTYPE_U16_RAW) {
+  if (b->dtype == GR_DTYPE_U16_RAW || b->dtype == GR_DTYPE_U16_LINEAR) {
     GR_CUDA(cudaMalloc(&d_flat, p->n_det * sizeof(float)));
     GR_CUDA(cudaMalloc(&d_dark, p->n_det * sizeof(float)));
     GR_CUDA(cudaMemcpy(d_flat, b->flat, p->n_det * sizeof(float), cudaMemcpyHostToDevice));

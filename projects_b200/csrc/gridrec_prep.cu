@@ -54,16 +54,16 @@ __device__ __forceinline__ double block_sum_d(double v, double* red) {
 //   r_i = mean_j x_ij,  g = mean_i r_i,  v_ij = x_ij g / r_i   (rows with r_i = 0 kept)
 //   c_j = mean_i v_ij,  t_j = c_j - (c_{j-1} + c_j + c_{j+1}) / 3   (t_0 = t_{n-1} = 0)
 //   x_ij <- v_ij - coeff t_j  where positive, else 0
-// Three launches per round: column partial sums over row chunks (v recomputed
-// on the fly), t_j, and the row update fused with the next round's row means.
-// The renormalised value is formed as (x g) / r in float, the reference's
-// expression, in both the column pass and the update, so both see equal v.
+// Two launches per round: the row update fused with the next round's row means
+// and column partial sums over chunks of rows, then the column means.  The
+// first round's partials come from a column pass over the input.  The
+// renormalised value is formed as (x g) / r in float, the reference's expression.
 
-int ring_chunks(int n_det, int n_ang, int n_slices) {
-  const int bx = (n_det + kPrepThreads - 1) / kPrepThreads;
-  const int want = (2 * 148 + bx * n_slices - 1) / (bx * n_slices);
-  return std::max(1, std::min({want, 32, n_ang}));
-}
+// Rows per chunk of the column passes (32: measured fastest of 4..32 at
+// 16 x 2048 x 1500; more row chunks add partial-sum traffic, fewer leave SMs idle).
+constexpr int kRingRows = 32;
+
+int ring_chunks(int n_ang) { return (n_ang + kRingRows - 1) / kRingRows; }
 
 __global__ void ring_rowmean_kernel(const float* data, float* rowmean, int n_det, int n_ang) {
   __shared__ float red[32];
@@ -105,35 +105,144 @@ __global__ void ring_colpart_kernel(const float* data, const float* rowmean, flo
   part[((size_t)s * R + r) * n_det + j] = acc;
 }
 
-__global__ void ring_tilt_kernel(const float* part, float* tilt, int n_det, int n_ang, int R) {
+// Column means c_j = g / n_ang * sum_q part[q][j] (32 columns x 8 chunk
+// strides per block).  scaled = 1: partials already include g (first round,
+// sums of v); scaled = 0: partials are sums of x / r_i and g, the mean of the
+// row means, is formed here and recorded for the next update.
+__global__ void __launch_bounds__(256) ring_colmean_kernel(const float* part, const float* rowmean,
+                                                          float* colmean, float* gmean, int n_det,
+                                                          int n_ang, int R, int scaled) {
+  __shared__ float red[32];
+  __shared__ float acc_s[8][33];
   const int s = blockIdx.y;
-  const int j = blockIdx.x * blockDim.x + threadIdx.x;
-  if (j >= n_det) return;
-  const float* p = part + (size_t)s * R * n_det;
-  float t = 0.f;
-  if (j > 0 && j < n_det - 1) {
-    float c[3] = {0.f, 0.f, 0.f};
-    for (int q = 0; q < R; ++q)
-      for (int d = 0; d < 3; ++d) c[d] += p[(size_t)q * n_det + j - 1 + d];
-    for (int d = 0; d < 3; ++d) c[d] /= n_ang;
-    t = c[1] - (c[0] + c[1] + c[2]) / 3.f;
+  float g = 1.f;
+  if (!scaled) {
+    g = slice_gmean(rowmean + (size_t)s * n_ang, n_ang, red);
+    if (threadIdx.x == 0 && threadIdx.y == 0 && blockIdx.x == 0) gmean[s] = g;
   }
-  tilt[(size_t)s * n_det + j] = t;
+  const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+  const int j = blockIdx.x * 32 + tx;
+  float acc = 0.f;
+  if (j < n_det) {
+    const float* p = part + (size_t)s * R * n_det + j;
+    for (int q = ty; q < R; q += 8) acc += p[(size_t)q * n_det];
+  }
+  acc_s[ty][tx] = acc;
+  __syncthreads();
+  if (ty == 0 && j < n_det) {
+    float c = 0.f;
+    for (int q = 0; q < 8; ++q) c += acc_s[q][tx];
+    colmean[(size_t)s * n_det + j] = c * g / n_ang;
+  }
 }
 
-__global__ void ring_update_kernel(float* data, float* rowmean, const float* tilt,
+// One round on rows [r * rows_per_chunk, ...) of slice s, all columns, fused
+// with the next round's column partials:
+//   t_j = c_j - (c_{j-1} + c_j + c_{j+1}) / 3 (0 at both edges),
+//   x <- max((x g) / r_i - coeff t_j, 0),  r_i <- mean of the new row,
+//   part[j] = sum over the chunk of x_new / r_i.
+// After a round every value is >= 0, so a row with r_i = 0 is all zeros and
+// adds nothing whether scaled or not.  KPT columns per thread, RB rows per
+// barrier (warp partials double-buffered).
+template <int KPT, int RB>
+__global__ void __launch_bounds__(kPrepThreads) ring_round_kernel(
+    float* data, float* rowmean, const float* colmean, const float* gmean, float* part, int n_det,
+    int n_ang, int rows_per_chunk, float coeff) {
+  constexpr int NW = kPrepThreads / 32;
+  __shared__ float red[2][RB][NW];
+  const int r = blockIdx.x, s = blockIdx.y, R = gridDim.x;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const float g = gmean[s];
+  const float* c = colmean + (size_t)s * n_det;
+  float d[KPT], acc[KPT];
+#pragma unroll
+  for (int k = 0; k < KPT; ++k) {
+    const int j = threadIdx.x + k * kPrepThreads;
+    float t = 0.f;
+    if (j > 0 && j < n_det - 1) t = c[j] - (c[j - 1] + c[j] + c[j + 1]) / 3.f;
+    d[k] = __fmul_rn(t, coeff);
+    acc[k] = 0.f;
+  }
+  float* rm = rowmean + (size_t)s * n_ang;
+  const int i0 = r * rows_per_chunk, i1 = min(n_ang, i0 + rows_per_chunk);
+  int buf = 0;
+  for (int ib = i0; ib < i1; ib += RB, buf ^= 1) {
+    float y[RB][KPT];
+    float ri[RB], sum[RB];
+    // all loads of the RB rows first, so they are in flight together
+#pragma unroll
+    for (int b = 0; b < RB; ++b) {
+      const int i = ib + b;
+      ri[b] = i < i1 ? rm[i] : 0.f;
+      const float* row = data + ((size_t)s * n_ang + i) * n_det;
+#pragma unroll
+      for (int k = 0; k < KPT; ++k) {
+        const int j = threadIdx.x + k * kPrepThreads;
+        y[b][k] = (i < i1 && j < n_det) ? row[j] : 0.f;
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < RB; ++b) {
+      const int i = ib + b;
+      sum[b] = 0.f;
+      float* row = data + ((size_t)s * n_ang + i) * n_det;
+#pragma unroll
+      for (int k = 0; k < KPT; ++k) {
+        const int j = threadIdx.x + k * kPrepThreads;
+        if (i < i1 && j < n_det) {
+          const float x = y[b][k];
+          const float v = ri[b] != 0.f ? __fdiv_rn(__fmul_rn(x, g), ri[b]) : x;
+          y[b][k] = __fsub_rn(v, d[k]) > 0.f ? __fsub_rn(v, d[k]) : 0.f;
+          row[j] = y[b][k];
+        }
+        sum[b] += y[b][k];
+      }
+    }
+#pragma unroll
+    for (int b = 0; b < RB; ++b) {
+      float v = sum[b];
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) red[buf][b][w] = v;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int b = 0; b < RB; ++b) {
+      float tot = 0.f;
+#pragma unroll
+      for (int q = 0; q < NW; ++q) tot += red[buf][b][q];
+      const float rn = tot / n_det;
+      const int i = ib + b;
+      if (i < i1) {
+        if (threadIdx.x == 0) rm[i] = rn;
+        if (rn != 0.f) {
+          const float inv = 1.f / rn;
+#pragma unroll
+          for (int k = 0; k < KPT; ++k) acc[k] += y[b][k] * inv;
+        }
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < KPT; ++k) {
+    const int j = threadIdx.x + k * kPrepThreads;
+    if (j < n_det) part[((size_t)s * R + r) * n_det + j] = acc[k];
+  }
+}
+
+__global__ void ring_update_kernel(float* data, float* rowmean, const float* colmean,
                                    const float* gmean, int n_det, int n_ang, float coeff) {
   __shared__ float red[32];
   const int i = blockIdx.x, s = blockIdx.y;
   float* row = data + ((size_t)s * n_ang + i) * n_det;
-  const float* t = tilt + (size_t)s * n_det;
+  const float* c = colmean + (size_t)s * n_det;
   const float ri = rowmean[(size_t)s * n_ang + i];
   const float g = gmean[s];
   float acc = 0.f;
   for (int j = threadIdx.x; j < n_det; j += blockDim.x) {
+    const float t = (j > 0 && j < n_det - 1) ? c[j] - (c[j - 1] + c[j] + c[j + 1]) / 3.f : 0.f;
     const float x = row[j];
     const float v = ri != 0.f ? __fdiv_rn(__fmul_rn(x, g), ri) : x;
-    const float d = __fmul_rn(t[j], coeff);
+    const float d = __fmul_rn(t, coeff);
     const float y = __fsub_rn(v, d) > 0.f ? __fsub_rn(v, d) : 0.f;
     row[j] = y;
     acc += y;
@@ -269,25 +378,29 @@ int check_launch(const char* what) {
   return e == cudaSuccess ? GR_OK : fail(GR_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
 }
 
-// Device buffers freed on scope exit (stream-ordered).
-struct AsyncBuf {
-  void* p = nullptr;
-  cudaStream_t st;
-  explicit AsyncBuf(cudaStream_t s) : st(s) {}
-  ~AsyncBuf() {
-    if (p) cudaFreeAsync(p, st);
+// Carves 256-byte aligned pieces out of one scratch allocation.
+struct Carve {
+  size_t off = 0;
+  char* base = nullptr;
+  template <class T> T* take(size_t count) {
+    off = (off + 255) & ~size_t(255);
+    T* p = reinterpret_cast<T*>(base + off);
+    off += count * sizeof(T);
+    return p;
   }
-  int alloc(size_t bytes) {
-    cudaError_t e = cudaMallocAsync(&p, bytes, st);
-    if (e != cudaSuccess) {
-      p = nullptr;
-      return fail(GR_ERR_NOMEM, "cudaMallocAsync(%zu bytes): %s", bytes, cudaGetErrorString(e));
-    }
-    return GR_OK;
-  }
-  template <class T> T* as() const { return static_cast<T*>(p); }
 };
 
+}  // namespace
+}  // namespace gr
+
+namespace gr {
+namespace {
+template <int KPT, int RB>
+void launch_ring_round(dim3 grid, cudaStream_t st, float* x, float* rm, const float* c,
+                       const float* g, float* part, int n_det, int n_ang, float coeff) {
+  ring_round_kernel<KPT, RB><<<grid, kPrepThreads, 0, st>>>(x, rm, c, g, part, n_det, n_ang,
+                                                            kRingRows, coeff);
+}
 }  // namespace
 }  // namespace gr
 
@@ -297,10 +410,11 @@ extern "C" {
 
 size_t gr_ring_workspace_bytes(int n_slices, int n_det, int n_ang) {
   if (n_slices < 1 || n_det < 1 || n_ang < 1) return 0;
-  const int R = ring_chunks(n_det, n_ang, n_slices);
+  const int R = ring_chunks(n_ang);
   const size_t floats = (size_t)n_slices * ((size_t)n_ang + (size_t)R * n_det + n_det + 1);
   return floats * sizeof(float);
 }
+
 
 int gr_ring_removal(float* sinos, int n_slices, int n_det, int n_ang, float ring_coeff,
                     int iterations, void* workspace, void* stream) {
@@ -310,21 +424,49 @@ int gr_ring_removal(float* sinos, int n_slices, int n_det, int n_ang, float ring
                             "iterations >= 0");
   if (iterations == 0) return GR_OK;
   cudaStream_t st = (cudaStream_t)stream;
-  const int R = ring_chunks(n_det, n_ang, n_slices);
-  const int rows_per = (n_ang + R - 1) / R;
+  const int R = ring_chunks(n_ang);
   float* rowmean = static_cast<float*>(workspace);
   float* part = rowmean + (size_t)n_slices * n_ang;
-  float* tilt = part + (size_t)n_slices * R * n_det;
-  float* gmean = tilt + (size_t)n_slices * n_det;
+  float* colmean = part + (size_t)n_slices * R * n_det;
+  float* gmean = colmean + (size_t)n_slices * n_det;
   const int bx = (n_det + kPrepThreads - 1) / kPrepThreads;
-  ring_rowmean_kernel<<<dim3(n_ang, n_slices), kPrepThreads, 0, st>>>(sinos, rowmean, n_det,
-                                                                       n_ang);
-  for (int m = 0; m < iterations; ++m) {
-    ring_colpart_kernel<<<dim3(bx, R, n_slices), kPrepThreads, 0, st>>>(
-        sinos, rowmean, part, gmean, n_det, n_ang, rows_per);
-    ring_tilt_kernel<<<dim3(bx, n_slices), kPrepThreads, 0, st>>>(part, tilt, n_det, n_ang, R);
-    ring_update_kernel<<<dim3(n_ang, n_slices), kPrepThreads, 0, st>>>(
-        sinos, rowmean, tilt, gmean, n_det, n_ang, ring_coeff);
+  const int cx = (n_det + 31) / 32;
+  const int kpt = bx <= 1 ? 1 : bx <= 2 ? 2 : bx <= 4 ? 4 : bx <= 8 ? 8 : 16;
+  const bool fused = bx <= 16;
+  {
+    const int ns = n_slices;
+    float* x = sinos;
+    float* rm = rowmean;
+    float* pt = part;
+    float* cm = colmean;
+    float* gm = gmean;
+    ring_rowmean_kernel<<<dim3(n_ang, ns), kPrepThreads, 0, st>>>(x, rm, n_det, n_ang);
+    ring_colpart_kernel<<<dim3(bx, R, ns), kPrepThreads, 0, st>>>(x, rm, pt, gm, n_det, n_ang,
+                                                                  kRingRows);
+    ring_colmean_kernel<<<dim3(cx, ns), 256, 0, st>>>(pt, rm, cm, gm, n_det, n_ang, R, 1);
+    for (int m = 0; m < iterations; ++m) {
+      if (fused) {
+        const dim3 grid(R, ns);
+        switch (kpt) {
+          case 1: launch_ring_round<1, 4>(grid, st, x, rm, cm, gm, pt, n_det, n_ang, ring_coeff); break;
+          case 2: launch_ring_round<2, 4>(grid, st, x, rm, cm, gm, pt, n_det, n_ang, ring_coeff); break;
+          case 4: launch_ring_round<4, 4>(grid, st, x, rm, cm, gm, pt, n_det, n_ang, ring_coeff); break;
+          case 8: launch_ring_round<8, 4>(grid, st, x, rm, cm, gm, pt, n_det, n_ang, ring_coeff); break;
+          default: launch_ring_round<16, 2>(grid, st, x, rm, cm, gm, pt, n_det, n_ang, ring_coeff);
+        }
+        if (m + 1 < iterations)
+          ring_colmean_kernel<<<dim3(cx, ns), 256, 0, st>>>(pt, rm, cm, gm, n_det, n_ang, R, 0);
+      } else {
+        // Rows wider than 4096: separate update and column passes.
+        if (m > 0) {
+          ring_colpart_kernel<<<dim3(bx, R, ns), kPrepThreads, 0, st>>>(x, rm, pt, gm, n_det,
+                                                                        n_ang, kRingRows);
+          ring_colmean_kernel<<<dim3(cx, ns), 256, 0, st>>>(pt, rm, cm, gm, n_det, n_ang, R, 1);
+        }
+        ring_update_kernel<<<dim3(n_ang, ns), kPrepThreads, 0, st>>>(x, rm, cm, gm, n_det, n_ang,
+                                                                     ring_coeff);
+      }
+    }
   }
   return check_launch("ring removal");
 }
@@ -383,26 +525,31 @@ int gr_reconstruct_padded(gr_plan* plan, const float* sinos, int n_slices, int n
   if (off + n_det > M0)
     return fail(GR_ERR_ARG, "padded: crop window [%d, %d) exceeds the image size %d", off,
                 off + n_det, M0);
+  DeviceGuard guard(dev);
   cudaStream_t st = (cudaStream_t)stream;
   const int chunk = std::min(n_slices, 2 * max_pairs);
-  AsyncBuf sp(st), rec(st);
-  if ((rc = sp.alloc((size_t)chunk * n_ang * pn * sizeof(float)))) return rc;
-  if ((rc = rec.alloc((size_t)chunk * M0 * M0 * sizeof(float)))) return rc;
+  Carve c;
+  c.take<float>((size_t)chunk * n_ang * pn);
+  c.take<float>((size_t)chunk * M0 * M0);
+  if ((rc = plan_scratch(plan, c.off + 256, (void**)&c.base))) return rc;
+  c.off = 0;
+  float* sp = c.take<float>((size_t)chunk * n_ang * pn);
+  float* rec = c.take<float>((size_t)chunk * M0 * M0);
   for (int s0 = 0; s0 < n_slices; s0 += chunk) {
     const int ns = std::min(chunk, n_slices - s0);
     shift_pad_kernel<<<dim3(n_ang, ns), kPrepThreads, 0, st>>>(
-        sinos + (size_t)s0 * n_ang * n_det, (long)n_ang * n_det, ns, nullptr, 1, xoffset,
-        sp.as<float>(), n_det, n_ang, pn);
+        sinos + (size_t)s0 * n_ang * n_det, (long)n_ang * n_det, ns, nullptr, 1, xoffset, sp,
+        n_det, n_ang, pn);
     if ((rc = check_launch("padded: shift/pad"))) return rc;
     gr_batch_desc b{};
     b.n_slices = ns;
     b.dtype = GR_DTYPE_F32;
-    b.sinos = sp.p;
-    b.outs = rec.as<float>();
+    b.sinos = sp;
+    b.outs = rec;
     b.out_stride = M0;
     if ((rc = gr_reconstruct_batch(plan, &b, st))) return rc;
     crop_kernel<<<dim3(n_det, ns), kPrepThreads, 0, st>>>(
-        rec.as<float>(), M0, (long)M0 * M0, outs + (size_t)s0 * n_det * out_stride, out_stride,
+        rec, M0, (long)M0 * M0, outs + (size_t)s0 * n_det * out_stride, out_stride,
         (long)n_det * out_stride, n_det, off, 0);
     if ((rc = check_launch("padded: crop"))) return rc;
   }
@@ -425,65 +572,74 @@ int gr_center_search(gr_plan* plan, const float* sino1, const float* sino2, int 
   if (off + n_det > M0)
     return fail(GR_ERR_ARG, "centre search: crop window [%d, %d) exceeds the image size %d", off,
                 off + n_det, M0);
+  DeviceGuard guard(dev);
   cudaStream_t st = (cudaStream_t)stream;
   const int chunk = std::min(n_cand, max_pairs);  // candidates per batch (one pair each)
   const long slice_in = (long)n_ang * n_det;
   const long slice_rec = (long)M0 * M0;
-  AsyncBuf pair(st), sp(st), rec(st), xo(st), gh(st), sc(st);
-  if ((rc = pair.alloc(2 * slice_in * sizeof(float)))) return rc;
-  if ((rc = sp.alloc((size_t)2 * chunk * n_ang * pn * sizeof(float)))) return rc;
-  if ((rc = rec.alloc((size_t)2 * chunk * slice_rec * sizeof(float)))) return rc;
-  if ((rc = xo.alloc((size_t)n_cand * sizeof(float)))) return rc;
-  if ((rc = gh.alloc((size_t)chunk * (nbins + 1) * sizeof(unsigned)))) return rc;
-  if ((rc = sc.alloc((size_t)n_cand * sizeof(float)))) return rc;
-  float* pr = pair.as<float>();
+  Carve c;
+  for (int pass = 0; pass < 2; ++pass) {
+    if (pass == 1) {
+      if ((rc = plan_scratch(plan, c.off + 256, (void**)&c.base))) return rc;
+      c.off = 0;
+    }
+    c.take<float>(2 * slice_in);
+    c.take<float>((size_t)2 * chunk * n_ang * pn);
+    c.take<float>((size_t)2 * chunk * slice_rec);
+    c.take<float>(n_cand);
+    c.take<unsigned>((size_t)chunk * (nbins + 1));
+    c.take<float>(n_cand);
+  }
+  c.off = 0;
+  float* pr = c.take<float>(2 * slice_in);
+  float* sp = c.take<float>((size_t)2 * chunk * n_ang * pn);
+  float* rec = c.take<float>((size_t)2 * chunk * slice_rec);
+  float* xo = c.take<float>(n_cand);
+  unsigned* gh = c.take<unsigned>((size_t)chunk * (nbins + 1));
+  float* sc = c.take<float>(n_cand);
   cudaError_t e = cudaMemcpyAsync(pr, sino1, slice_in * sizeof(float), cudaMemcpyDeviceToDevice, st);
   if (e == cudaSuccess)
     e = cudaMemcpyAsync(pr + slice_in, sino2, slice_in * sizeof(float), cudaMemcpyDeviceToDevice,
                         st);
   if (e == cudaSuccess)
-    e = cudaMemcpyAsync(xo.p, shifts, n_cand * sizeof(float), cudaMemcpyHostToDevice, st);
+    e = cudaMemcpyAsync(xo, shifts, n_cand * sizeof(float), cudaMemcpyHostToDevice, st);
   if (e != cudaSuccess) return cuda_fail(e, "centre search: copies");
   for (int c0 = 0; c0 < n_cand; c0 += chunk) {
     const int nc = std::min(chunk, n_cand - c0);
-    shift_pad_kernel<<<dim3(n_ang, 2 * nc), kPrepThreads, 0, st>>>(
-        pr, slice_in, 2, xo.as<float>() + c0, 2, 0.f, sp.as<float>(), n_det, n_ang, pn);
+    shift_pad_kernel<<<dim3(n_ang, 2 * nc), kPrepThreads, 0, st>>>(pr, slice_in, 2, xo + c0, 2,
+                                                                   0.f, sp, n_det, n_ang, pn);
     if ((rc = check_launch("centre search: shift/pad"))) return rc;
     gr_batch_desc b{};
     b.n_slices = 2 * nc;
     b.dtype = GR_DTYPE_F32;
-    b.sinos = sp.p;
-    b.outs = rec.as<float>();
+    b.sinos = sp;
+    b.outs = rec;
     b.out_stride = M0;
     if ((rc = gr_reconstruct_batch(plan, &b, st))) return rc;
-    Window w{rec.as<float>() + (size_t)off * M0 + off, M0, slice_rec, 2 * slice_rec, n_det,
-             n_det, 2};
-    if ((rc = launch_entropy(w, nc, hist_lo, hist_hi, nbins, gh.as<unsigned>(),
-                             sc.as<float>() + c0, st)))
-      return rc;
+    Window w{rec + (size_t)off * M0 + off, M0, slice_rec, 2 * slice_rec, n_det, n_det, 2};
+    if ((rc = launch_entropy(w, nc, hist_lo, hist_hi, nbins, gh, sc + c0, st))) return rc;
   }
-  e = cudaMemcpyAsync(scores, sc.p, n_cand * sizeof(float), cudaMemcpyDeviceToHost, st);
+  e = cudaMemcpyAsync(scores, sc, n_cand * sizeof(float), cudaMemcpyDeviceToHost, st);
   if (e == cudaSuccess) e = cudaStreamSynchronize(st);
   if (e != cudaSuccess) return cuda_fail(e, "centre search: scores");
   // First strict minimum, as the reference's `entropy_cur < entropy_optim` scan.
   int bi = 0;
-  for (int c = 1; c < n_cand; ++c)
-    if (scores[c] < scores[bi]) bi = c;
+  for (int k = 1; k < n_cand; ++k)
+    if (scores[k] < scores[bi]) bi = k;
   if (best) *best = bi;
   if (best_images) {
-    shift_pad_kernel<<<dim3(n_ang, 2), kPrepThreads, 0, st>>>(
-        pr, slice_in, 2, xo.as<float>() + bi, 2, 0.f, sp.as<float>(), n_det, n_ang, pn);
+    shift_pad_kernel<<<dim3(n_ang, 2), kPrepThreads, 0, st>>>(pr, slice_in, 2, xo + bi, 2, 0.f,
+                                                              sp, n_det, n_ang, pn);
     if ((rc = check_launch("centre search: shift/pad"))) return rc;
     gr_batch_desc b{};
     b.n_slices = 2;
     b.dtype = GR_DTYPE_F32;
-    b.sinos = sp.p;
-    b.outs = rec.as<float>();
+    b.sinos = sp;
+    b.outs = rec;
     b.out_stride = M0;
     if ((rc = gr_reconstruct_batch(plan, &b, st))) return rc;
-    crop_kernel<<<dim3(n_det, 2), kPrepThreads, 0, st>>>(rec.as<float>(), M0, slice_rec,
-                                                         best_images, n_det, (long)n_det * n_det,
-                                                         n_det, off, 0);
+    crop_kernel<<<dim3(n_det, 2), kPrepThreads, 0, st>>>(rec, M0, slice_rec, best_images, n_det,
+                                                         (long)n_det * n_det, n_det, off, 0);
     if ((rc = check_launch("centre search: crop"))) return rc;
   }
   return GR_OK;

@@ -21,7 +21,7 @@ STATUS = {0: "GR_OK", -1: "GR_ERR_ARG", -2: "GR_ERR_PSWF", -3: "GR_ERR_CUDA",
           -4: "GR_ERR_NOMEM", -5: "GR_ERR_UNSUPPORTED", -6: "GR_ERR_TIMEOUT"}
 
 FILTER_NONE, FILTER_SHEPP_LOGAN, FILTER_HANN, FILTER_HAMMING, FILTER_RAMP, FILTER_FBP = range(6)
-DTYPE_F32, DTYPE_F16, DTYPE_BF16, DTYPE_U16_RAW = range(4)
+DTYPE_F32, DTYPE_F16, DTYPE_BF16, DTYPE_U16_RAW, DTYPE_U16_LINEAR = range(5)
 
 # Functions declared in include/gridrec_b200.h (checked by the CPU tests).
 EXPORTS = ("gr_params_default", "gr_filter_code", "gr_plan_create", "gr_plan_destroy",

@@ -141,6 +141,35 @@ def test_raw_uint16_fused_normalisation():
     assert ph.rel_l2(got[1], o2[:, :plan.M0]) < TOL
 
 
+def test_raw_uint16_linear_normalisation_bit_exact():
+    """1 - (raw - dark)/(flat - dark) on load (tomo_recon.cpp:1871-1877, flat the mean of
+    two white fields): the images equal, bit for bit, those of the float32 sinograms
+    normalised on the host with the same float operations, and match float64 gridrec."""
+    n, a = 256, 120
+    th = ph.angles_deg(a)
+    rng = np.random.default_rng(21)
+    p = [ph.line_integrals(ph.random_ellipses(s), n, th, 128.0) / (n / 2) for s in range(2)]
+    raws = []
+    for s in range(2):
+        r, w1, dark = ph.raw_counts(p[s], seed=19)
+        raws.append(r)
+    raws = np.stack(raws)
+    w2 = (w1 * rng.uniform(0.98, 1.02, n)).astype(np.float32)
+    flat = (np.float32(0.5) * w1 + np.float32(0.5) * w2).astype(np.float32)
+    norm = (np.float32(1) - (raws.astype(np.float32) - dark) / (flat - dark)).astype(np.float32)
+    with G.Plan(n, a, th, center=128.0) as plan:
+        outs = torch.zeros((2, plan.M0, plan.M0), device="cuda")
+        plan.reconstruct_batch(_dev(raws.view(np.int16)), outs, flat=_dev(flat), dark=_dev(dark),
+                               dtype=G.DTYPE_U16_LINEAR)
+        ref = torch.zeros_like(outs)
+        plan.reconstruct_batch(_dev(norm), ref)
+        got, want = outs.cpu().numpy(), ref.cpu().numpy()
+    np.testing.assert_array_equal(got, want)
+    o1, o2 = O.port_gridrec_pair(norm[0], norm[1], th, center1=128.0, filter=1)
+    assert ph.rel_l2(got[0], o1[:, :plan.M0]) < TOL
+    assert ph.rel_l2(got[1], o2[:, :plan.M0]) < TOL
+
+
 def test_host_streaming_matches_device_batch():
     n, a = 128, 64
     th = ph.angles_deg(a)

@@ -77,6 +77,24 @@ def test_ring_removal_batch_against_oracle():
     assert np.array_equal(y.cpu().numpy(), s)
 
 
+def test_ring_removal_full_size_and_wide_rows():
+    """A batch of 2048 x 1500 slices, and rows wider than the fused round kernel
+    takes (separate update and column passes)."""
+    g = torch.Generator(device="cuda").manual_seed(11)
+    x = torch.rand((6, 1500, 2048), device="cuda", generator=g) + 0.5
+    x[:, :, 700] *= 1.1
+    src = x.cpu().numpy()
+    G.ring_removal(x, 1.0, 20)
+    out = x.cpu().numpy()
+    for i in (0, 5):
+        assert ph.rel_l2(out[i], O.port_ring_removal(src[i], 1.0, 20)) < 2e-5
+    rng = np.random.default_rng(12)
+    w = (rng.random((1, 20, 9000)) + 0.2).astype(np.float32)
+    y = _dev(w)
+    G.ring_removal(y, 1.0, 20)
+    assert ph.rel_l2(y.cpu().numpy()[0], O.port_ring_removal(w[0], 1.0, 20)) < 2e-5
+
+
 def test_crop_and_circle_mask():
     rng = np.random.default_rng(7)
     rec = rng.standard_normal((2, 70, 75)).astype(np.float32)
