@@ -131,6 +131,9 @@ int gr_reconstruct_pair(gr_plan* plan, const float* sino1, const float* sino2, f
  *              GR_DTYPE_U16_LINEAR: value = 1 - (raw - dark)/(flat - dark)
  *              (tomo_recon.cpp:1871-1877, where flat = 0.5 white1 + 0.5 white2)
  *   outs       n_slices images, each M0 rows of out_stride floats, contiguous
+ *   flat_stride floats between consecutive slices' flat/dark rows: 0 = one row
+ *              for all slices; n_det = one row per slice (each slice is a detector
+ *              row with its own white and dark, tomo_recon.cpp:1533-1541)
  * Pairs are processed max_pairs at a time on `stream`. */
 typedef struct {
   int n_slices;
@@ -141,6 +144,7 @@ typedef struct {
   const float* dark;
   float* outs;
   long out_stride;
+  long flat_stride;
 } gr_batch_desc;
 
 int gr_reconstruct_batch(gr_plan* plan, const gr_batch_desc* batch, void* stream);
@@ -206,10 +210,41 @@ const char* gr_last_error(void);
 /* Number of kernel launches the plan has issued since creation. */
 int gr_plan_launch_count(const gr_plan* plan, long* launches);
 
+/* Autotuner: times the gridding work-item cost cap (512..8192 sample slots per
+ * item: load balance against split-tile overhead) and the column-FFT group width
+ * (1..8 columns per CTA) on the plan's own workspaces, and keeps the fastest.
+ * Choices are cached per shape in the process, so later plans of the same shape
+ * tune instantly.  Synchronises `stream`; not for use inside stream capture.
+ * Results stay within the same tolerance; bitwise reproducibility holds per
+ * tuning (the item cap sets the gridding's summation order).  No reference
+ * counterpart (the reference has fixed launch shapes). */
+int gr_plan_autotune(gr_plan* plan, void* stream);
+int gr_plan_tuning(const gr_plan* plan, int* item_cap, int* cols_group);
+
 /* Shape of the gridding work list: work items (CTAs per pair), sample runs,
  * scratch slots of split tiles, and samples visited per pair (with halo). */
 int gr_plan_work_stats(const gr_plan* plan, int* n_items, int* n_runs, int* n_slots,
                        long* total_samples);
+
+/* ---- CUDA graphs: record once, replay with one launch.
+ * gr_graph_create records gr_reconstruct_batch(item.plan, &item.batch) for every
+ * item into one CUDA graph by stream capture.  Items of one plan run in order on
+ * one branch (they share its workspaces); items of different plans (different
+ * shapes: n_det, n_ang, dtype) run on parallel branches, so an uneven batch is
+ * one launch.  The batch buffers are baked into the graph: gr_graph_launch
+ * replays the same addresses on `stream`.  All plans must be on one device and
+ * have stage timing off.  No reference counterpart: the reference launches per
+ * slice pair (gridrec/GPU/tomo_recon.cpp:3846-3852). */
+typedef struct gr_graph gr_graph;
+typedef struct {
+  gr_plan* plan;
+  gr_batch_desc batch;
+} gr_graph_item;
+int gr_graph_create(const gr_graph_item* items, int n_items, gr_graph** graph);
+int gr_graph_launch(gr_graph* graph, void* stream);
+/* Kernel launches one replay performs. */
+int gr_graph_launch_count(const gr_graph* graph, long* launches);
+int gr_graph_destroy(gr_graph* graph);
 
 /* ---- Slice pipeline around gridrec (the reference's tomo_recon and find_shift
  * drivers).  Sinograms are n_ang rows of n_det float32, slices contiguous, in

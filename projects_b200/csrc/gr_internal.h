@@ -55,8 +55,9 @@ struct SpectraArgs {
   long pair_stride;      // elements between consecutive pairs' sinograms
   int n_slices_valid;    // slices that exist (2*pairs or 2*pairs-1)
   int slice_base;        // global index of slice 1 of pair 0 (for centres)
-  const float* flat;     // u16 raw only
+  const float* flat;     // u16 raw only: row of slice s at flat + s * flat_stride
   const float* dark;
+  long flat_stride;
   const float4* pq;      // [pair][J] (P.re, P.im, Q.re, Q.im)
   float2* spec;          // [pair][n_ang][2][J]
   const float2* tw;      // two-level twiddle table for pdim (see gridrec_kernels.cu)
@@ -93,6 +94,7 @@ struct ColArgs {
   const float2* tw;      // two-level twiddle table for M
   int M, pairs;
   int* err;              // device error word for bounded-wait timeouts (null: plain loads)
+  int G = 0;             // columns per CTA (0: cols_group(M))
 };
 
 struct RowArgs {

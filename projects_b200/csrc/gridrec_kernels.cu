@@ -394,14 +394,19 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
   const T* r2 = (2 * pair + 1 < a.n_slices_valid)
                     ? static_cast<const T*>(a.s2) + pair * a.pair_stride + (long)n * a.n_det
                     : nullptr;
+  const long fo = (long)(a.slice_base + 2 * pair) * a.flat_stride;  // slice 1's flat/dark row
+  const float* f1 = a.flat ? a.flat + fo : nullptr;
+  const float* d1 = a.dark ? a.dark + fo : nullptr;
+  const float* f2 = f1 ? f1 + a.flat_stride : nullptr;
+  const float* d2 = d1 ? d1 + a.flat_stride : nullptr;
   float2 v[16];
 #pragma unroll
   for (int r = 0; r < 16; ++r) {
     const int k = tid + r * nthr;
     float x = 0.f, y = 0.f;
     if (k < a.n_det) {
-      x = load_sino<T>(r1, k, a.flat, a.dark);
-      if (r2) y = load_sino<T>(r2, k, a.flat, a.dark);
+      x = load_sino<T>(r1, k, f1, d1);
+      if (r2) y = load_sino<T>(r2, k, f2, d2);
     }
     v[r] = make_float2(x, y);
   }
@@ -450,7 +455,7 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
 // shuffles), so the geometry -- positions, table lookups -- is computed once
 // for both pairs.  The samples of one step are taken P apart along the run
 // with P * max(|du|,|dv|) > L, so no two of them share a valid tap (taps lie
-// within L/2 of their sample); P per run comes from the host
+// within L/2 of their sample; P per run comes from the host), so
 // plain read-modify-write needs no atomics, and the summation order is fixed,
 // so the result is bitwise reproducible.  Float/int conversions use exact
 // magic-number rounding on the FP32 pipe.  Tiles split over several items
@@ -897,7 +902,7 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
 }
 
 cudaError_t launch_cols(const ColArgs& a, cudaStream_t s) {
-  const int G = cols_group(a.M);
+  const int G = a.G > 0 ? a.G : cols_group(a.M);
   const int threads = G * (a.M / 16);
   PFN_cuTensorMapEncodeTiled_v12000 encode = tensor_map_encoder();
   if (a.err && encode && G >= 2 && a.M >= 16 && ((uintptr_t)a.H % 16) == 0) {

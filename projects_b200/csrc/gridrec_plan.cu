@@ -8,6 +8,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -125,6 +126,10 @@ struct Plan {
   float2* d_spec = nullptr;
   float2* d_H = nullptr;
   float4* d_scratch = nullptr;
+  size_t scratch_cells = 0;         // float4 cells allocated in d_scratch
+  std::vector<double> dxy;          // per-direction (du, dv) steps, kept for rebuilding
+  int item_cap = kItemCap;          // gridding work-item cost cap (autotuned)
+  int cols_G = 0;                   // column-FFT group width (0 = cols_group(M); autotuned)
   float4* d_pq = nullptr;
   // host streaming (gr_reconstruct_host)
   void* h_in[2] = {nullptr, nullptr};
@@ -175,6 +180,15 @@ int upload(Plan* p, T** dptr, const std::vector<T>& h) {
   return GR_OK;
 }
 
+template <typename T>
+void dev_free(Plan* p, T** ptr) {
+  if (!*ptr) return;
+  auto it = std::find(p->allocs.begin(), p->allocs.end(), (void*)*ptr);
+  if (it != p->allocs.end()) p->allocs.erase(it);
+  cudaFree(*ptr);
+  *ptr = nullptr;
+}
+
 // The gridding work list: for each 32x32 tile, the runs of samples
 // (direction, j range) whose L x L footprint can reach the tile; tiles whose
 // runs exceed kItemCap samples are split into several items.
@@ -212,7 +226,7 @@ int run_spacing(double du, double dv, int n, double L, int spw, int* steps) {
 }
 
 void build_work_list(int M, int J, double L, int n_ang, const std::vector<double>& dxy,
-                     WorkList* wl) {
+                     WorkList* wl, int item_cap = kItemCap) {
   const int T = kTile;
   const double M2 = M / 2;
   const double L2 = L / 2 + 2e-3;  // box margin covers FP32 position rounding
@@ -283,7 +297,7 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
       cost += run_cost[r];
       total += wl->runs[r].jhi - wl->runs[r].jlo + 1;
     }
-    if (cost <= kItemCap) {
+    if (cost <= item_cap) {
       items.push_back({{t, b, e, -1}, cost});
       continue;
     }
@@ -291,7 +305,7 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
     long c = 0;
     for (int r = b; r < e; ++r) {
       const long rc = run_cost[r];
-      if (c > 0 && c + rc > kItemCap) {
+      if (c > 0 && c + rc > item_cap) {
         cuts.push_back({r, c});
         c = 0;
       }
@@ -313,6 +327,42 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
   wl->n_slots = n_slots;
   wl->n_split = n_split;
   wl->total = total;
+}
+
+// Builds the work list with the given item cap and (re)places it on the
+// device; grows the split-tile scratch when needed.
+int install_work_list(Plan* p, int item_cap) {
+  WorkList wl;
+  build_work_list(p->M, p->J, p->L, p->n_ang, p->dxy, &wl, item_cap);
+  std::vector<int4> split_list;
+  for (size_t t = 0; t < wl.splits.size(); ++t)
+    if (wl.splits[t].nsplit > 1)
+      split_list.push_back(make_int4((int)t, wl.splits[t].slot0, wl.splits[t].nsplit, 0));
+  dev_free(p, &p->d_items);
+  dev_free(p, &p->d_runs);
+  dev_free(p, &p->d_splits);
+  dev_free(p, &p->d_split_list);
+  int rc;
+  if ((rc = upload(p, &p->d_items, wl.items)) || (rc = upload(p, &p->d_runs, wl.runs)) ||
+      (rc = upload(p, &p->d_splits, wl.splits)) || (rc = upload(p, &p->d_split_list, split_list)))
+    return rc;
+  const size_t cells =
+      ((size_t)(p->max_pairs + 1) / 2) * (size_t)std::max(wl.n_slots, 1) * kTile * kTile;
+  if (cells > p->scratch_cells) {
+    dev_free(p, &p->d_scratch);
+    if ((rc = dev_alloc(p, &p->d_scratch, cells))) return rc;
+    p->scratch_cells = cells;
+  }
+  p->tiles_u = wl.tiles_u;
+  p->tiles_v = wl.tiles_v;
+  p->n_items = (int)wl.items.size();
+  p->n_runs = (int)wl.runs.size();
+  p->n_slots = wl.n_slots;
+  p->n_split = wl.n_split;
+  p->total_samples = wl.total;
+  p->n_split_tiles = (int)split_list.size();
+  p->item_cap = item_cap;
+  return GR_OK;
 }
 
 // Sizes exactly as GridRec::init (gridrec/GPU/gridrec.cu:243-268), in FP64.
@@ -393,13 +443,14 @@ cudaEvent_t next_event(Plan* p) {
 
 int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1,
                  const void* s2, long in_pair_stride, gr_dtype dt, const float* centers,
-                 const float* flat, const float* dark, float* o1, float* o2,
+                 const float* flat, const float* dark, long flat_stride, float* o1, float* o2,
                  long out_pair_stride, long out_stride, cudaStream_t st) {
   GR_MARK();
   PhaseArgs ph{centers, p->center, slice_base, n_valid, p->d_filt, p->d_pq, p->J, p->pdim, pairs};
   GR_CUDA(launch_phase(ph, st));
   GR_MARK();
-  SpectraArgs sa{s1, s2, in_pair_stride, n_valid, slice_base, flat, dark, p->d_pq, p->d_spec,
+  SpectraArgs sa{s1, s2, in_pair_stride, n_valid, slice_base, flat, dark, flat_stride, p->d_pq,
+                 p->d_spec,
                  p->d_tw_p, p->n_det, p->n_ang, p->pdim, p->J, pairs};
   GR_CUDA(launch_spectra(sa, dt, st));
   GR_MARK();
@@ -409,14 +460,15 @@ int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1
               (float)(2.0 * p->ltbl / p->L)};
   GR_CUDA(launch_grid(ga, p->ntaps, st));
   GR_MARK();
-  ColArgs ca{p->d_H, p->d_tw_m, p->M, pairs, p->d_err};
+  ColArgs ca{p->d_H, p->d_tw_m, p->M, pairs, p->d_err, p->cols_G};
   GR_CUDA(launch_cols(ca, st));
   GR_MARK();
   RowArgs ra{p->d_H, p->d_tw_m, p->d_winv, o1, o2, out_pair_stride, out_stride, n_valid,
              p->M, p->M0, p->M02, pairs};
   GR_CUDA(launch_rows(ra, st));
   GR_MARK();
-  p->launches += 5;
+  // phase, spectra, grid (+ split reduction when tiles are split), cols, rows
+  p->launches += 5 + (p->n_items > 0 && p->n_split_tiles > 0 ? 1 : 0);
   return GR_OK;
 }
 
@@ -439,6 +491,8 @@ int validate_batch(const Plan* p, const gr_batch_desc* b) {
   if (dtype_size(b->dtype) == 0) return fail(GR_ERR_ARG, "unknown dtype %d", (int)b->dtype);
   if ((b->dtype == GR_DTYPE_U16_RAW || b->dtype == GR_DTYPE_U16_LINEAR) && (!b->flat || !b->dark))
     return fail(GR_ERR_ARG, "raw uint16 dtypes need flat and dark rows");
+  if (b->flat_stride != 0 && b->flat_stride < p->n_det)
+    return fail(GR_ERR_ARG, "flat_stride %ld: 0 or >= n_det %d", b->flat_stride, p->n_det);
   return GR_OK;
 }
 
@@ -604,32 +658,17 @@ int gr_plan_create(const gr_params* prm, gr_plan** out) {
   std::vector<float2> dirs(2 * (size_t)prm->n_ang);
   for (size_t d = 0; d < dirs.size(); ++d)
     dirs[d] = make_float2((float)dxy[2 * d], (float)dxy[2 * d + 1]);
-  WorkList wl;
-  build_work_list(p->M, p->J, p->L, p->n_ang, dxy, &wl);
-  p->tiles_u = wl.tiles_u;
-  p->tiles_v = wl.tiles_v;
-  p->n_items = (int)wl.items.size();
-  p->n_runs = (int)wl.runs.size();
-  p->n_slots = wl.n_slots;
-  p->n_split = wl.n_split;
-  p->total_samples = wl.total;
-  std::vector<int4> split_list;
-  for (size_t t = 0; t < wl.splits.size(); ++t)
-    if (wl.splits[t].nsplit > 1)
-      split_list.push_back(make_int4((int)t, wl.splits[t].slot0, wl.splits[t].nsplit, 0));
-  p->n_split_tiles = (int)split_list.size();
+  p->dxy = dxy;
   if ((rc = upload(p, &p->d_wtbl, fw)) || (rc = upload(p, &p->d_winv, fi)) ||
       (rc = upload(p, &p->d_filt, filt)) || (rc = upload(p, &p->d_tw_p, twiddles((int)pdim))) ||
       (rc = upload(p, &p->d_tw_m, twiddles((int)M))) || (rc = upload(p, &p->d_dir, dirs)) ||
-      (rc = upload(p, &p->d_items, wl.items)) || (rc = upload(p, &p->d_runs, wl.runs)) ||
-      (rc = upload(p, &p->d_splits, wl.splits)) || (rc = upload(p, &p->d_split_list, split_list))) {
+      (rc = install_work_list(p, kItemCap))) {
     gr_plan_destroy(p);
     return rc;
   }
   const size_t P = (size_t)p->max_pairs;
   if ((rc = dev_alloc(p, &p->d_spec, P * p->n_ang * 2 * p->J)) ||
       (rc = dev_alloc(p, &p->d_H, P * (size_t)M * M)) ||
-      (rc = dev_alloc(p, &p->d_scratch, ((P + 1) / 2) * (size_t)std::max(p->n_slots, 1) * kTile * kTile)) ||
       (rc = dev_alloc(p, &p->d_pq, P * p->J)) ||
       (rc = dev_alloc(p, &p->d_queue, 1)) || (rc = dev_alloc(p, &p->d_err, 1))) {
     gr_plan_destroy(p);
@@ -743,6 +782,97 @@ int gr_plan_launch_count(const gr_plan* p, long* launches) {
   return GR_OK;
 }
 
+int gr_plan_autotune(gr_plan* p, void* stream) {
+  using namespace gr;
+  if (!p) return fail(GR_ERR_ARG, "null plan");
+  DeviceGuard g(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  // tuned choices depend on the work-list geometry and the chunk size: key on them
+  unsigned long long h = 1469598103934665603ull;
+  auto mix = [&](unsigned long long v) { h = (h ^ v) * 1099511628211ull; };
+  mix((unsigned long long)p->device);
+  mix((unsigned long long)p->M);
+  mix((unsigned long long)p->J);
+  mix((unsigned long long)p->n_ang);
+  mix((unsigned long long)p->max_pairs);
+  mix((unsigned long long)std::llround(p->L * 1e6));
+  for (double d : p->dxy) mix((unsigned long long)std::llround(d * 1e9));
+  static std::mutex mu;
+  static std::map<unsigned long long, std::pair<int, int>> cache;
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    auto it = cache.find(h);
+    if (it != cache.end()) {
+      int rc = it->second.first == p->item_cap ? GR_OK : install_work_list(p, it->second.first);
+      p->cols_G = it->second.second;
+      return rc;
+    }
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  GR_CUDA(cudaEventCreate(&e0));
+  GR_CUDA(cudaEventCreate(&e1));
+  auto time_ms = [&](auto&& launch) -> float {
+    float best = 1e30f;
+    for (int rep = 0; rep < 4; ++rep) {
+      cudaEventRecord(e0, st);
+      launch();
+      cudaEventRecord(e1, st);
+      cudaEventSynchronize(e1);
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, e0, e1);
+      if (rep > 0) best = std::min(best, ms);  // first run warms up
+    }
+    return best;
+  };
+  const int pairs = p->max_pairs;
+  cudaMemsetAsync(p->d_spec, 0, (size_t)pairs * p->n_ang * 2 * p->J * sizeof(float2), st);
+  cudaMemsetAsync(p->d_H, 0, (size_t)pairs * p->M * p->M * sizeof(float2), st);
+  int best_cap = p->item_cap, rc = GR_OK;
+  float best_t = 1e30f;
+  for (int cap : {512, 1024, 2048, 4096, 8192}) {
+    if ((rc = install_work_list(p, cap))) break;
+    GridArgs ga{p->d_spec, p->d_H, p->d_scratch, p->d_queue, p->d_items, p->d_runs,
+                p->d_split_list, p->n_split_tiles, p->d_dir, p->d_wtbl, p->n_items, pairs,
+                p->n_ang, p->J, p->M, p->tiles_v, p->n_slots, p->ltbl, (float)(p->L / 2),
+                (float)(2.0 * p->ltbl / p->L)};
+    const float t = time_ms([&] { launch_grid(ga, p->ntaps, st); });
+    if (t < best_t) {
+      best_t = t;
+      best_cap = cap;
+    }
+  }
+  if (rc == GR_OK && best_cap != p->item_cap) rc = install_work_list(p, best_cap);
+  int best_G = 0;
+  float best_c = 1e30f;
+  for (int G = 1; G <= 8 && rc == GR_OK; G *= 2) {
+    const int threads = G * (p->M / 16);
+    if (threads < 32 || threads > 512 || p->M % G) continue;
+    ColArgs ca{p->d_H, p->d_tw_m, p->M, pairs, p->d_err, G};
+    const float t = time_ms([&] { launch_cols(ca, st); });
+    if (t < best_c) {
+      best_c = t;
+      best_G = G;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaError_t e = cudaGetLastError();
+  if (rc == GR_OK && e != cudaSuccess) rc = fail(GR_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
+  if (rc == GR_OK) {
+    p->cols_G = best_G;
+    std::lock_guard<std::mutex> lk(mu);
+    cache[h] = {best_cap, best_G};
+  }
+  return rc;
+}
+
+int gr_plan_tuning(const gr_plan* p, int* item_cap, int* cols_group_width) {
+  if (!p) return gr::fail(GR_ERR_ARG, "null plan");
+  if (item_cap) *item_cap = p->item_cap;
+  if (cols_group_width) *cols_group_width = p->cols_G > 0 ? p->cols_G : gr::cols_group(p->M);
+  return GR_OK;
+}
+
 int gr_plan_work_stats(const gr_plan* p, int* n_items, int* n_runs, int* n_slots,
                        long* total_samples) {
   if (!p) return gr::fail(GR_ERR_ARG, "null plan");
@@ -761,7 +891,7 @@ int gr_reconstruct_pair(gr_plan* p, const float* sino1, const float* sino2, floa
   DeviceGuard g(p->device);
   const int n_valid = (sino2 && out2) ? 2 : 1;
   return launch_chunk(p, 1, n_valid, 0, sino1, sino2 ? sino2 : sino1, 0, GR_DTYPE_F32, nullptr,
-                      nullptr, nullptr, out1, out2 ? out2 : out1, 0, out_stride,
+                      nullptr, nullptr, 0, out1, out2 ? out2 : out1, 0, out_stride,
                       (cudaStream_t)stream);
 }
 
@@ -782,7 +912,8 @@ int gr_reconstruct_batch(gr_plan* p, const gr_batch_desc* b, void* stream) {
     const char* base = static_cast<const char*>(b->sinos) + (size_t)s0 * slice_in * es;
     float* ob = b->outs + (size_t)s0 * slice_out;
     rc = launch_chunk(p, pairs, n_valid, s0, base, base + slice_in * es, 2 * slice_in,
-                      b->dtype, b->centers, b->flat, b->dark, ob, ob + slice_out, 2 * slice_out,
+                      b->dtype, b->centers, b->flat, b->dark, b->flat_stride, ob, ob + slice_out,
+                      2 * slice_out,
                       b->out_stride, (cudaStream_t)stream);
     if (rc) return rc;
   }
@@ -857,10 +988,11 @@ int gr_reconstruct_host(gr_plan* p, const gr_batch_desc* b, void* stream) {
     GR_CUDA(cudaMemcpy(d_centers, b->centers, b->n_slices * sizeof(float), cudaMemcpyHostToDevice));
   }
   if (b->dtype == GR_DTYPE_U16_RAW || b->dtype == GR_DTYPE_U16_LINEAR) {
-    GR_CUDA(cudaMalloc(&d_flat, p->n_det * sizeof(float)));
-    GR_CUDA(cudaMalloc(&d_dark, p->n_det * sizeof(float)));
-    GR_CUDA(cudaMemcpy(d_flat, b->flat, p->n_det * sizeof(float), cudaMemcpyHostToDevice));
-    GR_CUDA(cudaMemcpy(d_dark, b->dark, p->n_det * sizeof(float), cudaMemcpyHostToDevice));
+    const size_t nf = (size_t)(b->n_slices - 1) * b->flat_stride + p->n_det;
+    GR_CUDA(cudaMalloc(&d_flat, nf * sizeof(float)));
+    GR_CUDA(cudaMalloc(&d_dark, nf * sizeof(float)));
+    GR_CUDA(cudaMemcpy(d_flat, b->flat, nf * sizeof(float), cudaMemcpyHostToDevice));
+    GR_CUDA(cudaMemcpy(d_dark, b->dark, nf * sizeof(float), cudaMemcpyHostToDevice));
   }
   const int n_pairs = (b->n_slices + 1) / 2;
   const int n_chunks = (n_pairs + p->max_pairs - 1) / p->max_pairs;
@@ -899,7 +1031,8 @@ int gr_reconstruct_host(gr_plan* p, const gr_batch_desc* b, void* stream) {
     const long slice_in_el = (long)p->n_ang * p->n_det;
     const long slice_out_el = (long)p->M0 * b->out_stride;
     rc = launch_chunk(p, pairs, n_valid, s0, dbase, dbase + slice_in, 2 * slice_in_el, b->dtype,
-                      d_centers, d_flat, d_dark, p->d_out[k], p->d_out[k] + slice_out_el,
+                      d_centers, d_flat, d_dark, b->flat_stride, p->d_out[k],
+                      p->d_out[k] + slice_out_el,
                       2 * slice_out_el, b->out_stride, st);
     if (rc) { cleanup(); return rc; }
     GR_CUDA(cudaEventRecord(p->ev_comp[k], st));
@@ -1005,7 +1138,7 @@ extern "C" int gr_reconstruct_pair_noalloc(gr_plan* p, const float* sino1, const
   // launch_grid zeroes the queue head in-stream before the gridding kernel
   PhaseArgs ph{nullptr, p->center, 0, n_valid, p->d_filt, pq, p->J, p->pdim, 1};
   GR_CUDA(launch_phase(ph, st));
-  SpectraArgs sa{sino1, s2, 0, n_valid, 0, nullptr, nullptr, pq, spec, p->d_tw_p, p->n_det,
+  SpectraArgs sa{sino1, s2, 0, n_valid, 0, nullptr, nullptr, 0, pq, spec, p->d_tw_p, p->n_det,
                  p->n_ang, p->pdim, p->J, 1};
   GR_CUDA(launch_spectra(sa, GR_DTYPE_F32, st));
   GridArgs ga{spec, H, part, queue, p->d_items, p->d_runs, p->d_split_list, p->n_split_tiles,
@@ -1021,3 +1154,124 @@ extern "C" int gr_reconstruct_pair_noalloc(gr_plan* p, const float* sino1, const
   p->launches += 5;
   return GR_OK;
 }
+
+// ------------------------------------------------------------------ CUDA graphs
+// A graph holds the launches of one or more batches, recorded once by stream
+// capture and replayed with one cudaGraphLaunch.  Batches of one plan run in
+// order on one branch (they share its workspaces); different plans get their
+// own branches, forked from and joined to the capture stream, so batches of
+// different shapes can overlap on the GPU.
+
+struct gr_graph {
+  int device = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long launches = 0;
+};
+
+extern "C" {
+
+int gr_graph_create(const gr_graph_item* items, int n_items, gr_graph** out) {
+  using namespace gr;
+  if (!items || n_items < 1 || !out) return fail(GR_ERR_ARG, "graph: items and out required");
+  *out = nullptr;
+  const int dev = items[0].plan ? items[0].plan->device : -1;
+  std::vector<gr_plan*> plans;
+  for (int i = 0; i < n_items; ++i) {
+    gr_plan* p = items[i].plan;
+    if (!p) return fail(GR_ERR_ARG, "graph: item %d has no plan", i);
+    if (p->device != dev) return fail(GR_ERR_ARG, "graph: all plans must be on one device");
+    if (p->timing) return fail(GR_ERR_ARG, "graph: disable stage timing before capture");
+    int rc = validate_batch(p, &items[i].batch);
+    if (rc) return rc;
+    if (std::find(plans.begin(), plans.end(), p) == plans.end()) plans.push_back(p);
+  }
+  DeviceGuard g(dev);
+  const size_t np = plans.size();
+  cudaStream_t s0 = nullptr;
+  std::vector<cudaStream_t> br(np, nullptr);
+  std::vector<cudaEvent_t> join(np, nullptr);
+  cudaEvent_t fork = nullptr;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  auto cleanup = [&]() {
+    for (auto s : br)
+      if (s) cudaStreamDestroy(s);
+    for (auto e : join)
+      if (e) cudaEventDestroy(e);
+    if (fork) cudaEventDestroy(fork);
+    if (s0) cudaStreamDestroy(s0);
+  };
+  cudaError_t e = cudaStreamCreateWithFlags(&s0, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaEventCreateWithFlags(&fork, cudaEventDisableTiming);
+  for (size_t k = 0; k < np && e == cudaSuccess; ++k) {
+    e = cudaStreamCreateWithFlags(&br[k], cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&join[k], cudaEventDisableTiming);
+  }
+  if (e != cudaSuccess) {
+    cleanup();
+    return fail(GR_ERR_CUDA, "graph set-up: %s", cudaGetErrorString(e));
+  }
+  long launches0 = 0;
+  for (auto p : plans) launches0 += p->launches;
+  e = cudaStreamBeginCapture(s0, cudaStreamCaptureModeRelaxed);
+  if (e != cudaSuccess) {
+    cleanup();
+    return fail(GR_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  }
+  int rc = GR_OK;
+  e = cudaEventRecord(fork, s0);
+  for (size_t k = 0; k < np && e == cudaSuccess && rc == GR_OK; ++k) {
+    e = cudaStreamWaitEvent(br[k], fork, 0);
+    for (int i = 0; i < n_items && e == cudaSuccess && rc == GR_OK; ++i)
+      if (items[i].plan == plans[k]) rc = gr_reconstruct_batch(plans[k], &items[i].batch, br[k]);
+    if (e == cudaSuccess && rc == GR_OK) e = cudaEventRecord(join[k], br[k]);
+    if (e == cudaSuccess && rc == GR_OK) e = cudaStreamWaitEvent(s0, join[k], 0);
+  }
+  const std::string err_rc = rc ? g_err : std::string();
+  cudaError_t ee = cudaStreamEndCapture(s0, &graph);
+  if (e == cudaSuccess) e = ee;
+  if (rc == GR_OK && e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+  cleanup();
+  long launches1 = 0;
+  for (auto p : plans) launches1 += p->launches;
+  if (rc != GR_OK || e != cudaSuccess) {
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    cudaGetLastError();
+    if (rc != GR_OK) return fail(rc, "graph capture: %s", err_rc.c_str());
+    return fail(GR_ERR_CUDA, "graph capture: %s", cudaGetErrorString(e));
+  }
+  gr_graph* gg = new gr_graph;
+  gg->device = dev;
+  gg->graph = graph;
+  gg->exec = exec;
+  gg->launches = launches1 - launches0;
+  *out = gg;
+  return GR_OK;
+}
+
+int gr_graph_launch(gr_graph* g, void* stream) {
+  using namespace gr;
+  if (!g) return fail(GR_ERR_ARG, "null graph");
+  DeviceGuard guard(g->device);
+  GR_CUDA(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+  return GR_OK;
+}
+
+int gr_graph_launch_count(const gr_graph* g, long* launches) {
+  if (!g || !launches) return gr::fail(GR_ERR_ARG, "null argument");
+  *launches = g->launches;
+  return GR_OK;
+}
+
+int gr_graph_destroy(gr_graph* g) {
+  if (!g) return GR_OK;
+  gr::DeviceGuard guard(g->device);
+  if (g->exec) cudaGraphExecDestroy(g->exec);
+  if (g->graph) cudaGraphDestroy(g->graph);
+  delete g;
+  return GR_OK;
+}
+
+}  // extern "C"

@@ -31,7 +31,9 @@ EXPORTS = ("gr_params_default", "gr_filter_code", "gr_plan_create", "gr_plan_des
            "gr_plan_set_timing", "gr_plan_stage_times", "gr_reconstruct_pair_noalloc",
            "gr_plan_device_status", "gr_selftest_wait_timeout", "gr_ring_workspace_bytes",
            "gr_ring_removal", "gr_shift_pad", "gr_crop_center", "gr_entropy_workspace_bytes",
-           "gr_entropy", "gr_reconstruct_padded", "gr_center_search")
+           "gr_entropy", "gr_reconstruct_padded", "gr_center_search", "gr_graph_create",
+           "gr_graph_launch", "gr_graph_launch_count", "gr_graph_destroy", "gr_plan_autotune",
+           "gr_plan_tuning")
 STAGES = ("phase", "spectra", "grid", "cols", "rows_deapod")
 
 
@@ -51,7 +53,11 @@ class GrParams(C.Structure):
 class GrBatch(C.Structure):
     _fields_ = [("n_slices", C.c_int), ("dtype", C.c_int), ("sinos", C.c_void_p),
                 ("centers", C.c_void_p), ("flat", C.c_void_p), ("dark", C.c_void_p),
-                ("outs", C.c_void_p), ("out_stride", C.c_long)]
+                ("outs", C.c_void_p), ("out_stride", C.c_long), ("flat_stride", C.c_long)]
+
+
+class GrGraphItem(C.Structure):
+    _fields_ = [("plan", C.c_void_p), ("batch", GrBatch)]
 
 
 _lib = None
@@ -102,6 +108,12 @@ def lib():
         L.gr_reconstruct_padded.argtypes = [vp, vp, i_, i_, i_, f_, vp, l_, vp]
         L.gr_center_search.argtypes = [vp, vp, vp, i_, i_, C.POINTER(f_), i_, f_, f_, i_,
                                        C.POINTER(f_), C.POINTER(i_), vp, vp]
+        L.gr_graph_create.argtypes = [C.c_void_p, i_, C.POINTER(C.c_void_p)]
+        L.gr_graph_launch.argtypes = [vp, vp]
+        L.gr_graph_launch_count.argtypes = [vp, C.POINTER(C.c_long)]
+        L.gr_graph_destroy.argtypes = [vp]
+        L.gr_plan_autotune.argtypes = [vp, vp]
+        L.gr_plan_tuning.argtypes = [vp, C.POINTER(i_), C.POINTER(i_)]
         _lib = L
     return _lib
 
@@ -240,6 +252,16 @@ class Plan:
         _check(lib().gr_plan_stage_times(self._h, ms, C.byref(n)), "gr_plan_stage_times")
         return dict(zip(STAGES, list(ms))), n.value
 
+    def autotune(self, stream=None):
+        """Times the gridding item cap and column-FFT group width; returns the choice."""
+        _check(lib().gr_plan_autotune(self._h, _stream_ptr(stream)), "gr_plan_autotune")
+        return self.tuning()
+
+    def tuning(self):
+        cap, g = C.c_int(), C.c_int()
+        _check(lib().gr_plan_tuning(self._h, C.byref(cap), C.byref(g)), "gr_plan_tuning")
+        return {"item_cap": cap.value, "cols_group": g.value}
+
     def work_stats(self):
         a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_long()
         _check(lib().gr_plan_work_stats(self._h, C.byref(a), C.byref(b), C.byref(c),
@@ -253,25 +275,36 @@ class Plan:
                                          _ptr(out2), stride, _stream_ptr(stream)),
                "gr_reconstruct_pair")
 
-    def _batch(self, n_slices, dtype, sinos, centers, flat, dark, outs, out_stride):
+    def _batch(self, n_slices, dtype, sinos, centers, flat, dark, outs, out_stride,
+               flat_stride=0):
         b = GrBatch()
         b.n_slices, b.dtype = int(n_slices), int(dtype)
         b.sinos, b.centers, b.flat, b.dark, b.outs = sinos, centers, flat, dark, outs
         b.out_stride = int(out_stride)
+        b.flat_stride = int(flat_stride)
         return b
 
     def reconstruct_batch(self, sinos, outs, centers=None, flat=None, dark=None, dtype=None,
                           stream=None):
         """Device tensors: sinos (S, n_ang, n_det) f32/f16/bf16/uint16, outs (S, M0, stride)."""
+        b = self.batch_desc(sinos, outs, centers, flat, dark, dtype)
+        _check(lib().gr_reconstruct_batch(self._h, C.byref(b), _stream_ptr(stream)),
+               "gr_reconstruct_batch")
+
+    def batch_desc(self, sinos, outs, centers=None, flat=None, dark=None, dtype=None):
+        """GrBatch for device tensors (as reconstruct_batch takes them)."""
         import torch
         if dtype is None:
             dtype = {torch.float32: DTYPE_F32, torch.float16: DTYPE_F16,
                      torch.bfloat16: DTYPE_BF16, torch.uint16: DTYPE_U16_RAW,
                      torch.int16: DTYPE_U16_RAW}[sinos.dtype]
-        b = self._batch(sinos.shape[0], dtype, _ptr(sinos), _ptr(centers), _ptr(flat),
-                        _ptr(dark), _ptr(outs), outs.shape[-1])
-        _check(lib().gr_reconstruct_batch(self._h, C.byref(b), _stream_ptr(stream)),
-               "gr_reconstruct_batch")
+        fs = flat.shape[-1] if flat is not None and flat.dim() == 2 else 0  # per-slice rows
+        return self._batch(sinos.shape[0], dtype, _ptr(sinos), _ptr(centers), _ptr(flat),
+                           _ptr(dark), _ptr(outs), outs.shape[-1], fs)
+
+    def capture_batch(self, sinos, outs, centers=None, flat=None, dark=None, dtype=None):
+        """A Graph that replays reconstruct_batch on these buffers with one launch."""
+        return Graph([(self, self.batch_desc(sinos, outs, centers, flat, dark, dtype))])
 
     def reconstruct_host(self, sinos: np.ndarray, outs: np.ndarray, centers=None, flat=None,
                          dark=None, dtype=None, stream=0):
@@ -290,9 +323,47 @@ class Plan:
         if centers is not None and isinstance(centers, np.ndarray):
             centers = np.ascontiguousarray(centers, np.float32)
             keep.append(centers)
+        fs = flat.shape[-1] if flat is not None and len(flat.shape) == 2 else 0
         b = self._batch(sinos.shape[0], dtype, addr(sinos), addr(centers), addr(flat), addr(dark),
-                        addr(outs), outs.shape[-1])
+                        addr(outs), outs.shape[-1], fs)
         _check(lib().gr_reconstruct_host(self._h, C.byref(b), stream), "gr_reconstruct_host")
+
+
+class Graph:
+    """Batches of one or more plans recorded into one CUDA graph (gr_graph_create).
+
+    items: list of (Plan, GrBatch).  The tensors behind the batches must stay
+    alive while the graph is used: their addresses are baked in."""
+
+    def __init__(self, items):
+        arr = (GrGraphItem * len(items))()
+        for k, (plan, b) in enumerate(items):
+            arr[k].plan = plan.handle
+            arr[k].batch = b
+        h = C.c_void_p()
+        _check(lib().gr_graph_create(C.cast(arr, C.c_void_p), len(items), C.byref(h)),
+               "gr_graph_create")
+        self._h = h
+        self._plans = [p for p, _ in items]
+
+    def launch(self, stream=None):
+        _check(lib().gr_graph_launch(self._h, _stream_ptr(stream)), "gr_graph_launch")
+
+    def launches(self) -> int:
+        n = C.c_long()
+        _check(lib().gr_graph_launch_count(self._h, C.byref(n)), "gr_graph_launch_count")
+        return n.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gr_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class GridRec:

@@ -146,6 +146,29 @@ def random_ellipse_sinogram(seed: int, n_det: int = 2048, n_ang: int = 1500,
     return poisson_log(p, photons, seed), center
 
 
+def random_ellipse_raw(seed: int, n_det: int, n_ang: int, device, flat_mean: float = 40000.0,
+                       flat_spread: float = 0.05, dark_mean: float = 100.0):
+    """Raw uint16 counts of the random-ellipse slice `seed` on a torch device:
+    Poisson(flat * exp(-p)) + dark, with this slice's own flat (flat_mean
+    +-flat_spread per pixel) and dark (dark_mean + N(0, 2)) rows.
+
+    Returns (raw as an int16 tensor view of the uint16 bits, flat, dark, center)."""
+    import torch
+    ell = random_ellipses(seed)
+    rng = np.random.default_rng(seed + 1_000_003)
+    center = n_det / 2.0 + float(rng.uniform(-2.0, 2.0))
+    p = line_integrals(ell, n_det, angles_deg(n_ang), center, device=device) / (n_det / 2.0)
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed) + 7)
+    u = torch.rand(n_det, generator=g, device=device, dtype=torch.float64)
+    flat = flat_mean * (1.0 + flat_spread * (2.0 * u - 1.0))
+    dark = dark_mean + 2.0 * torch.randn(n_det, generator=g, device=device, dtype=torch.float64)
+    counts = torch.poisson(flat[None, :] * torch.exp(-p), generator=g) + torch.round(dark)[None, :]
+    raw = counts.clamp(0, 65535).to(torch.int32)
+    raw = torch.where(raw > 32767, raw - 65536, raw).to(torch.int16)  # uint16 bits
+    return raw, flat.to(torch.float32), dark.to(torch.float32), center
+
+
 def raw_counts(p, seed: int = 0, flat_mean: float = 40000.0, flat_spread: float = 0.05,
                dark_mean: float = 100.0):
     """uint16 counts Poisson(flat*exp(-p)) + dark, plus the flat and dark rows.
