@@ -533,25 +533,30 @@ __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
     // Software pipeline over runs: the samples of run r+1 are loaded into
     // registers (lane l holds j = jlo + l and jlo + l + 32) while run r is
     // gridded from the shared staging buffer.
+    // The run record and its direction travel with the prefetch too, so no
+    // dependent global load sits at the start of a run.
     float2 nA0 = make_float2(0.f, 0.f), nA1 = nA0, nB0 = nA0, nB1 = nA0;
+    Run nrun{0, 0, -1, 1};
+    float2 ndir = make_float2(0.f, 0.f);
     auto prefetch = [&](int rr) {
       if (rr >= it.run_end) return;
-      const Run nr = a.runs[rr];
-      const float2* pa = specA + (size_t)nr.dir * a.J;
-      const float2* pb = specB + (size_t)nr.dir * a.J;
-      if (nr.jlo + lane <= nr.jhi) {
-        nA0 = __ldg(&pa[nr.jlo + lane]);
-        nB0 = __ldg(&pb[nr.jlo + lane]);
+      nrun = a.runs[rr];
+      ndir = __ldg(&a.dir[nrun.dir]);
+      const float2* pa = specA + (size_t)nrun.dir * a.J;
+      const float2* pb = specB + (size_t)nrun.dir * a.J;
+      if (nrun.jlo + lane <= nrun.jhi) {
+        nA0 = __ldg(&pa[nrun.jlo + lane]);
+        nB0 = __ldg(&pb[nrun.jlo + lane]);
       }
-      if (nr.jlo + 32 + lane <= nr.jhi) {
-        nA1 = __ldg(&pa[nr.jlo + 32 + lane]);
-        nB1 = __ldg(&pb[nr.jlo + 32 + lane]);
+      if (nrun.jlo + 32 + lane <= nrun.jhi) {
+        nA1 = __ldg(&pa[nrun.jlo + 32 + lane]);
+        nB1 = __ldg(&pb[nrun.jlo + 32 + lane]);
       }
     };
     prefetch(it.run_begin);
     for (int r = it.run_begin; r < it.run_end; ++r) {
-      const Run run = a.runs[r];
-      const float2 d = __ldg(&a.dir[run.dir]);
+      const Run run = nrun;
+      const float2 d = ndir;
       stage[lane] = make_float4(nA0.x, nA0.y, nB0.x, nB0.y);
       stage[32 + lane] = make_float4(nA1.x, nA1.y, nB1.x, nB1.y);
       __syncwarp();
