@@ -275,6 +275,21 @@ def measure_slice_pipeline(G, sinos, th, n, a, dev, stream, peak):
                                 "ms_per_candidate": 1000.0 * tc / len(shifts),
                                 "timing": "host wall clock (the call synchronises)"}
         p2.device_status()
+    # FBP comparator on 2 of the slices (n^2 x angles work per slice)
+    fb = G.FBP(n, a, th, max_slices=2, device=dev.index or 0)
+    t = timed(lambda: fb.reconstruct(src[:2], stream=stream), 2)
+    out["fbp_comparator"] = {"slices_per_s": 2 / t, "ms_per_slice": 1000.0 * t / 2}
+    fb.close()
+    # cross-correlation axis search: two n x 512 projections, 41 x 5 translations
+    tpl = src[0, :512].contiguous()
+    roi = (n // 8, n - n // 8 - 1, 64, 447)
+    troi = tpl[roi[2]:roi[3] + 1, roi[0]:roi[1] + 1].contiguous()
+    t0 = time.perf_counter()
+    G.xcorr_scores(troi, src[1, :512].contiguous(), roi, -20.0, -2.0, 1.0, 1.0, 41, 5,
+                   stream=stream)
+    out["xcorr_search"] = {"ms": 1000.0 * (time.perf_counter() - t0), "translations": 205,
+                           "image": f"{n}x512", "roi": list(roi),
+                           "timing": "host wall clock (the call synchronises)"}
     del x, src
     return out
 

@@ -304,6 +304,35 @@ int gr_center_search(gr_plan* plan, const float* sino1, const float* sino2, int 
                      const float* shifts, int n_cand, float hist_lo, float hist_hi, int nbins,
                      float* scores, int* best, float* best_images, void* stream);
 
+/* Rotation-axis search by cross-correlation <- find_shift's brute-force search
+ * (data_interp + cross_correlation, find_shift/src/main/find_shift.cpp:1975-2076;
+ * GPU twin cross_correlation.cu:19-413).  templ_roi: the (roi_y1-roi_y0+1) x
+ * (roi_x1-roi_x0+1) template (device, float); match: height x width (device).
+ * For every translation (tx0 + i dtx, ty0 + k dty), i < n_tx, k < n_ty, the match
+ * image is sampled at (nx - tx, ny - ty) over the ROI by weight-normalised bilinear
+ * interpolation and scored by normalised cross-correlation with the template
+ * (double arithmetic, as the reference's CPU path; the reference's GPU path uses
+ * 8-bit texture filtering weights instead).  scores: host, n_ty x n_tx doubles.
+ * Synchronises `stream`. */
+int gr_xcorr_scores(const float* templ_roi, const float* match, int width, int height, int roi_x0,
+                    int roi_x1, int roi_y0, int roi_y1, double tx0, double ty0, double dtx,
+                    double dty, int n_tx, int n_ty, double* scores, void* stream);
+
+/* FBP comparator <- OptimizedFBP, the reference's ReconAlgorithm filtered
+ * backprojection (gridrec/GPU/filteredbackprojection.cpp:190-330; tomo_recon's GPU
+ * FBP, gridrec/GPU/fbp.cu:22-169, is the same pipeline with a floor() sampler).
+ * Each projection row, gated to (-5, 5), is filtered by 1 - sqrt(|k - n/2|/(n/2))
+ * in frequency (unnormalised FFT pair), and pixel (x, y) of the n x n image sums
+ * filtered[a][(int)((r + 1) n/2)] over the angles, r = x cos + y sin with x, y in
+ * [-1, 1).  n_det a power of two in [16, 8192].  sinos: n_slices x n_ang x n_det
+ * (device); recons: n_slices x n_det x n_det (device, row = y).  One slice per
+ * call of the reference; max_slices per launch here. */
+typedef struct gr_fbp gr_fbp;
+int gr_fbp_create(int n_det, int n_ang, const float* theta_deg, int max_slices, int device,
+                  gr_fbp** fbp);
+int gr_fbp_reconstruct(gr_fbp* fbp, const float* sinos, int n_slices, float* recons, void* stream);
+int gr_fbp_destroy(gr_fbp* fbp);
+
 #ifdef __cplusplus
 }
 #endif

@@ -5,6 +5,8 @@
 #   oracle/_ref/libgridrec_ref64.so   the same sources with float -> double,
 #                                     made on temporary copies outside the repo
 #   oracle/_ref/libgridrec_refb.so    GridrecCPP 5.2 C API (centre, sampl, filter name)
+#   oracle/_ref/libfbp_ref.so         OptimizedFBP (CPU filtered backprojection, the
+#                                     ReconAlgorithm FBP comparator)
 #   oracle/_ref/libprep_ref.so        ring removal, shift/half-padding and entropy of the
 #                                     reference drivers (line ranges written to a
 #                                     temporary directory, see prep_ref_driver.cpp)
@@ -52,15 +54,21 @@ $CXX $FLAGS -fpermissive -I"$CPP" "$CPP/grid.cpp" "$CPP/fftgr.cpp" \
   "$CPP/filters.cpp" "$CPP/pswf.cpp" "$CPP/grid_math.cpp" "$HERE/refb_driver.cpp" \
   -o "$OUT/libgridrec_refb.so"
 
+# Oracle D: the reference's CPU OptimizedFBP.
+$CXX $FLAGS -I"$GPU" -x c++ "$GPU/filteredbackprojection.cpp" "$GPU/recon_algorithm.cpp" \
+  "$GPU/fft_nr.cpp" "$HERE/fbp_ref_driver.cpp" -o "$OUT/libfbp_ref.so"
+
 # Oracle C: slice-pipeline steps of tomo_recon / find_shift.
 FS="$REF/find_shift/src/main/find_shift.cpp"
 TR="$GPU/tomo_recon.cpp"
 sed -n '3905,3972p' "$TR" > "$TMP/ring_ref.inc"
 sed -n '2078,2115p' "$FS" > "$TMP/entropy_ref.inc"
 sed -n '3708,3807p' "$TR" > "$TMP/shiftpad_ref.inc"
+sed -n '1975,2076p' "$FS" > "$TMP/xcorr_ref.inc"
 grep -q 'void RingCorrectionSinogram' "$TMP/ring_ref.inc"
 grep -q 'float entropy( float\* data' "$TMP/entropy_ref.inc"
 grep -q 'float kk = k - xoffset' "$TMP/shiftpad_ref.inc"
+grep -q 'void data_interp' "$TMP/xcorr_ref.inc"
 $CXX $FLAGS -I"$TMP" "$HERE/prep_ref_driver.cpp" -o "$OUT/libprep_ref.so"
 
 echo "built: $(ls "$OUT")"

@@ -440,3 +440,112 @@ double orc_entropy(const float* data, long n, float vmin, float vmax, int num_hi
   free(hist);
   return e;
 }
+
+/* Cross-correlation score of find_shift's brute-force search (data_interp +
+ * cross_correlation, find_shift/src/main/find_shift.cpp:1975-2076), float64:
+ * the match image is sampled at (nx - tx, ny - ty) for every ROI pixel by
+ * bilinear interpolation over the in-image neighbours normalised by their
+ * weight (0 when the weight is <= 1e-5); with M_avg the ROI mean of the samples,
+ * score = sum (T - T_avg)(M - M_avg) / (T_rms sqrt(sum (M - M_avg)^2)), 0 when
+ * |T_rms| or the sum is <= 1e-5; T_rms = sqrt(sum (T - T_avg)^2) over the ROI
+ * template (roi_h x roi_w, row-major). */
+double orc_xcorr_score(const double* templ, const double* match, int width, int height, int x0,
+                       int x1, int y0, int y1, double tx, double ty) {
+  const int rw = x1 - x0 + 1, rh = y1 - y0 + 1;
+  const long area = (long)rw * rh;
+  double tavg = 0.0, trms = 0.0;
+  for (long i = 0; i < area; ++i) tavg += templ[i];
+  tavg /= (double)area;
+  for (long i = 0; i < area; ++i) trms += (templ[i] - tavg) * (templ[i] - tavg);
+  trms = sqrt(trms);
+  double* m = (double*)malloc(area * sizeof(double));
+  double mavg = 0.0;
+  for (int ny = y0; ny <= y1; ++ny)
+    for (int nx = x0; nx <= x1; ++nx) {
+      const double x = nx - tx, y = ny - ty;
+      const int a = (int)floor(x), b = (int)floor(y);
+      double pix = 0.0, w = 0.0;
+      const double ax = a + 1 - x, bx = x - a, ay = b + 1 - y, by = y - b;
+      const int xa = a >= 0 && a < width, xb = a + 1 >= 0 && a + 1 < width;
+      const int ya = b >= 0 && b < height, yb = b + 1 >= 0 && b + 1 < height;
+      if (xa && ya) { pix += match[(long)b * width + a] * ax * ay; w += ax * ay; }
+      if (xb && ya) { pix += match[(long)b * width + a + 1] * bx * ay; w += bx * ay; }
+      if (xa && yb) { pix += match[(long)(b + 1) * width + a] * ax * by; w += ax * by; }
+      if (xb && yb) { pix += match[(long)(b + 1) * width + a + 1] * bx * by; w += bx * by; }
+      pix = w > 1e-5 ? pix / w : 0.0;
+      m[(long)(ny - y0) * rw + nx - x0] = pix;
+      mavg += pix;
+    }
+  mavg /= (double)area;
+  double cc = 0.0, msq = 0.0;
+  for (long i = 0; i < area; ++i) {
+    cc += (templ[i] - tavg) * (m[i] - mavg);
+    msq += (m[i] - mavg) * (m[i] - mavg);
+  }
+  free(m);
+  return (fabs(trms) > 1e-5 && fabs(msq) > 1e-5) ? cc / (trms * sqrt(msq)) : 0.0;
+}
+
+/* OptimizedFBP (gridrec/GPU/filteredbackprojection.cpp:190-330): every projection
+ * row, gated to (-5, 5) (values outside become 0), is filtered by an FFT, a
+ * multiplication of bin k by 1 - sqrt(|(k - n/2) / (n/2)|), and an unnormalised
+ * inverse FFT (float64 here); pixel (x, y) of the n x n image (row y) then sums,
+ * over the angles in order, filtered[a][(int)((r + 1) n/2)] for -1 <= r < 1, with
+ * x = (col - n/2)/(n/2), y = (row - n/2)/(n/2), r = x cos + y sin -- all in float
+ * as the reference, whose sines/cosines come from the degree list via
+ * (theta * PI) / 180 stored as float.  n_det must be a power of two. */
+int orc_optimized_fbp(int n_det, int n_ang, const float* theta_deg, const float* sino,
+                      double* recon) {
+  const int n = n_det;
+  if (n < 2 || (n & (n - 1))) return -1;
+  const double PI_REF = 3.1415926535897932385;  /* fft.h:5 */
+  float* cs = (float*)malloc(n_ang * sizeof(float));
+  float* sn = (float*)malloc(n_ang * sizeof(float));
+  float* lut = (float*)malloc(n * sizeof(float));
+  double* row = (double*)malloc(2 * (size_t)n * sizeof(double));
+  double* filt = (double*)malloc((size_t)n_ang * n * sizeof(double));
+  for (int a = 0; a < n_ang; ++a) {
+    const float th = (float)((theta_deg[a] * PI_REF) / 180.0);
+    sn[a] = (float)sin(th);
+    cs[a] = (float)cos(th);
+  }
+  for (int k = 0; k < n; ++k) {
+    const float t = (float)(k - (float)(n / 2)) / ((float)(n / 2));
+    lut[k] = (float)(1 - sqrt(fabs(t)));
+  }
+  for (int a = 0; a < n_ang; ++a) {
+    for (int k = 0; k < n; ++k) {
+      const float v = sino[(long)a * n + k];
+      row[2 * k] = (v > -5.0f && v < 5.0f) ? v : 0.0;
+      row[2 * k + 1] = 0.0;
+    }
+    orc_fft1d(row, n, +1);
+    for (int k = 0; k < n; ++k) {
+      row[2 * k] *= lut[k];
+      row[2 * k + 1] *= lut[k];
+    }
+    orc_fft1d(row, n, -1);
+    for (int k = 0; k < n; ++k) filt[(long)a * n + k] = row[2 * k];
+  }
+  const float h = (float)n / 2.0f;
+  for (int yi = 0; yi < n; ++yi) {
+    const float y = ((float)(yi - h)) / h;
+    for (int xi = 0; xi < n; ++xi) {
+      const float x = ((float)(xi - h)) / h;
+      double acc = 0.0;
+      for (int a = 0; a < n_ang; ++a) {
+        const float xc = x * cs[a];
+        const float ys = y * sn[a];
+        const float r = xc + ys;
+        if (r >= -1 && r < 1) {
+          int k = (int)((r + 1) * h);
+          if (k > n - 1) k = n - 1; /* the reference reads outside the row there */
+          acc += filt[(long)a * n + k];
+        }
+      }
+      recon[(long)yi * n + xi] = acc;
+    }
+  }
+  free(cs); free(sn); free(lut); free(row); free(filt);
+  return 0;
+}

@@ -36,6 +36,10 @@ void orc_ring_removal(double* data, int n_det, int n_ang, double ring_coeff, int
 void orc_shift_pad(const float* in, float* out, int n_det, int n_ang, float xoffset, int out_width);
 void orc_crop(const float* rec, long rec_stride, float* out, int n, int offset, int radius);
 double orc_entropy(const float* data, long n, float vmin, float vmax, int num_hist_bin);
+int orc_optimized_fbp(int n_det, int n_ang, const float* theta_deg, const float* sino,
+                      double* recon);
+double orc_xcorr_score(const double* templ, const double* match, int width, int height, int x0,
+                       int x1, int y0, int y1, double tx, double ty);
 
 #ifdef __cplusplus
 }

@@ -62,6 +62,10 @@ def port_lib():
         lib.orc_crop.argtypes = [_fp, C.c_long, _fp, C.c_int, C.c_int, C.c_int]
         lib.orc_crop.restype = None
         lib.orc_entropy.argtypes = [_fp, C.c_long, C.c_float, C.c_float, C.c_int]
+        lib.orc_xcorr_score.argtypes = [_dp, _dp] + [C.c_int] * 6 + [C.c_double, C.c_double]
+        lib.orc_xcorr_score.restype = C.c_double
+        lib.orc_optimized_fbp.argtypes = [C.c_int, C.c_int, _fp, _fp, _dp]
+        lib.orc_optimized_fbp.restype = C.c_int
         lib.orc_entropy.restype = C.c_double
         _port = lib
     return _port
@@ -165,6 +169,25 @@ def port_entropy(img, vmin, vmax, nbins):
     return port_lib().orc_entropy(x, x.size, float(vmin), float(vmax), int(nbins))
 
 
+def port_optimized_fbp(sino, theta_deg):
+    """OptimizedFBP of one (n_ang, n_det) sinogram -> (n_det, n_det) float64 image."""
+    n_ang, n = sino.shape
+    out = np.zeros((n, n))
+    rc = port_lib().orc_optimized_fbp(n, n_ang, np.ascontiguousarray(theta_deg, np.float32),
+                                      np.ascontiguousarray(sino, np.float32), out)
+    if rc:
+        raise ValueError("orc_optimized_fbp: n_det must be a power of two")
+    return out
+
+
+def port_xcorr_score(templ_roi, match, roi, tx, ty):
+    """find_shift's brute-force score for one translation; roi = (x0, x1, y0, y1)."""
+    h, w = match.shape
+    return port_lib().orc_xcorr_score(np.ascontiguousarray(templ_roi, np.float64),
+                                      np.ascontiguousarray(match, np.float64), w, h, *roi,
+                                      float(tx), float(ty))
+
+
 # ---------------------------------------------------------------- reference builds
 
 def ref_available() -> bool:
@@ -188,6 +211,9 @@ def _ref_lib(name, real):
             lib.ref_entropy.restype = C.c_float
             lib.ref_shift_pad.argtypes = [rp, rp, C.c_int, C.c_int, C.c_float, rp]
             lib.ref_shift_pad.restype = None
+            dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+            lib.ref_xcorr_score.argtypes = [dp, dp] + [C.c_int] * 6 + [C.c_double, C.c_double]
+            lib.ref_xcorr_score.restype = C.c_double
         elif name == "libgridrec_refb.so":
             lib.refb_gridrec_pair.argtypes = [C.c_int, C.c_int, rp, C.c_float, C.c_char_p,
                                               C.c_float, C.c_float, C.c_int, rp, rp, rp, rp,
@@ -285,3 +311,34 @@ def ref_shift_pad(sino1, sino2, xoffset):
     lib.ref_shift_pad(np.ascontiguousarray(sino1, np.float32),
                       np.ascontiguousarray(sino2, np.float32), n_det, n_ang, float(xoffset), out)
     return out
+
+
+def ref_xcorr_score(templ_roi, match, roi, tx, ty):
+    """The reference's own data_interp + cross_correlation for one translation."""
+    lib = _ref_lib("libprep_ref.so", np.float32)
+    h, w = match.shape
+    return float(lib.ref_xcorr_score(np.ascontiguousarray(templ_roi, np.float64),
+                                     np.ascontiguousarray(match, np.float64), w, h, *roi,
+                                     float(tx), float(ty)))
+
+
+def ref_optimized_fbp(sino, theta_deg):
+    """The reference's own CPU OptimizedFBP -> (n_det, n_det) float32 image."""
+    path = os.path.join(_REF, "libfbp_ref.so")
+    if "fbp" not in _refs:
+        if not os.path.exists(path):
+            raise RuntimeError(f"reference oracle not built: {path}")
+        lib = C.CDLL(path)
+        fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+        lib.ref_optimized_fbp.argtypes = [C.c_int, C.c_int, fp, fp, fp]
+        lib.ref_optimized_fbp.restype = None
+        _refs["fbp"] = lib
+    n_ang, n = sino.shape
+    out = np.zeros((n, n), np.float32)
+    _refs["fbp"].ref_optimized_fbp(n, n_ang, np.ascontiguousarray(theta_deg, np.float32),
+                                   np.ascontiguousarray(sino, np.float32).copy(), out)
+    return out
+
+
+def fbp_ref_available() -> bool:
+    return os.path.exists(os.path.join(_REF, "libfbp_ref.so"))

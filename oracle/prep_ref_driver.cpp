@@ -6,6 +6,8 @@
 //   entropy_ref.inc   entropy()                find_shift/src/main/find_shift.cpp:2078-2115
 //   shiftpad_ref.inc  shift + half-padding     gridrec/GPU/tomo_recon.cpp:3708-3807
 //                     (body of GridRecSlices; expects the locals declared below)
+//   xcorr_ref.inc     data_interp + cross_correlation (brute-force axis search)
+//                                              find_shift/src/main/find_shift.cpp:1975-2076
 #include <cmath>
 #include <cstdlib>
 #include <vector>
@@ -13,6 +15,7 @@ using namespace std;  // the reference translation units see std names unqualifi
 
 #include "ring_ref.inc"
 #include "entropy_ref.inc"
+#include "xcorr_ref.inc"
 
 extern "C" {
 
@@ -49,6 +52,24 @@ void ref_shift_pad(const float* sino1, const float* sino2, int n_det, int n_ang,
   for (i = 0; i < 2 * num_ray_half_padding * n_ang; i++) sinogram[i] = 0.0f;
 #include "shiftpad_ref.inc"
   (void)i;
+}
+
+// One translation of the brute-force search, as find_shift.cpp:1333-1351 runs it
+// (template statistics as :902-973).
+double ref_xcorr_score(double* templ, double* match, int width, int height, int x0, int x1, int y0,
+                       int y1, double tx, double ty) {
+  const int rw = x1 - x0 + 1, rh = y1 - y0 + 1;
+  const long area = (long)rw * rh;
+  double tavg = 0.0, trms = 0.0;
+  for (long i = 0; i < area; ++i) tavg += templ[i];
+  tavg /= area;
+  for (long i = 0; i < area; ++i) trms += (templ[i] - tavg) * (templ[i] - tavg);
+  trms = sqrt(trms);
+  vector<double> roi(area);
+  double mavg = 0.0, res = 0.0;
+  data_interp(match, roi.data(), &mavg, tx, ty, x0, x1, y0, y1, width, height);
+  cross_correlation(roi.data(), templ, tavg, mavg, &res, x0, x1, y0, y1, trms);
+  return res;
 }
 
 }  // extern "C"

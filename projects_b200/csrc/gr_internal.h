@@ -109,6 +109,17 @@ struct RowArgs {
   int M, M0, M02, pairs;
 };
 
+// FBP comparator: OptimizedFBP's row filter on pairs of projection rows packed
+// as one complex line (gridrec_kernels.cu); backprojection in gridrec_fbp.cu.
+struct FbpFilterArgs {
+  const float* sino;     // [slice][n_ang][n]
+  float* filt;           // [slice][n_ang][n]
+  const float* lut;      // n filter weights
+  const float2* tw;      // two-level twiddle table for n
+  int n, n_ang, slices;
+};
+cudaError_t launch_fbp_filter(const FbpFilterArgs& a, cudaStream_t s);
+
 // Records a formatted message for gr_last_error() and returns code (gridrec_plan.cu).
 int fail(int code, const char* fmt, ...);
 

@@ -801,6 +801,66 @@ cudaError_t launch_wait_probe(int* err, int limit, cudaStream_t s) {
 
 static int fft_smem_bytes(int N) { return (kTwSlots + N) * (int)sizeof(float2); }
 
+// ------------------------------------------------------------------ FBP comparator filter
+// OptimizedFBP (gridrec/GPU/filteredbackprojection.cpp:280-300): each projection
+// row, gated to (-5, 5), goes through an FFT exp(+i), bin k times lut[k] =
+// 1 - sqrt(|k - n/2| / (n/2)), and an unnormalised FFT exp(-i), keeping the real
+// part.  lut[k] = lut[n - k] is real, so two rows packed as re + i im are
+// filtered together and come apart as the real and imaginary parts.
+// Grid: (row pairs, slices); n/16 threads.
+
+__device__ __forceinline__ float fbp_gate(float v) { return (v > -5.f && v < 5.f) ? v : 0.f; }
+
+template <int MAXT>
+__global__ void __launch_bounds__(MAXT, 1024 / MAXT) fbp_filter_kernel(FbpFilterArgs a) {
+  extern __shared__ float2 sm[];
+  float2* tw = sm;
+  float2* buf = sm + kTwSlots;
+  const int pr = blockIdx.x, s = blockIdx.y;
+  const int tid = threadIdx.x, nthr = blockDim.x;
+  const int n = a.n;
+  load_twiddles(tw, a.tw, n);
+  const int ra = 2 * pr, rb = 2 * pr + 1;
+  const float* xa = a.sino + ((size_t)s * a.n_ang + ra) * n;
+  const float* xb = rb < a.n_ang ? xa + n : nullptr;
+  float2 v[16];
+#pragma unroll
+  for (int r = 0; r < 16; ++r) {
+    const int k = tid + r * nthr;
+    v[r] = make_float2(fbp_gate(__ldg(&xa[k])), xb ? fbp_gate(__ldg(&xb[k])) : 0.f);
+  }
+  __syncthreads();
+  fft_reg<+1>(v, buf, n, tid, nthr, tw, tw + 64);
+  const int Rl = last_radix(n);
+  __syncthreads();
+#pragma unroll
+  for (int idx = 0; idx < 16; ++idx) {
+    const int k = tid + nthr * out_index(idx, Rl);
+    const float w = __ldg(&a.lut[k]);
+    buf[swz(k)] = make_float2(v[idx].x * w, v[idx].y * w);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int r = 0; r < 16; ++r) v[r] = buf[swz(tid + r * nthr)];
+  __syncthreads();
+  fft_reg<-1>(v, buf, n, tid, nthr, tw, tw + 64);
+  float* ya = a.filt + ((size_t)s * a.n_ang + ra) * n;
+#pragma unroll
+  for (int idx = 0; idx < 16; ++idx) {
+    const int k = tid + nthr * out_index(idx, Rl);
+    ya[k] = v[idx].x;
+    if (xb) ya[n + k] = v[idx].y;
+  }
+}
+
+cudaError_t launch_fbp_filter(const FbpFilterArgs& a, cudaStream_t s) {
+  const int smem = fft_smem_bytes(a.n);
+  dim3 grid((a.n_ang + 1) / 2, a.slices);
+  if (a.n <= 4096) fbp_filter_kernel<256><<<grid, a.n / 16, smem, s>>>(a);
+  else fbp_filter_kernel<512><<<grid, a.n / 16, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
 // Allows the dynamic-shared-memory kernels the device's opt-in maximum; called
 // once per device at plan creation so that launches need no attribute calls
 // (and can be captured in a CUDA graph).
@@ -821,7 +881,8 @@ cudaError_t init_kernel_attributes() {
                        (const void*)cols_kernel<256>, (const void*)cols_kernel<512>,
                        (const void*)cols_tma_kernel<256>, (const void*)cols_tma_kernel<512>,
                        (const void*)rows_kernel<256>, (const void*)rows_kernel<512>,
-                       (const void*)grid_kernel<4>, (const void*)grid_kernel<kMaxTaps>};
+                       (const void*)grid_kernel<4>, (const void*)grid_kernel<kMaxTaps>,
+                       (const void*)fbp_filter_kernel<256>, (const void*)fbp_filter_kernel<512>};
   for (const void* f : fns) {
     if (e != cudaSuccess) break;
     e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);

@@ -390,6 +390,155 @@ struct Carve {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Rotation-axis search by cross-correlation (find_shift's brute-force path:
+// data_interp + cross_correlation, find_shift/src/main/find_shift.cpp:1975-2076,
+// the CPU twin of cross_correlation.cu:19-413).  For translation (tx, ty) the
+// match image is sampled at (nx - tx, ny - ty) for every ROI pixel by bilinear
+// interpolation over the in-image neighbours, normalised by their weight
+// (0 when the weight is <= 1e-5); M_avg is the ROI mean of the samples, and
+//   score = sum (T - T_avg)(M - M_avg) / (T_rms sqrt(sum (M - M_avg)^2))
+// (0 when T_rms or the second sum is <= 1e-5), T_rms = sqrt(sum (T - T_avg)^2).
+// All arithmetic in double, as the reference's; two passes per translation
+// (mean, then centred sums), block partials summed in a fixed order.
+struct XcorrArgs {
+  const float* templ;   // roi_h x roi_w
+  const float* match;   // height x width
+  int width, height, x0, y0, roi_w, roi_h;
+  double tx0, ty0, dtx, dty;
+  int n_tx;
+  int rows_per_block;
+  double* part;         // [trans][block][2]
+  const double* mavg;   // [trans] (second pass)
+  const double* tavg;   // template mean
+};
+
+__device__ __forceinline__ double xcorr_sample(const XcorrArgs& a, double x, double y) {
+  const double fx = floor(x), fy = floor(y);
+  const int nxx = (int)fx, nyy = (int)fy;
+  double pix = 0.0, wsum = 0.0;
+  const double ax = (double)(nxx + 1) - x, bx = x - (double)nxx;
+  const double ay = (double)(nyy + 1) - y, by = y - (double)nyy;
+  const bool x0ok = nxx >= 0 && nxx < a.width, x1ok = nxx + 1 >= 0 && nxx + 1 < a.width;
+  const bool y0ok = nyy >= 0 && nyy < a.height, y1ok = nyy + 1 >= 0 && nyy + 1 < a.height;
+  const float* m = a.match;
+  if (x0ok && y0ok) {
+    pix += (double)__ldg(&m[(size_t)nyy * a.width + nxx]) * ax * ay;
+    wsum += ax * ay;
+  }
+  if (x1ok && y0ok) {
+    pix += (double)__ldg(&m[(size_t)nyy * a.width + nxx + 1]) * bx * ay;
+    wsum += bx * ay;
+  }
+  if (x0ok && y1ok) {
+    pix += (double)__ldg(&m[(size_t)(nyy + 1) * a.width + nxx]) * ax * by;
+    wsum += ax * by;
+  }
+  if (x1ok && y1ok) {
+    pix += (double)__ldg(&m[(size_t)(nyy + 1) * a.width + nxx + 1]) * bx * by;
+    wsum += bx * by;
+  }
+  return wsum > 1e-5 ? pix / wsum : 0.0;
+}
+
+// pass 0: sum of samples; pass 1: sum (T - T_avg)(M - M_avg) and sum (M - M_avg)^2
+template <int PASS>
+__global__ void __launch_bounds__(256) xcorr_kernel(XcorrArgs a) {
+  __shared__ double red[2][8];
+  const int blk = blockIdx.x, tr = blockIdx.y;
+  const double tx = a.tx0 + (tr % a.n_tx) * a.dtx;
+  const double ty = a.ty0 + (tr / a.n_tx) * a.dty;
+  const double mavg = PASS == 1 ? a.mavg[tr] : 0.0;
+  const double tavg = PASS == 1 ? *a.tavg : 0.0;
+  double s0 = 0.0, s1 = 0.0;
+  const int r0 = blk * a.rows_per_block, r1 = min(a.roi_h, r0 + a.rows_per_block);
+  for (int r = r0; r < r1; ++r) {
+    const double y = (double)(a.y0 + r) - ty;
+    for (int c = threadIdx.x; c < a.roi_w; c += blockDim.x) {
+      const double m = xcorr_sample(a, (double)(a.x0 + c) - tx, y);
+      if (PASS == 0) {
+        s0 += m;
+      } else {
+        const double dm = m - mavg;
+        s0 += ((double)__ldg(&a.templ[(size_t)r * a.roi_w + c]) - tavg) * dm;
+        s1 += dm * dm;
+      }
+    }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    s0 += __shfl_xor_sync(0xffffffffu, s0, o);
+    s1 += __shfl_xor_sync(0xffffffffu, s1, o);
+  }
+  const int w = threadIdx.x >> 5;
+  if ((threadIdx.x & 31) == 0) {
+    red[0][w] = s0;
+    red[1][w] = s1;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t0 = 0.0, t1 = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) {
+      t0 += red[0][k];
+      t1 += red[1][k];
+    }
+    double* p = a.part + ((size_t)tr * gridDim.x + blk) * 2;
+    p[0] = t0;
+    p[1] = t1;
+  }
+}
+
+// One thread per translation sums its block partials in order.  mode 0: mean
+// of the samples; mode 1: the score.
+__global__ void xcorr_finish_kernel(const double* part, int nblk, int n_trans, double area,
+                                    double* mavg, const double* trms, double* score, int mode) {
+  const int tr = blockIdx.x * blockDim.x + threadIdx.x;
+  if (tr >= n_trans) return;
+  double t0 = 0.0, t1 = 0.0;
+  for (int b = 0; b < nblk; ++b) {
+    t0 += part[((size_t)tr * nblk + b) * 2];
+    t1 += part[((size_t)tr * nblk + b) * 2 + 1];
+  }
+  if (mode == 0) {
+    mavg[tr] = t0 / area;
+  } else {
+    const double r = *trms;
+    score[tr] = (fabs(r) > 1e-5 && fabs(t1) > 1e-5) ? t0 / (r * sqrt(t1)) : 0.0;
+  }
+}
+
+// Template mean and T_rms = sqrt(sum (T - T_avg)^2), one block, fixed order.
+__global__ void __launch_bounds__(256) xcorr_template_kernel(const float* t, long n, double* out) {
+  __shared__ double red[8];
+  __shared__ double mean_s;
+  double s = 0.0;
+  for (long i = threadIdx.x; i < n; i += blockDim.x) s += (double)t[i];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int k = 0; k < 8; ++k) m += red[k];
+    mean_s = m / (double)n;
+    out[0] = mean_s;
+  }
+  __syncthreads();
+  const double mean = mean_s;
+  double q = 0.0;
+  for (long i = threadIdx.x; i < n; i += blockDim.x) {
+    const double d = (double)t[i] - mean;
+    q += d * d;
+  }
+  for (int o = 16; o > 0; o >>= 1) q += __shfl_xor_sync(0xffffffffu, q, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = q;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int k = 0; k < 8; ++k) m += red[k];
+    out[1] = sqrt(m);
+  }
+}
+
 }  // namespace
 }  // namespace gr
 
@@ -643,6 +792,48 @@ int gr_center_search(gr_plan* plan, const float* sino1, const float* sino2, int 
     if ((rc = check_launch("centre search: crop"))) return rc;
   }
   return GR_OK;
+}
+
+int gr_xcorr_scores(const float* templ_roi, const float* match, int width, int height, int roi_x0,
+                    int roi_x1, int roi_y0, int roi_y1, double tx0, double ty0, double dtx,
+                    double dty, int n_tx, int n_ty, double* scores, void* stream) {
+  if (!templ_roi || !match || !scores) return fail(GR_ERR_ARG, "xcorr: null pointer");
+  if (width < 1 || height < 1 || n_tx < 1 || n_ty < 1 || roi_x0 < 0 || roi_y0 < 0 ||
+      roi_x1 < roi_x0 || roi_y1 < roi_y0 || roi_x1 >= width || roi_y1 >= height)
+    return fail(GR_ERR_ARG, "xcorr: bad image, ROI or translation grid");
+  if ((long)n_tx * n_ty > 65535) return fail(GR_ERR_ARG, "xcorr: at most 65535 translations");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int roi_w = roi_x1 - roi_x0 + 1, roi_h = roi_y1 - roi_y0 + 1;
+  const int n_trans = n_tx * n_ty;
+  // enough blocks to fill the GPU: split the ROI rows when translations are few
+  const int want_blocks = 4 * 148;
+  int nblk = std::max(1, std::min(roi_h, (want_blocks + n_trans - 1) / n_trans));
+  const int rows_per = (roi_h + nblk - 1) / nblk;
+  nblk = (roi_h + rows_per - 1) / rows_per;
+  double* d = nullptr;
+  const size_t nd = (size_t)n_trans * nblk * 2 + n_trans * 2 + 2;
+  cudaError_t e = cudaMallocAsync(&d, nd * sizeof(double), st);
+  if (e != cudaSuccess) return fail(GR_ERR_NOMEM, "xcorr: %s", cudaGetErrorString(e));
+  double* part = d;
+  double* mavg = part + (size_t)n_trans * nblk * 2;
+  double* sc = mavg + n_trans;
+  double* tstat = sc + n_trans;  // T_avg, T_rms
+  XcorrArgs a{templ_roi, match, width, height, roi_x0, roi_y0, roi_w, roi_h,
+              tx0, ty0, dtx, dty, n_tx, rows_per, part, mavg, tstat};
+  const int fin = (n_trans + 255) / 256;
+  xcorr_template_kernel<<<1, 256, 0, st>>>(templ_roi, (long)roi_w * roi_h, tstat);
+  xcorr_kernel<0><<<dim3(nblk, n_trans), 256, 0, st>>>(a);
+  xcorr_finish_kernel<<<fin, 256, 0, st>>>(part, nblk, n_trans, (double)roi_w * roi_h, mavg,
+                                           tstat + 1, sc, 0);
+  xcorr_kernel<1><<<dim3(nblk, n_trans), 256, 0, st>>>(a);
+  xcorr_finish_kernel<<<fin, 256, 0, st>>>(part, nblk, n_trans, (double)roi_w * roi_h, mavg,
+                                           tstat + 1, sc, 1);
+  e = cudaGetLastError();
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(scores, sc, n_trans * sizeof(double), cudaMemcpyDeviceToHost, st);
+  cudaFreeAsync(d, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  return e == cudaSuccess ? GR_OK : cuda_fail(e, "xcorr");
 }
 
 }  // extern "C"

@@ -33,7 +33,8 @@ EXPORTS = ("gr_params_default", "gr_filter_code", "gr_plan_create", "gr_plan_des
            "gr_ring_removal", "gr_shift_pad", "gr_crop_center", "gr_entropy_workspace_bytes",
            "gr_entropy", "gr_reconstruct_padded", "gr_center_search", "gr_graph_create",
            "gr_graph_launch", "gr_graph_launch_count", "gr_graph_destroy", "gr_plan_autotune",
-           "gr_plan_tuning")
+           "gr_plan_tuning", "gr_xcorr_scores", "gr_fbp_create", "gr_fbp_reconstruct",
+           "gr_fbp_destroy")
 STAGES = ("phase", "spectra", "grid", "cols", "rows_deapod")
 
 
@@ -113,6 +114,12 @@ def lib():
         L.gr_graph_launch_count.argtypes = [vp, C.POINTER(C.c_long)]
         L.gr_graph_destroy.argtypes = [vp]
         L.gr_plan_autotune.argtypes = [vp, vp]
+        L.gr_fbp_create.argtypes = [i_, i_, C.POINTER(f_), i_, i_, C.POINTER(vp)]
+        L.gr_fbp_reconstruct.argtypes = [vp, vp, i_, vp, vp]
+        L.gr_fbp_destroy.argtypes = [vp]
+        d_ = C.c_double
+        L.gr_xcorr_scores.argtypes = [vp, vp] + [i_] * 6 + [d_] * 4 + [i_, i_,
+                                                                         C.POINTER(d_), vp]
         L.gr_plan_tuning.argtypes = [vp, C.POINTER(i_), C.POINTER(i_)]
         _lib = L
     return _lib
@@ -543,3 +550,75 @@ def center_search(plan: "Plan", sino1, sino2, shifts, hist_lo, hist_hi, nbins,
                                   int(nbins), scores.ctypes.data_as(fp), C.byref(best),
                                   _ptr(imgs), _stream_ptr(stream)), "gr_center_search")
     return scores, best.value, imgs
+
+
+def xcorr_scores(templ_roi, match, roi, tx0, ty0, dtx, dty, n_tx, n_ty, stream=None):
+    """find_shift's brute-force cross-correlation scores (find_shift.cpp:1975-2076) on
+    device tensors: templ_roi (roi_h, roi_w), match (height, width) float32; roi =
+    (x0, x1, y0, y1) inclusive.  Returns (n_ty, n_tx) float64 numpy scores."""
+    h, w = match.shape
+    out = np.zeros((n_ty, n_tx), np.float64)
+    _check(lib().gr_xcorr_scores(_ptr(templ_roi), _ptr(match), w, h, *[int(v) for v in roi],
+                                 float(tx0), float(ty0), float(dtx), float(dty), int(n_tx),
+                                 int(n_ty), out.ctypes.data_as(C.POINTER(C.c_double)),
+                                 _stream_ptr(stream)), "gr_xcorr_scores")
+    return out
+
+
+def find_shift_xcorr(templ_roi, match, roi, tx_range, ty_range, n_subpixel, stream=None):
+    """The translation search of find_shift (find_shift.cpp:1283-1480, GPU brute-force
+    branch): scores over tx_range = (start, end, step) x ty_range, the first maximum,
+    then 2 n_subpixel + 1 sub-pixel steps of step/n_subpixel in x from one coarse
+    step below it.  Returns (tx_subpixel, ty, coarse scores, sub-pixel scores); the
+    rotation axis offset the reference prints is tx_subpixel / 2."""
+    sx, ex, ix = tx_range
+    sy, ey, iy = ty_range
+    n_tx = int((ex - sx) / ix) + 1
+    n_ty = int((ey - sy) / iy) + 1
+    coarse = xcorr_scores(templ_roi, match, roi, sx, sy, ix, iy, n_tx, n_ty, stream)
+    best = int(np.argmax(coarse.reshape(-1)))  # first maximum, as the reference's scan
+    by, bx = divmod(best, n_tx)
+    ty = sy + by * iy
+    sub_step = ix / n_subpixel
+    start = sx + (bx - 1) * ix
+    sub = xcorr_scores(templ_roi, match, roi, start, ty, sub_step, iy, 2 * n_subpixel + 1, 1,
+                       stream)[0]
+    # The reference keeps the coarse best score as the bar for the sub-pixel scan
+    # (find_shift.cpp:1440-1455), so when no sub-pixel score beats it the result
+    # falls back to index 0, one coarse step low; the maximum is taken here.
+    bs = int(np.argmax(sub))
+    return start + bs * sub_step, ty, coarse, sub
+
+
+class FBP:
+    """The FBP comparator (OptimizedFBP, gridrec/GPU/filteredbackprojection.cpp:190-330)."""
+
+    def __init__(self, n_det, n_ang, theta_deg, max_slices=4, device=0):
+        th = np.ascontiguousarray(theta_deg, np.float32)
+        h = C.c_void_p()
+        _check(lib().gr_fbp_create(int(n_det), int(n_ang), th.ctypes.data_as(C.POINTER(C.c_float)),
+                                   int(max_slices), int(device), C.byref(h)), "gr_fbp_create")
+        self._h = h
+        self.n_det, self.n_ang = n_det, n_ang
+
+    def reconstruct(self, sinos, recons=None, stream=None):
+        """sinos (S, n_ang, n_det) float32 CUDA tensor -> (S, n_det, n_det)."""
+        import torch
+        S = sinos.shape[0]
+        if recons is None:
+            recons = torch.empty((S, self.n_det, self.n_det), dtype=torch.float32,
+                                 device=sinos.device)
+        _check(lib().gr_fbp_reconstruct(self._h, _ptr(sinos), S, _ptr(recons),
+                                        _stream_ptr(stream)), "gr_fbp_reconstruct")
+        return recons
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().gr_fbp_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

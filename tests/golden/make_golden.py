@@ -90,6 +90,25 @@ def prep_cases(rng):
     ent = np.array([O.ref_entropy(img, lo, hi, int(nb)) for lo, hi, nb in cfg], np.float64)
     np.savez_compressed(os.path.join(HERE, "prep_entropy_48x96.npz"), image=img, cfg=cfg,
                         entropy=ent)
+    # brute-force cross-correlation scores: a match image and the template cut from a
+    # shifted copy of it, several translations (integer, fractional, out of the image)
+    h, w = 40, 72
+    match = (rng.standard_normal((h, w)) * 0.3 + 1.0)
+    roi = (12, 55, 6, 31)
+    shifted = np.roll(match, (1, 3), axis=(0, 1))
+    templ = shifted[roi[2]:roi[3] + 1, roi[0]:roi[1] + 1].copy()
+    trans = np.array([[3.0, 1.0], [0.0, 0.0], [2.5, 1.0], [3.25, 0.75], [-4.5, 2.0],
+                      [30.0, -10.0], [70.0, 0.0]])
+    scores = np.array([O.ref_xcorr_score(templ, match, roi, tx, ty) for tx, ty in trans])
+    np.savez_compressed(os.path.join(HERE, "prep_xcorr_40x72.npz"), match=match, templ=templ,
+                        roi=np.array(roi), trans=trans, scores=scores)
+    # the reference's CPU OptimizedFBP (FBP comparator) on a Shepp-Logan sinogram
+    if O.fbp_ref_available():
+        n, a = 64, 45
+        th = ph.angles_deg(a)
+        sino = ph.shepp_logan_sinogram(n, a, center=n / 2, noise_seed=5)
+        np.savez_compressed(os.path.join(HERE, "prep_fbp_64x45.npz"), sino=sino, theta=th,
+                            recon=O.ref_optimized_fbp(sino, th))
 
 
 def main():

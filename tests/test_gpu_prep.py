@@ -165,3 +165,65 @@ def test_center_search_finds_axis_and_matches_oracle():
                                    lo, hi, nb) for v in shifts])
     assert np.abs(scores - ref).max() < 2e-2
     assert int(np.argmin(ref)) == best
+
+
+def test_xcorr_scores_against_reference_and_oracle():
+    z = _load("prep_xcorr_*.npz")[0]
+    roi = tuple(int(v) for v in z["roi"])
+    t = _dev(z["templ"].astype(np.float32))
+    m = _dev(z["match"].astype(np.float32))
+    for (tx, ty), ref in zip(z["trans"], z["scores"]):
+        got = G.xcorr_scores(t, m, roi, tx, ty, 1.0, 1.0, 1, 1)[0, 0]
+        # inputs rounded to float32 on the device: compare with the oracle on those
+        want = O.port_xcorr_score(z["templ"].astype(np.float32), z["match"].astype(np.float32),
+                                  roi, tx, ty)
+        assert abs(got - want) < 1e-12, (tx, ty, got, want)
+        assert abs(got - ref) < 1e-6
+    # a grid of translations in one call equals the per-translation oracle
+    got = G.xcorr_scores(t, m, roi, -2.0, -1.5, 0.75, 0.5, 9, 7)
+    for k in range(7):
+        for i in range(9):
+            want = O.port_xcorr_score(z["templ"].astype(np.float32),
+                                      z["match"].astype(np.float32), roi, -2.0 + 0.75 * i,
+                                      -1.5 + 0.5 * k)
+            assert abs(got[k, i] - want) < 1e-12
+
+
+def test_find_shift_xcorr_recovers_subpixel_translation():
+    """A projection pair whose true translation is 6.4 px in x, 0 in y: the coarse
+    grid finds 6, the sub-pixel pass 6.4 (step 0.2)."""
+    rng = np.random.default_rng(13)
+    h, w = 64, 256
+    xs = np.arange(w + 16, dtype=np.float64)
+    base = np.stack([np.interp(xs, np.sort(rng.uniform(0, w + 16, 40)),
+                               rng.uniform(0.2, 2.0, 40)) for _ in range(h)])
+    match = base[:, 8:8 + w]
+    true_tx = 6.4
+    xq = np.arange(w, dtype=np.float64) - true_tx + 8
+    shifted = np.stack([np.interp(xq, xs, base[r]) for r in range(h)])
+    roi = (40, 200, 8, 55)
+    templ = shifted[roi[2]:roi[3] + 1, roi[0]:roi[1] + 1]
+    tx, ty, coarse, sub = G.find_shift_xcorr(_dev(templ.astype(np.float32)),
+                                             _dev(match.astype(np.float32)), roi,
+                                             (-20.0, 20.0, 1.0), (-2.0, 2.0, 1.0), 5)
+    assert coarse.shape == (5, 41) and sub.shape == (11,)
+    assert ty == 0.0
+    assert abs(tx - true_tx) <= 0.1 + 1e-9
+
+
+def test_fbp_comparator_against_reference_and_oracle():
+    z = _load("prep_fbp_*.npz")[0]
+    f = G.FBP(64, 45, z["theta"], max_slices=2)
+    out = f.reconstruct(_dev(z["sino"][None])).cpu().numpy()[0]
+    assert ph.rel_l2(out, z["recon"]) < 1e-5
+    assert ph.rel_l2(out, O.port_optimized_fbp(z["sino"], z["theta"])) < 1e-5
+    f.close()
+    # a batch of three 256 x 180 slices (two launches of max_slices = 2)
+    n, a = 256, 180
+    th = ph.angles_deg(a)
+    sinos = np.stack([ph.shepp_logan_sinogram(n, a, center=n / 2, noise_seed=k) for k in range(3)])
+    f = G.FBP(n, a, th, max_slices=2)
+    out = f.reconstruct(_dev(sinos)).cpu().numpy()
+    for k in range(3):
+        assert ph.rel_l2(out[k], O.port_optimized_fbp(sinos[k], th)) < 1e-5
+    f.close()

@@ -21,6 +21,25 @@ def test_prep_fixtures_present():
     assert len(_load("prep_shift_pad_*.npz")) == 2
     assert len(_load("prep_ring_*.npz")) == 1
     assert len(_load("prep_entropy_*.npz")) == 1
+    assert len(_load("prep_xcorr_*.npz")) == 1
+    assert len(_load("prep_fbp_*.npz")) == 1
+
+
+def test_fbp_oracle_matches_reference_fixture():
+    """OptimizedFBP restated in float64: within the reference's float FFT noise."""
+    z = _load("prep_fbp_*.npz")[0]
+    got = O.port_optimized_fbp(z["sino"], z["theta"])
+    ref = z["recon"].astype(np.float64)
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-5
+
+
+def test_xcorr_oracle_matches_reference_fixture():
+    z = _load("prep_xcorr_*.npz")[0]
+    roi = tuple(int(v) for v in z["roi"])
+    for (tx, ty), ref in zip(z["trans"], z["scores"]):
+        got = O.port_xcorr_score(z["templ"], z["match"], roi, tx, ty)
+        assert abs(got - ref) <= 1e-12 * max(1.0, abs(ref)), (tx, ty, got, ref)
+    assert abs(z["scores"][0] - 1.0) < 1e-12  # the template's own translation
 
 
 @pytest.mark.parametrize("z", _load("prep_shift_pad_*.npz"))
@@ -96,6 +115,27 @@ def test_live_reference_shift_pad_and_ring():
         assert np.linalg.norm(out - ref) / np.linalg.norm(ref) < 1e-5
 
 
+@pytest.mark.skipif(not O.prep_ref_available(), reason="reference build absent")
+def test_live_reference_xcorr():
+    rng = np.random.default_rng(10)
+    m = rng.standard_normal((30, 50))
+    roi = (5, 40, 3, 25)
+    t = rng.standard_normal((23, 36))
+    for tx, ty in rng.uniform(-8, 8, (8, 2)):
+        assert O.port_xcorr_score(t, m, roi, tx, ty) == pytest.approx(
+            O.ref_xcorr_score(t, m, roi, tx, ty), rel=1e-12, abs=1e-14)
+
+
+@pytest.mark.skipif(not O.fbp_ref_available(), reason="reference build absent")
+def test_live_reference_fbp():
+    rng = np.random.default_rng(14)
+    th = np.sort(rng.uniform(0, 180, 37)).astype(np.float32)
+    sino = rng.uniform(-6, 6, (37, 32)).astype(np.float32)  # some values outside the gate
+    got = O.port_optimized_fbp(sino, th)
+    ref = O.ref_optimized_fbp(sino, th).astype(np.float64)
+    assert np.linalg.norm(got - ref) / np.linalg.norm(ref) < 1e-5
+
+
 # ---- C ABI argument checks (no GPU needed: they fail before any CUDA call)
 
 def test_prep_abi_rejects_bad_arguments():
@@ -110,6 +150,15 @@ def test_prep_abi_rejects_bad_arguments():
     assert "entropy" in G.last_error()
     assert L.gr_center_search(None, dummy, dummy, 64, 10, None, 3, 0.0, 1.0, 10, None, None,
                               None, None) == -1
+    import ctypes as C
+    out = (C.c_double * 4)()
+    assert L.gr_xcorr_scores(dummy, dummy, 64, 32, 0, 64, 0, 10, 0.0, 0.0, 1.0, 1.0, 2, 2,
+                             out, None) == -1  # roi_x1 beyond the image
+    assert L.gr_xcorr_scores(dummy, dummy, 64, 32, 0, 10, 0, 10, 0.0, 0.0, 1.0, 1.0, 300, 300,
+                             out, None) == -1  # more than 65535 translations
+    h = C.c_void_p()
+    th = (C.c_float * 10)()
+    assert L.gr_fbp_create(100, 10, th, 1, 0, C.byref(h)) == -1  # width not a power of two
     assert L.gr_ring_workspace_bytes(2, 64, 10) >= 4 * 2 * (64 + 10)
     assert L.gr_entropy_workspace_bytes(3, 100) == 3 * 101 * 4
     assert L.gr_entropy_workspace_bytes(0, 100) == 0
