@@ -23,6 +23,7 @@
 
 #include <algorithm>
 #include <mutex>
+#include <vector>
 
 #include "gr_internal.h"
 
@@ -246,6 +247,110 @@ __device__ __forceinline__ void fft_reg(float2 (&v)[16], float2* buf, int N, int
   }
 }
 
+// The same transform with N a compile-time constant: pass radices, strides,
+// twiddle steps and swizzle offsets fold into constants (fft_reg computes them
+// at run time).  Instantiated for N = 256 .. 8192.
+template <int R, int S, int N, int Ns, bool LAST>
+__device__ __forceinline__ void fft_pass_t(float2 (&v)[16], float2* buf, int tid, const float2* lo,
+                                           const float2* hi) {
+  constexpr int B = 16 / R, NR = N / R, nthr = N / 16, tstep = N / (Ns * R);
+#pragma unroll
+  for (int i = 0; i < B; ++i) {
+    const int j = tid + i * nthr;
+#pragma unroll
+    for (int r = 0; r < R; ++r) v[i * R + r] = buf[swz(j + r * NR)];
+  }
+#pragma unroll
+  for (int i = 0; i < B; ++i) {
+    const int j = tid + i * nthr;
+    const int k = j & (Ns - 1);
+    const int e = k * tstep;
+    const float2 w1 = twiddle<S>(lo, hi, e);
+    v[i * R + 1] = cmul(v[i * R + 1], w1);
+    if constexpr (R >= 4) {
+      const float2 w2 = twiddle<S>(lo, hi, 2 * e);
+      const float2 w3 = cmul(w1, w2);
+      v[i * R + 2] = cmul(v[i * R + 2], w2);
+      v[i * R + 3] = cmul(v[i * R + 3], w3);
+      if constexpr (R >= 8) {
+        const float2 w4 = twiddle<S>(lo, hi, 4 * e);
+        v[i * R + 4] = cmul(v[i * R + 4], w4);
+        v[i * R + 5] = cmul(v[i * R + 5], cmul(w1, w4));
+        v[i * R + 6] = cmul(v[i * R + 6], cmul(w2, w4));
+        v[i * R + 7] = cmul(v[i * R + 7], cmul(w3, w4));
+        if constexpr (R >= 16) {
+          const float2 w8 = twiddle<S>(lo, hi, 8 * e);
+          const float2 w12 = cmul(w4, w8);
+          v[i * R + 8] = cmul(v[i * R + 8], w8);
+          v[i * R + 9] = cmul(v[i * R + 9], cmul(w1, w8));
+          v[i * R + 10] = cmul(v[i * R + 10], cmul(w2, w8));
+          v[i * R + 11] = cmul(v[i * R + 11], cmul(w3, w8));
+          v[i * R + 12] = cmul(v[i * R + 12], w12);
+          v[i * R + 13] = cmul(v[i * R + 13], cmul(w1, w12));
+          v[i * R + 14] = cmul(v[i * R + 14], cmul(w2, w12));
+          v[i * R + 15] = cmul(v[i * R + 15], cmul(w3, w12));
+        }
+      }
+    }
+    dftR<R, S>(&v[i * R]);
+  }
+  if constexpr (!LAST) {
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < B; ++i) {
+      const int j = tid + i * nthr;
+      const int k = j & (Ns - 1);
+      const int base = (j - k) * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) buf[swz(base + r * Ns)] = v[i * R + r];
+    }
+    __syncthreads();
+  }
+}
+
+template <int S, int N, int Ns>
+__device__ __forceinline__ void fft_passes_t(float2 (&v)[16], float2* buf, int tid,
+                                             const float2* lo, const float2* hi) {
+  if constexpr (Ns < N) {
+    constexpr int rem = N / Ns;
+    constexpr int R = rem >= 16 ? 16 : rem;
+    fft_pass_t<R, S, N, Ns, Ns * R == N>(v, buf, tid, lo, hi);
+    fft_passes_t<S, N, Ns * R>(v, buf, tid, lo, hi);
+  }
+}
+
+template <int S, int N>
+__device__ __forceinline__ void fft_reg_t(float2 (&v)[16], float2* buf, int tid, const float2* lo,
+                                          const float2* hi) {
+  dft16<S>(v);
+  if constexpr (N > 16) {
+#pragma unroll
+    for (int r = 0; r < 16; ++r) buf[swz(tid * 16 + r)] = v[r];
+    __syncthreads();
+    fft_passes_t<S, N, 16>(v, buf, tid, lo, hi);
+  }
+}
+
+constexpr int last_radix_c(int N) {
+  return ((N == 16 || N == 256 || N == 4096) ? 16
+          : (N == 32 || N == 512 || N == 8192) ? 2
+          : (N == 64 || N == 1024) ? 4 : 8);
+}
+
+// One line of N points (NT = N known at compile time, or NT = 0: N at run time).
+template <int S, int NT>
+__device__ __forceinline__ void fft_line(float2 (&v)[16], float2* buf, int N, int tid, int nthr,
+                                         const float2* lo, const float2* hi) {
+  if constexpr (NT > 0) fft_reg_t<S, NT>(v, buf, tid, lo, hi);
+  else fft_reg<S>(v, buf, N, tid, nthr, lo, hi);
+}
+
+template <int NT>
+__device__ __forceinline__ int line_last_radix(int N) {
+  if constexpr (NT > 0) return last_radix_c(NT);
+  else return last_radix(N);
+}
+
 // Copies the two-level twiddle table (64 + max(1, N/64) entries) to shared memory.
 __device__ __forceinline__ void load_twiddles(float2* dst, const float2* src, int N) {
   const int n = 64 + max(1, N >> 6);
@@ -382,7 +487,7 @@ __device__ __forceinline__ float load_sino<U16Linear>(const U16Linear* row, int 
 
 // Lines of up to 4096 points run 64-register variants (several CTAs per SM);
 // 8192-point lines need 512 threads and use the MAXT = 512 variants.
-template <typename T, int MAXT>
+template <typename T, int MAXT, int NT>
 __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs a) {
   extern __shared__ float2 sm[];
   float2* tw = sm;
@@ -411,9 +516,9 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
     v[r] = make_float2(x, y);
   }
   __syncthreads();  // twiddle table ready
-  fft_reg<+1>(v, buf, a.pdim, tid, nthr, tw, tw + 64);
+  fft_line<+1, NT>(v, buf, a.pdim, tid, nthr, tw, tw + 64);
   // F[j] and F[pdim - j] meet through shared memory
-  const int Rl = last_radix(a.pdim);
+  const int Rl = line_last_radix<NT>(a.pdim);
   __syncthreads();
 #pragma unroll
   for (int idx = 0; idx < 16; ++idx) buf[swz(tid + nthr * out_index(idx, Rl))] = v[idx];
@@ -671,11 +776,11 @@ __global__ void __launch_bounds__(256) split_reduce_kernel(GridArgs a) {
 // Each column's exchange buffer has stride M + 16/G, which keeps the G lines
 // on distinct banks.
 
-template <int MAXT>
+template <int MAXT, int NT>
 __global__ void __launch_bounds__(MAXT, 1024 / MAXT) cols_kernel(ColArgs a, int G) {
   extern __shared__ float2 sm[];
   float2* tw = sm;
-  const int M = a.M;
+  const int M = NT ? NT : a.M;
   const int nthr = M >> 4;
   const int g = threadIdx.x % G, tid = threadIdx.x / G;
   float2* buf = sm + kTwSlots + g * (M + 16 / G);
@@ -686,8 +791,8 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) cols_kernel(ColArgs a, int 
 #pragma unroll
   for (int r = 0; r < 16; ++r) v[r] = Hp[(size_t)(tid + r * nthr) * M];
   __syncthreads();
-  fft_reg<-1>(v, buf, M, tid, nthr, tw, tw + 64);
-  const int Rl = last_radix(M);
+  fft_line<-1, NT>(v, buf, M, tid, nthr, tw, tw + 64);
+  const int Rl = line_last_radix<NT>(M);
 #pragma unroll
   for (int idx = 0; idx < 16; ++idx) Hp[(size_t)(tid + nthr * out_index(idx, Rl)) * M] = v[idx];
 }
@@ -698,11 +803,11 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) cols_kernel(ColArgs a, int 
 // twiddle table meanwhile.  The landing buffer then serves as the FFT
 // exchange buffers.  The wait is bounded; a timeout sets *err and the CTA
 // returns after giving the copies a second bounded wait.
-template <int MAXT>
+template <int MAXT, int NT>
 __global__ void __launch_bounds__(MAXT, 1024 / MAXT)
     cols_tma_kernel(const __grid_constant__ CUtensorMap tmap, ColArgs a, int G, int box_rows) {
   extern __shared__ __align__(128) float2 sm[];
-  const int M = a.M;
+  const int M = NT ? NT : a.M;
   const int nthr = M >> 4;
   float2* tw = sm;
   float2* land = sm + kTwSlots;  // [row][g], G * M values (+ 16 for exchange stride)
@@ -733,21 +838,21 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT)
 #pragma unroll
   for (int r = 0; r < 16; ++r) v[r] = land[(tid + r * nthr) * G + g];
   __syncthreads();  // inputs read before the landing buffer becomes the exchange buffer
-  fft_reg<-1>(v, land + g * (M + 16 / G), M, tid, nthr, tw, tw + 64);
+  fft_line<-1, NT>(v, land + g * (M + 16 / G), M, tid, nthr, tw, tw + 64);
   float2* Hp = a.H + (size_t)pair * M * M + q0 + g;
-  const int Rl = last_radix(M);
+  const int Rl = line_last_radix<NT>(M);
 #pragma unroll
   for (int idx = 0; idx < 16; ++idx) Hp[(size_t)(tid + nthr * out_index(idx, Rl)) * M] = v[idx];
 }
 
 // ------------------------------------------------------------------ second axis + deapod (K4)
 
-template <int MAXT>
+template <int MAXT, int NT>
 __global__ void __launch_bounds__(MAXT, 1024 / MAXT) rows_kernel(RowArgs a) {
   extern __shared__ float2 sm[];
   float2* tw = sm;
   float2* buf = sm + kTwSlots;
-  const int M = a.M;
+  const int M = NT ? NT : a.M;
   const int iu = blockIdx.x, pair = blockIdx.y;
   const int tid = threadIdx.x, nthr = blockDim.x;
   load_twiddles(tw, a.tw, M);
@@ -756,7 +861,7 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) rows_kernel(RowArgs a) {
 #pragma unroll
   for (int r = 0; r < 16; ++r) v[r] = row[tid + r * nthr];
   __syncthreads();
-  fft_reg<-1>(v, buf, M, tid, nthr, tw, tw + 64);
+  fft_line<-1, NT>(v, buf, M, tid, nthr, tw, tw + 64);
   // iu = (j - M02) mod M  (gridrec.cu:694-719)
   int j = iu + a.M02;
   if (j >= M) j -= M;
@@ -765,7 +870,7 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) rows_kernel(RowArgs a) {
   float* o1 = a.out1 + pair * a.pair_stride + (long)j * a.out_stride;
   float* o2 = (2 * pair + 1 < a.n_slices_valid) ? a.out2 + pair * a.pair_stride + (long)j * a.out_stride
                                                 : nullptr;
-  const int Rl = last_radix(M);
+  const int Rl = line_last_radix<NT>(M);
 #pragma unroll
   for (int idx = 0; idx < 16; ++idx) {
     const int iv = tid + nthr * out_index(idx, Rl);
@@ -801,6 +906,18 @@ cudaError_t launch_wait_probe(int* err, int limit, cudaStream_t s) {
 
 static int fft_smem_bytes(int N) { return (kTwSlots + N) * (int)sizeof(float2); }
 
+// Calls CALL(NT) with NT = N for the compiled line lengths, 0 (run-time N) otherwise.
+#define GR_DISPATCH_N(N, CALL)  \
+  switch (N) {                  \
+    case 256: CALL(256); break;   \
+    case 512: CALL(512); break;   \
+    case 1024: CALL(1024); break; \
+    case 2048: CALL(2048); break; \
+    case 4096: CALL(4096); break; \
+    case 8192: CALL(8192); break; \
+    default: CALL(0);             \
+  }
+
 // ------------------------------------------------------------------ FBP comparator filter
 // OptimizedFBP (gridrec/GPU/filteredbackprojection.cpp:280-300): each projection
 // row, gated to (-5, 5), goes through an FFT exp(+i), bin k times lut[k] =
@@ -811,14 +928,14 @@ static int fft_smem_bytes(int N) { return (kTwSlots + N) * (int)sizeof(float2); 
 
 __device__ __forceinline__ float fbp_gate(float v) { return (v > -5.f && v < 5.f) ? v : 0.f; }
 
-template <int MAXT>
+template <int MAXT, int NT>
 __global__ void __launch_bounds__(MAXT, 1024 / MAXT) fbp_filter_kernel(FbpFilterArgs a) {
   extern __shared__ float2 sm[];
   float2* tw = sm;
   float2* buf = sm + kTwSlots;
   const int pr = blockIdx.x, s = blockIdx.y;
   const int tid = threadIdx.x, nthr = blockDim.x;
-  const int n = a.n;
+  const int n = NT ? NT : a.n;
   load_twiddles(tw, a.tw, n);
   const int ra = 2 * pr, rb = 2 * pr + 1;
   const float* xa = a.sino + ((size_t)s * a.n_ang + ra) * n;
@@ -830,8 +947,8 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) fbp_filter_kernel(FbpFilter
     v[r] = make_float2(fbp_gate(__ldg(&xa[k])), xb ? fbp_gate(__ldg(&xb[k])) : 0.f);
   }
   __syncthreads();
-  fft_reg<+1>(v, buf, n, tid, nthr, tw, tw + 64);
-  const int Rl = last_radix(n);
+  fft_line<+1, NT>(v, buf, n, tid, nthr, tw, tw + 64);
+  const int Rl = line_last_radix<NT>(n);
   __syncthreads();
 #pragma unroll
   for (int idx = 0; idx < 16; ++idx) {
@@ -843,7 +960,7 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) fbp_filter_kernel(FbpFilter
 #pragma unroll
   for (int r = 0; r < 16; ++r) v[r] = buf[swz(tid + r * nthr)];
   __syncthreads();
-  fft_reg<-1>(v, buf, n, tid, nthr, tw, tw + 64);
+  fft_line<-1, NT>(v, buf, n, tid, nthr, tw, tw + 64);
   float* ya = a.filt + ((size_t)s * a.n_ang + ra) * n;
 #pragma unroll
   for (int idx = 0; idx < 16; ++idx) {
@@ -856,9 +973,36 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) fbp_filter_kernel(FbpFilter
 cudaError_t launch_fbp_filter(const FbpFilterArgs& a, cudaStream_t s) {
   const int smem = fft_smem_bytes(a.n);
   dim3 grid((a.n_ang + 1) / 2, a.slices);
-  if (a.n <= 4096) fbp_filter_kernel<256><<<grid, a.n / 16, smem, s>>>(a);
-  else fbp_filter_kernel<512><<<grid, a.n / 16, smem, s>>>(a);
+#define GR_FBP(NT)                                                                   \
+  if (a.n <= 4096) fbp_filter_kernel<256, NT><<<grid, a.n / 16, smem, s>>>(a);      \
+  else fbp_filter_kernel<(NT > 4096 || NT == 0) ? 512 : 256, NT><<<grid, a.n / 16, smem, s>>>(a)
+  GR_DISPATCH_N(a.n, GR_FBP)
+#undef GR_FBP
   return cudaGetLastError();
+}
+
+// Every FFT kernel instantiation for line length NT (both block-size variants:
+// the launchers choose by run-time N for NT = 0 and by the column group width).
+template <int NT>
+void add_fft_kernels(std::vector<const void*>& f) {
+  f.push_back((const void*)spectra_kernel<float, 256, NT>);
+  f.push_back((const void*)spectra_kernel<__half, 256, NT>);
+  f.push_back((const void*)spectra_kernel<__nv_bfloat16, 256, NT>);
+  f.push_back((const void*)spectra_kernel<uint16_t, 256, NT>);
+  f.push_back((const void*)spectra_kernel<U16Linear, 256, NT>);
+  f.push_back((const void*)spectra_kernel<float, 512, NT>);
+  f.push_back((const void*)spectra_kernel<__half, 512, NT>);
+  f.push_back((const void*)spectra_kernel<__nv_bfloat16, 512, NT>);
+  f.push_back((const void*)spectra_kernel<uint16_t, 512, NT>);
+  f.push_back((const void*)spectra_kernel<U16Linear, 512, NT>);
+  f.push_back((const void*)cols_kernel<256, NT>);
+  f.push_back((const void*)cols_kernel<512, NT>);
+  f.push_back((const void*)cols_tma_kernel<256, NT>);
+  f.push_back((const void*)cols_tma_kernel<512, NT>);
+  f.push_back((const void*)rows_kernel<256, NT>);
+  f.push_back((const void*)rows_kernel<512, NT>);
+  f.push_back((const void*)fbp_filter_kernel<256, NT>);
+  f.push_back((const void*)fbp_filter_kernel<512, NT>);
 }
 
 // Allows the dynamic-shared-memory kernels the device's opt-in maximum; called
@@ -868,21 +1012,16 @@ cudaError_t init_kernel_attributes() {
   int dev = 0, optin = 0;
   cudaError_t e = cudaGetDevice(&dev);
   if (e == cudaSuccess) e = cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  const void* fns[] = {(const void*)spectra_kernel<float, 256>,
-                       (const void*)spectra_kernel<__half, 256>,
-                       (const void*)spectra_kernel<__nv_bfloat16, 256>,
-                       (const void*)spectra_kernel<uint16_t, 256>,
-                       (const void*)spectra_kernel<U16Linear, 256>,
-                       (const void*)spectra_kernel<float, 512>,
-                       (const void*)spectra_kernel<__half, 512>,
-                       (const void*)spectra_kernel<__nv_bfloat16, 512>,
-                       (const void*)spectra_kernel<uint16_t, 512>,
-                       (const void*)spectra_kernel<U16Linear, 512>,
-                       (const void*)cols_kernel<256>, (const void*)cols_kernel<512>,
-                       (const void*)cols_tma_kernel<256>, (const void*)cols_tma_kernel<512>,
-                       (const void*)rows_kernel<256>, (const void*)rows_kernel<512>,
-                       (const void*)grid_kernel<4>, (const void*)grid_kernel<kMaxTaps>,
-                       (const void*)fbp_filter_kernel<256>, (const void*)fbp_filter_kernel<512>};
+  std::vector<const void*> fns;
+  add_fft_kernels<0>(fns);
+  add_fft_kernels<256>(fns);
+  add_fft_kernels<512>(fns);
+  add_fft_kernels<1024>(fns);
+  add_fft_kernels<2048>(fns);
+  add_fft_kernels<4096>(fns);
+  add_fft_kernels<8192>(fns);
+  fns.push_back((const void*)grid_kernel<4>);
+  fns.push_back((const void*)grid_kernel<kMaxTaps>);
   for (const void* f : fns) {
     if (e != cudaSuccess) break;
     e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
@@ -900,8 +1039,11 @@ template <typename T>
 static cudaError_t launch_spectra_t(const SpectraArgs& a, cudaStream_t s) {
   const int smem = fft_smem_bytes(a.pdim);
   dim3 grid(a.n_ang, a.pairs);
-  if (a.pdim <= 4096) spectra_kernel<T, 256><<<grid, a.pdim / 16, smem, s>>>(a);
-  else spectra_kernel<T, 512><<<grid, a.pdim / 16, smem, s>>>(a);
+#define GR_SPEC(NT)                                                                  \
+  if (a.pdim <= 4096) spectra_kernel<T, 256, NT><<<grid, a.pdim / 16, smem, s>>>(a); \
+  else spectra_kernel<T, (NT > 4096 || NT == 0) ? 512 : 256, NT><<<grid, a.pdim / 16, smem, s>>>(a)
+  GR_DISPATCH_N(a.pdim, GR_SPEC)
+#undef GR_SPEC
   return cudaGetLastError();
 }
 
@@ -985,23 +1127,32 @@ cudaError_t launch_cols(const ColArgs& a, cudaStream_t s) {
     if (r == CUDA_SUCCESS) {
       const int smem = (kTwSlots + G * a.M + 16) * (int)sizeof(float2) + (int)sizeof(uint64_t);
       dim3 grid(a.M / G, a.pairs);
-      if (threads <= 256) cols_tma_kernel<256><<<grid, threads, smem, s>>>(map, a, G, box_rows);
-      else cols_tma_kernel<512><<<grid, threads, smem, s>>>(map, a, G, box_rows);
+#define GR_COLT(NT)                                                                      \
+  if (threads <= 256) cols_tma_kernel<256, NT><<<grid, threads, smem, s>>>(map, a, G, box_rows); \
+  else cols_tma_kernel<512, NT><<<grid, threads, smem, s>>>(map, a, G, box_rows)
+      GR_DISPATCH_N(a.M, GR_COLT)
+#undef GR_COLT
       return cudaGetLastError();
     }
   }
   const int smem = (kTwSlots + G * (a.M + 16 / G)) * (int)sizeof(float2);
   dim3 grid(a.M / G, a.pairs);
-  if (G * (a.M / 16) <= 256) cols_kernel<256><<<grid, G * (a.M / 16), smem, s>>>(a, G);
-  else cols_kernel<512><<<grid, G * (a.M / 16), smem, s>>>(a, G);
+#define GR_COL(NT)                                                                       \
+  if (G * (a.M / 16) <= 256) cols_kernel<256, NT><<<grid, G * (a.M / 16), smem, s>>>(a, G); \
+  else cols_kernel<512, NT><<<grid, G * (a.M / 16), smem, s>>>(a, G)
+  GR_DISPATCH_N(a.M, GR_COL)
+#undef GR_COL
   return cudaGetLastError();
 }
 
 cudaError_t launch_rows(const RowArgs& a, cudaStream_t s) {
   const int smem = fft_smem_bytes(a.M);
   dim3 grid(a.M, a.pairs);
-  if (a.M <= 4096) rows_kernel<256><<<grid, a.M / 16, smem, s>>>(a);
-  else rows_kernel<512><<<grid, a.M / 16, smem, s>>>(a);
+#define GR_ROW(NT)                                                                   \
+  if (a.M <= 4096) rows_kernel<256, NT><<<grid, a.M / 16, smem, s>>>(a);            \
+  else rows_kernel<(NT > 4096 || NT == 0) ? 512 : 256, NT><<<grid, a.M / 16, smem, s>>>(a)
+  GR_DISPATCH_N(a.M, GR_ROW)
+#undef GR_ROW
   return cudaGetLastError();
 }
 
