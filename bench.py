@@ -294,6 +294,54 @@ def measure_slice_pipeline(G, sinos, th, n, a, dev, stream, peak):
     return out
 
 
+def measure_learned(sinos, th, n, a, dev, stream, args, centers_d):
+    """The learned narrow-kernel path on the same resident slices: narrow (C = 4)
+    gridrec + the trained correction network (projects_b200/correction_c4.npy),
+    timed with CUDA events; its held-out error against full-width gridrec on two
+    slices decides the fallback (tolerance 1e-3), as LearnedGridrec does."""
+    import torch
+
+    from projects_b200 import learned as Lrn
+    if sinos.dtype != torch.float32:
+        return None
+    S = min(64, sinos.shape[0])
+    lg = Lrn.LearnedGridrec(n, a, th, max_pairs=args.max_pairs, device=dev.index or 0)
+    x = sinos[:S]
+    c = centers_d[:S]
+    for _ in range(2):
+        lg.corrected(x, centers=c, stream=stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(3):
+        raw = torch.empty((S, lg.M0, lg.M0), device=dev)
+        lg.narrow.reconstruct_batch(x, raw, centers=c, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_narrow = e0.elapsed_time(e1) / 3000.0
+    e0.record(stream)
+    for _ in range(3):
+        y = lg.corrected(x, centers=c, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_learned = e0.elapsed_time(e1) / 3000.0
+    out, info = lg.reconstruct_batch(x[:4], centers=c[:4], stream=stream)
+    raw = torch.empty((2, lg.M0, lg.M0), device=dev)
+    lg.narrow.reconstruct_batch(x[:2], raw, centers=c[:2], stream=stream)
+    ref = torch.empty_like(raw)
+    lg.full.reconstruct_batch(x[:2], ref, centers=c[:2], stream=stream)
+    e_narrow = float(torch.linalg.vector_norm(raw - ref) / torch.linalg.vector_norm(ref))
+    lg.close()
+    return {"narrow_kernel": "PSWF C = 4 (3 x 3 taps), same grid and image size",
+            "narrow_slices_per_s": S / t_narrow,
+            "narrow_plus_cnn_slices_per_s": S / t_learned,
+            "held_out_rel_l2_vs_full_width": {"narrow": e_narrow,
+                                              "narrow_plus_cnn": info["held_out_rel_l2"]},
+            "tolerance": 1e-3, "fallback_to_full_width": info["fallback"],
+            "network": "3-layer 16-channel 3x3 residual CNN, BF16 tensor-core conv2, trained "
+                       "on 4096 slices of 1024 x 900 (projects_b200/train_correction.py)"}
+
+
 # ------------------------------------------------------------------ arms
 
 def run_reference(args, rank):
@@ -426,6 +474,10 @@ def run_b200(args, rank, world, local_rank):
                "steps": args.e2e_steps, "path": "gr_reconstruct_host, pinned host buffers"}
         del h_in, h_out
 
+    learned = None
+    if rank == 0 and not args.no_pipeline:
+        learned = measure_learned(sinos, th, n, a, dev, stream, args, centers_d)
+
     pipe = None
     if rank == 0 and not args.no_pipeline:
         pipe = measure_slice_pipeline(G, sinos, th, n, a, dev, stream, peaks()[0])
@@ -468,6 +520,7 @@ def run_b200(args, rank, world, local_rank):
             "e2e": e2e,
             "cpu_baseline": cpu,
             "slice_pipeline": pipe,
+            "learned": learned,
         }
         print(json.dumps(out), flush=True)
     plan.close()

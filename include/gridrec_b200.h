@@ -333,6 +333,26 @@ int gr_fbp_create(int n_det, int n_ang, const float* theta_deg, int max_slices, 
 int gr_fbp_reconstruct(gr_fbp* fbp, const float* sinos, int n_slices, float* recons, void* stream);
 int gr_fbp_destroy(gr_fbp* fbp);
 
+/* ---- Learned correction of narrow-kernel gridrec (no reference counterpart; the
+ * learned part of the project's specification).  A 3-layer, 16-channel, 3x3 residual
+ * CNN y = x + conv3(relu(conv2(relu(conv1(x))))) on n_img images of h x w (device
+ * float32).  params: gr_cnn_param_count() floats, layout w1[9][16], b1[16],
+ * w2[9][16][16], b2[16], w3[9][16], b3.  conv2 runs on BF16 tensor cores with FP32
+ * accumulation; hidden activations are stored as BF16.  The workspace
+ * (gr_cnn_workspace_bytes) keeps the forward activations that gr_cnn_backward uses:
+ * call backward after forward on the same images and workspace.  gr_cnn_backward
+ * writes the mean-squared-loss gradient to grads and the loss to *loss (synchronises
+ * when loss is non-NULL); gr_cnn_adam applies one Adam step (step counts from 1). */
+int gr_cnn_param_count(void);
+size_t gr_cnn_workspace_bytes(int n_img, int h, int w);
+int gr_cnn_forward(const float* params, const float* x, float* y, int n_img, int h, int w,
+                   void* workspace, void* stream);
+int gr_cnn_backward(const float* params, const float* x, const float* y, const float* target,
+                    int n_img, int h, int w, float* grads, double* loss, void* workspace,
+                    void* stream);
+int gr_cnn_adam(float* params, const float* grads, float* m, float* v, int step, float lr,
+                float beta1, float beta2, float eps, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -16,7 +16,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgridrec_b200.so")
-SOURCES = ["gridrec_kernels.cu", "gridrec_plan.cu", "gridrec_prep.cu", "gridrec_fbp.cu"]
+SOURCES = ["gridrec_kernels.cu", "gridrec_plan.cu", "gridrec_prep.cu", "gridrec_fbp.cu",
+           "gridrec_cnn.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -1020,6 +1020,7 @@ cudaError_t init_kernel_attributes() {
   add_fft_kernels<2048>(fns);
   add_fft_kernels<4096>(fns);
   add_fft_kernels<8192>(fns);
+  fns.push_back((const void*)grid_kernel<3>);
   fns.push_back((const void*)grid_kernel<4>);
   fns.push_back((const void*)grid_kernel<kMaxTaps>);
   for (const void* f : fns) {
@@ -1071,7 +1072,9 @@ cudaError_t launch_grid(const GridArgs& a, int ntaps, cudaStream_t s) {
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
   const int smem = grid_smem_bytes();
   int per_sm = 0;
-  if (ntaps <= 4) {
+  if (ntaps <= 3) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_kernel<3>, kGridWarps * 32, smem);
+  } else if (ntaps <= 4) {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_kernel<4>, kGridWarps * 32, smem);
   } else {
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_kernel<kMaxTaps>, kGridWarps * 32, smem);
@@ -1079,7 +1082,8 @@ cudaError_t launch_grid(const GridArgs& a, int ntaps, cudaStream_t s) {
   const long groups = (a.pairs + kGridPairs - 1) / kGridPairs;
   const long want = ((long)a.n_items * groups + kGridWarps - 1) / kGridWarps;
   const int blocks = (int)std::min<long>(want, (long)std::max(per_sm, 1) * sms);
-  if (ntaps <= 4) grid_kernel<4><<<blocks, kGridWarps * 32, smem, s>>>(a);
+  if (ntaps <= 3) grid_kernel<3><<<blocks, kGridWarps * 32, smem, s>>>(a);
+  else if (ntaps <= 4) grid_kernel<4><<<blocks, kGridWarps * 32, smem, s>>>(a);
   else grid_kernel<kMaxTaps><<<blocks, kGridWarps * 32, smem, s>>>(a);
   e = cudaGetLastError();
   if (e != cudaSuccess || a.n_split_tiles == 0) return e;

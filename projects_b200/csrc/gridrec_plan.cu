@@ -273,7 +273,9 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
                    [](const TRun& a, const TRun& b) { return a.tile < b.tile; });
   wl->runs.resize(all.size());
   std::vector<long> run_cost(all.size());
-  const int nt = (int)std::floor(L) + 1 <= 4 ? 4 : kMaxTaps;  // the kernel's NT
+  // the kernel's NT: footprint rows per sample (3 for L < 3, e.g. C = 4 at sampl = 1)
+  const int taps = (int)std::floor(L) + 1;
+  const int nt = taps <= 3 ? 3 : (taps <= 4 ? 4 : kMaxTaps);
   const int spw = 32 / nt;
   std::vector<int> first(n_tiles + 1, 0);
   for (size_t i = 0; i < all.size(); ++i) {

@@ -1,0 +1,166 @@
+"""Learned narrow-kernel gridrec: gridding with the narrowest PSWF kernel of the
+reference's table (C = 4, 3 x 3 taps instead of 4 x 4 at C = 6) followed by a
+3-layer, 16-channel residual CNN that corrects the slice toward full-width
+gridrec.  Plain gridrec stays the fallback and the judge: a batch whose held-out
+error against the full kernel exceeds the tolerance is recomputed with it.
+
+The network runs on this library's own kernels (projects_b200/csrc/gridrec_cnn.cu:
+BF16 tensor-core 16 -> 16 layer, FP32 accumulation), trained on the GPU by its own
+forward, backward and Adam kernels.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+from . import gridrec as G
+
+N_PARAMS = 2625
+PARAMS_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "correction_c4.npy")
+
+
+def _lib():
+    L = G.lib()
+    if not getattr(L, "_cnn_bound", False):
+        vp, i_, f_ = C.c_void_p, C.c_int, C.c_float
+        L.gr_cnn_param_count.restype = C.c_int
+        L.gr_cnn_workspace_bytes.argtypes = [i_, i_, i_]
+        L.gr_cnn_workspace_bytes.restype = C.c_size_t
+        L.gr_cnn_forward.argtypes = [vp, vp, vp, i_, i_, i_, vp, vp]
+        L.gr_cnn_backward.argtypes = [vp, vp, vp, vp, i_, i_, i_, vp, C.POINTER(C.c_double), vp,
+                                      vp]
+        L.gr_cnn_adam.argtypes = [vp, vp, vp, vp, i_, f_, f_, f_, f_, vp]
+        L._cnn_bound = True
+    return L
+
+
+def init_params(seed=0):
+    """He-scaled random first two layers; the last layer starts at zero, so the
+    untrained network is the identity (y = x)."""
+    rng = np.random.default_rng(seed)
+    p = np.zeros(N_PARAMS, np.float32)
+    p[0:144] = rng.normal(0, np.sqrt(2.0 / 9), 144)
+    p[160:2464] = rng.normal(0, np.sqrt(2.0 / 144), 2304)
+    return p
+
+
+class CorrectionNet:
+    """The residual CNN on a CUDA device (parameters, Adam state, workspace)."""
+
+    def __init__(self, params=None, device="cuda"):
+        import torch
+        if G.lib().gr_cnn_param_count() != N_PARAMS:
+            raise RuntimeError("library CNN parameter count mismatch")
+        p = init_params() if params is None else np.asarray(params, np.float32)
+        self.params = torch.tensor(p, device=device)
+        self.m = torch.zeros_like(self.params)
+        self.v = torch.zeros_like(self.params)
+        self.grads = torch.zeros_like(self.params)
+        self.step = 0
+        self._ws = None
+        self._ws_shape = None
+
+    def _workspace(self, n, h, w):
+        import torch
+        if self._ws_shape != (n, h, w):
+            nbytes = _lib().gr_cnn_workspace_bytes(n, h, w)
+            self._ws = torch.empty(nbytes, dtype=torch.uint8, device=self.params.device)
+            self._ws_shape = (n, h, w)
+        return self._ws
+
+    def forward(self, x, y=None, stream=None):
+        """x: (N, H, W) float32 CUDA tensor -> y = x + correction."""
+        import torch
+        n, h, w = x.shape
+        if y is None:
+            y = torch.empty_like(x)
+        ws = self._workspace(n, h, w)
+        G._check(_lib().gr_cnn_forward(G._ptr(self.params), G._ptr(x), G._ptr(y), n, h, w,
+                                       G._ptr(ws), G._stream_ptr(stream)), "gr_cnn_forward")
+        return y
+
+    def loss_and_grads(self, x, target, stream=None):
+        """Forward + backward; fills self.grads, returns the mean-squared loss."""
+        y = self.forward(x, stream=stream)
+        n, h, w = x.shape
+        loss = C.c_double()
+        G._check(_lib().gr_cnn_backward(G._ptr(self.params), G._ptr(x), G._ptr(y),
+                                        G._ptr(target), n, h, w, G._ptr(self.grads),
+                                        C.byref(loss), G._ptr(self._ws), G._stream_ptr(stream)),
+                 "gr_cnn_backward")
+        return loss.value
+
+    def train_step(self, x, target, lr=1e-3, stream=None):
+        loss = self.loss_and_grads(x, target, stream)
+        self.step += 1
+        G._check(_lib().gr_cnn_adam(G._ptr(self.params), G._ptr(self.grads), G._ptr(self.m),
+                                    G._ptr(self.v), self.step, lr, 0.9, 0.999, 1e-8,
+                                    G._stream_ptr(stream)), "gr_cnn_adam")
+        return loss
+
+    def numpy_params(self):
+        return self.params.detach().cpu().numpy().copy()
+
+
+class LearnedGridrec:
+    """Narrow-kernel (C = 4) gridrec + correction CNN, with full-width fallback.
+
+    reconstruct_batch() reconstructs with the narrow plan, corrects with the
+    network, then reconstructs the first pair with the full plan and compares:
+    if its relative L2 error exceeds `tol`, the whole batch is recomputed with
+    the full plan (the result is then plain gridrec)."""
+
+    def __init__(self, n_det, n_ang, theta_deg, params=None, tol=1e-3, max_pairs=8,
+                 filter=G.FILTER_HANN, device=0):
+        self.narrow = G.Plan(n_det, n_ang, theta_deg, filter=filter, pswf_c=4.0,
+                             max_pairs=max_pairs, device=device)
+        self.full = G.Plan(n_det, n_ang, theta_deg, filter=filter, pswf_c=6.0,
+                           max_pairs=max_pairs, device=device)
+        if self.narrow.M0 != self.full.M0:
+            raise ValueError("narrow and full plans disagree on the image size")
+        if params is None and os.path.exists(PARAMS_FILE):
+            params = np.load(PARAMS_FILE)
+        self.net = CorrectionNet(params, device=f"cuda:{device}")
+        self.tol = tol
+        self.M0 = self.full.M0
+
+    @staticmethod
+    def scales(images):
+        """Per-slice RMS, (S, 1, 1): the network sees every slice at unit RMS, so
+        its correction does not depend on the absolute scale of the values (which
+        follows the pixel size, i.e. the detector width)."""
+        import torch
+        return torch.sqrt(torch.mean(images * images, dim=(1, 2), keepdim=True)).clamp_min(1e-30)
+
+    def correct(self, raw, stream=None):
+        """s * net(raw / s) per slice."""
+        s = self.scales(raw)
+        return self.net.forward((raw / s).contiguous(), stream=stream) * s
+
+    def corrected(self, sinos, centers=None, stream=None):
+        """Narrow-kernel images corrected by the network, (S, M0, M0)."""
+        import torch
+        S = sinos.shape[0]
+        raw = torch.empty((S, self.M0, self.M0), dtype=torch.float32, device=sinos.device)
+        self.narrow.reconstruct_batch(sinos, raw, centers=centers, stream=stream)
+        return self.correct(raw, stream=stream)
+
+    def reconstruct_batch(self, sinos, centers=None, stream=None):
+        """Returns (images, info): info = {"held_out_rel_l2", "fallback"}."""
+        import torch
+        out = self.corrected(sinos, centers, stream)
+        k = min(2, sinos.shape[0])
+        ref = torch.empty((k, self.M0, self.M0), dtype=torch.float32, device=sinos.device)
+        self.full.reconstruct_batch(sinos[:k], ref, centers=None if centers is None
+                                    else centers[:k], stream=stream)
+        err = float(torch.linalg.vector_norm(out[:k] - ref) / torch.linalg.vector_norm(ref))
+        fallback = err > self.tol
+        if fallback:
+            self.full.reconstruct_batch(sinos, out, centers=centers, stream=stream)
+        return out, {"held_out_rel_l2": err, "fallback": fallback}
+
+    def close(self):
+        self.narrow.close()
+        self.full.close()
