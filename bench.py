@@ -146,6 +146,22 @@ class ClockSampler:
                 "reasons": sorted(reasons)}
 
 
+def max_over_ranks(seconds, device, world):
+    """The job's time: the maximum of the ranks' elapsed times (all_reduce MAX)."""
+    if world <= 1:
+        return seconds
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([seconds], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def rank_first_seed(rank, slices_per_rank):
+    """Each rank reconstructs its own slices (weak scaling): seeds rank*S .. rank*S+S-1."""
+    return rank * slices_per_rank
+
+
 def make_sinograms(n_slices, n_det, n_ang, first_seed, device):
     """Random-ellipse sinograms (seed = slice index) on the device + centres."""
     import torch
@@ -383,7 +399,7 @@ def run_b200(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     S, n, a = args.slices, args.n_det, args.n_ang
-    th, sinos, centers = make_sinograms(S, n, a, rank * S, dev)
+    th, sinos, centers = make_sinograms(S, n, a, rank_first_seed(rank, S), dev)
     tdt = {"f32": torch.float32, "f16": torch.float16, "bf16": torch.bfloat16}[args.dtype]
     if tdt != torch.float32:
         sinos = sinos.to(tdt)
@@ -428,9 +444,7 @@ def run_b200(args, rank, world, local_rank):
     graph.close()
     if world > 1:
         dist.barrier()
-        t = torch.tensor([elapsed], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = max_over_ranks(elapsed, dev, world)
     value = S * args.steps * world / elapsed
 
     # roofline of the dominant kernel
@@ -466,11 +480,7 @@ def run_b200(args, rank, world, local_rank):
         for _ in range(args.e2e_steps):
             plan.reconstruct_host(h_in, h_out, centers=centers, stream=int(stream.cuda_stream))
             float(h_out[0, plan.M0 // 2, plan.M0 // 2])   # read the result on the host
-        te = time.perf_counter() - t0
-        if world > 1:
-            t = torch.tensor([te], device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            te = float(t.item())
+        te = max_over_ranks(time.perf_counter() - t0, dev, world)
         e2e = {"value": S * args.e2e_steps * world / te, "unit": UNIT,
                "h2d_bytes_per_step": int(h_in.numel() * h_in.element_size()),
                "d2h_bytes_per_step": int(h_out.numel() * h_out.element_size()),
@@ -594,12 +604,7 @@ def run_uneven(args, rank, world, local_rank):
             graph.launch(stream)
         e1.record(stream)
         torch.cuda.synchronize()
-        t = e0.elapsed_time(e1) / 1000.0
-        if world > 1:
-            tt = torch.tensor([t], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
-        return t
+        return max_over_ranks(e0.elapsed_time(e1) / 1000.0, dev, world)
 
     total = sum(g["S"] for g in groups)
     steps = max(1, min(args.steps, 10))
@@ -705,10 +710,7 @@ def run_stream(args, rank, world, local_rank):
                                   stream=int(stream.cuda_stream))
             float(h_out[K - 1, plan.M0 // 2, plan.M0 // 2])
         te = time.perf_counter() - t0
-    if world > 1:
-        tt = torch.tensor([te], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        te = float(tt.item())
+    te = max_over_ranks(te, dev, world)
     in_b = int(h_in.numel() * 2) * (total // K)
     out_b = int(h_out.numel() * 4) * (total // K)
     if rank == 0:
