@@ -86,6 +86,10 @@ typedef struct {
   int ltbl;                /* convolvent table length (512) */
   int max_pairs;           /* slice pairs processed per launch (workspace size) */
   int device;              /* CUDA device ordinal (GridRec::setGPUDeviceID) */
+  int geom;                /* angle geometry of GridrecCPP's sg_struct: 0 = the theta_deg
+                              list; 1 / 2 = n_ang angles evenly over pi / 2 pi from its FP32
+                              rotation recurrence (Gridrec5.2/grid.cpp:540-553), theta_deg
+                              unused */
 } gr_params;
 
 typedef struct gr_plan gr_plan;

@@ -217,7 +217,7 @@ def _ref_lib(name, real):
         elif name == "libgridrec_refb.so":
             lib.refb_gridrec_pair.argtypes = [C.c_int, C.c_int, rp, C.c_float, C.c_char_p,
                                               C.c_float, C.c_float, C.c_int, rp, rp, rp, rp,
-                                              C.c_int]
+                                              C.c_int, C.c_int]
             lib.refb_gridrec_pair.restype = C.c_int
         else:
             lib.ref_gridrec_pair.argtypes = [C.c_int, C.c_int, rp, C.c_int, rp, rp, rp, rp,
@@ -265,7 +265,7 @@ def ref_gridrec_pairs(sinos, theta_deg, filter=1):
 
 
 def refb_gridrec_pair(sino1, sino2, theta_deg, center, filter_name="shlo", C_=6.0, sampl=1.2,
-                      ltbl=512):
+                      ltbl=512, geom=0):
     """GridrecCPP 5.2 (explicit centre/sampl/filter name).  Returns (out1, out2, M0)."""
     lib = _ref_lib("libgridrec_refb.so", np.float32)
     n_ang, n_det = sino1.shape
@@ -274,12 +274,12 @@ def refb_gridrec_pair(sino1, sino2, theta_deg, center, filter_name="shlo", C_=6.
     s2 = np.ascontiguousarray(sino2, np.float32)
     dummy = np.zeros(1, np.float32)
     m0 = lib.refb_gridrec_pair(n_det, n_ang, th, center, filter_name.encode(), C_, sampl, ltbl,
-                               s1, s2, dummy, dummy, 0)
+                               s1, s2, dummy, dummy, 0, int(geom))
     stride = max(m0, n_det)
     o1 = np.zeros((m0, stride), np.float32)
     o2 = np.zeros((m0, stride), np.float32)
     lib.refb_gridrec_pair(n_det, n_ang, th, center, filter_name.encode(), C_, sampl, ltbl,
-                          s1, s2, o1, o2, stride)
+                          s1, s2, o1, o2, stride, int(geom))
     return o1, o2, m0
 
 

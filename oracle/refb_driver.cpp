@@ -25,7 +25,7 @@ extern "C" {
 int refb_gridrec_pair(int n_det, int n_ang, float* theta_deg, float center,
                       const char* filter_name, float C, float sampl, int ltbl,
                       float* sino1, float* sino2, float* out1, float* out2,
-                      int out_stride) {
+                      int out_stride, int geom) {
   pswf_struct* pswf = nullptr;
   get_pswf(C, &pswf);
   grid_struct gp;
@@ -42,7 +42,7 @@ int refb_gridrec_pair(int n_det, int n_ang, float* theta_deg, float center,
   sg_struct sg;
   sg.n_ang = n_ang;
   sg.n_det = n_det;
-  sg.geom = 0;
+  sg.geom = geom;  // 0: the angle list; 1 / 2: uniform over pi / 2 pi
   sg.angles = theta_deg;
   sg.center = center;
   long im = 0;

@@ -400,8 +400,9 @@ int geometry(const gr_params* prm, const Pswf* pw, Geometry* g) {
 
 int check_params(const gr_params* prm, const Pswf** pw) {
   if (!prm) return fail(GR_ERR_ARG, "null argument");
-  if (prm->n_det < 9 || prm->n_ang < 1 || !prm->theta_deg)
-    return fail(GR_ERR_ARG, "need n_det >= 9, n_ang >= 1 and a theta list");
+  if (prm->geom < 0 || prm->geom > 2) return fail(GR_ERR_ARG, "geom must be 0, 1 or 2");
+  if (prm->n_det < 9 || prm->n_ang < 1 || (prm->geom == 0 && !prm->theta_deg))
+    return fail(GR_ERR_ARG, "need n_det >= 9, n_ang >= 1 and (geom 0) a theta list");
   if (prm->ltbl < 1 || prm->ltbl > 1024) return fail(GR_ERR_ARG, "ltbl must be in [1, 1024]");
   if (!(prm->sampl >= 1.0f) || prm->sampl > 4.0f)
     return fail(GR_ERR_ARG, "sampl must be in [1, 4]");
@@ -412,11 +413,35 @@ int check_params(const gr_params* prm, const Pswf** pw) {
 }
 
 // Direction vectors in grid units: half 0 = scale*(cos, sin), half 1 = mirrored.
+// geom 0: FP64 sin/cos of the degree list (the GridRec class, gridrec.cu:724-770).
+// geom 1 / 2: GridrecCPP's uniform angles over pi / 2 pi, generated by its FP32
+// rotation recurrence from (sin, cos) = (0, 1) (Gridrec5.2/grid.cpp:540-553, pi =
+// 3.14159265359), drift included, since that is what its gridding uses.
 std::vector<double> directions(const gr_params* prm, double scale) {
   std::vector<double> dxy(4 * (size_t)prm->n_ang);
+  std::vector<float> rs, rc;
+  if (prm->geom != 0) {
+    const float dtheta = (float)(prm->geom * 3.14159265359 / prm->n_ang);
+    const float dcos = (float)std::cos((double)dtheta), dsin = (float)std::sin((double)dtheta);
+    rs.assign(prm->n_ang, 0.f);
+    rc.assign(prm->n_ang, 1.f);
+    for (int j = 1; j < prm->n_ang; ++j) {
+      const float a = dcos * rs[j - 1], b = dsin * rc[j - 1];
+      const float c = dcos * rc[j - 1], d = dsin * rs[j - 1];
+      rs[j] = a + b;
+      rc[j] = c - d;
+    }
+  }
   for (int n = 0; n < prm->n_ang; ++n) {
-    const double th = (double)prm->theta_deg[n] * (M_PI / 180.0);
-    const double cs = std::cos(th) * scale, sn = std::sin(th) * scale;
+    double cs, sn;
+    if (prm->geom == 0) {
+      const double th = (double)prm->theta_deg[n] * (M_PI / 180.0);
+      cs = std::cos(th) * scale;
+      sn = std::sin(th) * scale;
+    } else {
+      cs = (double)rc[n] * scale;
+      sn = (double)rs[n] * scale;
+    }
     dxy[4 * n + 0] = cs;
     dxy[4 * n + 1] = sn;
     dxy[4 * n + 2] = -cs;

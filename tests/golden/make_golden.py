@@ -51,14 +51,16 @@ def case_gridrec_class(name, n, a, filt, seed, theta=None):
                         ref64_1=q1[:m0, :m0], ref64_2=q2[:m0, :m0])
 
 
-def case_gridrec_cpp(name, n, a, center, fname, C_, sampl, seed):
-    """GridrecCPP 5.2 with explicit centre, oversampling, PSWF C and filter name."""
+def case_gridrec_cpp(name, n, a, center, fname, C_, sampl, seed, geom=0):
+    """GridrecCPP 5.2 with explicit centre, oversampling, PSWF C and filter name; geom 1
+    generates its angles (uniform on [0, pi)) by its FP32 recurrence."""
     s1, s2, th = _pair_phantom(n, a, center, seed)
     b1, b2, m0 = O.refb_gridrec_pair(s1, s2, th, center=center, filter_name=fname, C_=C_,
-                                     sampl=sampl)
+                                     sampl=sampl, geom=geom)
     np.savez_compressed(os.path.join(HERE, f"case_{name}.npz"), kind="gridrec_cpp", sino1=s1,
                         sino2=s2, theta=th, n_det=n, n_ang=a, filter_name=fname, center=center,
-                        sampl=sampl, C=C_, M0=m0, refb_1=b1[:m0, :m0], refb_2=b2[:m0, :m0])
+                        sampl=sampl, C=C_, M0=m0, refb_1=b1[:m0, :m0], refb_2=b2[:m0, :m0],
+                        geom=geom)
 
 
 def prep_cases(rng):
@@ -125,6 +127,7 @@ def main():
     case_gridrec_cpp("b64x40_c31.7_C4_hann", 64, 40, 31.7, "hann", 4.0, 1.0, 22)
     case_gridrec_cpp("b120x72_c61.2_C7_s1.2_shepp", 120, 72, 61.2, "shepp", 7.0, 1.2, 23)
     case_gridrec_cpp("b72x45_c36.5_C5_hamming", 72, 45, 36.5, "hamming", 5.0, 1.0, 24)
+    case_gridrec_cpp("b96x90_c47.5_geom1_hann", 96, 90, 47.5, "hann", 6.0, 1.0, 25, geom=1)
     if O.prep_ref_available():
         prep_cases(np.random.default_rng(8))
     print("\n".join(sorted(f for f in os.listdir(HERE) if f.endswith(".npz"))))

@@ -38,7 +38,8 @@ def _gpu_pair(s1, s2, theta, **kw):
 @pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
 def test_pair_against_goldens(case):
     g1, g2 = _gpu_pair(case["sino1"], case["sino2"], case["theta"], center=case["center"],
-                       filter=case["filter"], pswf_c=case["C"], sampl=case["sampl"])
+                       filter=case["filter"], pswf_c=case["C"], sampl=case["sampl"],
+                       geom=case["geom"])
     m = case["M0"]
     assert g1.shape == (m, m)
     o1, o2 = O.port_gridrec_pair(case["sino1"], case["sino2"], case["theta"],

@@ -177,3 +177,18 @@ def _build_shim(tmp_path):
 def test_cxx_shim_compiles_against_the_c_abi(tmp_path):
     """include/gridrec_b200.hpp (the GridRec-compatible class) builds and links."""
     assert os.path.exists(_build_shim(tmp_path))
+
+
+def test_geom_recurrence_needs_no_angle_list():
+    """geom 1 (GridrecCPP's uniform angles from its FP32 recurrence) takes no theta list;
+    geom 3 is rejected.  Host-only (the work-list export)."""
+    ni, nr, tv = C.c_int(), C.c_int(), C.c_int()
+    p, _ = G.make_params(64, 30, np.zeros(30, np.float32))
+    p.theta_deg = None
+    p.geom = 1
+    assert G.lib().gr_worklist_export(C.byref(p), C.byref(ni), C.byref(nr), C.byref(tv), None,
+                                      None, None, 0, 0) == 0
+    assert ni.value > 0 and nr.value > 0
+    p.geom = 3
+    assert G.lib().gr_worklist_export(C.byref(p), C.byref(ni), C.byref(nr), C.byref(tv), None,
+                                      None, None, 0, 0) == -1
