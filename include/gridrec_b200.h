@@ -90,6 +90,12 @@ typedef struct {
                               list; 1 / 2 = n_ang angles evenly over pi / 2 pi from its FP32
                               rotation recurrence (Gridrec5.2/grid.cpp:540-553), theta_deg
                               unused */
+  /* GridrecCPP grid_struct extras (Gridrec5.2/grid.cpp:54-147, 225-275): */
+  float roi_size;          /* R: the reconstructed region spans R * n_det pixels (0 = 1) */
+  float pixel_size;        /* MaxPixSiz: M = next pow2 >= sampl * R * n_det / pixel_size
+                              (0 = 1) */
+  float roi_x0, roi_y0;    /* ROI offset X0, Y0: C1 times exp(-i j (X0 cos + Y0 sin) pi),
+                              C2 times its conjugate */
 } gr_params;
 
 typedef struct gr_plan gr_plan;

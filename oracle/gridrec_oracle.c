@@ -112,10 +112,12 @@ int orc_sizes(const orc_params* p, orc_sizes_t* s) {
   if (!pw) return -2;
   long pdim = 1, itmp = p->n_det - 1;
   while (itmp) { pdim <<= 1; itmp >>= 1; }              /* gridrec.cu:243-249 */
-  double D0 = p->n_det;                                   /* R = 1 */
+  const double R = p->roi_size > 0 ? p->roi_size : 1.0;
+  const double pix = p->pixel_size > 0 ? p->pixel_size : 1.0;
+  double D0 = R * p->n_det;                               /* grid.cpp:95-96 */
   double D1 = p->sampl * D0;
   long M = 1;
-  itmp = (long)(D1 - 1);                                  /* MaxPixSiz = 1 */
+  itmp = (long)(D1 / pix - 1);                            /* grid.cpp:100-106 */
   while (itmp) { M <<= 1; itmp >>= 1; }                   /* gridrec.cu:254-260 */
   long M02 = (long)floor((double)(M / 2) / p->sampl - 0.5);  /* gridrec.cu:262 */
   if (M02 < 0) M02 = 0;
@@ -259,7 +261,13 @@ int orc_grid(const orc_params* p, const double* theta_deg, const double* spec,
     double sn = sin(th), cs = cos(th);
     const double* c1 = spec + 2 * ((n * 2 + 0) * J);
     const double* c2 = spec + 2 * ((n * 2 + 1) * J);
+    /* ROI offset (GridrecCPP grid.cpp:237, 258-268): C1 times exp(-i j off), C2 times
+     * its conjugate, off = (X0 cos + Y0 sin) pi */
+    const double off = (p->x0 * cs + p->y0 * sn) * ORC_PI;
     for (long j = 1; j < J; ++j) {
+      const double pr = cos(j * off), pi = -sin(j * off);
+      const double a1r = c1[2 * j] * pr - c1[2 * j + 1] * pi, a1i = c1[2 * j] * pi + c1[2 * j + 1] * pr;
+      const double a2r = c2[2 * j] * pr + c2[2 * j + 1] * pi, a2i = -c2[2 * j] * pi + c2[2 * j + 1] * pr;
       double r = s.scale * j;
       double U = r * cs + M2, V = r * sn + M2;
       long iul = (long)ceil(U - L2), iuh = (long)floor(U + L2);
@@ -276,10 +284,10 @@ int orc_grid(const orc_params* p, const double* theta_deg, const double* spec,
           double w = wu * wv[k];
           double* h1 = H + 2 * (iu * M + iv);
           double* h2 = H + 2 * ((M - iu) * M + (M - iv));
-          h1[0] += w * c1[2 * j];
-          h1[1] += w * c1[2 * j + 1];
-          h2[0] += w * c2[2 * j];
-          h2[1] += w * c2[2 * j + 1];
+          h1[0] += w * a1r;
+          h1[1] += w * a1i;
+          h2[0] += w * a2r;
+          h2[1] += w * a2i;
         }
       }
     }

@@ -14,6 +14,11 @@ typedef struct {
   double C;                /* PSWF parameter: 4.0, 4.2, 5.0, 6.0 or 7.0 */
   double sampl;            /* oversampling request (1.0 = GridRec class default) */
   int ltbl;                /* convolvent table length (512) */
+  /* GridrecCPP grid_struct extras (Gridrec5.2/grid.cpp:54-147, 225-275); 0 selects the
+   * default of the first two (1.0) */
+  double roi_size;         /* R: ROI size as a fraction of n_det */
+  double pixel_size;       /* MaxPixSiz */
+  double x0, y0;           /* ROI offset */
 } orc_params;
 
 typedef struct {

@@ -25,7 +25,8 @@ _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 class OrcParams(C.Structure):
     _fields_ = [("n_det", C.c_int), ("n_ang", C.c_int), ("center1", C.c_double),
                 ("center2", C.c_double), ("filter", C.c_int), ("C", C.c_double),
-                ("sampl", C.c_double), ("ltbl", C.c_int)]
+                ("sampl", C.c_double), ("ltbl", C.c_int), ("roi_size", C.c_double),
+                ("pixel_size", C.c_double), ("x0", C.c_double), ("y0", C.c_double)]
 
 
 class OrcSizes(C.Structure):
@@ -71,12 +72,13 @@ def port_lib():
     return _port
 
 
-def params(n_det, n_ang, center1=None, center2=None, filter=1, C_=6.0, sampl=1.0, ltbl=512):
+def params(n_det, n_ang, center1=None, center2=None, filter=1, C_=6.0, sampl=1.0, ltbl=512,
+           roi_size=1.0, pixel_size=1.0, x0=0.0, y0=0.0):
     # GridRec::init: center = sinogram_x_dim / 2 in integer arithmetic (gridrec.cu:227)
     c1 = float(n_det // 2) if center1 is None else float(center1)
     c2 = c1 if center2 is None else float(center2)
     return OrcParams(int(n_det), int(n_ang), c1, c2, int(filter), float(C_), float(sampl),
-                     int(ltbl))
+                     int(ltbl), float(roi_size), float(pixel_size), float(x0), float(y0))
 
 
 def port_sizes(p: OrcParams) -> OrcSizes:
@@ -124,10 +126,12 @@ def port_fft2d(H):
 
 
 def port_gridrec_pair(sino1, sino2, theta_deg, center1=None, center2=None, filter=1,
-                      C_=6.0, sampl=1.0, ltbl=512, out_stride=None):
+                      C_=6.0, sampl=1.0, ltbl=512, out_stride=None, roi_size=1.0,
+                      pixel_size=1.0, x0=0.0, y0=0.0):
     """float64 gridrec of one pair; returns (out1, out2) of shape (M0, stride)."""
     n_ang, n_det = sino1.shape
-    p = params(n_det, n_ang, center1, center2, filter, C_, sampl, ltbl)
+    p = params(n_det, n_ang, center1, center2, filter, C_, sampl, ltbl, roi_size, pixel_size,
+               x0, y0)
     s = port_sizes(p)
     stride = max(n_det, s.M0) if out_stride is None else out_stride
     o1 = np.zeros((s.M0, stride))
@@ -217,7 +221,8 @@ def _ref_lib(name, real):
         elif name == "libgridrec_refb.so":
             lib.refb_gridrec_pair.argtypes = [C.c_int, C.c_int, rp, C.c_float, C.c_char_p,
                                               C.c_float, C.c_float, C.c_int, rp, rp, rp, rp,
-                                              C.c_int, C.c_int]
+                                              C.c_int, C.c_int, C.c_float, C.c_float, C.c_float,
+                                              C.c_float]
             lib.refb_gridrec_pair.restype = C.c_int
         else:
             lib.ref_gridrec_pair.argtypes = [C.c_int, C.c_int, rp, C.c_int, rp, rp, rp, rp,
@@ -265,7 +270,7 @@ def ref_gridrec_pairs(sinos, theta_deg, filter=1):
 
 
 def refb_gridrec_pair(sino1, sino2, theta_deg, center, filter_name="shlo", C_=6.0, sampl=1.2,
-                      ltbl=512, geom=0):
+                      ltbl=512, geom=0, roi_size=1.0, pixel_size=1.0, x0=0.0, y0=0.0):
     """GridrecCPP 5.2 (explicit centre/sampl/filter name).  Returns (out1, out2, M0)."""
     lib = _ref_lib("libgridrec_refb.so", np.float32)
     n_ang, n_det = sino1.shape
@@ -274,12 +279,12 @@ def refb_gridrec_pair(sino1, sino2, theta_deg, center, filter_name="shlo", C_=6.
     s2 = np.ascontiguousarray(sino2, np.float32)
     dummy = np.zeros(1, np.float32)
     m0 = lib.refb_gridrec_pair(n_det, n_ang, th, center, filter_name.encode(), C_, sampl, ltbl,
-                               s1, s2, dummy, dummy, 0, int(geom))
+                               s1, s2, dummy, dummy, 0, int(geom), roi_size, pixel_size, x0, y0)
     stride = max(m0, n_det)
     o1 = np.zeros((m0, stride), np.float32)
     o2 = np.zeros((m0, stride), np.float32)
     lib.refb_gridrec_pair(n_det, n_ang, th, center, filter_name.encode(), C_, sampl, ltbl,
-                          s1, s2, o1, o2, stride, int(geom))
+                          s1, s2, o1, o2, stride, int(geom), roi_size, pixel_size, x0, y0)
     return o1, o2, m0
 
 

@@ -25,17 +25,18 @@ extern "C" {
 int refb_gridrec_pair(int n_det, int n_ang, float* theta_deg, float center,
                       const char* filter_name, float C, float sampl, int ltbl,
                       float* sino1, float* sino2, float* out1, float* out2,
-                      int out_stride, int geom) {
+                      int out_stride, int geom, float roi_size, float pixel_size, float x0,
+                      float y0) {
   pswf_struct* pswf = nullptr;
   get_pswf(C, &pswf);
   grid_struct gp;
   std::memset(&gp, 0, sizeof(gp));
   gp.pswf = pswf;
   gp.sampl = sampl;
-  gp.MaxPixSiz = 1.0f;
-  gp.R = 1.0f;
-  gp.X0 = 0.0f;
-  gp.Y0 = 0.0f;
+  gp.MaxPixSiz = pixel_size;
+  gp.R = roi_size;
+  gp.X0 = x0;
+  gp.Y0 = y0;
   std::strncpy(gp.fname, filter_name, sizeof(gp.fname) - 1);
   gp.filter = get_filter(gp.fname);
   gp.ltbl = ltbl;

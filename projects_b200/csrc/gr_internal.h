@@ -62,6 +62,7 @@ struct SpectraArgs {
   float2* spec;          // [pair][n_ang][2][J]
   const float2* tw;      // two-level twiddle table for pdim (see gridrec_kernels.cu)
   int n_det, n_ang, pdim, J, pairs;
+  const double* roi_off; // per angle (X0 cos + Y0 sin) pi of the ROI offset, or null
 };
 
 struct PhaseArgs {

@@ -537,6 +537,13 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
       c1.y = q.x * F.y + q.y * F.x - q.z * G.y + q.w * G.x;
       c2.x = q.x * G.x + q.y * G.y + q.z * F.x - q.w * F.y;
       c2.y = q.x * G.y - q.y * G.x - q.z * F.y - q.w * F.x;
+      if (a.roi_off) {  // ROI offset: C1 exp(-i j off), C2 exp(+i j off) (GridrecCPP)
+        double sn, cs;
+        sincos((double)j * a.roi_off[n], &sn, &cs);
+        const float pr = (float)cs, pi = (float)-sn;
+        c1 = make_float2(c1.x * pr - c1.y * pi, c1.x * pi + c1.y * pr);
+        c2 = make_float2(c2.x * pr + c2.y * pi, c2.y * pr - c2.x * pi);
+      }
     }
     o1[j] = c1;
     o2[j] = c2;

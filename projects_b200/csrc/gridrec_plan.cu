@@ -112,6 +112,7 @@ struct Plan {
   float2* d_tw_p = nullptr;
   float2* d_tw_m = nullptr;
   float2* d_dir = nullptr;
+  double* d_roi_off = nullptr;  // per-angle ROI offset phase step, or null
   // gridding work list
   int tiles_u = 0, tiles_v = 0, n_items = 0, n_runs = 0, n_slots = 0, n_split = 0;
   long total_samples = 0;
@@ -377,10 +378,12 @@ struct Geometry {
 int geometry(const gr_params* prm, const Pswf* pw, Geometry* g) {
   long pdim = 1, itmp = prm->n_det - 1;
   while (itmp) { pdim <<= 1; itmp >>= 1; }
-  const double D0 = prm->n_det;
+  const double R = prm->roi_size > 0.f ? prm->roi_size : 1.0;
+  const double pix = prm->pixel_size > 0.f ? prm->pixel_size : 1.0;
+  const double D0 = R * prm->n_det;  // GridrecCPP grid.cpp:95-106 (R = MaxPixSiz = 1: GridRec)
   const double D1 = (double)prm->sampl * D0;
   long M = 1;
-  itmp = (long)(D1 - 1);
+  itmp = (long)(D1 / pix - 1);
   while (itmp) { M <<= 1; itmp >>= 1; }
   long M02 = (long)std::floor((double)(M / 2) / (double)prm->sampl - 0.5);
   if (M02 < 0) M02 = 0;
@@ -407,6 +410,8 @@ int check_params(const gr_params* prm, const Pswf** pw) {
   if (!(prm->sampl >= 1.0f) || prm->sampl > 4.0f)
     return fail(GR_ERR_ARG, "sampl must be in [1, 4]");
   if (prm->max_pairs < 1) return fail(GR_ERR_ARG, "max_pairs must be >= 1");
+  if (prm->roi_size < 0.f || prm->roi_size > 4.f || prm->pixel_size < 0.f || prm->pixel_size > 16.f)
+    return fail(GR_ERR_ARG, "roi_size in [0, 4] and pixel_size in [0, 16] (0 = 1)");
   *pw = find_pswf(prm->pswf_c);
   if (!*pw) return fail(GR_ERR_PSWF, "Prolate parameter C = %f not in data base", prm->pswf_c);
   return GR_OK;
@@ -478,7 +483,7 @@ int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1
   GR_MARK();
   SpectraArgs sa{s1, s2, in_pair_stride, n_valid, slice_base, flat, dark, flat_stride, p->d_pq,
                  p->d_spec,
-                 p->d_tw_p, p->n_det, p->n_ang, p->pdim, p->J, pairs};
+                 p->d_tw_p, p->n_det, p->n_ang, p->pdim, p->J, pairs, p->d_roi_off};
   GR_CUDA(launch_spectra(sa, dt, st));
   GR_MARK();
   GridArgs ga{p->d_spec, p->d_H, p->d_scratch, p->d_queue, p->d_items, p->d_runs,
@@ -585,6 +590,8 @@ int gr_params_default(gr_params* p, int n_det, int n_ang, const float* theta_deg
   p->ltbl = 512;
   p->max_pairs = 1;
   p->device = 0;
+  p->roi_size = 1.0f;
+  p->pixel_size = 1.0f;
   return GR_OK;
 }
 
@@ -686,6 +693,17 @@ int gr_plan_create(const gr_params* prm, gr_plan** out) {
   for (size_t d = 0; d < dirs.size(); ++d)
     dirs[d] = make_float2((float)dxy[2 * d], (float)dxy[2 * d + 1]);
   p->dxy = dxy;
+  if (prm->roi_x0 != 0.f || prm->roi_y0 != 0.f) {
+    // (X0 cos + Y0 sin) pi per angle, from the unscaled direction (GridrecCPP grid.cpp:237)
+    std::vector<double> off(prm->n_ang);
+    for (int n = 0; n < prm->n_ang; ++n)
+      off[n] = ((double)prm->roi_x0 * dxy[4 * n] + (double)prm->roi_y0 * dxy[4 * n + 1]) /
+               p->scale * M_PI;
+    if ((rc = upload(p, &p->d_roi_off, off))) {
+      gr_plan_destroy(p);
+      return rc;
+    }
+  }
   if ((rc = upload(p, &p->d_wtbl, fw)) || (rc = upload(p, &p->d_winv, fi)) ||
       (rc = upload(p, &p->d_filt, filt)) || (rc = upload(p, &p->d_tw_p, twiddles((int)pdim))) ||
       (rc = upload(p, &p->d_tw_m, twiddles((int)M))) || (rc = upload(p, &p->d_dir, dirs)) ||
@@ -1166,7 +1184,7 @@ extern "C" int gr_reconstruct_pair_noalloc(gr_plan* p, const float* sino1, const
   PhaseArgs ph{nullptr, p->center, 0, n_valid, p->d_filt, pq, p->J, p->pdim, 1};
   GR_CUDA(launch_phase(ph, st));
   SpectraArgs sa{sino1, s2, 0, n_valid, 0, nullptr, nullptr, 0, pq, spec, p->d_tw_p, p->n_det,
-                 p->n_ang, p->pdim, p->J, 1};
+                 p->n_ang, p->pdim, p->J, 1, p->d_roi_off};
   GR_CUDA(launch_spectra(sa, GR_DTYPE_F32, st));
   GridArgs ga{spec, H, part, queue, p->d_items, p->d_runs, p->d_split_list, p->n_split_tiles,
               p->d_dir, p->d_wtbl, p->n_items, 1, p->n_ang, p->J, p->M, p->tiles_v, p->n_slots,

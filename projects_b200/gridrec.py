@@ -49,7 +49,8 @@ class GrParams(C.Structure):
     _fields_ = [("n_det", C.c_int), ("n_ang", C.c_int), ("theta_deg", C.POINTER(C.c_float)),
                 ("center", C.c_float), ("filter", C.c_int), ("pswf_c", C.c_float),
                 ("sampl", C.c_float), ("ltbl", C.c_int), ("max_pairs", C.c_int),
-                ("device", C.c_int), ("geom", C.c_int)]
+                ("device", C.c_int), ("geom", C.c_int), ("roi_size", C.c_float),
+                ("pixel_size", C.c_float), ("roi_x0", C.c_float), ("roi_y0", C.c_float)]
 
 
 class GrBatch(C.Structure):
@@ -141,7 +142,8 @@ def filter_code(name: str) -> int:
 
 
 def make_params(n_det: int, n_ang: int, theta_deg, center=None, filter=FILTER_SHEPP_LOGAN,
-                pswf_c=6.0, sampl=1.0, ltbl=512, max_pairs=1, device=0, geom=0):
+                pswf_c=6.0, sampl=1.0, ltbl=512, max_pairs=1, device=0, geom=0, roi_size=1.0,
+                pixel_size=1.0, roi_x0=0.0, roi_y0=0.0):
     """GrParams plus the float32 theta array that must outlive plan creation."""
     th = np.ascontiguousarray(theta_deg, dtype=np.float32)
     if th.shape != (n_ang,):
@@ -158,6 +160,8 @@ def make_params(n_det: int, n_ang: int, theta_deg, center=None, filter=FILTER_SH
     p.max_pairs = int(max_pairs)
     p.device = int(device)
     p.geom = int(geom)
+    p.roi_size, p.pixel_size = float(roi_size), float(pixel_size)
+    p.roi_x0, p.roi_y0 = float(roi_x0), float(roi_y0)
     return p, th
 
 
@@ -202,9 +206,10 @@ class Plan:
 
     def __init__(self, n_det: int, n_ang: int, theta_deg, center=None,
                  filter=FILTER_SHEPP_LOGAN, pswf_c=6.0, sampl=1.0, ltbl=512, max_pairs=1,
-                 device=0, geom=0):
+                 device=0, geom=0, roi_size=1.0, pixel_size=1.0, roi_x0=0.0, roi_y0=0.0):
         self._params, self._theta = make_params(n_det, n_ang, theta_deg, center, filter,
-                                                pswf_c, sampl, ltbl, max_pairs, device, geom)
+                                                pswf_c, sampl, ltbl, max_pairs, device, geom,
+                                                roi_size, pixel_size, roi_x0, roi_y0)
         h = C.c_void_p()
         _check(lib().gr_plan_create(C.byref(self._params), C.byref(h)), "gr_plan_create")
         self._h = h

@@ -51,16 +51,18 @@ def case_gridrec_class(name, n, a, filt, seed, theta=None):
                         ref64_1=q1[:m0, :m0], ref64_2=q2[:m0, :m0])
 
 
-def case_gridrec_cpp(name, n, a, center, fname, C_, sampl, seed, geom=0):
+def case_gridrec_cpp(name, n, a, center, fname, C_, sampl, seed, geom=0, roi=(1.0, 1.0, 0.0, 0.0)):
     """GridrecCPP 5.2 with explicit centre, oversampling, PSWF C and filter name; geom 1
-    generates its angles (uniform on [0, pi)) by its FP32 recurrence."""
+    generates its angles (uniform on [0, pi)) by its FP32 recurrence; roi = (R, MaxPixSiz,
+    X0, Y0) of its grid_struct."""
     s1, s2, th = _pair_phantom(n, a, center, seed)
     b1, b2, m0 = O.refb_gridrec_pair(s1, s2, th, center=center, filter_name=fname, C_=C_,
-                                     sampl=sampl, geom=geom)
+                                     sampl=sampl, geom=geom, roi_size=roi[0], pixel_size=roi[1],
+                                     x0=roi[2], y0=roi[3])
     np.savez_compressed(os.path.join(HERE, f"case_{name}.npz"), kind="gridrec_cpp", sino1=s1,
                         sino2=s2, theta=th, n_det=n, n_ang=a, filter_name=fname, center=center,
                         sampl=sampl, C=C_, M0=m0, refb_1=b1[:m0, :m0], refb_2=b2[:m0, :m0],
-                        geom=geom)
+                        geom=geom, roi=np.array(roi))
 
 
 def prep_cases(rng):
@@ -128,6 +130,10 @@ def main():
     case_gridrec_cpp("b120x72_c61.2_C7_s1.2_shepp", 120, 72, 61.2, "shepp", 7.0, 1.2, 23)
     case_gridrec_cpp("b72x45_c36.5_C5_hamming", 72, 45, 36.5, "hamming", 5.0, 1.0, 24)
     case_gridrec_cpp("b96x90_c47.5_geom1_hann", 96, 90, 47.5, "hann", 6.0, 1.0, 25, geom=1)
+    case_gridrec_cpp("b96x80_c48_R0.75_X0.04_Y-0.03_hann", 96, 80, 48.0, "hann", 6.0, 1.0, 26,
+                     roi=(0.75, 1.0, 0.04, -0.03))
+    case_gridrec_cpp("b96x80_c48_R0.8_pix1.5_X0.05_Y0.02_shlo", 96, 80, 48.0, "shlo", 6.0, 1.0,
+                     27, roi=(0.8, 1.5, 0.05, 0.02))
     if O.prep_ref_available():
         prep_cases(np.random.default_rng(8))
     print("\n".join(sorted(f for f in os.listdir(HERE) if f.endswith(".npz"))))

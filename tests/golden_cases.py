@@ -16,7 +16,8 @@ def cases():
         case = {"name": os.path.basename(f)[5:-4], "sino1": z["sino1"], "sino2": z["sino2"],
                 "theta": z["theta"], "n_det": int(z["n_det"]), "n_ang": int(z["n_ang"]),
                 "center": float(z["center"]), "sampl": float(z["sampl"]), "C": float(z["C"]),
-                "M0": int(z["M0"]), "geom": int(z["geom"]) if "geom" in z else 0}
+                "M0": int(z["M0"]), "geom": int(z["geom"]) if "geom" in z else 0,
+                "roi": tuple(float(v) for v in z["roi"]) if "roi" in z else (1.0, 1.0, 0.0, 0.0)}
         if str(z["kind"]) == "gridrec":
             case["filter"] = int(z["filter"])
             case["ref32"] = (z["ref32_1"], z["ref32_2"])

@@ -37,14 +37,15 @@ def _gpu_pair(s1, s2, theta, **kw):
 
 @pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
 def test_pair_against_goldens(case):
+    R, pix, x0, y0 = case["roi"]
     g1, g2 = _gpu_pair(case["sino1"], case["sino2"], case["theta"], center=case["center"],
                        filter=case["filter"], pswf_c=case["C"], sampl=case["sampl"],
-                       geom=case["geom"])
+                       geom=case["geom"], roi_size=R, pixel_size=pix, roi_x0=x0, roi_y0=y0)
     m = case["M0"]
     assert g1.shape == (m, m)
     o1, o2 = O.port_gridrec_pair(case["sino1"], case["sino2"], case["theta"],
                                  center1=case["center"], filter=case["filter"], C_=case["C"],
-                                 sampl=case["sampl"])
+                                 sampl=case["sampl"], roi_size=R, pixel_size=pix, x0=x0, y0=y0)
     assert ph.rel_l2(g1, o1[:, :m]) < TOL
     assert ph.rel_l2(g2, o2[:, :m]) < TOL
     # and against the reference's own FP32 output

@@ -11,9 +11,10 @@ CASES = cases()
 
 @pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
 def test_port_against_reference_goldens(case):
+    R, pix, x0, y0 = case["roi"]
     o1, o2 = O.port_gridrec_pair(case["sino1"], case["sino2"], case["theta"],
                                  center1=case["center"], filter=case["filter"], C_=case["C"],
-                                 sampl=case["sampl"])
+                                 sampl=case["sampl"], roi_size=R, pixel_size=pix, x0=x0, y0=y0)
     m = case["M0"]
     assert o1.shape[0] == m
     if case["ref64"] is not None:
