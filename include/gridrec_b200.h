@@ -228,7 +228,7 @@ int gr_plan_launch_count(const gr_plan* plan, long* launches);
  * Results stay within the same tolerance; bitwise reproducibility holds per
  * tuning (the item cap sets the gridding's summation order).  No reference
  * counterpart (the reference has fixed launch shapes). */
-int gr_plan_autotune(gr_plan* plan, void* stream);
+int gr_plan_autotune(gr_plan* plan, void* stream);  /* GR_ERR_ARG while a gr_graph holds the plan */
 int gr_plan_tuning(const gr_plan* plan, int* item_cap, int* cols_group);
 
 /* Shape of the gridding work list: work items (CTAs per pair), sample runs,
@@ -251,7 +251,7 @@ typedef struct {
   gr_batch_desc batch;
 } gr_graph_item;
 int gr_graph_create(const gr_graph_item* items, int n_items, gr_graph** graph);
-int gr_graph_launch(gr_graph* graph, void* stream);
+int gr_graph_launch(gr_graph* graph, void* stream);  /* GR_ERR_ARG once a plan it holds is destroyed */
 /* Kernel launches one replay performs. */
 int gr_graph_launch_count(const gr_graph* graph, long* launches);
 int gr_graph_destroy(gr_graph* graph);
@@ -354,7 +354,8 @@ int gr_fbp_destroy(gr_fbp* fbp);
  * writes the mean-squared-loss gradient to grads and the loss to *loss (synchronises
  * when loss is non-NULL); gr_cnn_adam applies one Adam step (step counts from 1). */
 int gr_cnn_param_count(void);
-size_t gr_cnn_workspace_bytes(int n_img, int h, int w);
+size_t gr_cnn_workspace_bytes(int n_img, int h, int w);          /* forward + backward */
+size_t gr_cnn_forward_workspace_bytes(int n_img, int h, int w);  /* forward only */
 int gr_cnn_forward(const float* params, const float* x, float* y, int n_img, int h, int w,
                    void* workspace, void* stream);
 int gr_cnn_backward(const float* params, const float* x, const float* y, const float* target,

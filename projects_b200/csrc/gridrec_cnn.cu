@@ -378,6 +378,10 @@ size_t gr_cnn_workspace_bytes(int n_img, int h, int w) {
   return 4 * px * kC * 2 + px * 4 + (size_t)segs * kCnnParams * 4 + 1024 * 8 + 1024;
 }
 
+size_t gr_cnn_forward_workspace_bytes(int n_img, int h, int w) {
+  return 2 * (size_t)n_img * h * w * kC * 2;  // h1, h2 (BF16 x 16)
+}
+
 int gr_cnn_forward(const float* params, const float* x, float* y, int n_img, int h, int w,
                    void* workspace, void* stream) {
   int rc = cnn_check(n_img, h, w);

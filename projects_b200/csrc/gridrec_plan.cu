@@ -131,6 +131,7 @@ struct Plan {
   std::vector<double> dxy;          // per-direction (du, dv) steps, kept for rebuilding
   int item_cap = kItemCap;          // gridding work-item cost cap (autotuned)
   int cols_G = 0;                   // column-FFT group width (0 = cols_group(M); autotuned)
+  std::vector<gr_graph*> graphs;    // live CUDA graphs replaying this plan's buffers
   float4* d_pq = nullptr;
   // host streaming (gr_reconstruct_host)
   void* h_in[2] = {nullptr, nullptr};
@@ -534,6 +535,15 @@ int validate_batch(const Plan* p, const gr_batch_desc* b) {
 using gr::Plan;
 struct gr_plan : public Plan {};
 
+struct gr_graph {
+  int device = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  long launches = 0;
+  std::vector<gr_plan*> plans;  // the plans whose buffers the graph replays
+  bool dead = false;            // a plan it replays was destroyed: launch refused
+};
+
 namespace gr {
 int plan_shape(const gr_plan* p, int* n_det, int* n_ang, int* M0, int* max_pairs, int* device) {
   if (!p) return fail(GR_ERR_ARG, "null plan");
@@ -598,6 +608,12 @@ int gr_params_default(gr_params* p, int n_det, int n_ang, const float* theta_deg
 int gr_plan_destroy(gr_plan* plan) {
   if (!plan) return GR_OK;
   gr::DeviceGuard g(plan->device);
+  // graphs that replay this plan can no longer run; they forget the plan so
+  // that destroying them later touches nothing freed here
+  for (gr_graph* gg : plan->graphs) {
+    gg->dead = true;
+    gg->plans.erase(std::find(gg->plans.begin(), gg->plans.end(), plan));
+  }
   for (void* ptr : plan->allocs) cudaFree(ptr);
   for (int b = 0; b < 2; ++b) {
     if (plan->h_in[b]) cudaFreeHost(plan->h_in[b]);
@@ -830,6 +846,9 @@ int gr_plan_launch_count(const gr_plan* p, long* launches) {
 int gr_plan_autotune(gr_plan* p, void* stream) {
   using namespace gr;
   if (!p) return fail(GR_ERR_ARG, "null plan");
+  if (!p->graphs.empty())
+    return fail(GR_ERR_ARG, "autotune replaces buffers that %d live graph(s) replay: tune before "
+                "capture", (int)p->graphs.size());
   DeviceGuard g(p->device);
   cudaStream_t st = (cudaStream_t)stream;
   // tuned choices depend on the work-list geometry and the chunk size: key on them
@@ -1207,12 +1226,6 @@ extern "C" int gr_reconstruct_pair_noalloc(gr_plan* p, const float* sino1, const
 // own branches, forked from and joined to the capture stream, so batches of
 // different shapes can overlap on the GPU.
 
-struct gr_graph {
-  int device = 0;
-  cudaGraph_t graph = nullptr;
-  cudaGraphExec_t exec = nullptr;
-  long launches = 0;
-};
 
 extern "C" {
 
@@ -1292,6 +1305,8 @@ int gr_graph_create(const gr_graph_item* items, int n_items, gr_graph** out) {
   gg->graph = graph;
   gg->exec = exec;
   gg->launches = launches1 - launches0;
+  gg->plans = plans;
+  for (auto p : plans) p->graphs.push_back(gg);
   *out = gg;
   return GR_OK;
 }
@@ -1299,6 +1314,7 @@ int gr_graph_create(const gr_graph_item* items, int n_items, gr_graph** out) {
 int gr_graph_launch(gr_graph* g, void* stream) {
   using namespace gr;
   if (!g) return fail(GR_ERR_ARG, "null graph");
+  if (g->dead) return fail(GR_ERR_ARG, "graph replays a destroyed plan's buffers");
   DeviceGuard guard(g->device);
   GR_CUDA(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
   return GR_OK;
@@ -1315,6 +1331,7 @@ int gr_graph_destroy(gr_graph* g) {
   gr::DeviceGuard guard(g->device);
   if (g->exec) cudaGraphExecDestroy(g->exec);
   if (g->graph) cudaGraphDestroy(g->graph);
+  for (auto p : g->plans) p->graphs.erase(std::find(p->graphs.begin(), p->graphs.end(), g));
   delete g;
   return GR_OK;
 }

@@ -652,8 +652,8 @@ int gr_entropy(const float* images, int n_groups, int group, int rows, int cols,
                long image_stride, long group_stride, float vmin, float vmax, int nbins,
                float* entropies, void* workspace, void* stream) {
   if (!images || !entropies || !workspace) return fail(GR_ERR_ARG, "entropy: null pointer");
-  if (n_groups < 1 || group < 1 || rows < 1 || cols < 1 || row_stride < cols || nbins < 1 ||
-      nbins > kMaxBins || !(vmax > vmin))
+  if (n_groups < 1 || n_groups > 65535 || group < 1 || rows < 1 || cols < 1 ||
+      row_stride < cols || nbins < 1 || nbins > kMaxBins || !(vmax > vmin))
     return fail(GR_ERR_ARG, "entropy: bad sizes or range (nbins in [1, %d], vmax > vmin)",
                 kMaxBins);
   Window w{images, row_stride, image_stride, group_stride, rows, cols, group};

@@ -34,7 +34,8 @@ EXPORTS = ("gr_params_default", "gr_filter_code", "gr_plan_create", "gr_plan_des
            "gr_entropy", "gr_reconstruct_padded", "gr_center_search", "gr_graph_create",
            "gr_graph_launch", "gr_graph_launch_count", "gr_graph_destroy", "gr_plan_autotune",
            "gr_plan_tuning", "gr_xcorr_scores", "gr_fbp_create", "gr_fbp_reconstruct",
-           "gr_fbp_destroy", "gr_cnn_param_count", "gr_cnn_workspace_bytes", "gr_cnn_forward",
+           "gr_fbp_destroy", "gr_cnn_param_count", "gr_cnn_workspace_bytes",
+           "gr_cnn_forward_workspace_bytes", "gr_cnn_forward",
            "gr_cnn_backward", "gr_cnn_adam")
 STAGES = ("phase", "spectra", "grid", "cols", "rows_deapod")
 

@@ -28,6 +28,8 @@ def _lib():
         L.gr_cnn_param_count.restype = C.c_int
         L.gr_cnn_workspace_bytes.argtypes = [i_, i_, i_]
         L.gr_cnn_workspace_bytes.restype = C.c_size_t
+        L.gr_cnn_forward_workspace_bytes.argtypes = [i_, i_, i_]
+        L.gr_cnn_forward_workspace_bytes.restype = C.c_size_t
         L.gr_cnn_forward.argtypes = [vp, vp, vp, i_, i_, i_, vp, vp]
         L.gr_cnn_backward.argtypes = [vp, vp, vp, vp, i_, i_, i_, vp, C.POINTER(C.c_double), vp,
                                       vp]
@@ -62,28 +64,34 @@ class CorrectionNet:
         self._ws = None
         self._ws_shape = None
 
-    def _workspace(self, n, h, w):
+    def _workspace(self, n, h, w, train=False):
+        """Forward-only workspace (the activations) unless training needs the
+        gradient buffers too; grows to the larger kind when asked for it."""
         import torch
-        if self._ws_shape != (n, h, w):
-            nbytes = _lib().gr_cnn_workspace_bytes(n, h, w)
+        key = (n, h, w, train)
+        have = self._ws_shape
+        if have is None or have[:3] != (n, h, w) or (train and not have[3]):
+            nbytes = (_lib().gr_cnn_workspace_bytes(n, h, w) if train
+                      else _lib().gr_cnn_forward_workspace_bytes(n, h, w))
+            self._ws = None
             self._ws = torch.empty(nbytes, dtype=torch.uint8, device=self.params.device)
-            self._ws_shape = (n, h, w)
+            self._ws_shape = key
         return self._ws
 
-    def forward(self, x, y=None, stream=None):
+    def forward(self, x, y=None, stream=None, train=False):
         """x: (N, H, W) float32 CUDA tensor -> y = x + correction."""
         import torch
         n, h, w = x.shape
         if y is None:
             y = torch.empty_like(x)
-        ws = self._workspace(n, h, w)
+        ws = self._workspace(n, h, w, train)
         G._check(_lib().gr_cnn_forward(G._ptr(self.params), G._ptr(x), G._ptr(y), n, h, w,
                                        G._ptr(ws), G._stream_ptr(stream)), "gr_cnn_forward")
         return y
 
     def loss_and_grads(self, x, target, stream=None):
         """Forward + backward; fills self.grads, returns the mean-squared loss."""
-        y = self.forward(x, stream=stream)
+        y = self.forward(x, stream=stream, train=True)
         n, h, w = x.shape
         loss = C.c_double()
         G._check(_lib().gr_cnn_backward(G._ptr(self.params), G._ptr(x), G._ptr(y),

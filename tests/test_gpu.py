@@ -398,3 +398,31 @@ def test_autotune_keeps_parity_and_caches():
         with G.Plan(512, 360, th, center=256.3, filter=G.FILTER_SHEPP_LOGAN,
                     max_pairs=2) as again:
             assert again.autotune() == t  # cached for the shape
+
+
+def test_autotune_refused_while_a_graph_holds_the_plan():
+    n, a = 64, 40
+    th = ph.angles_deg(a)
+    s = _dev(np.stack([ph.random_ellipse_sinogram(k, n, a, center=32.0)[0] for k in range(2)]))
+    with G.Plan(n, a, th, center=32.0) as plan:
+        outs = torch.zeros((2, plan.M0, n), device="cuda")
+        g = plan.capture_batch(s, outs)
+        with pytest.raises(G.GrError):
+            plan.autotune()
+        g.close()
+        plan.autotune()  # fine once the graph is gone
+
+
+def test_graph_refused_after_its_plan_is_destroyed():
+    n, a = 64, 40
+    th = ph.angles_deg(a)
+    s = _dev(np.stack([ph.random_ellipse_sinogram(k, n, a, center=32.0)[0] for k in range(2)]))
+    plan = G.Plan(n, a, th, center=32.0)
+    outs = torch.zeros((2, plan.M0, n), device="cuda")
+    g = plan.capture_batch(s, outs)
+    g.launch()
+    torch.cuda.synchronize()
+    plan.close()
+    with pytest.raises(G.GrError):
+        g.launch()
+    g.close()
