@@ -96,6 +96,10 @@ typedef struct {
                               (0 = 1) */
   float roi_x0, roi_y0;    /* ROI offset X0, Y0: C1 times exp(-i j (X0 cos + Y0 sin) pi),
                               C2 times its conjugate */
+  int wide_grid;           /* gridding kernel: 0 = 16-pair kernel for chunks of >= 8 pairs
+                              (default), 1 = for every chunk, -1 = never (2 pairs per warp
+                              over 32 x 32 tiles); same taps and weights, the sums differ
+                              only in FP32 summation order */
 } gr_params;
 
 typedef struct gr_plan gr_plan;
@@ -213,6 +217,12 @@ int gr_plan_stage_times(gr_plan* plan, double* ms5, long* chunks);
  * {counter, slot0, nsplit, 0} per tile (tile = tu * tiles_v + tv, 32 x 32 cells). */
 int gr_worklist_export(const gr_params* p, int* n_items, int* n_runs, int* tiles_v, int* items,
                        int* runs, int* splits, int cap_items, int cap_runs);
+/* The same for the 16-pair gridding kernel's list: tiles of 8 x 8 cells, runs of at
+ * most 32 samples, step spacing 1. */
+int gr_worklist_export_wide(const gr_params* p, int* n_items, int* n_runs, int* tiles_v,
+                            int* items, int* runs, int* splits, int cap_items, int cap_runs);
+/* *wide = 1 when a chunk of `pairs` pairs grids with the 16-pair kernel. */
+int gr_plan_grid_kernel(const gr_plan* plan, int pairs, int* wide);
 
 /* Text of the last error recorded on this thread (never NULL). */
 const char* gr_last_error(void);

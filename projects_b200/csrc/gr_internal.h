@@ -23,6 +23,18 @@ constexpr int kRunMax = 64;
 // sample slots (steps x samples per step).
 constexpr int kItemCap = 2048;
 
+// The 16-pair gridding kernel (grid_wide_kernel): a warp's lanes carry the
+// (re, im) components of 16 slice pairs and hold a kTileW x kTileW sub-tile
+// of cells in registers.
+constexpr int kTileW = 8;
+constexpr int kWidePairs = 16;
+// Longest run it stages at once (longer runs are split on the host).
+constexpr int kRunMaxW = 32;
+// Work per item before a sub-tile is split (samples + per-run overhead).
+constexpr int kItemCapW = 1024;
+// Chunks of at least this many pairs use it when gr_params.wide_grid is 0.
+constexpr int kWideMinPairs = 8;
+
 // One run of samples: direction d (= 2*angle + half), samples j in [jlo, jhi],
 // gridded in steps of samples P apart (footprints of one step disjoint).
 struct Run {
@@ -59,10 +71,11 @@ struct SpectraArgs {
   const float* dark;
   long flat_stride;
   const float4* pq;      // [pair][J] (P.re, P.im, Q.re, Q.im)
-  float2* spec;          // [pair][n_ang][2][J]
+  float2* spec;          // [pair][n_ang][2][J], or (wide) [pair / 16][2 n_ang][J / 4][16][4]
   const float2* tw;      // two-level twiddle table for pdim (see gridrec_kernels.cu)
   int n_det, n_ang, pdim, J, pairs;
   const double* roi_off; // per angle (X0 cos + Y0 sin) pi of the ROI offset, or null
+  int wide = 0;          // spec in the 16-pair kernel's interleaved layout
 };
 
 struct PhaseArgs {
@@ -146,7 +159,11 @@ struct DeviceGuard {
 cudaError_t init_kernel_attributes();
 cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t s);
 cudaError_t launch_spectra(const SpectraArgs& a, gr_dtype dt, cudaStream_t s);
+// Gridding: grid_kernel over 32 x 32 tiles (two pairs per warp) or
+// grid_wide_kernel over 8 x 8 sub-tiles (16 pairs per warp), each followed by
+// its split-tile reduction when tiles are split.
 cudaError_t launch_grid(const GridArgs& a, int ntaps, cudaStream_t s);
+cudaError_t launch_grid_wide(const GridArgs& a, cudaStream_t s);
 int cols_group(int M);
 cudaError_t launch_cols(const ColArgs& a, cudaStream_t s);
 cudaError_t launch_rows(const RowArgs& a, cudaStream_t s);

@@ -524,9 +524,26 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
   for (int idx = 0; idx < 16; ++idx) buf[swz(tid + nthr * out_index(idx, Rl))] = v[idx];
   __syncthreads();
   const float4* pq = a.pq + (size_t)pair * a.J;
-  float2* o1 = a.spec + ((size_t)pair * a.n_ang + n) * 2 * a.J;
-  float2* o2 = o1 + a.J;
+  // plain: [pair][dir][j]; wide: [pair / 16][dir][j / 4][pair % 16][j % 4], so each
+  // pair still writes whole 32-byte sectors and the 16-pair gridding kernel
+  // stages a run of 16 pairs as one contiguous range
+  float2* o1;
+  float2* o2;
+  int qshift, qmask;
+  if (a.wide) {
+    const size_t per_dir = (size_t)(a.J >> 2) * 64;
+    o1 = a.spec + ((size_t)(pair >> 4) * 2 * a.n_ang + 2 * n) * per_dir + (pair & 15) * 4;
+    o2 = o1 + per_dir;
+    qshift = 2;
+    qmask = 3;
+  } else {
+    o1 = a.spec + ((size_t)pair * a.n_ang + n) * 2 * a.J;
+    o2 = o1 + a.J;
+    qshift = 30;
+    qmask = 0x3fffffff;
+  }
   for (int j = tid; j < a.J; j += nthr) {
+    const int oj = ((j >> qshift) << 6) + (j & qmask);
     float2 c1 = make_float2(0.f, 0.f), c2 = make_float2(0.f, 0.f);
     if (j > 0) {
       const float2 F = buf[swz(j)];
@@ -545,8 +562,8 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
         c2 = make_float2(c2.x * pr + c2.y * pi, c2.y * pr - c2.x * pi);
       }
     }
-    o1[j] = c1;
-    o2[j] = c2;
+    o1[oj] = c1;
+    o2[oj] = c2;
   }
 }
 
@@ -774,6 +791,239 @@ __global__ void __launch_bounds__(256) split_reduce_kernel(GridArgs a) {
     if (p == 0 || q == 0) sum = make_float4(0.f, 0.f, 0.f, 0.f);
     HA[(size_t)p * a.M + q] = make_float2(sum.x, sum.y);
     if (hasB) HB[(size_t)p * a.M + q] = make_float2(sum.z, sum.w);
+  }
+}
+
+// ------------------------------------------------------------------ gridding, 16 pairs per warp
+// The same gather as grid_kernel -- the work-list geometry, tap set and
+// nearest-neighbour weights of gridrec.cu:546-566 -- organised for chunks of
+// many slice pairs.  Lane l of a warp carries component l & 1 (re, im) of pair
+// l >> 1 of a group of kWidePairs pairs, so all lanes apply the same taps, each
+// to its own value:
+// * the geometry and weights of a sample are warp-uniform and computed once
+//   for all 16 pairs (16 lanes per sample, one weight each, exchanged through
+//   a small shared record);
+// * a work item is one kTileW x kTileW sub-tile whose cells stay in registers
+//   for all its runs: no shared-memory read-modify-write and no atomics.
+// Every sample carries one weight per sub-tile row and per column,
+// w(|u - row|) and w(|v - col|), zero where the distance exceeds L/2 -- the
+// test that selects the taps -- and is applied to the whole 8 x 8 register
+// tile with packed FP32x2 FMAs: no per-sample branches or offsets, and any
+// footprint width up to 8 taps.  A tap adds wv * (wu * value), the rounding
+// of grid_kernel, at positions formed as grid_kernel forms them, so the two
+// kernels differ only in summation order.  Each cell sums its taps in a fixed
+// order (runs in work-list order, samples in j order; split sub-tiles by
+// slot): results are bitwise reproducible.  The run's values for the 16 pairs
+// are one contiguous range of the interleaved spectra layout
+// ([group][dir][j / 4][pair][j % 4]), staged by 16-byte cp.async and double
+// buffered against the previous run.
+
+constexpr int kWideWarps = 4;
+// staging: up to kRunMaxW samples span kWideQuads quads of 4 j x 16 pairs
+constexpr int kWideQuads = (kRunMaxW + 3) / 4 + 1;
+constexpr int kWideStage = kWideQuads * 16 * 4 * 2;  // floats per buffer
+// per warp: staging [2][kWideStage] + weights [kRunMaxW][16]
+constexpr int kWideWarpFloats = 2 * kWideStage + kRunMaxW * 16;
+
+__device__ __forceinline__ void cp_async16(float* dst_smem, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+__device__ __forceinline__ unsigned long long pack2(float lo, float hi) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+  return r;
+}
+__device__ __forceinline__ float2 unpack2(unsigned long long v) {
+  float2 r;
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(r.x), "=f"(r.y) : "l"(v));
+  return r;
+}
+// acc += a * b elementwise on packed float pairs (one rounding per element)
+__device__ __forceinline__ void ffma2(unsigned long long& acc, unsigned long long a,
+                                      unsigned long long b) {
+  asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(a), "l"(b));
+}
+
+// 4 CTAs per SM: 128 registers a thread (no spills), 16 warps
+__global__ void __launch_bounds__(kWideWarps * 32, 4) grid_wide_kernel(GridArgs a) {
+  constexpr int T = kTileW;
+  extern __shared__ float4 smw4[];
+  float* s_wtbl = reinterpret_cast<float*>(smw4);  // table: up to 1028 floats
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  float* wbase = reinterpret_cast<float*>(smw4 + 257) + warp * kWideWarpFloats;
+  float* stage = wbase;                     // [2][kWideQuads][16][4][2]
+  float* rec = wbase + 2 * kWideStage;      // [kRunMaxW][16]: rows 0..7, columns 8..15
+  for (int i = threadIdx.x; i <= a.ltbl; i += blockDim.x) s_wtbl[i] = __ldg(&a.wtbl[i]);
+  __syncthreads();
+  const float L2 = a.L2, ts = a.tblspcg;
+  const int ltbl = a.ltbl;
+  const float half_m = (float)(a.M / 2);
+  const int groups = (a.pairs + kWidePairs - 1) / kWidePairs;
+  const unsigned total = (unsigned)a.n_items * (unsigned)groups;
+  const size_t per_dir = (size_t)(a.J >> 2) * 64;  // float2 per direction and group
+  const size_t MM = (size_t)a.M * a.M;
+  // weight pass: lanes 0-15 serve sample s0, 16-31 sample s0 + 1; lane k & 15
+  // computes row k (k < 8) or column k - 8
+  const int w_s = lane >> 4, w_k = lane & 15;
+  const bool w_row = w_k < 8;
+  const float w_cell = (float)(w_k & 7);
+  const int pl = lane >> 1, cl = lane & 1;
+  for (;;) {
+    unsigned w = 0;
+    if (lane == 0) w = atomicAdd(a.queue, 1u);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    if (w >= total) break;
+    const int grp = (int)(w / (unsigned)a.n_items);
+    const Item it = a.items[w - (unsigned)grp * (unsigned)a.n_items];
+    const int pg0 = grp * kWidePairs;
+    const int np = min(kWidePairs, a.pairs - pg0);
+    const int tu = it.tile / a.tiles_v;
+    const int tv = it.tile - tu * a.tiles_v;
+    const int p0 = tu * T, q0 = tv * T;
+    // positions as grid_kernel forms them (relative to the enclosing 32 x 32
+    // tile), then moved to the sub-tile by an exact integer: both kernels see
+    // the same |d| and table indices
+    const float offu = half_m - (float)(p0 & ~(kTile - 1));
+    const float offv = half_m - (float)(q0 & ~(kTile - 1));
+    const float subu = (float)(p0 & (kTile - 1)), subv = (float)(q0 & (kTile - 1));
+    const float2* specg = a.spec + (size_t)grp * 2 * a.n_ang * per_dir;
+    unsigned long long acc[T][T / 2];  // (cell c, cell c + 1) of row r
+#pragma unroll
+    for (int r = 0; r < T; ++r)
+#pragma unroll
+      for (int c = 0; c < T / 2; ++c) acc[r][c] = 0ull;
+    // the quads of run rn -> staging buffer b
+    auto stage_run = [&](const Run& rn, int b) {
+      const int nq = (rn.jhi >> 2) - (rn.jlo >> 2) + 1;
+      float* dst = stage + b * kWideStage;
+      const float2* src = specg + (size_t)rn.dir * per_dir + (size_t)(rn.jlo >> 2) * 64;
+      for (int i = lane; i < nq * 32; i += 32) cp_async16(dst + i * 4, src + i * 2);
+    };
+    // run records travel two runs ahead of their use, staging one run ahead
+    const int rb = it.run_begin, re = it.run_end;
+    Run run1 = a.runs[rb];
+    float2 dir1 = __ldg(&a.dir[run1.dir]);
+    Run run2 = run1;
+    float2 dir2 = dir1;
+    if (rb + 1 < re) {
+      run2 = a.runs[rb + 1];
+      dir2 = __ldg(&a.dir[run2.dir]);
+    }
+    stage_run(run1, 0);
+    cp_async_commit();
+    for (int r = rb; r < re; ++r) {
+      const Run run = run1;
+      const float2 d = dir1;
+      const int b = (r - rb) & 1;
+      run1 = run2;
+      dir1 = dir2;
+      if (r + 1 < re) stage_run(run1, b ^ 1);
+      cp_async_commit();  // possibly empty: keeps one group per run
+      if (r + 2 < re) {
+        run2 = a.runs[r + 2];
+        dir2 = __ldg(&a.dir[run2.dir]);
+      }
+      // row and column weights of this run's samples
+      const int n = run.jhi - run.jlo + 1;
+      for (int s0 = 0; s0 < n; s0 += 2) {
+        const int s = s0 + w_s;
+        if (s < n) {
+          const float fj = (float)(run.jlo + s);
+          const float pos = w_row ? fmaf(fj, d.x, offu) - subu : fmaf(fj, d.y, offv) - subv;
+          const float dd = fabsf(pos - w_cell);
+          const float wt = s_wtbl[min(table_index(dd, ts), ltbl)];
+          rec[s * 16 + w_k] = dd <= L2 ? wt : 0.f;
+        }
+      }
+      cp_async_wait<1>();  // this run's values have landed (the next run's may be in flight)
+      __syncwarp();
+      const float* st = stage + b * kWideStage;
+      const int jq0 = run.jlo & ~3;
+      for (int s = 0; s < n; ++s) {
+        const int jr = run.jlo + s - jq0;  // j relative to the first staged quad
+        const float val = st[(((jr >> 2) * 16 + pl) * 4 + (jr & 3)) * 2 + cl];
+        const float4 wr0 = *reinterpret_cast<const float4*>(rec + s * 16);
+        const float4 wr1 = *reinterpret_cast<const float4*>(rec + s * 16 + 4);
+        const float4 wc0 = *reinterpret_cast<const float4*>(rec + s * 16 + 8);
+        const float4 wc1 = *reinterpret_cast<const float4*>(rec + s * 16 + 12);
+        const float wr[T] = {wr0.x, wr0.y, wr0.z, wr0.w, wr1.x, wr1.y, wr1.z, wr1.w};
+        const unsigned long long wc[T / 2] = {pack2(wc0.x, wc0.y), pack2(wc0.z, wc0.w),
+                                              pack2(wc1.x, wc1.y), pack2(wc1.z, wc1.w)};
+#pragma unroll
+        for (int rr = 0; rr < T; ++rr) {
+          const float x = wr[rr] * val;  // wu * value
+          const unsigned long long x2 = pack2(x, x);
+#pragma unroll
+          for (int c = 0; c < T / 2; ++c) ffma2(acc[rr][c], wc[c], x2);  // += wv * (wu * value)
+        }
+      }
+      __syncwarp();
+    }
+    cp_async_wait<0>();
+    if (it.slot < 0) {
+      // lane pairs trade halves so each lane stores one complex cell:
+      // lane 2p+0 stores cell (r, c), lane 2p+1 cell (r, c+1)
+      float2* Hp = a.H + (size_t)(pg0 + min(pl, np - 1)) * MM;
+#pragma unroll
+      for (int r = 0; r < T; ++r) {
+#pragma unroll
+        for (int c2 = 0; c2 < T / 2; ++c2) {
+          const float2 v = unpack2(acc[r][c2]);  // cells (r, 2 c2), (r, 2 c2 + 1)
+          const float give = cl ? v.x : v.y;
+          const float got = __shfl_xor_sync(0xffffffffu, give, 1);
+          float2 val = cl ? make_float2(got, v.y) : make_float2(v.x, got);
+          const int p = p0 + r, q = q0 + 2 * c2 + cl;
+          if (p == 0 || q == 0) val = make_float2(0.f, 0.f);
+          if (pl < np) Hp[(size_t)p * a.M + q] = val;
+        }
+      }
+    } else {
+      // partial sub-tile of a split sub-tile: [cell][lane], summed by split_reduce_wide_kernel
+      float* part = reinterpret_cast<float*>(a.scratch) +
+                    ((size_t)grp * a.n_slots + it.slot) * (T * T * 32);
+#pragma unroll
+      for (int r = 0; r < T; ++r)
+#pragma unroll
+        for (int c2 = 0; c2 < T / 2; ++c2) {
+          const float2 v = unpack2(acc[r][c2]);
+          part[(r * T + 2 * c2) * 32 + lane] = v.x;
+          part[(r * T + 2 * c2 + 1) * 32 + lane] = v.y;
+        }
+    }
+    __syncwarp();
+  }
+}
+
+// Sums the partial sub-tiles of every split sub-tile in slot order and writes H.
+// Grid: (split sub-tiles, pair groups of 16); 256 threads over (cell, lane).
+__global__ void __launch_bounds__(256) split_reduce_wide_kernel(GridArgs a) {
+  constexpr int T = kTileW;
+  const int4 sp = a.split_list[blockIdx.x];  // (tile, slot0, nsplit, -)
+  const int grp = blockIdx.y;
+  const int pg0 = grp * kWidePairs;
+  const int np = min(kWidePairs, a.pairs - pg0);
+  const int tu = sp.x / a.tiles_v, tv = sp.x - (sp.x / a.tiles_v) * a.tiles_v;
+  const int p0 = tu * T, q0 = tv * T;
+  const float* base = reinterpret_cast<const float*>(a.scratch) +
+                      ((size_t)grp * a.n_slots + sp.y) * (T * T * 32);
+  const size_t MM = (size_t)a.M * a.M;
+  for (int i = threadIdx.x; i < T * T * 32; i += blockDim.x) {
+    const int cell = i >> 5, l = i & 31;
+    if ((l >> 1) >= np) continue;
+    float sum = 0.f;
+    for (int k = 0; k < sp.z; ++k) sum += __ldg(&base[(size_t)k * (T * T * 32) + i]);
+    const int p = p0 + cell / T, q = q0 + cell % T;
+    if (p == 0 || q == 0) sum = 0.f;
+    float* Hf = reinterpret_cast<float*>(a.H + (size_t)(pg0 + (l >> 1)) * MM);
+    Hf[((size_t)p * a.M + q) * 2 + (l & 1)] = sum;
   }
 }
 
@@ -1030,6 +1280,7 @@ cudaError_t init_kernel_attributes() {
   fns.push_back((const void*)grid_kernel<3>);
   fns.push_back((const void*)grid_kernel<4>);
   fns.push_back((const void*)grid_kernel<kMaxTaps>);
+  fns.push_back((const void*)grid_wide_kernel);
   for (const void* f : fns) {
     if (e != cudaSuccess) break;
     e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
@@ -1096,6 +1347,31 @@ cudaError_t launch_grid(const GridArgs& a, int ntaps, cudaStream_t s) {
   if (e != cudaSuccess || a.n_split_tiles == 0) return e;
   dim3 rgrid(a.n_split_tiles, (unsigned)groups);
   split_reduce_kernel<<<rgrid, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+static int grid_wide_smem_bytes() {
+  return 257 * (int)sizeof(float4) + kWideWarps * kWideWarpFloats * (int)sizeof(float);
+}
+
+cudaError_t launch_grid_wide(const GridArgs& a, cudaStream_t s) {
+  if (a.n_items == 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(a.queue, 0, sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int smem = grid_wide_smem_bytes();
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_wide_kernel, kWideWarps * 32, smem);
+  const long groups = (a.pairs + kWidePairs - 1) / kWidePairs;
+  const long want = ((long)a.n_items * groups + kWideWarps - 1) / kWideWarps;
+  const int blocks = (int)std::min<long>(want, (long)std::max(per_sm, 1) * sms);
+  grid_wide_kernel<<<blocks, kWideWarps * 32, smem, s>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess || a.n_split_tiles == 0) return e;
+  dim3 rgrid(a.n_split_tiles, (unsigned)groups);
+  split_reduce_wide_kernel<<<rgrid, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -130,6 +130,17 @@ struct Plan {
   size_t scratch_cells = 0;         // float4 cells allocated in d_scratch
   std::vector<double> dxy;          // per-direction (du, dv) steps, kept for rebuilding
   int item_cap = kItemCap;          // gridding work-item cost cap (autotuned)
+  // 16-pair gridding (grid_wide_kernel): its own work list over 8 x 8 sub-tiles,
+  // present when chunks can be wide enough to use it (gr_params.wide_grid)
+  int wide_mode = 0;                // gr_params.wide_grid: 0 auto, 1 always, -1 never
+  int w_tiles_v = 0, w_items = 0, w_runs = 0, w_slots = 0, w_split_tiles = 0;
+  int w_item_cap = kItemCapW;
+  Item* d_w_items = nullptr;
+  Run* d_w_runs = nullptr;
+  int4* d_w_split_list = nullptr;
+  float4* d_w_scratch = nullptr;    // [pair group of 16][slot][64 cells x 32 lanes] floats
+  size_t w_scratch_cells = 0;
+  int spec_pairs = 0;               // pairs the spectra workspace holds
   int cols_G = 0;                   // column-FFT group width (0 = cols_group(M); autotuned)
   std::vector<gr_graph*> graphs;    // live CUDA graphs replaying this plan's buffers
   float4* d_pq = nullptr;
@@ -191,9 +202,10 @@ void dev_free(Plan* p, T** ptr) {
   *ptr = nullptr;
 }
 
-// The gridding work list: for each 32x32 tile, the runs of samples
+// The gridding work list: for each T x T tile, the runs of samples
 // (direction, j range) whose L x L footprint can reach the tile; tiles whose
-// runs exceed kItemCap samples are split into several items.
+// runs exceed the item cap are split into several items.  T = kTile (32) for
+// grid_kernel, kTileW (8) for grid_wide_kernel.
 struct WorkList {
   std::vector<Item> items;
   std::vector<Run> runs;
@@ -228,8 +240,9 @@ int run_spacing(double du, double dv, int n, double L, int spw, int* steps) {
 }
 
 void build_work_list(int M, int J, double L, int n_ang, const std::vector<double>& dxy,
-                     WorkList* wl, int item_cap = kItemCap) {
-  const int T = kTile;
+                     WorkList* wl, int item_cap = kItemCap, bool wide = false) {
+  const int T = wide ? kTileW : kTile;
+  const int run_max = wide ? kRunMaxW : kRunMax;
   const double M2 = M / 2;
   const double L2 = L / 2 + 2e-3;  // box margin covers FP32 position rounding
   wl->tiles_u = (M + T - 1) / T;
@@ -266,8 +279,8 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
         if (!slab(M2, dy, y0, y1, sa, sb)) continue;
         const int jlo = std::max(1, (int)std::ceil(sa - 1e-6));
         const int jhi = std::min(J - 1, (int)std::floor(sb + 1e-6));
-        for (int j0 = jlo; j0 <= jhi; j0 += kRunMax)  // runs of at most kRunMax samples
-          all.push_back({tu * wl->tiles_v + tv, d, j0, std::min(jhi, j0 + kRunMax - 1)});
+        for (int j0 = jlo; j0 <= jhi; j0 += run_max)  // runs of at most run_max samples
+          all.push_back({tu * wl->tiles_v + tv, d, j0, std::min(jhi, j0 + run_max - 1)});
       }
     }
   }
@@ -281,11 +294,17 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
   const int spw = 32 / nt;
   std::vector<int> first(n_tiles + 1, 0);
   for (size_t i = 0; i < all.size(); ++i) {
-    int steps = 0;
-    const int P = run_spacing(dxy[2 * all[i].dir], dxy[2 * all[i].dir + 1],
-                              all[i].jhi - all[i].jlo + 1, L, spw, &steps);
-    wl->runs[i] = {all[i].dir, all[i].jlo, all[i].jhi, P};
-    run_cost[i] = (long)steps * spw + 4;  // sample slots + per-run overhead
+    const int n = all[i].jhi - all[i].jlo + 1;
+    if (wide) {
+      // one warp-uniform pass per sample; the run's staging and weight pass
+      wl->runs[i] = {all[i].dir, all[i].jlo, all[i].jhi, 1};
+      run_cost[i] = n + 6;
+    } else {
+      int steps = 0;
+      const int P = run_spacing(dxy[2 * all[i].dir], dxy[2 * all[i].dir + 1], n, L, spw, &steps);
+      wl->runs[i] = {all[i].dir, all[i].jlo, all[i].jhi, P};
+      run_cost[i] = (long)steps * spw + 4;  // sample slots + per-run overhead
+    }
     first[all[i].tile + 1]++;
   }
   for (int t = 0; t < n_tiles; ++t) first[t + 1] += first[t];
@@ -369,6 +388,56 @@ int install_work_list(Plan* p, int item_cap) {
   return GR_OK;
 }
 
+// The 16-pair kernel's work list (8 x 8 sub-tiles), placed on the device.
+int install_work_list_wide(Plan* p, int item_cap) {
+  WorkList wl;
+  build_work_list(p->M, p->J, p->L, p->n_ang, p->dxy, &wl, item_cap, true);
+  std::vector<int4> split_list;
+  for (size_t t = 0; t < wl.splits.size(); ++t)
+    if (wl.splits[t].nsplit > 1)
+      split_list.push_back(make_int4((int)t, wl.splits[t].slot0, wl.splits[t].nsplit, 0));
+  dev_free(p, &p->d_w_items);
+  dev_free(p, &p->d_w_runs);
+  dev_free(p, &p->d_w_split_list);
+  int rc;
+  if ((rc = upload(p, &p->d_w_items, wl.items)) || (rc = upload(p, &p->d_w_runs, wl.runs)) ||
+      (rc = upload(p, &p->d_w_split_list, split_list)))
+    return rc;
+  // 64 cells x 32 lanes floats = 512 float4 per slot and group of 16 pairs
+  const size_t groups = (size_t)(p->max_pairs + kWidePairs - 1) / kWidePairs;
+  const size_t cells = groups * (size_t)std::max(wl.n_slots, 1) * (kTileW * kTileW * 32 / 4);
+  if (cells > p->w_scratch_cells) {
+    dev_free(p, &p->d_w_scratch);
+    if ((rc = dev_alloc(p, &p->d_w_scratch, cells))) return rc;
+    p->w_scratch_cells = cells;
+  }
+  p->w_tiles_v = wl.tiles_v;
+  p->w_items = (int)wl.items.size();
+  p->w_runs = (int)wl.runs.size();
+  p->w_slots = wl.n_slots;
+  p->w_split_tiles = (int)split_list.size();
+  p->w_item_cap = item_cap;
+  return GR_OK;
+}
+
+// Whether a chunk of `pairs` pairs grids with grid_wide_kernel.
+bool use_wide(const Plan* p, int pairs) {
+  if (p->w_items == 0 || p->wide_mode < 0) return false;
+  return p->wide_mode > 0 || pairs >= kWideMinPairs;
+}
+
+GridArgs grid_args(const Plan* p, int pairs, bool wide) {
+  if (wide)
+    return GridArgs{p->d_spec, p->d_H, p->d_w_scratch, p->d_queue, p->d_w_items, p->d_w_runs,
+                    p->d_w_split_list, p->w_split_tiles, p->d_dir, p->d_wtbl, p->w_items, pairs,
+                    p->n_ang, p->J, p->M, p->w_tiles_v, p->w_slots, p->ltbl, (float)(p->L / 2),
+                    (float)(2.0 * p->ltbl / p->L)};
+  return GridArgs{p->d_spec, p->d_H, p->d_scratch, p->d_queue, p->d_items, p->d_runs,
+                  p->d_split_list, p->n_split_tiles, p->d_dir, p->d_wtbl, p->n_items, pairs,
+                  p->n_ang, p->J, p->M, p->tiles_v, p->n_slots, p->ltbl, (float)(p->L / 2),
+                  (float)(2.0 * p->ltbl / p->L)};
+}
+
 // Sizes exactly as GridRec::init (gridrec/GPU/gridrec.cu:243-268), in FP64.
 struct Geometry {
   long pdim, M, M02, M0;
@@ -411,6 +480,8 @@ int check_params(const gr_params* prm, const Pswf** pw) {
   if (!(prm->sampl >= 1.0f) || prm->sampl > 4.0f)
     return fail(GR_ERR_ARG, "sampl must be in [1, 4]");
   if (prm->max_pairs < 1) return fail(GR_ERR_ARG, "max_pairs must be >= 1");
+  if (prm->wide_grid < -1 || prm->wide_grid > 1)
+    return fail(GR_ERR_ARG, "wide_grid must be -1, 0 or 1");
   if (prm->roi_size < 0.f || prm->roi_size > 4.f || prm->pixel_size < 0.f || prm->pixel_size > 16.f)
     return fail(GR_ERR_ARG, "roi_size in [0, 4] and pixel_size in [0, 16] (0 = 1)");
   *pw = find_pswf(prm->pswf_c);
@@ -482,16 +553,14 @@ int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1
   PhaseArgs ph{centers, p->center, slice_base, n_valid, p->d_filt, p->d_pq, p->J, p->pdim, pairs};
   GR_CUDA(launch_phase(ph, st));
   GR_MARK();
+  const bool wide = use_wide(p, pairs);
   SpectraArgs sa{s1, s2, in_pair_stride, n_valid, slice_base, flat, dark, flat_stride, p->d_pq,
                  p->d_spec,
-                 p->d_tw_p, p->n_det, p->n_ang, p->pdim, p->J, pairs, p->d_roi_off};
+                 p->d_tw_p, p->n_det, p->n_ang, p->pdim, p->J, pairs, p->d_roi_off, wide ? 1 : 0};
   GR_CUDA(launch_spectra(sa, dt, st));
   GR_MARK();
-  GridArgs ga{p->d_spec, p->d_H, p->d_scratch, p->d_queue, p->d_items, p->d_runs,
-              p->d_split_list, p->n_split_tiles, p->d_dir, p->d_wtbl, p->n_items, pairs,
-              p->n_ang, p->J, p->M, p->tiles_v, p->n_slots, p->ltbl, (float)(p->L / 2),
-              (float)(2.0 * p->ltbl / p->L)};
-  GR_CUDA(launch_grid(ga, p->ntaps, st));
+  const GridArgs ga = grid_args(p, pairs, wide);
+  GR_CUDA(wide ? launch_grid_wide(ga, st) : launch_grid(ga, p->ntaps, st));
   GR_MARK();
   ColArgs ca{p->d_H, p->d_tw_m, p->M, pairs, p->d_err, p->cols_G};
   GR_CUDA(launch_cols(ca, st));
@@ -501,7 +570,7 @@ int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1
   GR_CUDA(launch_rows(ra, st));
   GR_MARK();
   // phase, spectra, grid (+ split reduction when tiles are split), cols, rows
-  p->launches += 5 + (p->n_items > 0 && p->n_split_tiles > 0 ? 1 : 0);
+  p->launches += 5 + (ga.n_items > 0 && ga.n_split_tiles > 0 ? 1 : 0);
   return GR_OK;
 }
 
@@ -655,6 +724,7 @@ int gr_plan_create(const gr_params* prm, gr_plan** out) {
   p->ltbl = prm->ltbl;
   p->filter = prm->filter;
   p->max_pairs = prm->max_pairs;
+  p->wide_mode = prm->wide_grid;
   p->center = prm->center < 0 ? (float)(prm->n_det / 2) : prm->center;
   const long pdim = geo.pdim, M = geo.M, M02 = geo.M02;
   p->pdim = (int)pdim;
@@ -723,12 +793,17 @@ int gr_plan_create(const gr_params* prm, gr_plan** out) {
   if ((rc = upload(p, &p->d_wtbl, fw)) || (rc = upload(p, &p->d_winv, fi)) ||
       (rc = upload(p, &p->d_filt, filt)) || (rc = upload(p, &p->d_tw_p, twiddles((int)pdim))) ||
       (rc = upload(p, &p->d_tw_m, twiddles((int)M))) || (rc = upload(p, &p->d_dir, dirs)) ||
-      (rc = install_work_list(p, kItemCap))) {
+      (rc = install_work_list(p, kItemCap)) ||
+      ((p->wide_mode > 0 || (p->wide_mode == 0 && p->max_pairs >= kWideMinPairs)) &&
+       (rc = install_work_list_wide(p, kItemCapW)))) {
     gr_plan_destroy(p);
     return rc;
   }
   const size_t P = (size_t)p->max_pairs;
-  if ((rc = dev_alloc(p, &p->d_spec, P * p->n_ang * 2 * p->J)) ||
+  // the 16-pair kernel's spectra layout holds whole groups of 16 pairs
+  const size_t P_spec = p->w_items ? (P + kWidePairs - 1) / kWidePairs * kWidePairs : P;
+  p->spec_pairs = (int)P_spec;
+  if ((rc = dev_alloc(p, &p->d_spec, P_spec * p->n_ang * 2 * p->J)) ||
       (rc = dev_alloc(p, &p->d_H, P * (size_t)M * M)) ||
       (rc = dev_alloc(p, &p->d_pq, P * p->J)) ||
       (rc = dev_alloc(p, &p->d_queue, 1)) || (rc = dev_alloc(p, &p->d_err, 1))) {
@@ -745,8 +820,9 @@ int gr_plan_create(const gr_params* prm, gr_plan** out) {
   return GR_OK;
 }
 
-int gr_worklist_export(const gr_params* prm, int* n_items, int* n_runs, int* tiles_v,
-                       int* items, int* runs, int* splits, int cap_items, int cap_runs) {
+static int worklist_export(const gr_params* prm, bool wide, int* n_items, int* n_runs,
+                           int* tiles_v, int* items, int* runs, int* splits, int cap_items,
+                           int cap_runs) {
   using namespace gr;
   const Pswf* pw = nullptr;
   int rc = check_params(prm, &pw);
@@ -755,7 +831,7 @@ int gr_worklist_export(const gr_params* prm, int* n_items, int* n_runs, int* til
   if ((rc = geometry(prm, pw, &geo))) return rc;
   WorkList wl;
   build_work_list((int)geo.M, (int)(geo.pdim / 2), geo.L, prm->n_ang, directions(prm, geo.scale),
-                  &wl);
+                  &wl, wide ? kItemCapW : kItemCap, wide);
   if (n_items) *n_items = (int)wl.items.size();
   if (n_runs) *n_runs = (int)wl.runs.size();
   if (tiles_v) *tiles_v = wl.tiles_v;
@@ -765,6 +841,24 @@ int gr_worklist_export(const gr_params* prm, int* n_items, int* n_runs, int* til
   std::memcpy(items, wl.items.data(), wl.items.size() * sizeof(Item));
   std::memcpy(runs, wl.runs.data(), wl.runs.size() * sizeof(Run));
   std::memcpy(splits, wl.splits.data(), wl.splits.size() * sizeof(Split));
+  return GR_OK;
+}
+
+int gr_worklist_export(const gr_params* prm, int* n_items, int* n_runs, int* tiles_v,
+                       int* items, int* runs, int* splits, int cap_items, int cap_runs) {
+  return worklist_export(prm, false, n_items, n_runs, tiles_v, items, runs, splits, cap_items,
+                         cap_runs);
+}
+
+int gr_worklist_export_wide(const gr_params* prm, int* n_items, int* n_runs, int* tiles_v,
+                            int* items, int* runs, int* splits, int cap_items, int cap_runs) {
+  return worklist_export(prm, true, n_items, n_runs, tiles_v, items, runs, splits, cap_items,
+                         cap_runs);
+}
+
+int gr_plan_grid_kernel(const gr_plan* p, int pairs, int* wide) {
+  if (!p || !wide) return gr::fail(GR_ERR_ARG, "null argument");
+  *wide = gr::use_wide(p, std::min(std::max(pairs, 1), p->max_pairs)) ? 1 : 0;
   return GR_OK;
 }
 
@@ -859,17 +953,23 @@ int gr_plan_autotune(gr_plan* p, void* stream) {
   mix((unsigned long long)p->J);
   mix((unsigned long long)p->n_ang);
   mix((unsigned long long)p->max_pairs);
+  mix((unsigned long long)(p->wide_mode + 1));
   mix((unsigned long long)std::llround(p->L * 1e6));
   for (double d : p->dxy) mix((unsigned long long)std::llround(d * 1e9));
   static std::mutex mu;
-  static std::map<unsigned long long, std::pair<int, int>> cache;
+  struct Tuned { int cap, G; };  // cap: item cap of the kernel a full chunk uses
+  static std::map<unsigned long long, Tuned> cache;
+  const bool wide = use_wide(p, p->max_pairs);
+  auto install = [&](int cap) {
+    if (wide) return cap == p->w_item_cap ? GR_OK : install_work_list_wide(p, cap);
+    return cap == p->item_cap ? GR_OK : install_work_list(p, cap);
+  };
   {
     std::lock_guard<std::mutex> lk(mu);
     auto it = cache.find(h);
     if (it != cache.end()) {
-      int rc = it->second.first == p->item_cap ? GR_OK : install_work_list(p, it->second.first);
-      p->cols_G = it->second.second;
-      return rc;
+      p->cols_G = it->second.G;
+      return install(it->second.cap);
     }
   }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
@@ -889,23 +989,25 @@ int gr_plan_autotune(gr_plan* p, void* stream) {
     return best;
   };
   const int pairs = p->max_pairs;
-  cudaMemsetAsync(p->d_spec, 0, (size_t)pairs * p->n_ang * 2 * p->J * sizeof(float2), st);
+  cudaMemsetAsync(p->d_spec, 0, (size_t)p->spec_pairs * p->n_ang * 2 * p->J * sizeof(float2), st);
   cudaMemsetAsync(p->d_H, 0, (size_t)pairs * p->M * p->M * sizeof(float2), st);
-  int best_cap = p->item_cap, rc = GR_OK;
+  int best_cap = wide ? p->w_item_cap : p->item_cap, rc = GR_OK;
   float best_t = 1e30f;
-  for (int cap : {512, 1024, 2048, 4096, 8192}) {
-    if ((rc = install_work_list(p, cap))) break;
-    GridArgs ga{p->d_spec, p->d_H, p->d_scratch, p->d_queue, p->d_items, p->d_runs,
-                p->d_split_list, p->n_split_tiles, p->d_dir, p->d_wtbl, p->n_items, pairs,
-                p->n_ang, p->J, p->M, p->tiles_v, p->n_slots, p->ltbl, (float)(p->L / 2),
-                (float)(2.0 * p->ltbl / p->L)};
-    const float t = time_ms([&] { launch_grid(ga, p->ntaps, st); });
+  const std::vector<int> caps = wide ? std::vector<int>{256, 512, 1024, 2048, 4096}
+                                     : std::vector<int>{512, 1024, 2048, 4096, 8192};
+  for (int cap : caps) {
+    if ((rc = install(cap))) break;
+    const GridArgs ga = grid_args(p, pairs, wide);
+    const float t = time_ms([&] {
+      if (wide) launch_grid_wide(ga, st);
+      else launch_grid(ga, p->ntaps, st);
+    });
     if (t < best_t) {
       best_t = t;
       best_cap = cap;
     }
   }
-  if (rc == GR_OK && best_cap != p->item_cap) rc = install_work_list(p, best_cap);
+  if (rc == GR_OK) rc = install(best_cap);
   int best_G = 0;
   float best_c = 1e30f;
   for (int G = 1; G <= 8 && rc == GR_OK; G *= 2) {
@@ -932,7 +1034,7 @@ int gr_plan_autotune(gr_plan* p, void* stream) {
 
 int gr_plan_tuning(const gr_plan* p, int* item_cap, int* cols_group_width) {
   if (!p) return gr::fail(GR_ERR_ARG, "null plan");
-  if (item_cap) *item_cap = p->item_cap;
+  if (item_cap) *item_cap = gr::use_wide(p, p->max_pairs) ? p->w_item_cap : p->item_cap;
   if (cols_group_width) *cols_group_width = p->cols_G > 0 ? p->cols_G : gr::cols_group(p->M);
   return GR_OK;
 }

@@ -28,6 +28,7 @@ EXPORTS = ("gr_params_default", "gr_filter_code", "gr_plan_create", "gr_plan_des
            "gr_plan_sizes", "gr_plan_device_bytes", "gr_reconstruct_pair",
            "gr_reconstruct_batch", "gr_reconstruct_host", "gr_last_error",
            "gr_plan_launch_count", "gr_plan_work_stats", "gr_worklist_export",
+           "gr_worklist_export_wide", "gr_plan_grid_kernel",
            "gr_plan_set_timing", "gr_plan_stage_times", "gr_reconstruct_pair_noalloc",
            "gr_plan_device_status", "gr_selftest_wait_timeout", "gr_ring_workspace_bytes",
            "gr_ring_removal", "gr_shift_pad", "gr_crop_center", "gr_entropy_workspace_bytes",
@@ -51,7 +52,8 @@ class GrParams(C.Structure):
                 ("center", C.c_float), ("filter", C.c_int), ("pswf_c", C.c_float),
                 ("sampl", C.c_float), ("ltbl", C.c_int), ("max_pairs", C.c_int),
                 ("device", C.c_int), ("geom", C.c_int), ("roi_size", C.c_float),
-                ("pixel_size", C.c_float), ("roi_x0", C.c_float), ("roi_y0", C.c_float)]
+                ("pixel_size", C.c_float), ("roi_x0", C.c_float), ("roi_y0", C.c_float),
+                ("wide_grid", C.c_int)]
 
 
 class GrBatch(C.Structure):
@@ -100,6 +102,8 @@ def lib():
         ip = C.POINTER(C.c_int)
         L.gr_worklist_export.argtypes = [P, ip, ip, ip, C.c_void_p, C.c_void_p, C.c_void_p,
                                          C.c_int, C.c_int]
+        L.gr_worklist_export_wide.argtypes = L.gr_worklist_export.argtypes
+        L.gr_plan_grid_kernel.argtypes = [C.c_void_p, C.c_int, ip]
         vp, i_, l_, f_ = C.c_void_p, C.c_int, C.c_long, C.c_float
         L.gr_ring_workspace_bytes.argtypes = [i_, i_, i_]
         L.gr_ring_workspace_bytes.restype = C.c_size_t
@@ -144,7 +148,7 @@ def filter_code(name: str) -> int:
 
 def make_params(n_det: int, n_ang: int, theta_deg, center=None, filter=FILTER_SHEPP_LOGAN,
                 pswf_c=6.0, sampl=1.0, ltbl=512, max_pairs=1, device=0, geom=0, roi_size=1.0,
-                pixel_size=1.0, roi_x0=0.0, roi_y0=0.0):
+                pixel_size=1.0, roi_x0=0.0, roi_y0=0.0, wide_grid=0):
     """GrParams plus the float32 theta array that must outlive plan creation."""
     th = np.ascontiguousarray(theta_deg, dtype=np.float32)
     if th.shape != (n_ang,):
@@ -163,24 +167,27 @@ def make_params(n_det: int, n_ang: int, theta_deg, center=None, filter=FILTER_SH
     p.geom = int(geom)
     p.roi_size, p.pixel_size = float(roi_size), float(pixel_size)
     p.roi_x0, p.roi_y0 = float(roi_x0), float(roi_y0)
+    p.wide_grid = int(wide_grid)
     return p, th
 
 
-def worklist(n_det, n_ang, theta_deg, sampl=1.0, pswf_c=6.0):
+def worklist(n_det, n_ang, theta_deg, sampl=1.0, pswf_c=6.0, wide=False):
     """Host-only gridding work list: (items[n,4], runs[n,4], splits[tiles,4], tiles_v).
 
     runs rows are (direction, jlo, jhi, P): direction = 2*angle + half, samples
-    jlo..jhi, processed in steps of samples P apart."""
+    jlo..jhi, processed in steps of samples P apart.  wide=True: the 16-pair
+    kernel's list (8 x 8 tiles, P = 1)."""
     p, th = make_params(n_det, n_ang, theta_deg, sampl=sampl, pswf_c=pswf_c)
     ni, nr, tv = C.c_int(), C.c_int(), C.c_int()
-    _check(lib().gr_worklist_export(C.byref(p), C.byref(ni), C.byref(nr), C.byref(tv), None,
-                                    None, None, 0, 0), "gr_worklist_export")
+    fn = lib().gr_worklist_export_wide if wide else lib().gr_worklist_export
+    _check(fn(C.byref(p), C.byref(ni), C.byref(nr), C.byref(tv), None,
+              None, None, 0, 0), "gr_worklist_export")
     items = np.zeros((ni.value, 4), np.int32)
     runs = np.zeros((nr.value, 4), np.int32)
     splits = np.zeros((tv.value * tv.value, 4), np.int32)
-    _check(lib().gr_worklist_export(C.byref(p), C.byref(ni), C.byref(nr), C.byref(tv),
-                                    items.ctypes.data, runs.ctypes.data, splits.ctypes.data,
-                                    ni.value, nr.value), "gr_worklist_export")
+    _check(fn(C.byref(p), C.byref(ni), C.byref(nr), C.byref(tv),
+              items.ctypes.data, runs.ctypes.data, splits.ctypes.data,
+              ni.value, nr.value), "gr_worklist_export")
     return items, runs, splits, tv.value
 
 
@@ -207,10 +214,11 @@ class Plan:
 
     def __init__(self, n_det: int, n_ang: int, theta_deg, center=None,
                  filter=FILTER_SHEPP_LOGAN, pswf_c=6.0, sampl=1.0, ltbl=512, max_pairs=1,
-                 device=0, geom=0, roi_size=1.0, pixel_size=1.0, roi_x0=0.0, roi_y0=0.0):
+                 device=0, geom=0, roi_size=1.0, pixel_size=1.0, roi_x0=0.0, roi_y0=0.0,
+                 wide_grid=0):
         self._params, self._theta = make_params(n_det, n_ang, theta_deg, center, filter,
                                                 pswf_c, sampl, ltbl, max_pairs, device, geom,
-                                                roi_size, pixel_size, roi_x0, roi_y0)
+                                                roi_size, pixel_size, roi_x0, roi_y0, wide_grid)
         h = C.c_void_p()
         _check(lib().gr_plan_create(C.byref(self._params), C.byref(h)), "gr_plan_create")
         self._h = h
@@ -242,6 +250,13 @@ class Plan:
     @property
     def handle(self):
         return self._h
+
+    def grid_kernel(self, pairs=None) -> str:
+        """'wide' (16 pairs per warp) or 'tiles' for a chunk of `pairs` pairs."""
+        w = C.c_int()
+        _check(lib().gr_plan_grid_kernel(self._h, int(pairs or self.max_pairs), C.byref(w)),
+               "gr_plan_grid_kernel")
+        return "wide" if w.value else "tiles"
 
     def device_bytes(self) -> int:
         b = C.c_size_t()

@@ -26,6 +26,7 @@ def _dev(a):
 def _gpu_pair(s1, s2, theta, **kw):
     n_ang, n_det = s1.shape
     with G.Plan(n_det, n_ang, theta, **kw) as plan:
+        assert plan.grid_kernel(1) == ("wide" if kw.get("wide_grid", 0) > 0 else "tiles")
         o1 = torch.zeros((plan.M0, max(plan.M0, n_det)), device="cuda")
         o2 = torch.zeros_like(o1)
         plan.reconstruct_pair(_dev(s1), _dev(s2), o1, o2)
@@ -35,12 +36,16 @@ def _gpu_pair(s1, s2, theta, **kw):
         return o1.cpu().numpy()[:, :plan.M0], o2.cpu().numpy()[:, :plan.M0]
 
 
+@pytest.mark.parametrize("grid", ["tiles", "wide"])
 @pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
-def test_pair_against_goldens(case):
+def test_pair_against_goldens(case, grid):
+    """Every golden case through both gridding kernels (the 16-pair kernel forced
+    on a single pair: one lane pair live, the others carry unused values)."""
     R, pix, x0, y0 = case["roi"]
     g1, g2 = _gpu_pair(case["sino1"], case["sino2"], case["theta"], center=case["center"],
                        filter=case["filter"], pswf_c=case["C"], sampl=case["sampl"],
-                       geom=case["geom"], roi_size=R, pixel_size=pix, roi_x0=x0, roi_y0=y0)
+                       geom=case["geom"], roi_size=R, pixel_size=pix, roi_x0=x0, roi_y0=y0,
+                       wide_grid=1 if grid == "wide" else -1)
     m = case["M0"]
     assert g1.shape == (m, m)
     o1, o2 = O.port_gridrec_pair(case["sino1"], case["sino2"], case["theta"],
@@ -426,3 +431,97 @@ def test_graph_refused_after_its_plan_is_destroyed():
     with pytest.raises(G.GrError):
         g.launch()
     g.close()
+
+
+# the two gridding kernels against each other: same taps and weights, FP32 sums in
+# a different order.  It shows as an image-wide offset from the centre cells of the
+# grid, where the filtered terms of every direction nearly cancel; seen up to
+# 7.3e-5 at C = 7 (each kernel is ~1e-4 from float64 there).
+KERNEL_TOL = 2e-4
+
+
+def _ellipse_batch(n, a, S, seed=0):
+    rng = np.random.default_rng(seed)
+    centers = (n / 2 + rng.uniform(-1.5, 1.5, S)).astype(np.float32)
+    sinos = np.stack([ph.random_ellipse_sinogram(seed + s, n, a, center=float(c))[0]
+                      for s, c in enumerate(centers)])
+    return sinos, centers
+
+
+def _oracle_batch(sinos, centers, th, M0, **kw):
+    refs = []
+    for i in range(0, len(sinos), 2):
+        o1, o2 = O.port_gridrec_pair(sinos[i], sinos[i + 1], th, center1=float(centers[i]),
+                                     center2=float(centers[i + 1]), **kw)
+        refs += [o1[:, :M0], o2[:, :M0]]
+    return refs
+
+
+@pytest.mark.parametrize("n,a,C_", [(96, 80, 6.0), (72, 50, 4.0), (90, 45, 7.0)])
+def test_wide_kernel_16_pairs_against_oracle(n, a, C_):
+    """A full chunk of 16 pairs grids with the 16-pair kernel (lanes = pairs x
+    re/im, 8 x 8 register sub-tiles); every slice against float64 gridrec, and
+    against the 32 x 32 tile kernel on the same input."""
+    th = ph.angles_deg(a)
+    sinos, centers = _ellipse_batch(n, a, 32, seed=n + a)
+    outs = {}
+    for mode in (0, -1):
+        with G.Plan(n, a, th, filter=G.FILTER_HANN, pswf_c=C_, max_pairs=16,
+                    wide_grid=mode) as plan:
+            assert plan.grid_kernel() == ("wide" if mode == 0 else "tiles")
+            o = torch.zeros((32, plan.M0, max(plan.M0, n)), device="cuda")
+            plan.reconstruct_batch(_dev(sinos), o, centers=_dev(centers))
+            torch.cuda.synchronize()
+            plan.device_status()
+            outs[mode] = o.cpu().numpy()[:, :, :plan.M0]
+            M0 = plan.M0
+    refs = _oracle_batch(sinos, centers, th, M0, filter=2, C_=C_)
+    for i in range(32):
+        assert ph.rel_l2(outs[0][i], refs[i]) < TOL, i
+        assert ph.rel_l2(outs[0][i], outs[-1][i]) < KERNEL_TOL, i
+
+
+def test_wide_kernel_mixed_chunks_and_reproducible():
+    """20 pairs with max_pairs 16: a wide chunk of 16 then a tile-kernel chunk of
+    4, one odd slice at the end; three runs bitwise identical."""
+    n, a = 64, 48
+    th = ph.angles_deg(a)
+    sinos, centers = _ellipse_batch(n, a, 39, seed=7)
+    with G.Plan(n, a, th, filter=G.FILTER_HANN, max_pairs=16) as plan:
+        assert plan.grid_kernel(16) == "wide" and plan.grid_kernel(4) == "tiles"
+        o = [torch.zeros((39, plan.M0, n), device="cuda") for _ in range(3)]
+        for k in range(3):
+            plan.reconstruct_batch(_dev(sinos), o[k], centers=_dev(centers))
+        torch.cuda.synchronize()
+        M0 = plan.M0
+    assert torch.equal(o[0], o[1]) and torch.equal(o[0], o[2])
+    got = o[0].cpu().numpy()[:, :, :M0]
+    ext_s = np.concatenate([sinos, np.zeros_like(sinos[:1])])
+    ext_c = np.concatenate([centers, centers[-1:]])
+    refs = _oracle_batch(ext_s, ext_c, th, M0, filter=2)
+    for i in range(39):
+        assert ph.rel_l2(got[i], refs[i]) < TOL, i
+
+
+def test_wide_kernel_split_subtiles_2048x1500():
+    """Full-size geometry: the centre sub-tiles are split over many items and
+    summed by the split reduction; a 16-pair chunk matches the tile kernel on the
+    same input."""
+    n, a = 2048, 1500
+    th = ph.angles_deg(a)
+    S = 32
+    base = [ph.line_integrals(ph.random_ellipses(s), n, th, n / 2.0 + 0.3 * s, device="cuda")
+            for s in range(2)]
+    sinos = torch.stack([base[s % 2] * (1.0 + 0.01 * s) for s in range(S)]).float().contiguous()
+    del base
+    outs = {}
+    for mode in (0, -1):
+        with G.Plan(n, a, th, filter=G.FILTER_HANN, max_pairs=16, wide_grid=mode) as plan:
+            o = torch.zeros((S, plan.M0, n), device="cuda")
+            plan.reconstruct_batch(sinos, o)
+            torch.cuda.synchronize()
+            plan.device_status()
+            outs[mode] = o
+    for i in range(S):
+        d = torch.linalg.vector_norm(outs[0][i] - outs[-1][i]) / torch.linalg.vector_norm(outs[-1][i])
+        assert float(d) < KERNEL_TOL, i

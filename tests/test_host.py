@@ -118,6 +118,56 @@ def test_worklist_gather_arbitrary_angles():
     assert _emulate_gather(48, len(th), th) < 1e-14
 
 
+def _emulate_wide(n, a, theta, sampl=1.0, pswf_c=6.0):
+    """Float64 execution of grid_wide_kernel's scheme over the exported 8 x 8 list:
+    every sample weights all 8 rows and 8 columns of the sub-tile by w(|d|), zero
+    for |d| > L/2, and adds the outer product; compared with the oracle's scatter."""
+    p = O.params(n, a, None, None, 1, pswf_c, sampl)
+    sz = O.port_sizes(p)
+    rng = np.random.default_rng(n + a)
+    spec = O.port_spectra(p, rng.random((a, n)), rng.random((a, n)))
+    href = O.port_grid(p, theta, spec)
+    items, runs, splits, tiles_v = G.worklist(n, a, theta, sampl=sampl, pswf_c=pswf_c, wide=True)
+    assert np.all(runs[:, 3] == 1) and np.all(runs[:, 2] - runs[:, 1] < 32)
+    M, L2 = sz.M, sz.L / 2
+    ts = 2 * 512 / sz.L
+    wtbl, _ = O.port_tables(p)
+    cells = np.arange(8)
+    wt = lambda d: np.where(d <= L2, wtbl[np.minimum((d * ts + 0.5).astype(int), 512)], 0.0)
+    H = np.zeros((M, M), complex)
+    T = 8
+    seen = np.zeros(len(runs), int)
+    for tile, rb, re_, slot in items:
+        tu, tv = divmod(tile, tiles_v)
+        p0, q0 = tu * T, tv * T
+        seen[rb:re_] += 1
+        for d, jlo, jhi, _ in runs[rb:re_]:
+            nn, h = divmod(d, 2)
+            t = np.deg2rad(float(theta[nn]))
+            sg = -1.0 if h else 1.0
+            for j in range(jlo, jhi + 1):
+                u = M / 2 + sg * sz.scale * j * np.cos(t) - p0
+                v = M / 2 + sg * sz.scale * j * np.sin(t) - q0
+                H[p0:p0 + T, q0:q0 + T] += np.outer(wt(np.abs(u - cells)),
+                                                    wt(np.abs(v - cells))) * spec[nn, h, j]
+    assert np.all(seen == 1), "every run belongs to exactly one item"
+    H[0, :] = 0
+    H[:, 0] = 0
+    return np.linalg.norm(H - href) / np.linalg.norm(href)
+
+
+@pytest.mark.parametrize("n,a,sampl,C_", [(64, 48, 1.0, 6.0), (100, 37, 1.2, 6.0),
+                                          (72, 30, 1.0, 4.0), (90, 25, 1.2, 7.0)])
+def test_wide_worklist_gather_equals_scatter(n, a, sampl, C_):
+    th = ph.angles_deg(a)
+    assert _emulate_wide(n, a, th, sampl, C_) < 1e-14
+
+
+def test_wide_worklist_arbitrary_angles():
+    th = np.array([-30.0, 0.0, 12.5, 90.0, 179.9, 200.0, 359.0, 45.0], np.float32)
+    assert _emulate_wide(48, len(th), th) < 1e-14
+
+
 def _steps(n, P, spw=8):
     return sum(min(P, n - b) for b in range(0, n, spw * P))
 
