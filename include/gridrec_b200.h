@@ -98,8 +98,9 @@ typedef struct {
                               C2 times its conjugate */
   int wide_grid;           /* gridding kernel: 0 = 16-pair kernel for chunks of >= 8 pairs
                               (default), 1 = for every chunk, -1 = never (2 pairs per warp
-                              over 32 x 32 tiles); same taps and weights, the sums differ
-                              only in FP32 summation order */
+                              over 32 x 32 tiles), 2 = tensor-core kernel (tcgen05, 3xTF32)
+                              for every chunk; same taps and weights, the sums differ only
+                              in order (and, for 2, in ~2^-22 relative rounding per term) */
 } gr_params;
 
 typedef struct gr_plan gr_plan;
@@ -221,7 +222,8 @@ int gr_worklist_export(const gr_params* p, int* n_items, int* n_runs, int* tiles
  * most 32 samples, step spacing 1. */
 int gr_worklist_export_wide(const gr_params* p, int* n_items, int* n_runs, int* tiles_v,
                             int* items, int* runs, int* splits, int cap_items, int cap_runs);
-/* *wide = 1 when a chunk of `pairs` pairs grids with the 16-pair kernel. */
+/* *wide = 0 (tile kernel), 1 (16-pair kernel) or 2 (tensor-core kernel) for a chunk of
+ * `pairs` pairs. */
 int gr_plan_grid_kernel(const gr_plan* plan, int pairs, int* wide);
 
 /* Text of the last error recorded on this thread (never NULL). */

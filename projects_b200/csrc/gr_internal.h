@@ -35,6 +35,15 @@ constexpr int kItemCapW = 1024;
 // Chunks of at least this many pairs use it when gr_params.wide_grid is 0.
 constexpr int kWideMinPairs = 8;
 
+// The tensor-core gridding kernel (grid_tc_kernel): a CTA accumulates a
+// kTcRows x kTcCols sub-tile (128 cells, the MMA M) for 16 pairs x (re, im)
+// (the MMA N) in tensor memory, 8 samples (the MMA K) per step.
+constexpr int kTcRows = 16;
+constexpr int kTcCols = 8;
+constexpr int kItemCapT = 2048;
+// Work-list kinds (gridrec_plan.cu).
+constexpr int kListTiles = 0, kListWide = 1, kListTensor = 2;
+
 // One run of samples: direction d (= 2*angle + half), samples j in [jlo, jhi],
 // gridded in steps of samples P apart (footprints of one step disjoint).
 struct Run {
@@ -101,6 +110,8 @@ struct GridArgs {
   const float* wtbl;     // ltbl + 1
   int n_items, pairs, n_ang, J, M, tiles_v, n_slots, ltbl;
   float L2, tblspcg;
+  const unsigned* codes = nullptr;  // grid_tc_kernel: flat (direction << 13 | j) per sample
+  int* err = nullptr;               // device error word for bounded-wait timeouts
 };
 
 struct ColArgs {
@@ -164,6 +175,7 @@ cudaError_t launch_spectra(const SpectraArgs& a, gr_dtype dt, cudaStream_t s);
 // its split-tile reduction when tiles are split.
 cudaError_t launch_grid(const GridArgs& a, int ntaps, cudaStream_t s);
 cudaError_t launch_grid_wide(const GridArgs& a, cudaStream_t s);
+cudaError_t launch_grid_tc(const GridArgs& a, cudaStream_t s);
 int cols_group(int M);
 cudaError_t launch_cols(const ColArgs& a, cudaStream_t s);
 cudaError_t launch_rows(const RowArgs& a, cudaStream_t s);

@@ -1027,6 +1027,295 @@ __global__ void __launch_bounds__(256) split_reduce_wide_kernel(GridArgs a) {
   }
 }
 
+// ------------------------------------------------------------------ gridding on the tensor cores
+// The gather of grid_wide_kernel as a dense product per work item.  For a
+// kTcRows x kTcCols sub-tile (128 cells) and the item's samples s,
+//   H[cell][value] = sum_s A[cell][s] B[s][value],
+//   A[(r, c)][s] = w(|u_s - r|) w(|v_s - c|)   (zero where a distance exceeds L/2),
+//   B[s][2 p + re/im] = spectrum of pair p at sample s,
+// so each tcgen05.mma (kind::tf32, M = 128 cells, N = 32 values, K = 8
+// samples) applies eight samples to the whole sub-tile for 16 pairs.  The
+// accumulator stays in tensor memory for the whole item.  FP32 accuracy comes
+// from three TF32 products per step, A_hi B_hi + A_hi B_lo + A_lo B_hi with
+// x_hi = x with the low 13 mantissa bits cleared and x_lo = x - x_hi (exact),
+// so each term keeps ~22 bits.  Positions, distances and table indices are
+// those of grid_kernel (positions relative to the enclosing 32 x 32 tile,
+// moved by exact integers).  A CTA of 128 threads handles one item at a time:
+// thread t owns cell t of A, one weight, and two values of B per step; the
+// operands are double-buffered and each buffer is released by tcgen05.commit
+// on its own mbarrier (bounded waits, device error word on timeout).  Items
+// list their samples as one flat array of (direction << 13 | j) codes padded
+// to a multiple of 8 with j = 0, whose spectrum is zero.  Operands use the
+// no-swizzle K-major layout: 8-row x 16-byte core matrices, the two K halves
+// 128 bytes apart (LBO), 8-row groups 256 bytes apart (SBO).
+
+constexpr int kTcThreads = 128;
+constexpr int kTcStages = 2;                    // operand buffers in flight
+constexpr int kTcStage = 2 * 4096 + 2 * 1024;  // A_hi, A_lo (128 x 8), B_hi, B_lo (32 x 8) bytes
+constexpr int kTcSmem = 4224 + kTcStages * kTcStage + 16 * 8 * 4 + 8 * 8 * 4 + 8 * kTcStages + 16;
+
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+  // start >> 4 [0,14), LBO 128 >> 4 [16,30), SBO 256 >> 4 [32,46), version 1 [46,48), no swizzle
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)(128 >> 4) << 16) |
+         ((uint64_t)(256 >> 4) << 32) | (1ull << 46);
+}
+// instruction descriptor: D f32, A/B tf32, both K-major, N = 32, M = 128
+constexpr uint32_t kTcIdesc = (1u << 4) | (2u << 7) | (2u << 10) | ((32u >> 3) << 17) | ((128u >> 4) << 24);
+
+__device__ __forceinline__ void tc_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+      "l"(da), "l"(db), "r"(kTcIdesc), "r"(acc));
+}
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+}
+__device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
+
+__global__ void __launch_bounds__(kTcThreads) grid_tc_kernel(GridArgs a) {
+  constexpr int TR = kTcRows, TC = kTcCols;
+  extern __shared__ __align__(128) unsigned char smt[];
+  float* s_wtbl = reinterpret_cast<float*>(smt);                  // up to 1028 floats
+  unsigned char* stg = smt + 4224;                                // [kTcStages][kTcStage]
+  float* s_wu = reinterpret_cast<float*>(stg + kTcStages * kTcStage);  // [TR][8]: row weights
+  float* s_wv = s_wu + TR * 8;                                    // [TC][8]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(s_wv + TC * 8);     // [kTcStages]
+  unsigned* s_misc = reinterpret_cast<unsigned*>(bar + kTcStages);  // [0] tmem base, [1] item
+  const int tid = threadIdx.x, warp = tid >> 5;
+  for (int i = tid; i <= a.ltbl; i += kTcThreads) s_wtbl[i] = __ldg(&a.wtbl[i]);
+  if (tid == 0) {
+    for (int b = 0; b < kTcStages; ++b) mbar_init(&bar[b], 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 32;" ::"r"(
+                     smem_u32(&s_misc[0]))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_misc[0];
+  const float L2 = a.L2, ts = a.tblspcg;
+  const int ltbl = a.ltbl;
+  const float half_m = (float)(a.M / 2);
+  const int groups = (a.pairs + kWidePairs - 1) / kWidePairs;
+  const unsigned total = (unsigned)a.n_items * (unsigned)groups;
+  const size_t per_dir = (size_t)(a.J >> 2) * 64;
+  const size_t MM = (size_t)a.M * a.M;
+  const unsigned* codes = a.codes;
+  // roles: weights (thread -> sample k = tid >> 4, row tid & 15; tid < 64 also
+  // sample tid >> 3, column tid & 7); B (value n = tid >> 2, samples kb, kb + 1);
+  // A (cell tid = r * TC + c)
+  const int wk = tid >> 4, wr = tid & 15, vk = (tid >> 3) & 7, vc = tid & 7;
+  const int bn = tid >> 2, bk = (tid & 3) * 2;
+  const int bp = bn >> 1, bc = bn & 1;
+  unsigned uses[kTcStages] = {};
+  int last_buf = -1;
+  bool ok = true;
+  for (;;) {
+    if (tid == 0) s_misc[1] = atomicAdd(a.queue, 1u);
+    __syncthreads();
+    const unsigned w = s_misc[1];
+    if (w >= total) break;
+    const int grp = (int)(w / (unsigned)a.n_items);
+    const Item it = a.items[w - (unsigned)grp * (unsigned)a.n_items];
+    const int pg0 = grp * kWidePairs;
+    const int np = min(kWidePairs, a.pairs - pg0);
+    const int tu = it.tile / a.tiles_v, tv = it.tile - (it.tile / a.tiles_v) * a.tiles_v;
+    const int p0 = tu * TR, q0 = tv * TC;
+    const float offu = half_m - (float)(p0 & ~(kTile - 1)), offv = half_m - (float)(q0 & ~(kTile - 1));
+    const float subu = (float)(p0 & (kTile - 1)), subv = (float)(q0 & (kTile - 1));
+    const float* specg = reinterpret_cast<const float*>(a.spec + (size_t)grp * 2 * a.n_ang * per_dir);
+    const int nchunk = (it.run_end - it.run_begin) >> 3;
+    // a step's codes (this thread's weight samples and its two B samples) are
+    // loaded two steps ahead, its B values one step ahead
+    struct Codes { unsigned w, v, b0, b1; };
+    auto load_codes = [&](int ch) {
+      Codes c{0u, 0u, 0u, 0u};
+      if (ch < nchunk) {
+        const unsigned* cs = codes + it.run_begin + ch * 8;
+        c = Codes{__ldg(&cs[wk]), __ldg(&cs[vk]), __ldg(&cs[bk]), __ldg(&cs[bk + 1])};
+      }
+      return c;
+    };
+    auto load_val = [&](unsigned code) {
+      const int j = code & 8191;
+      return __ldg(&specg[(((code >> 13) * per_dir + (j >> 2) * 64 + bp * 4 + (j & 3)) << 1) + bc]);
+    };
+    Codes cur = load_codes(0), nxt = load_codes(1);
+    float b0 = load_val(cur.b0), b1 = load_val(cur.b1);
+    float dwx = __ldg(&a.dir[cur.w >> 13]).x, dvy = __ldg(&a.dir[cur.v >> 13]).y;
+    for (int ch = 0; ch < nchunk && ok; ++ch) {
+      const int buf = ch % kTcStages;
+      const unsigned cw = cur.w, cv = cur.v;
+      const float cdx = dwx, cdy = dvy;
+      unsigned char* sb = stg + buf * kTcStage;
+      // the MMAs that last read this buffer are done
+      bool got = true;
+      if (uses[buf] > 0) got = mbar_wait(&bar[buf], (uses[buf] - 1) & 1);
+      // weights of this step's samples
+      {
+        const float fj = (float)(cw & 8191);
+        const float u = fmaf(fj, cdx, offu) - subu;
+        const float dd = fabsf(u - (float)wr);
+        const float wt = s_wtbl[min(table_index(dd, ts), ltbl)];
+        s_wu[wr * 8 + wk] = dd <= L2 ? wt : 0.f;
+        if (tid < 64) {
+          const float fjv = (float)(cv & 8191);
+          const float v = fmaf(fjv, cdy, offv) - subv;
+          const float ddv = fabsf(v - (float)vc);
+          const float wtv = s_wtbl[min(table_index(ddv, ts), ltbl)];
+          s_wv[vc * 8 + vk] = ddv <= L2 ? wtv : 0.f;
+        }
+      }
+      // B (K-major: value n's 4 samples per 16-byte row), hi and lo parts
+      {
+        const int off = (bn >> 3) * 256 + (bk >> 2) * 128 + (bn & 7) * 16 + (bk & 3) * 4;
+        const float h0 = tf32_hi(b0), h1 = tf32_hi(b1);
+        *reinterpret_cast<float2*>(sb + 8192 + off) = make_float2(h0, h1);
+        *reinterpret_cast<float2*>(sb + 9216 + off) = make_float2(b0 - h0, b1 - h1);
+      }
+      // next step's values (codes loaded a step ago), codes of the step after
+      const float nb0 = load_val(nxt.b0), nb1 = load_val(nxt.b1);
+      dwx = __ldg(&a.dir[nxt.w >> 13]).x;
+      dvy = __ldg(&a.dir[nxt.v >> 13]).y;
+      cur = nxt;
+      nxt = load_codes(ch + 2);
+      if (__syncthreads_or(!got)) {
+        ok = false;
+        break;
+      }
+      // A: cell tid = (r, c), its 8 products, hi and lo parts
+      {
+        const int r = tid >> 3, c = tid & 7;
+        const float4 u0 = *reinterpret_cast<const float4*>(s_wu + r * 8);
+        const float4 u1 = *reinterpret_cast<const float4*>(s_wu + r * 8 + 4);
+        const float4 v0 = *reinterpret_cast<const float4*>(s_wv + c * 8);
+        const float4 v1 = *reinterpret_cast<const float4*>(s_wv + c * 8 + 4);
+        const float4 p0v = make_float4(u0.x * v0.x, u0.y * v0.y, u0.z * v0.z, u0.w * v0.w);
+        const float4 p1v = make_float4(u1.x * v1.x, u1.y * v1.y, u1.z * v1.z, u1.w * v1.w);
+        const float4 h0 = make_float4(tf32_hi(p0v.x), tf32_hi(p0v.y), tf32_hi(p0v.z), tf32_hi(p0v.w));
+        const float4 h1 = make_float4(tf32_hi(p1v.x), tf32_hi(p1v.y), tf32_hi(p1v.z), tf32_hi(p1v.w));
+        const int off = (tid >> 3) * 256 + (tid & 7) * 16;
+        *reinterpret_cast<float4*>(sb + off) = h0;
+        *reinterpret_cast<float4*>(sb + off + 128) = h1;
+        *reinterpret_cast<float4*>(sb + 4096 + off) =
+            make_float4(p0v.x - h0.x, p0v.y - h0.y, p0v.z - h0.z, p0v.w - h0.w);
+        *reinterpret_cast<float4*>(sb + 4096 + off + 128) =
+            make_float4(p1v.x - h1.x, p1v.y - h1.y, p1v.z - h1.z, p1v.w - h1.w);
+      }
+      // generic-proxy writes -> visible to the tensor core (async proxy)
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      __syncthreads();
+      if (tid == 0) {
+        tc_fence_after();
+        const uint32_t base = smem_u32(sb);
+        const uint64_t a_hi = tc_desc(base), a_lo = tc_desc(base + 4096);
+        const uint64_t b_hi = tc_desc(base + 8192), b_lo = tc_desc(base + 9216);
+        tc_mma(tmem, a_lo, b_hi, ch > 0 ? 1u : 0u);
+        tc_mma(tmem, a_hi, b_lo, 1u);
+        tc_mma(tmem, a_hi, b_hi, 1u);
+        tc_commit(&bar[buf]);
+      }
+      uses[buf]++;
+      last_buf = buf;
+      b0 = nb0;
+      b1 = nb1;
+    }
+    if (!ok) break;
+    float v[32];
+#pragma unroll
+    for (int k = 0; k < 32; ++k) v[k] = 0.f;
+    if (nchunk > 0) {  // a tile that no sample reaches has an empty item: zeros
+      // all MMAs of the item are done: the last commit covers the earlier ones
+      const bool got = mbar_wait(&bar[last_buf], (uses[last_buf] - 1) & 1);
+      if (__syncthreads_or(!got)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      unsigned r[32];
+      const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+      asm volatile(
+          "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+          "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+          : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+            "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+            "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+            "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+            "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+            "=r"(r[31])
+          : "r"(taddr));
+      asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+      for (int k = 0; k < 32; ++k) v[k] = __uint_as_float(r[k]);
+    }
+    const int cr = tid >> 3, cc = tid & 7;  // this thread's cell
+    if (it.slot < 0) {
+      const int p = p0 + cr, q = q0 + cc;
+      const bool zero = p == 0 || q == 0;
+#pragma unroll
+      for (int pp = 0; pp < kWidePairs; ++pp)
+        if (pp < np)
+          a.H[(size_t)(pg0 + pp) * MM + (size_t)p * a.M + q] =
+              zero ? make_float2(0.f, 0.f) : make_float2(v[2 * pp], v[2 * pp + 1]);
+    } else {
+      float4* part = reinterpret_cast<float4*>(a.scratch) +
+                     (((size_t)grp * a.n_slots + it.slot) * (TR * TC) + tid) * 8;
+#pragma unroll
+      for (int k = 0; k < 8; ++k) part[k] = make_float4(v[4 * k], v[4 * k + 1], v[4 * k + 2], v[4 * k + 3]);
+    }
+    // every thread has read the accumulator before the next item overwrites it
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(a.err, 1);
+    // let MMAs in flight finish before the tensor memory is released
+    if (last_buf >= 0) mbar_wait(&bar[last_buf], (uses[last_buf] - 1) & 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 32;" ::"r"(tmem) : "memory");
+}
+
+// Sums the partial sub-tiles of every split sub-tile of grid_tc_kernel in slot order.
+__global__ void __launch_bounds__(256) split_reduce_tc_kernel(GridArgs a) {
+  constexpr int TR = kTcRows, TC = kTcCols;
+  const int4 sp = a.split_list[blockIdx.x];  // (tile, slot0, nsplit, -)
+  const int grp = blockIdx.y;
+  const int pg0 = grp * kWidePairs;
+  const int np = min(kWidePairs, a.pairs - pg0);
+  const int tu = sp.x / a.tiles_v, tv = sp.x - (sp.x / a.tiles_v) * a.tiles_v;
+  const int p0 = tu * TR, q0 = tv * TC;
+  const float* base = reinterpret_cast<const float*>(a.scratch) +
+                      ((size_t)grp * a.n_slots + sp.y) * (TR * TC * 32);
+  const size_t MM = (size_t)a.M * a.M;
+  for (int i = threadIdx.x; i < TR * TC * 32; i += blockDim.x) {
+    const int cell = i >> 5, l = i & 31;
+    if ((l >> 1) >= np) continue;
+    float sum = 0.f;
+    for (int k = 0; k < sp.z; ++k) sum += __ldg(&base[(size_t)k * (TR * TC * 32) + i]);
+    const int p = p0 + cell / TC, q = q0 + cell % TC;
+    if (p == 0 || q == 0) sum = 0.f;
+    float* Hf = reinterpret_cast<float*>(a.H + (size_t)(pg0 + (l >> 1)) * MM);
+    Hf[((size_t)p * a.M + q) * 2 + (l & 1)] = sum;
+  }
+}
+
 // ------------------------------------------------------------------ 2-D FFT, first axis (K3)
 // G columns of H per CTA: thread t works on column g = t % G (so a warp's
 // loads cover G adjacent columns of several rows) and line position t / G.
@@ -1281,6 +1570,7 @@ cudaError_t init_kernel_attributes() {
   fns.push_back((const void*)grid_kernel<4>);
   fns.push_back((const void*)grid_kernel<kMaxTaps>);
   fns.push_back((const void*)grid_wide_kernel);
+  fns.push_back((const void*)grid_tc_kernel);
   for (const void* f : fns) {
     if (e != cudaSuccess) break;
     e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
@@ -1372,6 +1662,30 @@ cudaError_t launch_grid_wide(const GridArgs& a, cudaStream_t s) {
   if (e != cudaSuccess || a.n_split_tiles == 0) return e;
   dim3 rgrid(a.n_split_tiles, (unsigned)groups);
   split_reduce_wide_kernel<<<rgrid, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grid_tc(const GridArgs& a, cudaStream_t s) {
+  if (a.n_items == 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(a.queue, 0, sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  // CTAs per SM from its shared memory (1 KB reserved per CTA) and tensor
+  // memory (32 of the 512 columns each); 128 threads and 56 registers allow more
+  int smem_sm = 0;
+  cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+  int per_sm = std::min(smem_sm / (kTcSmem + 1024), 16);
+  per_sm = std::max(per_sm, 1);
+  const long groups = (a.pairs + kWidePairs - 1) / kWidePairs;
+  const long want = (long)a.n_items * groups;
+  const int blocks = (int)std::min<long>(want, (long)per_sm * sms);
+  grid_tc_kernel<<<blocks, kTcThreads, kTcSmem, s>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess || a.n_split_tiles == 0) return e;
+  dim3 rgrid(a.n_split_tiles, (unsigned)groups);
+  split_reduce_tc_kernel<<<rgrid, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 

@@ -141,6 +141,14 @@ struct Plan {
   float4* d_w_scratch = nullptr;    // [pair group of 16][slot][64 cells x 32 lanes] floats
   size_t w_scratch_cells = 0;
   int spec_pairs = 0;               // pairs the spectra workspace holds
+  // tensor-core gridding (grid_tc_kernel, gr_params.wide_grid = 2): 16 x 8
+  // sub-tiles, each item's samples as one flat code array padded to 8
+  int t_tiles_v = 0, t_items = 0, t_slots = 0, t_split_tiles = 0, t_item_cap = kItemCapT;
+  Item* d_t_items = nullptr;
+  unsigned* d_t_codes = nullptr;
+  int4* d_t_split_list = nullptr;
+  float4* d_t_scratch = nullptr;    // [group of 16][slot][128 cells][32 values] floats
+  size_t t_scratch_cells = 0;
   int cols_G = 0;                   // column-FFT group width (0 = cols_group(M); autotuned)
   std::vector<gr_graph*> graphs;    // live CUDA graphs replaying this plan's buffers
   float4* d_pq = nullptr;
@@ -239,14 +247,18 @@ int run_spacing(double du, double dv, int n, double L, int spw, int* steps) {
   return P;
 }
 
+// kind: kListTiles (32 x 32, grid_kernel), kListWide (8 x 8, grid_wide_kernel) or
+// kListTensor (16 x 8, grid_tc_kernel; its runs are flattened by build_tc_list).
 void build_work_list(int M, int J, double L, int n_ang, const std::vector<double>& dxy,
-                     WorkList* wl, int item_cap = kItemCap, bool wide = false) {
-  const int T = wide ? kTileW : kTile;
-  const int run_max = wide ? kRunMaxW : kRunMax;
+                     WorkList* wl, int item_cap = kItemCap, int kind = kListTiles) {
+  const bool wide = kind != kListTiles;
+  const int Tu = kind == kListTiles ? kTile : (kind == kListWide ? kTileW : kTcRows);
+  const int Tv = kind == kListTiles ? kTile : (kind == kListWide ? kTileW : kTcCols);
+  const int run_max = kind == kListWide ? kRunMaxW : kRunMax;
   const double M2 = M / 2;
   const double L2 = L / 2 + 2e-3;  // box margin covers FP32 position rounding
-  wl->tiles_u = (M + T - 1) / T;
-  wl->tiles_v = wl->tiles_u;
+  wl->tiles_u = (M + Tu - 1) / Tu;
+  wl->tiles_v = (M + Tv - 1) / Tv;
   const int n_tiles = wl->tiles_u * wl->tiles_v;
   const int n_dir = 2 * n_ang;
   struct TRun { int tile, dir, jlo, jhi; };
@@ -263,18 +275,18 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
   for (int d = 0; d < n_dir; ++d) {
     const double dx = dxy[2 * d], dy = dxy[2 * d + 1];
     for (int tu = 0; tu < wl->tiles_u; ++tu) {
-      const double x0 = tu * T - L2, x1 = std::min(tu * T + T, M) - 1 + L2;
+      const double x0 = tu * Tu - L2, x1 = std::min(tu * Tu + Tu, M) - 1 + L2;
       double ta = 1.0, tb = J - 1.0;
       if (!slab(M2, dx, x0, x1, ta, tb)) continue;
       // y extent of the samples in this x slab -> candidate tile columns
       const double ya = M2 + ta * dy, yb = M2 + tb * dy;
       const double ymin = std::min(ya, yb), ymax = std::max(ya, yb);
-      int tv0 = (int)std::floor((ymin - L2) / T) - 1;
-      int tv1 = (int)std::floor((ymax + L2) / T) + 1;
+      int tv0 = (int)std::floor((ymin - L2) / Tv) - 1;
+      int tv1 = (int)std::floor((ymax + L2) / Tv) + 1;
       tv0 = std::max(tv0, 0);
       tv1 = std::min(tv1, wl->tiles_v - 1);
       for (int tv = tv0; tv <= tv1; ++tv) {
-        const double y0 = tv * T - L2, y1 = std::min(tv * T + T, M) - 1 + L2;
+        const double y0 = tv * Tv - L2, y1 = std::min(tv * Tv + Tv, M) - 1 + L2;
         double sa = ta, sb = tb;
         if (!slab(M2, dy, y0, y1, sa, sb)) continue;
         const int jlo = std::max(1, (int)std::ceil(sa - 1e-6));
@@ -391,7 +403,7 @@ int install_work_list(Plan* p, int item_cap) {
 // The 16-pair kernel's work list (8 x 8 sub-tiles), placed on the device.
 int install_work_list_wide(Plan* p, int item_cap) {
   WorkList wl;
-  build_work_list(p->M, p->J, p->L, p->n_ang, p->dxy, &wl, item_cap, true);
+  build_work_list(p->M, p->J, p->L, p->n_ang, p->dxy, &wl, item_cap, kListWide);
   std::vector<int4> split_list;
   for (size_t t = 0; t < wl.splits.size(); ++t)
     if (wl.splits[t].nsplit > 1)
@@ -420,10 +432,66 @@ int install_work_list_wide(Plan* p, int item_cap) {
   return GR_OK;
 }
 
+// The tensor-core kernel's work list: 16 x 8 sub-tiles; each item's runs
+// flattened into (direction << 13 | j) codes, padded with j = 0 (a zero
+// spectrum) to a whole number of 8-sample steps.
+int install_work_list_tc(Plan* p, int item_cap) {
+  WorkList wl;
+  build_work_list(p->M, p->J, p->L, p->n_ang, p->dxy, &wl, item_cap, kListTensor);
+  std::vector<unsigned> codes;
+  codes.reserve((size_t)wl.total + 8 * wl.items.size());
+  std::vector<Item> items(wl.items.size());
+  for (size_t i = 0; i < wl.items.size(); ++i) {
+    const Item& it = wl.items[i];
+    const int begin = (int)codes.size();
+    for (int r = it.run_begin; r < it.run_end; ++r)
+      for (int j = wl.runs[r].jlo; j <= wl.runs[r].jhi; ++j)
+        codes.push_back(((unsigned)wl.runs[r].dir << 13) | (unsigned)j);
+    while ((codes.size() - begin) % 8) codes.push_back(0u);
+    items[i] = {it.tile, begin, (int)codes.size(), it.slot};
+  }
+  std::vector<int4> split_list;
+  for (size_t t = 0; t < wl.splits.size(); ++t)
+    if (wl.splits[t].nsplit > 1)
+      split_list.push_back(make_int4((int)t, wl.splits[t].slot0, wl.splits[t].nsplit, 0));
+  dev_free(p, &p->d_t_items);
+  dev_free(p, &p->d_t_codes);
+  dev_free(p, &p->d_t_split_list);
+  int rc;
+  if ((rc = upload(p, &p->d_t_items, items)) || (rc = upload(p, &p->d_t_codes, codes)) ||
+      (rc = upload(p, &p->d_t_split_list, split_list)))
+    return rc;
+  const size_t groups = (size_t)(p->max_pairs + kWidePairs - 1) / kWidePairs;
+  const size_t cells = groups * (size_t)std::max(wl.n_slots, 1) * (kTcRows * kTcCols * 32 / 4);
+  if (cells > p->t_scratch_cells) {
+    dev_free(p, &p->d_t_scratch);
+    if ((rc = dev_alloc(p, &p->d_t_scratch, cells))) return rc;
+    p->t_scratch_cells = cells;
+  }
+  p->t_tiles_v = wl.tiles_v;
+  p->t_items = (int)items.size();
+  p->t_slots = wl.n_slots;
+  p->t_split_tiles = (int)split_list.size();
+  p->t_item_cap = item_cap;
+  return GR_OK;
+}
+
+bool use_tc(const Plan* p, int pairs) {
+  (void)pairs;
+  return p->t_items > 0 && p->wide_mode == 2;
+}
+
 // Whether a chunk of `pairs` pairs grids with grid_wide_kernel.
 bool use_wide(const Plan* p, int pairs) {
-  if (p->w_items == 0 || p->wide_mode < 0) return false;
+  if (p->w_items == 0 || p->wide_mode < 0 || use_tc(p, pairs)) return false;
   return p->wide_mode > 0 || pairs >= kWideMinPairs;
+}
+
+GridArgs grid_args_tc(const Plan* p, int pairs) {
+  return GridArgs{p->d_spec, p->d_H, p->d_t_scratch, p->d_queue, p->d_t_items, nullptr,
+                  p->d_t_split_list, p->t_split_tiles, p->d_dir, p->d_wtbl, p->t_items, pairs,
+                  p->n_ang, p->J, p->M, p->t_tiles_v, p->t_slots, p->ltbl, (float)(p->L / 2),
+                  (float)(2.0 * p->ltbl / p->L), p->d_t_codes, p->d_err};
 }
 
 GridArgs grid_args(const Plan* p, int pairs, bool wide) {
@@ -480,8 +548,8 @@ int check_params(const gr_params* prm, const Pswf** pw) {
   if (!(prm->sampl >= 1.0f) || prm->sampl > 4.0f)
     return fail(GR_ERR_ARG, "sampl must be in [1, 4]");
   if (prm->max_pairs < 1) return fail(GR_ERR_ARG, "max_pairs must be >= 1");
-  if (prm->wide_grid < -1 || prm->wide_grid > 1)
-    return fail(GR_ERR_ARG, "wide_grid must be -1, 0 or 1");
+  if (prm->wide_grid < -1 || prm->wide_grid > 2)
+    return fail(GR_ERR_ARG, "wide_grid must be -1, 0, 1 or 2");
   if (prm->roi_size < 0.f || prm->roi_size > 4.f || prm->pixel_size < 0.f || prm->pixel_size > 16.f)
     return fail(GR_ERR_ARG, "roi_size in [0, 4] and pixel_size in [0, 16] (0 = 1)");
   *pw = find_pswf(prm->pswf_c);
@@ -553,14 +621,17 @@ int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1
   PhaseArgs ph{centers, p->center, slice_base, n_valid, p->d_filt, p->d_pq, p->J, p->pdim, pairs};
   GR_CUDA(launch_phase(ph, st));
   GR_MARK();
+  const bool tc = use_tc(p, pairs);
   const bool wide = use_wide(p, pairs);
   SpectraArgs sa{s1, s2, in_pair_stride, n_valid, slice_base, flat, dark, flat_stride, p->d_pq,
                  p->d_spec,
-                 p->d_tw_p, p->n_det, p->n_ang, p->pdim, p->J, pairs, p->d_roi_off, wide ? 1 : 0};
+                 p->d_tw_p, p->n_det, p->n_ang, p->pdim, p->J, pairs, p->d_roi_off,
+                 (wide || tc) ? 1 : 0};
   GR_CUDA(launch_spectra(sa, dt, st));
   GR_MARK();
-  const GridArgs ga = grid_args(p, pairs, wide);
-  GR_CUDA(wide ? launch_grid_wide(ga, st) : launch_grid(ga, p->ntaps, st));
+  const GridArgs ga = tc ? grid_args_tc(p, pairs) : grid_args(p, pairs, wide);
+  GR_CUDA(tc ? launch_grid_tc(ga, st)
+             : (wide ? launch_grid_wide(ga, st) : launch_grid(ga, p->ntaps, st)));
   GR_MARK();
   ColArgs ca{p->d_H, p->d_tw_m, p->M, pairs, p->d_err, p->cols_G};
   GR_CUDA(launch_cols(ca, st));
@@ -794,14 +865,16 @@ int gr_plan_create(const gr_params* prm, gr_plan** out) {
       (rc = upload(p, &p->d_filt, filt)) || (rc = upload(p, &p->d_tw_p, twiddles((int)pdim))) ||
       (rc = upload(p, &p->d_tw_m, twiddles((int)M))) || (rc = upload(p, &p->d_dir, dirs)) ||
       (rc = install_work_list(p, kItemCap)) ||
-      ((p->wide_mode > 0 || (p->wide_mode == 0 && p->max_pairs >= kWideMinPairs)) &&
+      (p->wide_mode == 2 && (rc = install_work_list_tc(p, kItemCapT))) ||
+      ((p->wide_mode == 1 || (p->wide_mode == 0 && p->max_pairs >= kWideMinPairs)) &&
        (rc = install_work_list_wide(p, kItemCapW)))) {
     gr_plan_destroy(p);
     return rc;
   }
   const size_t P = (size_t)p->max_pairs;
   // the 16-pair kernel's spectra layout holds whole groups of 16 pairs
-  const size_t P_spec = p->w_items ? (P + kWidePairs - 1) / kWidePairs * kWidePairs : P;
+  const size_t P_spec =
+      (p->w_items || p->t_items) ? (P + kWidePairs - 1) / kWidePairs * kWidePairs : P;
   p->spec_pairs = (int)P_spec;
   if ((rc = dev_alloc(p, &p->d_spec, P_spec * p->n_ang * 2 * p->J)) ||
       (rc = dev_alloc(p, &p->d_H, P * (size_t)M * M)) ||
@@ -831,7 +904,7 @@ static int worklist_export(const gr_params* prm, bool wide, int* n_items, int* n
   if ((rc = geometry(prm, pw, &geo))) return rc;
   WorkList wl;
   build_work_list((int)geo.M, (int)(geo.pdim / 2), geo.L, prm->n_ang, directions(prm, geo.scale),
-                  &wl, wide ? kItemCapW : kItemCap, wide);
+                  &wl, wide ? kItemCapW : kItemCap, wide ? kListWide : kListTiles);
   if (n_items) *n_items = (int)wl.items.size();
   if (n_runs) *n_runs = (int)wl.runs.size();
   if (tiles_v) *tiles_v = wl.tiles_v;
@@ -858,7 +931,8 @@ int gr_worklist_export_wide(const gr_params* prm, int* n_items, int* n_runs, int
 
 int gr_plan_grid_kernel(const gr_plan* p, int pairs, int* wide) {
   if (!p || !wide) return gr::fail(GR_ERR_ARG, "null argument");
-  *wide = gr::use_wide(p, std::min(std::max(pairs, 1), p->max_pairs)) ? 1 : 0;
+  const int pr = std::min(std::max(pairs, 1), p->max_pairs);
+  *wide = gr::use_tc(p, pr) ? 2 : (gr::use_wide(p, pr) ? 1 : 0);
   return GR_OK;
 }
 
