@@ -218,8 +218,9 @@ int gr_plan_stage_times(gr_plan* plan, double* ms5, long* chunks);
  * {counter, slot0, nsplit, 0} per tile (tile = tu * tiles_v + tv, 32 x 32 cells). */
 int gr_worklist_export(const gr_params* p, int* n_items, int* n_runs, int* tiles_v, int* items,
                        int* runs, int* splits, int cap_items, int cap_runs);
-/* The same for the 16-pair gridding kernel's list: tiles of 8 x 8 cells, runs of at
- * most 32 samples, step spacing 1. */
+/* The same for the 16-pair gridding kernel's list: tiles of 4 x 8 cells (tile index
+ * tu * tiles_v + tv, 4 rows by 8 columns), runs of at most 16 samples, step spacing 1;
+ * splits then holds 2 * tiles_v * tiles_v records (M/4 tile rows of M/8 tiles). */
 int gr_worklist_export_wide(const gr_params* p, int* n_items, int* n_runs, int* tiles_v,
                             int* items, int* runs, int* splits, int cap_items, int cap_runs);
 /* *wide = 0 (tile kernel), 1 (16-pair kernel) or 2 (tensor-core kernel) for a chunk of

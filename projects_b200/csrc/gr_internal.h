@@ -24,12 +24,14 @@ constexpr int kRunMax = 64;
 constexpr int kItemCap = 2048;
 
 // The 16-pair gridding kernel (grid_wide_kernel): a warp's lanes carry the
-// (re, im) components of 16 slice pairs and hold a kTileW x kTileW sub-tile
-// of cells in registers.
-constexpr int kTileW = 8;
+// (re, im) components of 16 slice pairs and hold a kWideRows x kWideCols
+// sub-tile of cells in registers (kWideCols = 8: four packed column pairs).
+constexpr int kWideRows = 4;
+constexpr int kWideCols = 8;
+constexpr int kWideMinBlocks = 6;
 constexpr int kWidePairs = 16;
 // Longest run it stages at once (longer runs are split on the host).
-constexpr int kRunMaxW = 32;
+constexpr int kRunMaxW = 16;
 // Work per item before a sub-tile is split (samples + per-run overhead).
 constexpr int kItemCapW = 1024;
 // Chunks of at least this many pairs use it when gr_params.wide_grid is 0.

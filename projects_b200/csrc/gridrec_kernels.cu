@@ -803,7 +803,7 @@ __global__ void __launch_bounds__(256) split_reduce_kernel(GridArgs a) {
 // * the geometry and weights of a sample are warp-uniform and computed once
 //   for all 16 pairs (16 lanes per sample, one weight each, exchanged through
 //   a small shared record);
-// * a work item is one kTileW x kTileW sub-tile whose cells stay in registers
+// * a work item is one kWideRows x kWideCols sub-tile whose cells stay in registers
 //   for all its runs: no shared-memory read-modify-write and no atomics.
 // Every sample carries one weight per sub-tile row and per column,
 // w(|u - row|) and w(|v - col|), zero where the distance exceeds L/2 -- the
@@ -852,9 +852,9 @@ __device__ __forceinline__ void ffma2(unsigned long long& acc, unsigned long lon
   asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(a), "l"(b));
 }
 
-// 4 CTAs per SM: 128 registers a thread (no spills), 16 warps
-__global__ void __launch_bounds__(kWideWarps * 32, 4) grid_wide_kernel(GridArgs a) {
-  constexpr int T = kTileW;
+// kWideMinBlocks CTAs per SM (registers capped accordingly, no spills)
+__global__ void __launch_bounds__(kWideWarps * 32, kWideMinBlocks) grid_wide_kernel(GridArgs a) {
+  constexpr int TR = kWideRows, TC = kWideCols;
   extern __shared__ float4 smw4[];
   float* s_wtbl = reinterpret_cast<float*>(smw4);  // table: up to 1028 floats
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -887,7 +887,7 @@ __global__ void __launch_bounds__(kWideWarps * 32, 4) grid_wide_kernel(GridArgs 
     const int np = min(kWidePairs, a.pairs - pg0);
     const int tu = it.tile / a.tiles_v;
     const int tv = it.tile - tu * a.tiles_v;
-    const int p0 = tu * T, q0 = tv * T;
+    const int p0 = tu * TR, q0 = tv * TC;
     // positions as grid_kernel forms them (relative to the enclosing 32 x 32
     // tile), then moved to the sub-tile by an exact integer: both kernels see
     // the same |d| and table indices
@@ -895,11 +895,11 @@ __global__ void __launch_bounds__(kWideWarps * 32, 4) grid_wide_kernel(GridArgs 
     const float offv = half_m - (float)(q0 & ~(kTile - 1));
     const float subu = (float)(p0 & (kTile - 1)), subv = (float)(q0 & (kTile - 1));
     const float2* specg = a.spec + (size_t)grp * 2 * a.n_ang * per_dir;
-    unsigned long long acc[T][T / 2];  // (cell c, cell c + 1) of row r
+    unsigned long long acc[TR][TC / 2];  // (cell c, cell c + 1) of row r
 #pragma unroll
-    for (int r = 0; r < T; ++r)
+    for (int r = 0; r < TR; ++r)
 #pragma unroll
-      for (int c = 0; c < T / 2; ++c) acc[r][c] = 0ull;
+      for (int c = 0; c < TC / 2; ++c) acc[r][c] = 0ull;
     // the quads of run rn -> staging buffer b
     auto stage_run = [&](const Run& rn, int b) {
       const int nq = (rn.jhi >> 2) - (rn.jlo >> 2) + 1;
@@ -907,17 +907,23 @@ __global__ void __launch_bounds__(kWideWarps * 32, 4) grid_wide_kernel(GridArgs 
       const float2* src = specg + (size_t)rn.dir * per_dir + (size_t)(rn.jlo >> 2) * 64;
       for (int i = lane; i < nq * 32; i += 32) cp_async16(dst + i * 4, src + i * 2);
     };
-    // run records travel two runs ahead of their use, staging one run ahead
+    // run records travel two runs ahead of their use, staging one run ahead;
+    // a tile that no sample reaches has an empty item (rb == re, possibly one
+    // past the last run): nothing is read and its cells are written as zeros
     const int rb = it.run_begin, re = it.run_end;
-    Run run1 = a.runs[rb];
-    float2 dir1 = __ldg(&a.dir[run1.dir]);
-    Run run2 = run1;
-    float2 dir2 = dir1;
+    Run run1{0, 1, 0, 1}, run2{0, 1, 0, 1};
+    float2 dir1 = make_float2(0.f, 0.f), dir2 = dir1;
+    if (rb < re) {
+      run1 = a.runs[rb];
+      dir1 = __ldg(&a.dir[run1.dir]);
+      run2 = run1;
+      dir2 = dir1;
+      stage_run(run1, 0);
+    }
     if (rb + 1 < re) {
       run2 = a.runs[rb + 1];
       dir2 = __ldg(&a.dir[run2.dir]);
     }
-    stage_run(run1, 0);
     cp_async_commit();
     for (int r = rb; r < re; ++r) {
       const Run run = run1;
@@ -950,19 +956,23 @@ __global__ void __launch_bounds__(kWideWarps * 32, 4) grid_wide_kernel(GridArgs 
       for (int s = 0; s < n; ++s) {
         const int jr = run.jlo + s - jq0;  // j relative to the first staged quad
         const float val = st[(((jr >> 2) * 16 + pl) * 4 + (jr & 3)) * 2 + cl];
+        float wr[8];
         const float4 wr0 = *reinterpret_cast<const float4*>(rec + s * 16);
-        const float4 wr1 = *reinterpret_cast<const float4*>(rec + s * 16 + 4);
+        wr[0] = wr0.x; wr[1] = wr0.y; wr[2] = wr0.z; wr[3] = wr0.w;
+        if constexpr (TR > 4) {
+          const float4 wr1 = *reinterpret_cast<const float4*>(rec + s * 16 + 4);
+          wr[4] = wr1.x; wr[5] = wr1.y; wr[6] = wr1.z; wr[7] = wr1.w;
+        }
         const float4 wc0 = *reinterpret_cast<const float4*>(rec + s * 16 + 8);
         const float4 wc1 = *reinterpret_cast<const float4*>(rec + s * 16 + 12);
-        const float wr[T] = {wr0.x, wr0.y, wr0.z, wr0.w, wr1.x, wr1.y, wr1.z, wr1.w};
-        const unsigned long long wc[T / 2] = {pack2(wc0.x, wc0.y), pack2(wc0.z, wc0.w),
-                                              pack2(wc1.x, wc1.y), pack2(wc1.z, wc1.w)};
+        const unsigned long long wc[4] = {pack2(wc0.x, wc0.y), pack2(wc0.z, wc0.w),
+                                          pack2(wc1.x, wc1.y), pack2(wc1.z, wc1.w)};
 #pragma unroll
-        for (int rr = 0; rr < T; ++rr) {
+        for (int rr = 0; rr < TR; ++rr) {
           const float x = wr[rr] * val;  // wu * value
           const unsigned long long x2 = pack2(x, x);
 #pragma unroll
-          for (int c = 0; c < T / 2; ++c) ffma2(acc[rr][c], wc[c], x2);  // += wv * (wu * value)
+          for (int c = 0; c < TC / 2; ++c) ffma2(acc[rr][c], wc[c], x2);  // += wv * (wu * value)
         }
       }
       __syncwarp();
@@ -973,9 +983,9 @@ __global__ void __launch_bounds__(kWideWarps * 32, 4) grid_wide_kernel(GridArgs 
       // lane 2p+0 stores cell (r, c), lane 2p+1 cell (r, c+1)
       float2* Hp = a.H + (size_t)(pg0 + min(pl, np - 1)) * MM;
 #pragma unroll
-      for (int r = 0; r < T; ++r) {
+      for (int r = 0; r < TR; ++r) {
 #pragma unroll
-        for (int c2 = 0; c2 < T / 2; ++c2) {
+        for (int c2 = 0; c2 < TC / 2; ++c2) {
           const float2 v = unpack2(acc[r][c2]);  // cells (r, 2 c2), (r, 2 c2 + 1)
           const float give = cl ? v.x : v.y;
           const float got = __shfl_xor_sync(0xffffffffu, give, 1);
@@ -988,14 +998,14 @@ __global__ void __launch_bounds__(kWideWarps * 32, 4) grid_wide_kernel(GridArgs 
     } else {
       // partial sub-tile of a split sub-tile: [cell][lane], summed by split_reduce_wide_kernel
       float* part = reinterpret_cast<float*>(a.scratch) +
-                    ((size_t)grp * a.n_slots + it.slot) * (T * T * 32);
+                    ((size_t)grp * a.n_slots + it.slot) * (TR * TC * 32);
 #pragma unroll
-      for (int r = 0; r < T; ++r)
+      for (int r = 0; r < TR; ++r)
 #pragma unroll
-        for (int c2 = 0; c2 < T / 2; ++c2) {
+        for (int c2 = 0; c2 < TC / 2; ++c2) {
           const float2 v = unpack2(acc[r][c2]);
-          part[(r * T + 2 * c2) * 32 + lane] = v.x;
-          part[(r * T + 2 * c2 + 1) * 32 + lane] = v.y;
+          part[(r * TC + 2 * c2) * 32 + lane] = v.x;
+          part[(r * TC + 2 * c2 + 1) * 32 + lane] = v.y;
         }
     }
     __syncwarp();
@@ -1005,22 +1015,22 @@ __global__ void __launch_bounds__(kWideWarps * 32, 4) grid_wide_kernel(GridArgs 
 // Sums the partial sub-tiles of every split sub-tile in slot order and writes H.
 // Grid: (split sub-tiles, pair groups of 16); 256 threads over (cell, lane).
 __global__ void __launch_bounds__(256) split_reduce_wide_kernel(GridArgs a) {
-  constexpr int T = kTileW;
+  constexpr int TR = kWideRows, TC = kWideCols;
   const int4 sp = a.split_list[blockIdx.x];  // (tile, slot0, nsplit, -)
   const int grp = blockIdx.y;
   const int pg0 = grp * kWidePairs;
   const int np = min(kWidePairs, a.pairs - pg0);
   const int tu = sp.x / a.tiles_v, tv = sp.x - (sp.x / a.tiles_v) * a.tiles_v;
-  const int p0 = tu * T, q0 = tv * T;
+  const int p0 = tu * TR, q0 = tv * TC;
   const float* base = reinterpret_cast<const float*>(a.scratch) +
-                      ((size_t)grp * a.n_slots + sp.y) * (T * T * 32);
+                      ((size_t)grp * a.n_slots + sp.y) * (TR * TC * 32);
   const size_t MM = (size_t)a.M * a.M;
-  for (int i = threadIdx.x; i < T * T * 32; i += blockDim.x) {
+  for (int i = threadIdx.x; i < TR * TC * 32; i += blockDim.x) {
     const int cell = i >> 5, l = i & 31;
     if ((l >> 1) >= np) continue;
     float sum = 0.f;
-    for (int k = 0; k < sp.z; ++k) sum += __ldg(&base[(size_t)k * (T * T * 32) + i]);
-    const int p = p0 + cell / T, q = q0 + cell % T;
+    for (int k = 0; k < sp.z; ++k) sum += __ldg(&base[(size_t)k * (TR * TC * 32) + i]);
+    const int p = p0 + cell / TC, q = q0 + cell % TC;
     if (p == 0 || q == 0) sum = 0.f;
     float* Hf = reinterpret_cast<float*>(a.H + (size_t)(pg0 + (l >> 1)) * MM);
     Hf[((size_t)p * a.M + q) * 2 + (l & 1)] = sum;

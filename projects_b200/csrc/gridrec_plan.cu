@@ -213,7 +213,7 @@ void dev_free(Plan* p, T** ptr) {
 // The gridding work list: for each T x T tile, the runs of samples
 // (direction, j range) whose L x L footprint can reach the tile; tiles whose
 // runs exceed the item cap are split into several items.  T = kTile (32) for
-// grid_kernel, kTileW (8) for grid_wide_kernel.
+// grid_kernel, kWideRows x kWideCols (4 x 8) for grid_wide_kernel.
 struct WorkList {
   std::vector<Item> items;
   std::vector<Run> runs;
@@ -252,8 +252,8 @@ int run_spacing(double du, double dv, int n, double L, int spw, int* steps) {
 void build_work_list(int M, int J, double L, int n_ang, const std::vector<double>& dxy,
                      WorkList* wl, int item_cap = kItemCap, int kind = kListTiles) {
   const bool wide = kind != kListTiles;
-  const int Tu = kind == kListTiles ? kTile : (kind == kListWide ? kTileW : kTcRows);
-  const int Tv = kind == kListTiles ? kTile : (kind == kListWide ? kTileW : kTcCols);
+  const int Tu = kind == kListTiles ? kTile : (kind == kListWide ? kWideRows : kTcRows);
+  const int Tv = kind == kListTiles ? kTile : (kind == kListWide ? kWideCols : kTcCols);
   const int run_max = kind == kListWide ? kRunMaxW : kRunMax;
   const double M2 = M / 2;
   const double L2 = L / 2 + 2e-3;  // box margin covers FP32 position rounding
@@ -417,7 +417,7 @@ int install_work_list_wide(Plan* p, int item_cap) {
     return rc;
   // 64 cells x 32 lanes floats = 512 float4 per slot and group of 16 pairs
   const size_t groups = (size_t)(p->max_pairs + kWidePairs - 1) / kWidePairs;
-  const size_t cells = groups * (size_t)std::max(wl.n_slots, 1) * (kTileW * kTileW * 32 / 4);
+  const size_t cells = groups * (size_t)std::max(wl.n_slots, 1) * (kWideRows * kWideCols * 32 / 4);
   if (cells > p->w_scratch_cells) {
     dev_free(p, &p->d_w_scratch);
     if ((rc = dev_alloc(p, &p->d_w_scratch, cells))) return rc;

@@ -176,7 +176,7 @@ def worklist(n_det, n_ang, theta_deg, sampl=1.0, pswf_c=6.0, wide=False):
 
     runs rows are (direction, jlo, jhi, P): direction = 2*angle + half, samples
     jlo..jhi, processed in steps of samples P apart.  wide=True: the 16-pair
-    kernel's list (8 x 8 tiles, P = 1)."""
+    kernel's list (4 x 8 tiles, P = 1)."""
     p, th = make_params(n_det, n_ang, theta_deg, sampl=sampl, pswf_c=pswf_c)
     ni, nr, tv = C.c_int(), C.c_int(), C.c_int()
     fn = lib().gr_worklist_export_wide if wide else lib().gr_worklist_export
@@ -184,7 +184,9 @@ def worklist(n_det, n_ang, theta_deg, sampl=1.0, pswf_c=6.0, wide=False):
               None, None, 0, 0), "gr_worklist_export")
     items = np.zeros((ni.value, 4), np.int32)
     runs = np.zeros((nr.value, 4), np.int32)
-    splits = np.zeros((tv.value * tv.value, 4), np.int32)
+    # one split record per tile: tiles_v x tiles_v square tiles, or 2 tiles_v rows of
+    # 4 x 8 tiles for the 16-pair list
+    splits = np.zeros(((2 if wide else 1) * tv.value * tv.value, 4), np.int32)
     _check(fn(C.byref(p), C.byref(ni), C.byref(nr), C.byref(tv),
               items.ctypes.data, runs.ctypes.data, splits.ctypes.data,
               ni.value, nr.value), "gr_worklist_export")

@@ -119,27 +119,28 @@ def test_worklist_gather_arbitrary_angles():
 
 
 def _emulate_wide(n, a, theta, sampl=1.0, pswf_c=6.0):
-    """Float64 execution of grid_wide_kernel's scheme over the exported 8 x 8 list:
-    every sample weights all 8 rows and 8 columns of the sub-tile by w(|d|), zero
-    for |d| > L/2, and adds the outer product; compared with the oracle's scatter."""
+    """Float64 execution of grid_wide_kernel's scheme over the exported 4 x 8 list:
+    every sample weights all rows and columns of the sub-tile by w(|d|), zero for
+    |d| > L/2, and adds the outer product; compared with the oracle's scatter."""
     p = O.params(n, a, None, None, 1, pswf_c, sampl)
     sz = O.port_sizes(p)
     rng = np.random.default_rng(n + a)
     spec = O.port_spectra(p, rng.random((a, n)), rng.random((a, n)))
     href = O.port_grid(p, theta, spec)
     items, runs, splits, tiles_v = G.worklist(n, a, theta, sampl=sampl, pswf_c=pswf_c, wide=True)
-    assert np.all(runs[:, 3] == 1) and np.all(runs[:, 2] - runs[:, 1] < 32)
+    assert np.all(runs[:, 3] == 1) and np.all(runs[:, 2] - runs[:, 1] < 16)
     M, L2 = sz.M, sz.L / 2
     ts = 2 * 512 / sz.L
     wtbl, _ = O.port_tables(p)
-    cells = np.arange(8)
+    TR, TC = 4, 8
+    assert tiles_v == M // TC
+    rows, cols = np.arange(TR), np.arange(TC)
     wt = lambda d: np.where(d <= L2, wtbl[np.minimum((d * ts + 0.5).astype(int), 512)], 0.0)
     H = np.zeros((M, M), complex)
-    T = 8
     seen = np.zeros(len(runs), int)
     for tile, rb, re_, slot in items:
         tu, tv = divmod(tile, tiles_v)
-        p0, q0 = tu * T, tv * T
+        p0, q0 = tu * TR, tv * TC
         seen[rb:re_] += 1
         for d, jlo, jhi, _ in runs[rb:re_]:
             nn, h = divmod(d, 2)
@@ -148,8 +149,8 @@ def _emulate_wide(n, a, theta, sampl=1.0, pswf_c=6.0):
             for j in range(jlo, jhi + 1):
                 u = M / 2 + sg * sz.scale * j * np.cos(t) - p0
                 v = M / 2 + sg * sz.scale * j * np.sin(t) - q0
-                H[p0:p0 + T, q0:q0 + T] += np.outer(wt(np.abs(u - cells)),
-                                                    wt(np.abs(v - cells))) * spec[nn, h, j]
+                H[p0:p0 + TR, q0:q0 + TC] += np.outer(wt(np.abs(u - rows)),
+                                                      wt(np.abs(v - cols))) * spec[nn, h, j]
     assert np.all(seen == 1), "every run belongs to exactly one item"
     H[0, :] = 0
     H[:, 0] = 0
@@ -242,3 +243,13 @@ def test_geom_recurrence_needs_no_angle_list():
     p.geom = 3
     assert G.lib().gr_worklist_export(C.byref(p), C.byref(ni), C.byref(nr), C.byref(tv), None,
                                       None, None, 0, 0) == -1
+
+
+def test_wide_worklist_has_empty_items_past_the_runs():
+    """Tiles that no sample reaches (the grid's corners) get empty items whose
+    run_begin can equal the run count: the 16-pair kernel must read no run record
+    for them (the GPU goldens run such a case)."""
+    items, runs, splits, tv = G.worklist(120, 72, ph.angles_deg(72), sampl=1.2, pswf_c=7.0,
+                                         wide=True)
+    empty = items[items[:, 1] == items[:, 2]]
+    assert len(empty) > 0 and (empty[:, 1] == len(runs)).any()
