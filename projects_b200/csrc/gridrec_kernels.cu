@@ -492,7 +492,9 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
   extern __shared__ float2 sm[];
   float2* tw = sm;
   float2* buf = sm + kTwSlots;
-  const int n = blockIdx.x, pair = blockIdx.y;
+  // wide layout: pairs vary fastest, so the 16 pairs sharing each 512-byte span
+  // of the interleaved spectra write it at about the same time
+  const int n = a.wide ? blockIdx.y : blockIdx.x, pair = a.wide ? blockIdx.x : blockIdx.y;
   const int tid = threadIdx.x, nthr = blockDim.x;
   load_twiddles(tw, a.tw, a.pdim);
   const T* r1 = static_cast<const T*>(a.s1) + pair * a.pair_stride + (long)n * a.n_det;
@@ -1597,7 +1599,7 @@ cudaError_t launch_phase(const PhaseArgs& a, cudaStream_t s) {
 template <typename T>
 static cudaError_t launch_spectra_t(const SpectraArgs& a, cudaStream_t s) {
   const int smem = fft_smem_bytes(a.pdim);
-  dim3 grid(a.n_ang, a.pairs);
+  const dim3 grid = a.wide ? dim3(a.pairs, a.n_ang) : dim3(a.n_ang, a.pairs);
 #define GR_SPEC(NT)                                                                  \
   if (a.pdim <= 4096) spectra_kernel<T, 256, NT><<<grid, a.pdim / 16, smem, s>>>(a); \
   else spectra_kernel<T, (NT > 4096 || NT == 0) ? 512 : 256, NT><<<grid, a.pdim / 16, smem, s>>>(a)
