@@ -190,6 +190,42 @@ def algorithmic_bytes_per_pair(n_det, n_ang, pdim, M, M0, in_bytes=4):
     }
 
 
+class gpu_local_cpus:
+    """Runs the enclosed allocations on the host CPUs local to the GPU (its PCI
+    device's local_cpulist in sysfs), so that pinned host buffers, placed on first
+    touch, sit on the GPU's NUMA node: host<->device copies then avoid the
+    inter-socket link.  The previous affinity is restored on exit; where the
+    information is missing nothing changes.  `self.cpus` records what was used."""
+
+    def __init__(self, device):
+        self.device, self.cpus, self._old = device, None, None
+
+    def __enter__(self):
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.device)
+            bdf = "%04x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+            with open(f"/sys/bus/pci/devices/{bdf}/local_cpulist") as f:
+                spec = f.read().strip()
+            cpus = set()
+            for part in spec.split(","):
+                lo, _, hi = part.partition("-")
+                cpus.update(range(int(lo), int(hi or lo) + 1))
+            old = os.sched_getaffinity(0)
+            use = cpus & old
+            if use and use != old:
+                os.sched_setaffinity(0, use)
+                self._old, self.cpus = old, spec
+        except (OSError, ValueError, AttributeError, RuntimeError):
+            pass
+        return self
+
+    def __exit__(self, *exc):
+        if self._old:
+            os.sched_setaffinity(0, self._old)
+        return False
+
+
 def traffic_from_profile(stage, pairs_per_launch, n_det, n_ang):
     """DRAM bytes per launch (ncu read + write per pair, scaled by the pairs of
     one launch) from the committed profile summary of this workload."""
@@ -469,9 +505,10 @@ def run_b200(args, rank, world, local_rank):
     # end to end through the host-buffer entry point
     e2e = None
     if not args.no_e2e:
-        h_in = torch.empty(sinos.shape, dtype=sinos.dtype).pin_memory()
+        with gpu_local_cpus(local_rank) as host_node:
+            h_in = torch.empty(sinos.shape, dtype=sinos.dtype).pin_memory()
+            h_out = torch.empty(outs.shape, dtype=torch.float32).pin_memory()
         h_in.copy_(sinos.cpu())
-        h_out = torch.empty(outs.shape, dtype=torch.float32).pin_memory()
         plan.reconstruct_host(h_in, h_out, centers=centers, stream=int(stream.cuda_stream))
         if world > 1:
             dist.barrier()
@@ -484,7 +521,8 @@ def run_b200(args, rank, world, local_rank):
         e2e = {"value": S * args.e2e_steps * world / te, "unit": UNIT,
                "h2d_bytes_per_step": int(h_in.numel() * h_in.element_size()),
                "d2h_bytes_per_step": int(h_out.numel() * h_out.element_size()),
-               "steps": args.e2e_steps, "path": "gr_reconstruct_host, pinned host buffers"}
+               "steps": args.e2e_steps, "path": "gr_reconstruct_host, pinned host buffers",
+               "host_buffers_on_cpus": host_node.cpus}
         del h_in, h_out
 
     learned = None
@@ -693,10 +731,11 @@ def run_stream(args, rank, world, local_rank):
     e1.record(stream)
     torch.cuda.synchronize()
     kernel_only = 3 * K / (e0.elapsed_time(e1) / 1000.0)
-    h_in = torch.empty(raw.shape, dtype=torch.int16).pin_memory()
+    with gpu_local_cpus(local_rank) as host_node:
+        h_in = torch.empty(raw.shape, dtype=torch.int16).pin_memory()
+        h_out = torch.empty(outs.shape, dtype=torch.float32).pin_memory()
     h_in.copy_(raw.cpu())
     h_flat, h_dark = flat.cpu().numpy(), dark.cpu().numpy()
-    h_out = torch.empty(outs.shape, dtype=torch.float32).pin_memory()
     del raw, outs
     torch.cuda.empty_cache()
     plan.reconstruct_host(h_in, h_out, flat=h_flat, dark=h_dark, dtype=G.DTYPE_U16_RAW,
@@ -728,7 +767,8 @@ def run_stream(args, rank, world, local_rank):
                        "path": "plain gridrec (the learned path falls back to it)"},
             "e2e": {"value": total * world / te, "unit": UNIT, "h2d_bytes_per_step":
                     in_b // (total // K), "d2h_bytes_per_step": out_b // (total // K),
-                    "path": "gr_reconstruct_host, double-buffered, separate H2D/D2H streams"},
+                    "path": "gr_reconstruct_host, double-buffered, separate H2D/D2H streams",
+                    "host_buffers_on_cpus": host_node.cpus},
             "kernel_only_slices_per_s": kernel_only,
             "pcie_gbs": {"h2d": in_b / te / 1e9, "d2h": out_b / te / 1e9},
             "clocks": clk.summary(),
