@@ -592,7 +592,7 @@ def run_uneven(args, rank, world, local_rank):
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     stream = torch.cuda.current_stream()
-    pairs_by_n = {1024: 32, 2048: 16, 4096: 8}
+    pairs_by_n = {1024: 32, 2048: 16, 4096: 16}
     groups = []
     seed0 = rank * 100000
     for n, a, S in UNEVEN_SHAPES:
