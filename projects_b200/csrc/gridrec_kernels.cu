@@ -461,15 +461,16 @@ __device__ __forceinline__ float load_sino<__nv_bfloat16>(const __nv_bfloat16* r
 }
 // Raw uint16 counts with flat/dark: the normalisation of
 // gridrec/GPU/tomo_recon.cpp:1533-1541 (log((flat-dark)/(raw-dark)), 0 when
-// raw <= dark or the ratio is not positive).
+// raw <= dark or the ratio is not positive), as the difference of two fast
+// logarithms (no division; ~1e-6 absolute on line integrals of a few units):
+// the load runs inside the issue-bound spectra FFT kernel.
 template <>
 __device__ __forceinline__ float load_sino<uint16_t>(const uint16_t* row, int k, const float* flat,
                                                      const float* dark) {
   const float d = __ldg(&dark[k]);
   const float v = (float)row[k] - d;
-  if (v <= 0.f) return 0.f;
-  const float r = (__ldg(&flat[k]) - d) / v;
-  return r > 0.f ? logf(r) : 0.f;
+  const float fd = __ldg(&flat[k]) - d;
+  return (v > 0.f && fd > 0.f) ? __logf(fd) - __logf(v) : 0.f;
 }
 // Raw uint16 counts, linear normalisation of the HDF5 path of
 // gridrec/GPU/tomo_recon.cpp:1871-1877 and :2019: 1 - (raw - dark) / (flat - dark)

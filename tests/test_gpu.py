@@ -144,8 +144,13 @@ def test_raw_uint16_fused_normalisation():
         plan.reconstruct_batch(_dev(raws.view(np.int16)), outs, flat=_dev(flat), dark=_dev(dark),
                                dtype=G.DTYPE_U16_RAW)
         got = outs.cpu().numpy()
+        # the same slices normalised on the host in float64 and passed as f32
+        plan.reconstruct_batch(_dev(norm), outs)
+        host = outs.cpu().numpy()
     assert ph.rel_l2(got[0], o1[:, :plan.M0]) < TOL
     assert ph.rel_l2(got[1], o2[:, :plan.M0]) < TOL
+    # the fused normalisation (fast logarithms) against the host one
+    assert ph.rel_l2(got, host) < 2e-5
 
 
 def test_raw_uint16_linear_normalisation_bit_exact():
