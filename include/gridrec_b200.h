@@ -297,6 +297,25 @@ int gr_crop_center(const float* recon, long recon_stride, long recon_slice_elems
                    long out_stride, long out_slice_elems, int n_slices, int n, int offset,
                    int radius, void* stream);
 
+/* Output thresholds <- the 8-bit slice writer of tomo_recon.cpp:2282-2311: lohi[0] /
+ * lohi[1] (device, 2 floats) = min / max over every pixel of the n_slices images
+ * (rows x cols, strides in floats; NaN skipped), then hi capped at upper_clamp and
+ * lo raised to lower_clamp (RECON_THRESHOLD_UPPER/LOWER_VALUE).  workspace: device,
+ * gr_threshold_workspace_bytes() bytes. */
+size_t gr_threshold_workspace_bytes(void);
+int gr_threshold_range(const float* images, int n_slices, int rows, int cols, long row_stride,
+                       long slice_stride, float lower_clamp, float upper_clamp, float* lohi,
+                       void* workspace, void* stream);
+/* 8-bit slices <- tomo_recon.cpp:2338-2361: 0 below lo, 255 above hi, else
+ * (unsigned char)(255 * (p - lo) / (hi - lo)) in float; with radius > 0 the
+ * writer's cropped copy: pixels with (x - cols/2)^2 + (y - rows/2)^2 > radius^2 set
+ * to 0 (this writer keeps the boundary circle, gr_crop_center's float crop does
+ * not).  lohi from gr_threshold_range (device).  Bit-exact with the reference's
+ * float arithmetic; a NaN result gives 0. */
+int gr_to_u8(const float* images, int n_slices, int rows, int cols, long row_stride,
+             long slice_stride, const float* lohi, int radius, unsigned char* out,
+             long out_row_stride, long out_slice_stride, void* stream);
+
 /* Histogram entropy <- entropy()  find_shift/src/main/find_shift.cpp:2078-2115.
  * For each of n_groups groups of `group` image windows (rows x cols, row_stride;
  * images image_stride apart, groups group_stride apart, all in floats): nbins + 1

@@ -425,6 +425,49 @@ void orc_crop(const float* rec, long rec_stride, float* out, int n, int offset, 
     }
 }
 
+/* Output thresholds of the reference's 8-bit (BMP/TIFF) slice writer
+ * (gridrec/GPU/tomo_recon.cpp:2282-2311): lo / hi start at 1e10 / -1e10 and take the
+ * min / max of every pixel of the slices written together (NaN compares false and
+ * is skipped); hi is then capped by RECON_THRESHOLD_UPPER_VALUE and lo raised to
+ * RECON_THRESHOLD_LOWER_VALUE. */
+void orc_minmax(const float* img, long n, float lower_clamp, float upper_clamp, float* lo,
+                float* hi) {
+  float up = -1e10f, low = 1e10f;
+  for (long i = 0; i < n; ++i) {
+    if (up < img[i]) up = img[i];
+    if (low > img[i]) low = img[i];
+  }
+  if (up > upper_clamp) up = upper_clamp;
+  if (low < lower_clamp) low = lower_clamp;
+  *lo = low;
+  *hi = up;
+}
+
+/* Its 8-bit conversion (tomo_recon.cpp:2338-2361): 0 below lo, 255 above hi, else
+ * (unsigned char)(255 * (p - lo) / (hi - lo)) in float, left to right; with
+ * radius > 0 the cropped copy keeps pixels with (x - w/2)^2 + (y - h/2)^2 <= radius^2
+ * (x the column, y the row, integer halves) and zeroes the rest.  A value the
+ * reference would convert from NaN (a NaN pixel, or hi == lo) gives 0 here. */
+void orc_to_u8(const float* img, int rows, int cols, long row_stride, float lo, float hi,
+               int radius, unsigned char* out) {
+  for (int y = 0; y < rows; ++y)
+    for (int x = 0; x < cols; ++x) {
+      const float p = img[(long)y * row_stride + x];
+      unsigned char v;
+      if (p < lo) v = 0;
+      else if (p > hi) v = 255;
+      else {
+        const float q = 255.0f * (p - lo) / (hi - lo);
+        v = (q == q) ? (unsigned char)q : 0;
+      }
+      if (radius > 0) {
+        const long dx = x - cols / 2, dy = y - rows / 2;
+        if (dx * dx + dy * dy > (long)radius * radius) v = 0;
+      }
+      out[(long)y * cols + x] = v;
+    }
+}
+
 /* Histogram entropy of find_shift (find_shift/src/main/find_shift.cpp:2078-2115):
  * num_hist_bin + 1 bins, bin = (int)((x - min) / inv) computed in float with
  * inv = (max - min) / num_hist_bin (truncation toward zero; bins outside

@@ -40,6 +40,10 @@ int orc_gridrec_pair(const orc_params* p, const double* theta_deg, const double*
 void orc_ring_removal(double* data, int n_det, int n_ang, double ring_coeff, int iterations);
 void orc_shift_pad(const float* in, float* out, int n_det, int n_ang, float xoffset, int out_width);
 void orc_crop(const float* rec, long rec_stride, float* out, int n, int offset, int radius);
+void orc_minmax(const float* img, long n, float lower_clamp, float upper_clamp, float* lo,
+                float* hi);
+void orc_to_u8(const float* img, int rows, int cols, long row_stride, float lo, float hi,
+               int radius, unsigned char* out);
 double orc_entropy(const float* data, long n, float vmin, float vmax, int num_hist_bin);
 int orc_optimized_fbp(int n_det, int n_ang, const float* theta_deg, const float* sino,
                       double* recon);

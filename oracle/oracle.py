@@ -62,6 +62,12 @@ def port_lib():
         lib.orc_shift_pad.restype = None
         lib.orc_crop.argtypes = [_fp, C.c_long, _fp, C.c_int, C.c_int, C.c_int]
         lib.orc_crop.restype = None
+        lib.orc_minmax.argtypes = [_fp, C.c_long, C.c_float, C.c_float, C.POINTER(C.c_float),
+                                   C.POINTER(C.c_float)]
+        lib.orc_minmax.restype = None
+        lib.orc_to_u8.argtypes = [_fp, C.c_int, C.c_int, C.c_long, C.c_float, C.c_float, C.c_int,
+                                  C.c_void_p]
+        lib.orc_to_u8.restype = None
         lib.orc_entropy.argtypes = [_fp, C.c_long, C.c_float, C.c_float, C.c_int]
         lib.orc_xcorr_score.argtypes = [_dp, _dp] + [C.c_int] * 6 + [C.c_double, C.c_double]
         lib.orc_xcorr_score.restype = C.c_double
@@ -158,6 +164,21 @@ def port_shift_pad(sino, xoffset, out_width=None):
     port_lib().orc_shift_pad(np.ascontiguousarray(sino, np.float32), out, n_det, n_ang,
                              float(xoffset), w)
     return out
+
+
+def port_to_u8(images, lower_clamp=-1e30, upper_clamp=1e30, radius=0):
+    """8-bit slices of the reference's BMP/TIFF writer: thresholds from all the
+    given slices (S, rows, cols), then the conversion (and crop) per slice."""
+    imgs = np.ascontiguousarray(images, np.float32)
+    lo, hi = C.c_float(), C.c_float()
+    port_lib().orc_minmax(imgs, imgs.size, float(lower_clamp), float(upper_clamp), C.byref(lo),
+                          C.byref(hi))
+    S, rows, cols = imgs.shape
+    out = np.zeros((S, rows, cols), np.uint8)
+    for s in range(S):
+        port_lib().orc_to_u8(imgs[s], rows, cols, cols, lo.value, hi.value, int(radius),
+                             out[s].ctypes.data)
+    return out, (lo.value, hi.value)
 
 
 def port_crop(rec, n, offset, radius=0):

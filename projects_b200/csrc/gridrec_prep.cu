@@ -303,6 +303,86 @@ __global__ void crop_kernel(const float* rec, long rec_stride, long rec_slice, f
 }
 
 // ---------------------------------------------------------------------------
+// Output thresholds and 8-bit slices of the reference's BMP/TIFF writer
+// (gridrec/GPU/tomo_recon.cpp:2282-2361).  lo / hi: min / max over every pixel
+// of the given slices (start 1e10 / -1e10; NaN compares false and is skipped),
+// then capped by the configured upper / raised to the configured lower value.
+// Min and max do not depend on the order of evaluation, so the block partials
+// give the reference's values exactly.
+constexpr int kMinMaxBlocks = 1024;
+
+__global__ void __launch_bounds__(kPrepThreads) minmax_partial_kernel(
+    const float* img, int n_slices, int rows, int cols, long row_stride, long slice_stride,
+    float2* part) {
+  float lo = 1e10f, hi = -1e10f;
+  const long per_slice = (long)rows * cols;
+  const long total = per_slice * n_slices;
+  for (long i = (long)blockIdx.x * blockDim.x + threadIdx.x; i < total;
+       i += (long)gridDim.x * blockDim.x) {
+    const long s = i / per_slice, r = (i - s * per_slice) / cols;
+    const long c = i - s * per_slice - r * cols;
+    const float p = img[s * slice_stride + r * row_stride + c];
+    if (hi < p) hi = p;
+    if (lo > p) lo = p;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    const float l2 = __shfl_xor_sync(0xffffffffu, lo, o), h2 = __shfl_xor_sync(0xffffffffu, hi, o);
+    lo = fminf(lo, l2);
+    hi = fmaxf(hi, h2);
+  }
+  __shared__ float2 s_part[kPrepThreads / 32];
+  if ((threadIdx.x & 31) == 0) s_part[threadIdx.x >> 5] = make_float2(lo, hi);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int w = 1; w < kPrepThreads / 32; ++w) {
+      lo = fminf(lo, s_part[w].x);
+      hi = fmaxf(hi, s_part[w].y);
+    }
+    part[blockIdx.x] = make_float2(lo, hi);
+  }
+}
+
+__global__ void minmax_final_kernel(const float2* part, int n, float lower_clamp, float upper_clamp,
+                                    float* lohi) {
+  float lo = 1e10f, hi = -1e10f;
+  for (int i = 0; i < n; ++i) {
+    lo = fminf(lo, part[i].x);
+    hi = fmaxf(hi, part[i].y);
+  }
+  if (hi > upper_clamp) hi = upper_clamp;
+  if (lo < lower_clamp) lo = lower_clamp;
+  lohi[0] = lo;
+  lohi[1] = hi;
+}
+
+// 0 below lo, 255 above hi, else (unsigned char)(255 * (p - lo) / (hi - lo)) in
+// float left to right (a NaN value, which the reference's cast leaves undefined,
+// gives 0); with radius > 0, pixels with (x - cols/2)^2 + (y - rows/2)^2 > radius^2
+// are 0 (the writer's cropped copy keeps the boundary, unlike crop_kernel).
+__global__ void to_u8_kernel(const float* img, int cols, int rows, long row_stride,
+                             long slice_stride, const float* lohi, int radius, unsigned char* out,
+                             long out_row_stride, long out_slice_stride) {
+  const int y = blockIdx.x, s = blockIdx.y;
+  const float lo = lohi[0], hi = lohi[1];
+  const float* src = img + (size_t)s * slice_stride + (size_t)y * row_stride;
+  unsigned char* dst = out + (size_t)s * out_slice_stride + (size_t)y * out_row_stride;
+  const long long r2 = (long long)radius * radius;
+  const long long dy = (long long)(y - rows / 2) * (y - rows / 2);
+  for (int x = threadIdx.x; x < cols; x += blockDim.x) {
+    const float p = src[x];
+    unsigned char v;
+    if (p < lo) v = 0;
+    else if (p > hi) v = 255;
+    else {
+      const float q = __fdiv_rn(__fmul_rn(255.f, __fsub_rn(p, lo)), __fsub_rn(hi, lo));
+      v = (q == q) ? (unsigned char)q : 0;
+    }
+    if (radius > 0 && (long long)(x - cols / 2) * (x - cols / 2) + dy > r2) v = 0;
+    dst[x] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
 // Histogram entropy of a group of image windows: nbins + 1 bins of width
 // inv = (vmax - vmin) / nbins, bin = (int)((x - vmin) / inv) in float
 // (truncation toward zero, values outside [0, nbins] ignored), entropy =
@@ -641,6 +721,41 @@ int gr_crop_center(const float* recon, long recon_stride, long recon_slice_elems
   crop_kernel<<<dim3(n, n_slices), kPrepThreads, 0, (cudaStream_t)stream>>>(
       recon, recon_stride, recon_slice_elems, out, out_stride, out_slice_elems, n, offset, radius);
   return check_launch("crop");
+}
+
+size_t gr_threshold_workspace_bytes(void) { return kMinMaxBlocks * sizeof(float2); }
+
+int gr_threshold_range(const float* images, int n_slices, int rows, int cols, long row_stride,
+                       long slice_stride, float lower_clamp, float upper_clamp, float* lohi,
+                       void* workspace, void* stream) {
+  if (!images || !lohi || !workspace) return fail(GR_ERR_ARG, "threshold: null pointer");
+  if (n_slices < 1 || rows < 1 || cols < 1 || row_stride < cols ||
+      (n_slices > 1 && slice_stride < (long)rows * row_stride))
+    return fail(GR_ERR_ARG, "threshold: bad sizes (rows=%d cols=%d row_stride=%ld)", rows, cols,
+                row_stride);
+  const long total = (long)n_slices * rows * cols;
+  const int blocks = (int)std::min<long>(kMinMaxBlocks, (total + kPrepThreads - 1) / kPrepThreads);
+  cudaStream_t st = (cudaStream_t)stream;
+  float2* part = static_cast<float2*>(workspace);
+  minmax_partial_kernel<<<blocks, kPrepThreads, 0, st>>>(images, n_slices, rows, cols, row_stride,
+                                                         slice_stride, part);
+  int rc = check_launch("threshold: min/max");
+  if (rc) return rc;
+  minmax_final_kernel<<<1, 1, 0, st>>>(part, blocks, lower_clamp, upper_clamp, lohi);
+  return check_launch("threshold: final");
+}
+
+int gr_to_u8(const float* images, int n_slices, int rows, int cols, long row_stride,
+             long slice_stride, const float* lohi, int radius, unsigned char* out,
+             long out_row_stride, long out_slice_stride, void* stream) {
+  if (!images || !lohi || !out) return fail(GR_ERR_ARG, "to_u8: null pointer");
+  if (n_slices < 1 || n_slices > 65535 || rows < 1 || cols < 1 || row_stride < cols ||
+      out_row_stride < cols || radius < 0)
+    return fail(GR_ERR_ARG, "to_u8: bad sizes (rows=%d cols=%d)", rows, cols);
+  to_u8_kernel<<<dim3(rows, n_slices), kPrepThreads, 0, (cudaStream_t)stream>>>(
+      images, cols, rows, row_stride, slice_stride, lohi, radius, out, out_row_stride,
+      out_slice_stride);
+  return check_launch("to_u8");
 }
 
 size_t gr_entropy_workspace_bytes(int n_groups, int nbins) {

@@ -35,6 +35,7 @@ EXPORTS = ("gr_params_default", "gr_filter_code", "gr_plan_create", "gr_plan_des
            "gr_entropy", "gr_reconstruct_padded", "gr_center_search", "gr_graph_create",
            "gr_graph_launch", "gr_graph_launch_count", "gr_graph_destroy", "gr_plan_autotune",
            "gr_plan_tuning", "gr_xcorr_scores", "gr_fbp_create", "gr_fbp_reconstruct",
+           "gr_threshold_workspace_bytes", "gr_threshold_range", "gr_to_u8",
            "gr_fbp_destroy", "gr_cnn_param_count", "gr_cnn_workspace_bytes",
            "gr_cnn_forward_workspace_bytes", "gr_cnn_forward",
            "gr_cnn_backward", "gr_cnn_adam")
@@ -110,6 +111,9 @@ def lib():
         L.gr_ring_removal.argtypes = [vp, i_, i_, i_, f_, i_, vp, vp]
         L.gr_shift_pad.argtypes = [vp, vp, i_, i_, i_, vp, i_, vp]
         L.gr_crop_center.argtypes = [vp, l_, l_, vp, l_, l_, i_, i_, i_, i_, vp]
+        L.gr_threshold_workspace_bytes.restype = C.c_size_t
+        L.gr_threshold_range.argtypes = [vp, i_, i_, i_, l_, l_, f_, f_, vp, vp, vp]
+        L.gr_to_u8.argtypes = [vp, i_, i_, i_, l_, l_, vp, i_, vp, l_, l_, vp]
         L.gr_entropy_workspace_bytes.argtypes = [i_, i_]
         L.gr_entropy_workspace_bytes.restype = C.c_size_t
         L.gr_entropy.argtypes = [vp, i_, i_, i_, i_, l_, l_, l_, f_, f_, i_, vp, vp, vp]
@@ -525,6 +529,38 @@ def crop_center(recs, n, offset, radius=0, stream=None):
         raise ValueError("crop window exceeds the image rows")
     _check(lib().gr_crop_center(_ptr(recs), stride, rows * stride, _ptr(out), n, n * n, S, n,
                                 offset, int(radius), _stream_ptr(stream)), "gr_crop_center")
+    return out
+
+
+def threshold_range(images, lower_clamp=-1e30, upper_clamp=1e30, stream=None):
+    """(lo, hi) of the reference's 8-bit slice writer for images (S, rows, cols),
+    a CUDA float32 tensor or a view with unit column stride, as a (2,) float32 CUDA
+    tensor (tomo_recon.cpp:2282-2311)."""
+    import torch
+    S, rows, cols = images.shape
+    if images.stride(2) != 1:
+        raise ValueError("images need unit column stride")
+    ws = torch.empty(lib().gr_threshold_workspace_bytes(), dtype=torch.uint8, device=images.device)
+    lohi = torch.empty(2, dtype=torch.float32, device=images.device)
+    _check(lib().gr_threshold_range(_ptr(images), S, rows, cols, images.stride(1),
+                                    images.stride(0), float(lower_clamp), float(upper_clamp),
+                                    _ptr(lohi), _ptr(ws), _stream_ptr(stream)),
+           "gr_threshold_range")
+    return lohi
+
+
+def to_u8(images, lohi, radius=0, out=None, stream=None):
+    """8-bit slices (S, rows, cols) uint8 of the reference's BMP/TIFF writer
+    (tomo_recon.cpp:2338-2361), optionally its cropped copy (radius > 0)."""
+    import torch
+    S, rows, cols = images.shape
+    if images.stride(2) != 1:
+        raise ValueError("images need unit column stride")
+    if out is None:
+        out = torch.empty((S, rows, cols), dtype=torch.uint8, device=images.device)
+    _check(lib().gr_to_u8(_ptr(images), S, rows, cols, images.stride(1), images.stride(0),
+                          _ptr(lohi), int(radius), _ptr(out), out.stride(1), out.stride(0),
+                          _stream_ptr(stream)), "gr_to_u8")
     return out
 
 

@@ -227,3 +227,21 @@ def test_fbp_comparator_against_reference_and_oracle():
     for k in range(3):
         assert ph.rel_l2(out[k], O.port_optimized_fbp(sinos[k], th)) < 1e-5
     f.close()
+
+
+@pytest.mark.parametrize("clamps,radius", [((-1e30, 1e30), 0), ((-0.2, 0.9), 0), ((-0.5, 2.0), 37)])
+def test_threshold_u8_bit_exact(clamps, radius):
+    """8-bit slices of the reference's BMP/TIFF writer (thresholds from all slices,
+    clamped; the cropped copy) against the oracle, byte for byte; NaN included."""
+    rng = np.random.default_rng(5)
+    imgs = rng.normal(0.3, 0.5, size=(3, 101, 96)).astype(np.float32)
+    imgs[1, 5, 7] = np.nan
+    imgs[2, 50, 50] = 7.0
+    ref, (lo, hi) = O.port_to_u8(imgs, *clamps, radius=radius)
+    d = torch.zeros((3, 101, 128), device="cuda")
+    d[:, :, :96] = torch.as_tensor(imgs).cuda()
+    view = d[:, :, :96]
+    lohi = G.threshold_range(view, *clamps)
+    got = G.to_u8(view, lohi, radius=radius).cpu().numpy()
+    assert tuple(lohi.cpu().numpy().tolist()) == (lo, hi)
+    assert np.array_equal(got, ref)
