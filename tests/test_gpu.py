@@ -539,3 +539,60 @@ def test_wide_kernel_split_subtiles_2048x1500():
             d = (torch.linalg.vector_norm(outs[mode][i] - outs[-1][i]) /
                  torch.linalg.vector_norm(outs[-1][i]))
             assert float(d) < (TENSOR_TOL if mode == 2 else KERNEL_TOL), (mode, i)
+
+
+@pytest.mark.parametrize("dtype", ["float16", "bfloat16", "u16raw"])
+def test_wide_kernel_input_types(dtype):
+    """Reduced-precision and raw-count inputs through the 16-pair kernel (a chunk of
+    16 pairs): the same images as the tile kernel from the same input, within the
+    cross-kernel bound."""
+    n, a = 96, 64
+    th = ph.angles_deg(a)
+    S = 32
+    if dtype == "u16raw":
+        p = [ph.line_integrals(ph.random_ellipses(s), n, th, 48.0) / (n / 2) for s in range(S)]
+        raws, flats, darks = zip(*[ph.raw_counts(p[s], seed=s) for s in range(S)])
+        src = _dev(np.stack(raws).view(np.int16))
+        kw = dict(flat=_dev(np.stack(flats)), dark=_dev(np.stack(darks)), dtype=G.DTYPE_U16_RAW)
+    else:
+        sinos = np.stack([ph.random_ellipse_sinogram(s, n, a, center=48.0)[0] for s in range(S)])
+        src = _dev(sinos).to(getattr(torch, dtype))
+        kw = {}
+    outs = {}
+    for mode in (0, -1):
+        with G.Plan(n, a, th, center=48.0, filter=G.FILTER_HANN, max_pairs=16,
+                    wide_grid=mode) as plan:
+            o = torch.zeros((S, plan.M0, 128), device="cuda")
+            plan.reconstruct_batch(src, o, **kw)
+            torch.cuda.synchronize()
+            plan.device_status()
+            outs[mode] = o.cpu().numpy()[:, :, :plan.M0]
+    for i in range(S):
+        assert ph.rel_l2(outs[0][i], outs[-1][i]) < KERNEL_TOL, i
+
+
+def test_wide_kernel_host_streaming_and_graph():
+    """gr_reconstruct_host (pinned and pageable buffers) and a captured graph on a
+    plan whose chunks use the 16-pair kernel: bitwise equal to the device batch."""
+    n, a = 64, 48
+    th = ph.angles_deg(a)
+    S = 70  # two chunks of 16 pairs, then 3 pairs (tile kernel)
+    sinos = np.stack([ph.random_ellipse_sinogram(s, n, a, center=32.0)[0] for s in range(S)])
+    with G.Plan(n, a, th, center=32.0, max_pairs=16) as plan:
+        assert plan.grid_kernel(16) == "wide" and plan.grid_kernel(3) == "tiles"
+        dev_out = torch.zeros((S, plan.M0, n), device="cuda")
+        plan.reconstruct_batch(_dev(sinos), dev_out)
+        host_out = np.zeros((S, plan.M0, n), np.float32)
+        plan.reconstruct_host(sinos, host_out)
+        pinned_out = torch.zeros((S, plan.M0, n)).pin_memory()
+        plan.reconstruct_host(torch.from_numpy(sinos).pin_memory(), pinned_out)
+        d_in = _dev(sinos)
+        g_out = torch.zeros_like(dev_out)
+        g = plan.capture_batch(d_in, g_out)
+        g.launch()
+        torch.cuda.synchronize()
+        g.close()
+    d = dev_out.cpu().numpy()
+    np.testing.assert_array_equal(host_out, d)
+    np.testing.assert_array_equal(pinned_out.numpy(), d)
+    np.testing.assert_array_equal(g_out.cpu().numpy(), d)
