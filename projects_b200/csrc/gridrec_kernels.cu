@@ -1558,6 +1558,7 @@ void add_fft_kernels(std::vector<const void*>& f) {
   f.push_back((const void*)cols_kernel<512, NT>);
   f.push_back((const void*)cols_tma_kernel<256, NT>);
   f.push_back((const void*)cols_tma_kernel<512, NT>);
+  f.push_back((const void*)cols_tma_kernel<1024, NT>);
   f.push_back((const void*)rows_kernel<256, NT>);
   f.push_back((const void*)rows_kernel<512, NT>);
   f.push_back((const void*)fbp_filter_kernel<256, NT>);
@@ -1743,17 +1744,21 @@ cudaError_t launch_cols(const ColArgs& a, cudaStream_t s) {
       dim3 grid(a.M / G, a.pairs);
 #define GR_COLT(NT)                                                                      \
   if (threads <= 256) cols_tma_kernel<256, NT><<<grid, threads, smem, s>>>(map, a, G, box_rows); \
-  else cols_tma_kernel<512, NT><<<grid, threads, smem, s>>>(map, a, G, box_rows)
+  else if (threads <= 512) cols_tma_kernel<512, NT><<<grid, threads, smem, s>>>(map, a, G, box_rows); \
+  else cols_tma_kernel<1024, NT><<<grid, threads, smem, s>>>(map, a, G, box_rows)
       GR_DISPATCH_N(a.M, GR_COLT)
 #undef GR_COLT
       return cudaGetLastError();
     }
   }
-  const int smem = (kTwSlots + G * (a.M + 16 / G)) * (int)sizeof(float2);
-  dim3 grid(a.M / G, a.pairs);
-#define GR_COL(NT)                                                                       \
-  if (G * (a.M / 16) <= 256) cols_kernel<256, NT><<<grid, G * (a.M / 16), smem, s>>>(a, G); \
-  else cols_kernel<512, NT><<<grid, G * (a.M / 16), smem, s>>>(a, G)
+  // the plain kernel takes at most 512 threads: narrower column groups if needed
+  int Gp = G;
+  while (Gp > 1 && Gp * (a.M / 16) > 512) Gp >>= 1;
+  const int smem = (kTwSlots + Gp * (a.M + 16 / Gp)) * (int)sizeof(float2);
+  dim3 grid(a.M / Gp, a.pairs);
+#define GR_COL(NT)                                                                         \
+  if (Gp * (a.M / 16) <= 256) cols_kernel<256, NT><<<grid, Gp * (a.M / 16), smem, s>>>(a, Gp); \
+  else cols_kernel<512, NT><<<grid, Gp * (a.M / 16), smem, s>>>(a, Gp)
   GR_DISPATCH_N(a.M, GR_COL)
 #undef GR_COL
   return cudaGetLastError();

@@ -1086,7 +1086,8 @@ int gr_plan_autotune(gr_plan* p, void* stream) {
   float best_c = 1e30f;
   for (int G = 1; G <= 8 && rc == GR_OK; G *= 2) {
     const int threads = G * (p->M / 16);
-    if (threads < 32 || threads > 512 || p->M % G) continue;
+    // up to 1024 threads (the TMA-fed kernel); the plain one stops at 512
+    if (threads < 32 || threads > 1024 || p->M % G) continue;
     ColArgs ca{p->d_H, p->d_tw_m, p->M, pairs, p->d_err, G};
     const float t = time_ms([&] { launch_cols(ca, st); });
     if (t < best_c) {
