@@ -253,3 +253,17 @@ def test_wide_worklist_has_empty_items_past_the_runs():
                                          wide=True)
     empty = items[items[:, 1] == items[:, 2]]
     assert len(empty) > 0 and (empty[:, 1] == len(runs)).any()
+
+
+@pytest.mark.parametrize("seed", [11, 12, 13])
+def test_wide_worklist_random_geometries(seed):
+    """Seeded random geometries (width, angle count, irregular angle list,
+    oversampling, PSWF parameter): the 16-pair kernel's 4 x 8 work list covers
+    exactly the oracle's scatter, in float64."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(40, 110))
+    a = int(rng.integers(12, 40))
+    th = np.sort(rng.uniform(-20.0, 200.0, a)).astype(np.float32)
+    sampl = float(rng.choice([1.0, 1.2, 1.5]))
+    C_ = float(rng.choice([4.0, 5.0, 6.0, 7.0]))
+    assert _emulate_wide(n, a, th, sampl, C_) < 1e-14
