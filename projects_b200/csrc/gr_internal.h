@@ -110,10 +110,13 @@ struct GridArgs {
   const Run* runs;
   const int4* split_list;  // per split tile: (tile, slot0, nsplit, 0)
   int n_split_tiles;
-  const float2* dir;     // per direction (scale*dx, scale*dy)
+  // Tap geometry is FP64, as the FP64 restatement forms it: sample j of
+  // direction d sits at u = j * dir[d] + (M/2 - tile origin), and its tap in
+  // cell c weighs wtbl[(int)(|u - c| * tblspcg + 0.5)] where |u - c| <= L2.
+  const double2* dir;    // per direction (scale*dx, scale*dy)
   const float* wtbl;     // ltbl + 1
   int n_items, pairs, n_ang, J, M, tiles_v, n_slots, ltbl;
-  float L2, tblspcg;
+  double L2, tblspcg;    // L/2, 2 ltbl / L
   const unsigned* codes = nullptr;  // grid_tc_kernel: flat (direction << 13 | j) per sample
   int* err = nullptr;               // device error word for bounded-wait timeouts
 };

@@ -589,37 +589,23 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
 // with P * max(|du|,|dv|) > L, so no two of them share a valid tap (taps lie
 // within L/2 of their sample; P per run comes from the host), so
 // plain read-modify-write needs no atomics, and the summation order is fixed,
-// so the result is bitwise reproducible.  Float/int conversions use exact
-// magic-number rounding on the FP32 pipe.  Tiles split over several items
+// so the result is bitwise reproducible.  Tap positions and table indices are
+// FP64, as the FP64 restatement of the algorithm forms them: FP32 positions put some taps on
+// the other side of a table-bin boundary (a position error of 2^-12 at
+// |u| ~ 2048 moves the index when |u - c| * tblspcg lies that close to a
+// half-integer), which alone costs ~5e-4 relative L2.  Tiles split over several items
 // leave partial tiles in scratch, summed in slot order by split_reduce_kernel.
 
 constexpr int kTileStride = kTile + 1;
 constexpr int kGridWarps = 4;
 constexpr int kGridPairs = 2;   // slice pairs gridded together from one set of weights
-constexpr float kMagic = 12582912.0f;  // 1.5 * 2^23: x + kMagic rounds x to an integer
-constexpr int kMagicBits = 0x4B400000;
-
-// ceil(x) as float and int, exact for |x| < 2^22.
-__device__ __forceinline__ float ceil_exact(float x, int& xi) {
-  const float y = x + kMagic;
-  float r = y - kMagic;
-  int i = __float_as_int(y) - kMagicBits;
-  if (r < x) {
-    r += 1.f;
-    i += 1;
-  }
-  xi = i;
-  return r;
-}
 
 // (int)(d * ts + 0.5) for d >= 0 -- the nearest-neighbour table index of
-// gridrec.h:53 -- exact for arguments below 2^22.
-__device__ __forceinline__ int table_index(float d, float ts) {
-  const float y = fmaf(d, ts, 0.5f);
-  const float r = (y + kMagic) - kMagic;
-  int i = __float_as_int(y + kMagic) - kMagicBits;
-  if (r > y) i -= 1;
-  return i;
+// gridrec.h:53 -- in FP64 with the product and the sum rounded separately, as
+// the FP64 restatement forms them; capped so that far taps stay in int range
+// (callers clamp to the table length and zero taps beyond L/2).
+__device__ __forceinline__ int table_index64(double d, double ts) {
+  return (int)fmin(__dadd_rn(__dmul_rn(d, ts), 0.5), 2.0e9);
 }
 
 template <int NT>
@@ -638,10 +624,8 @@ __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
   const int t = lane - slot_k * NT;      // footprint row of this lane
   const int lane0 = slot_k * NT;         // first lane of this sample
   const bool lane_used = slot_k < SPW;
-  const float ft = (float)t, fslot = (float)slot_k;
-  const float L2 = a.L2, ts = a.tblspcg;
+  const double L2d = a.L2, tsd = a.tblspcg;
   const int ltbl = a.ltbl;
-  const float half_m = (float)(a.M / 2);
   const int groups = (a.pairs + kGridPairs - 1) / kGridPairs;
   const unsigned total = (unsigned)a.n_items * (unsigned)groups;
   const size_t spec_pair = (size_t)a.n_ang * 2 * a.J;
@@ -659,7 +643,7 @@ __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
     const int p0 = tu * kTile, q0 = tv * kTile;
     for (int i = lane; i < kTile * kTileStride; i += 32) tile[i] = make_float4(0.f, 0.f, 0.f, 0.f);
     __syncwarp();
-    const float offu = half_m - (float)p0, offv = half_m - (float)q0;
+    const double offu = (double)(a.M / 2 - p0), offv = (double)(a.M / 2 - q0);
     const float2* specA = a.spec + (size_t)pA * spec_pair;
     const float2* specB = hasB ? specA + spec_pair : specA;
     // Software pipeline over runs: the samples of run r+1 are loaded into
@@ -669,7 +653,7 @@ __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
     // dependent global load sits at the start of a run.
     float2 nA0 = make_float2(0.f, 0.f), nA1 = nA0, nB0 = nA0, nB1 = nA0;
     Run nrun{0, 0, -1, 1};
-    float2 ndir = make_float2(0.f, 0.f);
+    double2 ndir = make_double2(0.0, 0.0);
     auto prefetch = [&](int rr) {
       if (rr >= it.run_end) return;
       nrun = a.runs[rr];
@@ -688,7 +672,7 @@ __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
     prefetch(it.run_begin);
     for (int r = it.run_begin; r < it.run_end; ++r) {
       const Run run = nrun;
-      const float2 d = ndir;
+      const double2 d = ndir;
       stage[lane] = make_float4(nA0.x, nA0.y, nB0.x, nB0.y);
       stage[32 + lane] = make_float4(nA1.x, nA1.y, nB1.x, nB1.y);
       __syncwarp();
@@ -696,26 +680,23 @@ __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
       // run.P: samples P apart never share a valid tap (P * max(|du|,|dv|)
       // > L with margin), chosen on the host to minimise the steps
       const int P = run.P;
-      const float fP = (float)P;
       for (int blk = run.jlo; blk <= run.jhi; blk += SPW * P) {
-        const float fblk = (float)blk;
         for (int ph = 0; ph < P && blk + ph <= run.jhi; ++ph) {
           const int j = blk + ph + P * slot_k;
           const bool active = lane_used && j <= run.jhi;
-          const float fj = fmaf(fP, fslot, fblk + (float)ph);
-          const float u = fmaf(fj, d.x, offu);
-          const float v = fmaf(fj, d.y, offv);
-          int iu0, iv0;
-          const float fu0 = ceil_exact(u - L2, iu0);
-          const float fv0 = ceil_exact(v - L2, iv0);
+          // positions, taps and table indices in FP64 (tile-relative, exact
+          // offsets), as the float64 algorithm forms them
+          const double fj = (double)j;
+          const double u = fma(fj, d.x, offu), v = fma(fj, d.y, offv);
+          const int iu0 = (int)ceil(u - L2d), iv0 = (int)ceil(v - L2d);
           const int row = iu0 + t;
           const int col = iv0 + t;
-          const float du = fabsf(u - (fu0 + ft));
-          const float dv = fabsf(v - (fv0 + ft));
-          const float wtu = s_wtbl[min(table_index(du, ts), ltbl)];
-          const float wtv = s_wtbl[min(table_index(dv, ts), ltbl)];
-          const float wu = (active && du <= L2 && (unsigned)row < (unsigned)kTile) ? wtu : 0.f;
-          const float wvt = (active && dv <= L2 && (unsigned)col < (unsigned)kTile) ? wtv : 0.f;
+          const double du = fabs(u - (double)row);
+          const double dv = fabs(v - (double)col);
+          const float wtu = s_wtbl[min(table_index64(du, tsd), ltbl)];
+          const float wtv = s_wtbl[min(table_index64(dv, tsd), ltbl)];
+          const float wu = (active && du <= L2d && (unsigned)row < (unsigned)kTile) ? wtu : 0.f;
+          const float wvt = (active && dv <= L2d && (unsigned)col < (unsigned)kTile) ? wtv : 0.f;
           float4 cc = make_float4(0.f, 0.f, 0.f, 0.f);
           if (wu != 0.f) cc = stage[j - run.jlo];
           const float4 c4 = make_float4(wu * cc.x, wu * cc.y, wu * cc.z, wu * cc.w);
@@ -866,9 +847,8 @@ __global__ void __launch_bounds__(kWideWarps * 32, kWideMinBlocks) grid_wide_ker
   float* rec = wbase + 2 * kWideStage;      // [kRunMaxW][16]: rows 0..7, columns 8..15
   for (int i = threadIdx.x; i <= a.ltbl; i += blockDim.x) s_wtbl[i] = __ldg(&a.wtbl[i]);
   __syncthreads();
-  const float L2 = a.L2, ts = a.tblspcg;
+  const double L2d = a.L2, tsd = a.tblspcg;
   const int ltbl = a.ltbl;
-  const float half_m = (float)(a.M / 2);
   const int groups = (a.pairs + kWidePairs - 1) / kWidePairs;
   const unsigned total = (unsigned)a.n_items * (unsigned)groups;
   const size_t per_dir = (size_t)(a.J >> 2) * 64;  // float2 per direction and group
@@ -877,7 +857,7 @@ __global__ void __launch_bounds__(kWideWarps * 32, kWideMinBlocks) grid_wide_ker
   // computes row k (k < 8) or column k - 8
   const int w_s = lane >> 4, w_k = lane & 15;
   const bool w_row = w_k < 8;
-  const float w_cell = (float)(w_k & 7);
+  const double w_cell = (double)(w_k & 7);
   const int pl = lane >> 1, cl = lane & 1;
   for (;;) {
     unsigned w = 0;
@@ -891,12 +871,11 @@ __global__ void __launch_bounds__(kWideWarps * 32, kWideMinBlocks) grid_wide_ker
     const int tu = it.tile / a.tiles_v;
     const int tv = it.tile - tu * a.tiles_v;
     const int p0 = tu * TR, q0 = tv * TC;
-    // positions as grid_kernel forms them (relative to the enclosing 32 x 32
-    // tile), then moved to the sub-tile by an exact integer: both kernels see
-    // the same |d| and table indices
-    const float offu = half_m - (float)(p0 & ~(kTile - 1));
-    const float offv = half_m - (float)(q0 & ~(kTile - 1));
-    const float subu = (float)(p0 & (kTile - 1)), subv = (float)(q0 & (kTile - 1));
+    // FP64 positions as grid_kernel forms them (relative to the enclosing
+    // 32 x 32 tile), then moved to the sub-tile by an integer (exact for every
+    // tap within L/2): both kernels see the same |d| and table indices
+    const double w_off = (double)(a.M / 2 - (w_row ? (p0 & ~(kTile - 1)) : (q0 & ~(kTile - 1))));
+    const double w_sub = (double)(w_row ? (p0 & (kTile - 1)) : (q0 & (kTile - 1)));
     const float2* specg = a.spec + (size_t)grp * 2 * a.n_ang * per_dir;
     unsigned long long acc[TR][TC / 2];  // (cell c, cell c + 1) of row r
 #pragma unroll
@@ -915,22 +894,22 @@ __global__ void __launch_bounds__(kWideWarps * 32, kWideMinBlocks) grid_wide_ker
     // past the last run): nothing is read and its cells are written as zeros
     const int rb = it.run_begin, re = it.run_end;
     Run run1{0, 1, 0, 1}, run2{0, 1, 0, 1};
-    float2 dir1 = make_float2(0.f, 0.f), dir2 = dir1;
+    double dir1 = 0.0, dir2 = 0.0;  // this lane's component of the run's direction
     if (rb < re) {
       run1 = a.runs[rb];
-      dir1 = __ldg(&a.dir[run1.dir]);
+      dir1 = w_row ? __ldg(&a.dir[run1.dir].x) : __ldg(&a.dir[run1.dir].y);
       run2 = run1;
       dir2 = dir1;
       stage_run(run1, 0);
     }
     if (rb + 1 < re) {
       run2 = a.runs[rb + 1];
-      dir2 = __ldg(&a.dir[run2.dir]);
+      dir2 = w_row ? __ldg(&a.dir[run2.dir].x) : __ldg(&a.dir[run2.dir].y);
     }
     cp_async_commit();
     for (int r = rb; r < re; ++r) {
       const Run run = run1;
-      const float2 d = dir1;
+      const double d = dir1;
       const int b = (r - rb) & 1;
       run1 = run2;
       dir1 = dir2;
@@ -938,18 +917,17 @@ __global__ void __launch_bounds__(kWideWarps * 32, kWideMinBlocks) grid_wide_ker
       cp_async_commit();  // possibly empty: keeps one group per run
       if (r + 2 < re) {
         run2 = a.runs[r + 2];
-        dir2 = __ldg(&a.dir[run2.dir]);
+        dir2 = w_row ? __ldg(&a.dir[run2.dir].x) : __ldg(&a.dir[run2.dir].y);
       }
       // row and column weights of this run's samples
       const int n = run.jhi - run.jlo + 1;
       for (int s0 = 0; s0 < n; s0 += 2) {
         const int s = s0 + w_s;
         if (s < n) {
-          const float fj = (float)(run.jlo + s);
-          const float pos = w_row ? fmaf(fj, d.x, offu) - subu : fmaf(fj, d.y, offv) - subv;
-          const float dd = fabsf(pos - w_cell);
-          const float wt = s_wtbl[min(table_index(dd, ts), ltbl)];
-          rec[s * 16 + w_k] = dd <= L2 ? wt : 0.f;
+          const double pos = fma((double)(run.jlo + s), d, w_off) - w_sub;
+          const double dd = fabs(pos - w_cell);
+          const float wt = s_wtbl[min(table_index64(dd, tsd), ltbl)];
+          rec[s * 16 + w_k] = dd <= L2d ? wt : 0.f;
         }
       }
       cp_async_wait<1>();  // this run's values have landed (the next run's may be in flight)
@@ -1119,9 +1097,8 @@ __global__ void __launch_bounds__(kTcThreads) grid_tc_kernel(GridArgs a) {
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_misc[0];
-  const float L2 = a.L2, ts = a.tblspcg;
+  const double L2d = a.L2, tsd = a.tblspcg;
   const int ltbl = a.ltbl;
-  const float half_m = (float)(a.M / 2);
   const int groups = (a.pairs + kWidePairs - 1) / kWidePairs;
   const unsigned total = (unsigned)a.n_items * (unsigned)groups;
   const size_t per_dir = (size_t)(a.J >> 2) * 64;
@@ -1147,8 +1124,9 @@ __global__ void __launch_bounds__(kTcThreads) grid_tc_kernel(GridArgs a) {
     const int np = min(kWidePairs, a.pairs - pg0);
     const int tu = it.tile / a.tiles_v, tv = it.tile - (it.tile / a.tiles_v) * a.tiles_v;
     const int p0 = tu * TR, q0 = tv * TC;
-    const float offu = half_m - (float)(p0 & ~(kTile - 1)), offv = half_m - (float)(q0 & ~(kTile - 1));
-    const float subu = (float)(p0 & (kTile - 1)), subv = (float)(q0 & (kTile - 1));
+    // FP64 positions formed as grid_kernel forms them (see grid_wide_kernel)
+    const double offu = (double)(a.M / 2 - (p0 & ~(kTile - 1))), offv = (double)(a.M / 2 - (q0 & ~(kTile - 1)));
+    const double subu = (double)(p0 & (kTile - 1)), subv = (double)(q0 & (kTile - 1));
     const float* specg = reinterpret_cast<const float*>(a.spec + (size_t)grp * 2 * a.n_ang * per_dir);
     const int nchunk = (it.run_end - it.run_begin) >> 3;
     // a step's codes (this thread's weight samples and its two B samples) are
@@ -1168,28 +1146,26 @@ __global__ void __launch_bounds__(kTcThreads) grid_tc_kernel(GridArgs a) {
     };
     Codes cur = load_codes(0), nxt = load_codes(1);
     float b0 = load_val(cur.b0), b1 = load_val(cur.b1);
-    float dwx = __ldg(&a.dir[cur.w >> 13]).x, dvy = __ldg(&a.dir[cur.v >> 13]).y;
+    double dwx = __ldg(&a.dir[cur.w >> 13].x), dvy = __ldg(&a.dir[cur.v >> 13].y);
     for (int ch = 0; ch < nchunk && ok; ++ch) {
       const int buf = ch % kTcStages;
       const unsigned cw = cur.w, cv = cur.v;
-      const float cdx = dwx, cdy = dvy;
+      const double cdx = dwx, cdy = dvy;
       unsigned char* sb = stg + buf * kTcStage;
       // the MMAs that last read this buffer are done
       bool got = true;
       if (uses[buf] > 0) got = mbar_wait(&bar[buf], (uses[buf] - 1) & 1);
       // weights of this step's samples
       {
-        const float fj = (float)(cw & 8191);
-        const float u = fmaf(fj, cdx, offu) - subu;
-        const float dd = fabsf(u - (float)wr);
-        const float wt = s_wtbl[min(table_index(dd, ts), ltbl)];
-        s_wu[wr * 8 + wk] = dd <= L2 ? wt : 0.f;
+        const double u = fma((double)(cw & 8191), cdx, offu) - subu;
+        const double dd = fabs(u - (double)wr);
+        const float wt = s_wtbl[min(table_index64(dd, tsd), ltbl)];
+        s_wu[wr * 8 + wk] = dd <= L2d ? wt : 0.f;
         if (tid < 64) {
-          const float fjv = (float)(cv & 8191);
-          const float v = fmaf(fjv, cdy, offv) - subv;
-          const float ddv = fabsf(v - (float)vc);
-          const float wtv = s_wtbl[min(table_index(ddv, ts), ltbl)];
-          s_wv[vc * 8 + vk] = ddv <= L2 ? wtv : 0.f;
+          const double v = fma((double)(cv & 8191), cdy, offv) - subv;
+          const double ddv = fabs(v - (double)vc);
+          const float wtv = s_wtbl[min(table_index64(ddv, tsd), ltbl)];
+          s_wv[vc * 8 + vk] = ddv <= L2d ? wtv : 0.f;
         }
       }
       // B (K-major: value n's 4 samples per 16-byte row), hi and lo parts
@@ -1201,8 +1177,8 @@ __global__ void __launch_bounds__(kTcThreads) grid_tc_kernel(GridArgs a) {
       }
       // next step's values (codes loaded a step ago), codes of the step after
       const float nb0 = load_val(nxt.b0), nb1 = load_val(nxt.b1);
-      dwx = __ldg(&a.dir[nxt.w >> 13]).x;
-      dvy = __ldg(&a.dir[nxt.v >> 13]).y;
+      dwx = __ldg(&a.dir[nxt.w >> 13].x);
+      dvy = __ldg(&a.dir[nxt.v >> 13].y);
       cur = nxt;
       nxt = load_codes(ch + 2);
       if (__syncthreads_or(!got)) {

@@ -111,7 +111,7 @@ struct Plan {
   float* d_filt = nullptr;
   float2* d_tw_p = nullptr;
   float2* d_tw_m = nullptr;
-  float2* d_dir = nullptr;
+  double2* d_dir = nullptr;         // per direction (scale*dx, scale*dy): tap positions
   double* d_roi_off = nullptr;  // per-angle ROI offset phase step, or null
   // gridding work list
   int tiles_u = 0, tiles_v = 0, n_items = 0, n_runs = 0, n_slots = 0, n_split = 0;
@@ -488,22 +488,24 @@ bool use_wide(const Plan* p, int pairs) {
 }
 
 GridArgs grid_args_tc(const Plan* p, int pairs) {
-  return GridArgs{p->d_spec, p->d_H, p->d_t_scratch, p->d_queue, p->d_t_items, nullptr,
-                  p->d_t_split_list, p->t_split_tiles, p->d_dir, p->d_wtbl, p->t_items, pairs,
-                  p->n_ang, p->J, p->M, p->t_tiles_v, p->t_slots, p->ltbl, (float)(p->L / 2),
-                  (float)(2.0 * p->ltbl / p->L), p->d_t_codes, p->d_err};
+  GridArgs g{p->d_spec, p->d_H, p->d_t_scratch, p->d_queue, p->d_t_items, nullptr,
+             p->d_t_split_list, p->t_split_tiles, p->d_dir, p->d_wtbl, p->t_items, pairs,
+             p->n_ang, p->J, p->M, p->t_tiles_v, p->t_slots, p->ltbl, p->L / 2,
+             2.0 * p->ltbl / p->L, p->d_t_codes, p->d_err};
+  return g;
 }
 
 GridArgs grid_args(const Plan* p, int pairs, bool wide) {
-  if (wide)
-    return GridArgs{p->d_spec, p->d_H, p->d_w_scratch, p->d_queue, p->d_w_items, p->d_w_runs,
-                    p->d_w_split_list, p->w_split_tiles, p->d_dir, p->d_wtbl, p->w_items, pairs,
-                    p->n_ang, p->J, p->M, p->w_tiles_v, p->w_slots, p->ltbl, (float)(p->L / 2),
-                    (float)(2.0 * p->ltbl / p->L)};
-  return GridArgs{p->d_spec, p->d_H, p->d_scratch, p->d_queue, p->d_items, p->d_runs,
-                  p->d_split_list, p->n_split_tiles, p->d_dir, p->d_wtbl, p->n_items, pairs,
-                  p->n_ang, p->J, p->M, p->tiles_v, p->n_slots, p->ltbl, (float)(p->L / 2),
-                  (float)(2.0 * p->ltbl / p->L)};
+  GridArgs g =
+      wide ? GridArgs{p->d_spec, p->d_H, p->d_w_scratch, p->d_queue, p->d_w_items, p->d_w_runs,
+                      p->d_w_split_list, p->w_split_tiles, p->d_dir, p->d_wtbl, p->w_items, pairs,
+                      p->n_ang, p->J, p->M, p->w_tiles_v, p->w_slots, p->ltbl, p->L / 2,
+                      2.0 * p->ltbl / p->L}
+           : GridArgs{p->d_spec, p->d_H, p->d_scratch, p->d_queue, p->d_items, p->d_runs,
+                      p->d_split_list, p->n_split_tiles, p->d_dir, p->d_wtbl, p->n_items, pairs,
+                      p->n_ang, p->J, p->M, p->tiles_v, p->n_slots, p->ltbl, p->L / 2,
+                      2.0 * p->ltbl / p->L};
+  return g;
 }
 
 // Sizes exactly as GridRec::init (gridrec/GPU/gridrec.cu:243-268), in FP64.
@@ -846,9 +848,8 @@ int gr_plan_create(const gr_params* prm, gr_plan** out) {
     return t;
   };
   const std::vector<double> dxy = directions(prm, p->scale);
-  std::vector<float2> dirs(2 * (size_t)prm->n_ang);
-  for (size_t d = 0; d < dirs.size(); ++d)
-    dirs[d] = make_float2((float)dxy[2 * d], (float)dxy[2 * d + 1]);
+  std::vector<double2> dirs(2 * (size_t)prm->n_ang);
+  for (size_t d = 0; d < dirs.size(); ++d) dirs[d] = make_double2(dxy[2 * d], dxy[2 * d + 1]);
   p->dxy = dxy;
   if (prm->roi_x0 != 0.f || prm->roi_y0 != 0.f) {
     // (X0 cos + Y0 sin) pi per angle, from the unscaled direction (GridrecCPP grid.cpp:237)
@@ -1384,7 +1385,7 @@ extern "C" int gr_reconstruct_pair_noalloc(gr_plan* p, const float* sino1, const
   GR_CUDA(launch_spectra(sa, GR_DTYPE_F32, st));
   GridArgs ga{spec, H, part, queue, p->d_items, p->d_runs, p->d_split_list, p->n_split_tiles,
               p->d_dir, p->d_wtbl, p->n_items, 1, p->n_ang, p->J, p->M, p->tiles_v, p->n_slots,
-              p->ltbl, (float)(p->L / 2), (float)(2.0 * p->ltbl / p->L)};
+              p->ltbl, p->L / 2, 2.0 * p->ltbl / p->L};
   GR_CUDA(launch_grid(ga, p->ntaps, st));
   int* err = reinterpret_cast<int*>(base + off_queue + 64);
   GR_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));

@@ -16,6 +16,7 @@ torch = pytest.importorskip("torch")
 pytestmark = pytest.mark.gpu
 
 TOL = 1e-3
+FULL_SIZE_TOL = 1e-4
 CASES = cases()
 
 
@@ -278,7 +279,9 @@ def test_full_size_2048x1500_and_linearity():
     r1, r2 = O.port_gridrec_pair(s1, s2, th, filter=2)
     e1, e2 = ph.rel_l2(g[0], r1[:, :2047]), ph.rel_l2(g[1], r2[:, :2047])
     print(f"2048x1500 relL2 vs float64: {e1:.2e} {e2:.2e}")
-    assert e1 < TOL and e2 < TOL
+    # FP64 tap geometry keeps the benchmark shape an order of magnitude inside the
+    # parity bound (measured 1.6e-5; the reference's FP32 build is 4.8e-4 here)
+    assert e1 < FULL_SIZE_TOL and e2 < FULL_SIZE_TOL
     assert ph.rel_l2(gl[0], 2 * g[0] - g[1]) < TOL
 
 
@@ -596,3 +599,50 @@ def test_wide_kernel_host_streaming_and_graph():
     np.testing.assert_array_equal(host_out, d)
     np.testing.assert_array_equal(pinned_out.numpy(), d)
     np.testing.assert_array_equal(g_out.cpu().numpy(), d)
+
+
+@pytest.mark.parametrize("seed", [21, 22, 23])
+@pytest.mark.parametrize("mode", [-1, 0, 2])
+def test_wide_and_tensor_random_geometries(seed, mode):
+    """Seeded random widths, irregular angle lists, oversampling, PSWF parameter,
+    filter and centres through the 32 x 32 tile (mode -1), 16-pair (mode 0) and
+    tensor-core (mode 2) gridding kernels: every slice of a 16-pair chunk within
+    the parity bound of float64, and the worst slice no further from float64 than
+    the reference's own FP32 build's worst slice (GridrecCPP, one centre per pair).
+    Tap positions and table indices are FP64 in every kernel; FP32 positions move
+    taps across table-bin boundaries, which put FP32 gridrec near 1e-3 on these
+    sparse irregular angle sets (seed 22: 9.9e-4 for the reference's build)."""
+    rng = np.random.default_rng(seed)
+    n = int(rng.integers(60, 140))
+    a = int(rng.integers(30, 90))
+    th = np.sort(rng.uniform(0.0, 180.0, a)).astype(np.float32)
+    sampl = float(rng.choice([1.0, 1.2]))
+    C_ = float(rng.choice([4.0, 6.0, 7.0]))
+    filt = int(rng.integers(1, 5))
+    S = 32
+    centers = np.repeat(n / 2 + rng.uniform(-1.5, 1.5, S // 2), 2).astype(np.float32)
+    sinos = np.stack([ph.line_integrals(ph.random_ellipses(seed * 100 + s), n, th, float(c))
+                      / (n / 2) for s, c in enumerate(centers)]).astype(np.float32)
+    with G.Plan(n, a, th, filter=filt, pswf_c=C_, sampl=sampl, max_pairs=16,
+                wide_grid=mode) as plan:
+        assert plan.grid_kernel() == {-1: "tiles", 0: "wide", 2: "tensor"}[mode]
+        o = torch.zeros((S, plan.M0, max(plan.M0, n)), device="cuda")
+        plan.reconstruct_batch(_dev(sinos), o, centers=_dev(centers))
+        torch.cuda.synchronize()
+        plan.device_status()
+        got = o.cpu().numpy()[:, :, :plan.M0]
+        M0 = plan.M0
+    refs = _oracle_batch(sinos, centers, th, M0, filter=filt, C_=C_, sampl=sampl)
+    names = {1: "shlo", 2: "hann", 3: "hamm", 4: "ramp"}
+    errs, ref_errs = [], []
+    for i in range(0, S, 2):
+        r1, r2, m0 = O.refb_gridrec_pair(sinos[i], sinos[i + 1], th, float(centers[i]),
+                                         names[filt], C_, sampl)
+        for k, r in ((i, r1), (i + 1, r2)):
+            e_ref = ph.rel_l2(r[:, :m0], refs[k])
+            e = ph.rel_l2(got[k], refs[k])
+            assert e < TOL, (k, e, e_ref)
+            errs.append(e)
+            ref_errs.append(e_ref)
+    print(f"seed {seed} mode {mode}: worst slice {max(errs):.2e}, reference FP32 worst {max(ref_errs):.2e}")
+    assert max(errs) < max(ref_errs), (max(errs), max(ref_errs))
