@@ -836,6 +836,34 @@ __device__ __forceinline__ void ffma2(unsigned long long& acc, unsigned long lon
   asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(a), "l"(b));
 }
 
+// Applies the n samples of one staged run to the 4 x 8 register tile, over
+// column pairs C0..C1 only.  Lane (pl, cl) carries component cl of pair pl;
+// the run's first sample is jr0 into the first staged quad; rec holds per
+// sample 4 row weights (slots 0-3) and 8 column weights (slots 8-15).
+template <int C0, int C1>
+__device__ __forceinline__ void wide_apply_run(unsigned long long (&acc)[kWideRows][kWideCols / 2],
+                                               const float* st, const float* rec, int n, int jr0,
+                                               int pl, int cl) {
+  static_assert(kWideRows == 4 && kWideCols == 8, "weight record layout");
+  for (int s = 0; s < n; ++s) {
+    const int jr = jr0 + s;
+    const float val = st[(((jr >> 2) * 16 + pl) * 4 + (jr & 3)) * 2 + cl];
+    const float4 wr = *reinterpret_cast<const float4*>(rec + s * 16);
+    const float wrs[4] = {wr.x, wr.y, wr.z, wr.w};
+    const float4 wc0 = *reinterpret_cast<const float4*>(rec + s * 16 + 8);
+    const float4 wc1 = *reinterpret_cast<const float4*>(rec + s * 16 + 12);
+    const unsigned long long wc[4] = {pack2(wc0.x, wc0.y), pack2(wc0.z, wc0.w),
+                                      pack2(wc1.x, wc1.y), pack2(wc1.z, wc1.w)};
+#pragma unroll
+    for (int rr = 0; rr < kWideRows; ++rr) {
+      const float x = wrs[rr] * val;  // wu * value
+      const unsigned long long x2 = pack2(x, x);
+#pragma unroll
+      for (int c = C0; c <= C1; ++c) ffma2(acc[rr][c], wc[c], x2);  // += wv * (wu * value)
+    }
+  }
+}
+
 // kWideMinBlocks CTAs per SM (registers capped accordingly, no spills)
 __global__ void __launch_bounds__(kWideWarps * 32, kWideMinBlocks) grid_wide_kernel(GridArgs a) {
   constexpr int TR = kWideRows, TC = kWideCols;
@@ -921,6 +949,7 @@ __global__ void __launch_bounds__(kWideWarps * 32, kWideMinBlocks) grid_wide_ker
       }
       // row and column weights of this run's samples
       const int n = run.jhi - run.jlo + 1;
+      bool touched = false;  // some sample of the run reaches this lane's row / column
       for (int s0 = 0; s0 < n; s0 += 2) {
         const int s = s0 + w_s;
         if (s < n) {
@@ -928,32 +957,31 @@ __global__ void __launch_bounds__(kWideWarps * 32, kWideMinBlocks) grid_wide_ker
           const double dd = fabs(pos - w_cell);
           const float wt = s_wtbl[min(table_index64(dd, tsd), ltbl)];
           rec[s * 16 + w_k] = dd <= L2d ? wt : 0.f;
+          touched |= dd <= L2d;
         }
       }
       cp_async_wait<1>();  // this run's values have landed (the next run's may be in flight)
       __syncwarp();
-      const float* st = stage + b * kWideStage;
-      const int jq0 = run.jlo & ~3;
-      for (int s = 0; s < n; ++s) {
-        const int jr = run.jlo + s - jq0;  // j relative to the first staged quad
-        const float val = st[(((jr >> 2) * 16 + pl) * 4 + (jr & 3)) * 2 + cl];
-        float wr[8];
-        const float4 wr0 = *reinterpret_cast<const float4*>(rec + s * 16);
-        wr[0] = wr0.x; wr[1] = wr0.y; wr[2] = wr0.z; wr[3] = wr0.w;
-        if constexpr (TR > 4) {
-          const float4 wr1 = *reinterpret_cast<const float4*>(rec + s * 16 + 4);
-          wr[4] = wr1.x; wr[5] = wr1.y; wr[6] = wr1.z; wr[7] = wr1.w;
-        }
-        const float4 wc0 = *reinterpret_cast<const float4*>(rec + s * 16 + 8);
-        const float4 wc1 = *reinterpret_cast<const float4*>(rec + s * 16 + 12);
-        const unsigned long long wc[4] = {pack2(wc0.x, wc0.y), pack2(wc0.z, wc0.w),
-                                          pack2(wc1.x, wc1.y), pack2(wc1.z, wc1.w)};
-#pragma unroll
-        for (int rr = 0; rr < TR; ++rr) {
-          const float x = wr[rr] * val;  // wu * value
-          const unsigned long long x2 = pack2(x, x);
-#pragma unroll
-          for (int c = 0; c < TC / 2; ++c) ffma2(acc[rr][c], wc[c], x2);  // += wv * (wu * value)
+      // the run's samples over the column pairs some sample reaches (column
+      // lanes 8-15 and 24-31 report nonzero weights); the other pairs would
+      // only add zero products
+      const unsigned reach = __ballot_sync(0xffffffffu, touched);
+      const unsigned cols = ((reach >> 8) | (reach >> 24)) & 0xFFu;
+      if (cols) {
+        const float* st = stage + b * kWideStage;
+        const int jr0 = run.jlo - (run.jlo & ~3);  // j relative to the first staged quad
+        const int c2lo = (__ffs(cols) - 1) >> 1, c2hi = (31 - __clz(cols)) >> 1;
+        switch (c2lo * 4 + c2hi) {
+          case 0: wide_apply_run<0, 0>(acc, st, rec, n, jr0, pl, cl); break;
+          case 1: wide_apply_run<0, 1>(acc, st, rec, n, jr0, pl, cl); break;
+          case 2: wide_apply_run<0, 2>(acc, st, rec, n, jr0, pl, cl); break;
+          case 3: wide_apply_run<0, 3>(acc, st, rec, n, jr0, pl, cl); break;
+          case 5: wide_apply_run<1, 1>(acc, st, rec, n, jr0, pl, cl); break;
+          case 6: wide_apply_run<1, 2>(acc, st, rec, n, jr0, pl, cl); break;
+          case 7: wide_apply_run<1, 3>(acc, st, rec, n, jr0, pl, cl); break;
+          case 10: wide_apply_run<2, 2>(acc, st, rec, n, jr0, pl, cl); break;
+          case 11: wide_apply_run<2, 3>(acc, st, rec, n, jr0, pl, cl); break;
+          default: wide_apply_run<3, 3>(acc, st, rec, n, jr0, pl, cl); break;
         }
       }
       __syncwarp();

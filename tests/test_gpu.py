@@ -489,6 +489,9 @@ def test_wide_kernel_16_pairs_against_oracle(n, a, C_):
             outs[mode] = o.cpu().numpy()[:, :, :plan.M0]
             M0 = plan.M0
     refs = _oracle_batch(sinos, centers, th, M0, filter=2, C_=C_)
+    e64 = {m: max(ph.rel_l2(outs[m][i], refs[i]) for i in range(32)) for m in outs}
+    e_tiles = {m: max(ph.rel_l2(outs[m][i], outs[-1][i]) for i in range(32)) for m in (0, 2)}
+    print(f"n={n} a={a} C={C_}: worst vs float64 {e64}; worst vs the tile kernel {e_tiles}")
     for i in range(32):
         assert ph.rel_l2(outs[0][i], refs[i]) < TOL, i
         assert ph.rel_l2(outs[2][i], refs[i]) < TOL, i
