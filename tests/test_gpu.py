@@ -444,7 +444,8 @@ def test_graph_refused_after_its_plan_is_destroyed():
 # the two gridding kernels against each other: same taps and weights, FP32 sums in
 # a different order.  It shows as an image-wide offset from the centre cells of the
 # grid, where the filtered terms of every direction nearly cancel; seen up to
-# 7.3e-5 at C = 7 (each kernel is ~1e-4 from float64 there).
+# 1.3e-4 at C = 7 with 45 angles (the kernels are 1.7e-4 and 2.8e-4 from float64
+# there).
 KERNEL_TOL = 2e-4
 # the tensor-core kernel adds the 3xTF32 rounding (lo x lo dropped, lo parts in TF32)
 # and the tensor core's own FP32 accumulation, which rounds more coarsely than one
