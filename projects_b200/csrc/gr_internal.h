@@ -28,7 +28,10 @@ constexpr int kItemCap = 2048;
 // sub-tile of cells in registers (kWideCols = 8: four packed column pairs).
 constexpr int kWideRows = 4;
 constexpr int kWideCols = 8;
-constexpr int kWideMinBlocks = 6;
+// precomputed weights per (run, sample) of the 16-pair list: 4 row + 8 column
+constexpr int kWideRec = kWideRows + kWideCols;
+constexpr int kWideNoReach = 16;  // column-pair range code of a run that reaches no column
+constexpr int kWideMinBlocks = 5;
 constexpr int kWidePairs = 16;
 // Longest run it stages at once (longer runs are split on the host).
 constexpr int kRunMaxW = 16;
@@ -119,6 +122,10 @@ struct GridArgs {
   double L2, tblspcg;    // L/2, 2 ltbl / L
   const unsigned* codes = nullptr;  // grid_tc_kernel: flat (direction << 13 | j) per sample
   int* err = nullptr;               // device error word for bounded-wait timeouts
+  // grid_wide_kernel: weights per (run, sample), 4 row + 8 column, and per run
+  // {first sample's record, column-pair range}, from launch_wide_weights
+  const float* wts = nullptr;
+  const int2* wmeta = nullptr;
 };
 
 struct ColArgs {
@@ -182,6 +189,10 @@ cudaError_t launch_spectra(const SpectraArgs& a, gr_dtype dt, cudaStream_t s);
 // its split-tile reduction when tiles are split.
 cudaError_t launch_grid(const GridArgs& a, int ntaps, cudaStream_t s);
 cudaError_t launch_grid_wide(const GridArgs& a, cudaStream_t s);
+// Weights of the 16-pair work list (once per list): meta[r] = {record base,
+// sub-tile index} on entry; .y becomes the run's column-pair range code.
+cudaError_t launch_wide_weights(const GridArgs& a, int n_runs, float* wts, int2* meta,
+                                cudaStream_t s);
 cudaError_t launch_grid_tc(const GridArgs& a, cudaStream_t s);
 int cols_group(int M);
 cudaError_t launch_cols(const ColArgs& a, cudaStream_t s);

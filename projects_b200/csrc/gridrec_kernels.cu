@@ -784,30 +784,37 @@ __global__ void __launch_bounds__(256) split_reduce_kernel(GridArgs a) {
 // many slice pairs.  Lane l of a warp carries component l & 1 (re, im) of pair
 // l >> 1 of a group of kWidePairs pairs, so all lanes apply the same taps, each
 // to its own value:
-// * the geometry and weights of a sample are warp-uniform and computed once
-//   for all 16 pairs (16 lanes per sample, one weight each, exchanged through
-//   a small shared record);
+// * the geometry and weights of a sample are warp-uniform and shared by all
+//   16 pairs; they depend on the geometry only, so wide_weights_kernel
+//   computes them once per work list, with each run's column-pair range, and
+//   the kernel copies them in beside the values;
 // * a work item is one kWideRows x kWideCols sub-tile whose cells stay in registers
 //   for all its runs: no shared-memory read-modify-write and no atomics.
 // Every sample carries one weight per sub-tile row and per column,
 // w(|u - row|) and w(|v - col|), zero where the distance exceeds L/2 -- the
-// test that selects the taps -- and is applied to the whole 8 x 8 register
-// tile with packed FP32x2 FMAs: no per-sample branches or offsets, and any
-// footprint width up to 8 taps.  A tap adds wv * (wu * value), the rounding
+// test that selects the taps -- and is applied to the register tile with
+// packed FP32x2 FMAs over the column pairs its run reaches: no per-sample
+// branches or offsets.  A tap adds wv * (wu * value), the rounding
 // of grid_kernel, at positions formed as grid_kernel forms them, so the two
 // kernels differ only in summation order.  Each cell sums its taps in a fixed
 // order (runs in work-list order, samples in j order; split sub-tiles by
 // slot): results are bitwise reproducible.  The run's values for the 16 pairs
 // are one contiguous range of the interleaved spectra layout
-// ([group][dir][j / 4][pair][j % 4]), staged by 16-byte cp.async and double
-// buffered against the previous run.
+// ([group][dir][j / 4][pair][j % 4]), staged by 16-byte cp.async one run ahead
+// and then moved sample-major (one 32-value row per sample) into a second
+// buffer, so the FMA loop reads a sample's values with one conflict-free load
+// at a fixed stride.
 
 constexpr int kWideWarps = 4;
 // staging: up to kRunMaxW samples span kWideQuads quads of 4 j x 16 pairs
 constexpr int kWideQuads = (kRunMaxW + 3) / 4 + 1;
-constexpr int kWideStage = kWideQuads * 16 * 4 * 2;  // floats per buffer
-// per warp: staging [2][kWideStage] + weights [kRunMaxW][16]
-constexpr int kWideWarpFloats = 2 * kWideStage + kRunMaxW * 16;
+constexpr int kWideStage = kWideQuads * 16 * 4 * 2;  // floats of one staged run
+// sample-major rows: 32 values + 8 pad floats, so the rows a restaging store
+// writes at once (t and t + 2 of a quad) fall on disjoint banks
+constexpr int kWideRowStride = 40;
+constexpr int kWideSamp = kWideQuads * 4 * kWideRowStride;
+// per warp: staging [kWideStage] + sample rows [kWideSamp] + weights [2][kRunMaxW][kWideRec]
+constexpr int kWideWarpFloats = kWideStage + kWideSamp + 2 * kRunMaxW * kWideRec;
 
 __device__ __forceinline__ void cp_async16(float* dst_smem, const void* src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
@@ -836,22 +843,20 @@ __device__ __forceinline__ void ffma2(unsigned long long& acc, unsigned long lon
   asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(acc) : "l"(a), "l"(b));
 }
 
-// Applies the n samples of one staged run to the 4 x 8 register tile, over
-// column pairs C0..C1 only.  Lane (pl, cl) carries component cl of pair pl;
-// the run's first sample is jr0 into the first staged quad; rec holds per
-// sample 4 row weights (slots 0-3) and 8 column weights (slots 8-15).
+// Applies the n samples of one restaged run to the 4 x 8 register tile, over
+// column pairs C0..C1 only.  sv points at this lane's value of the run's
+// first sample (rows kWideRowStride floats apart); rec holds per sample
+// kWideRec floats: 4 row weights, then 8 column weights.
 template <int C0, int C1>
 __device__ __forceinline__ void wide_apply_run(unsigned long long (&acc)[kWideRows][kWideCols / 2],
-                                               const float* st, const float* rec, int n, int jr0,
-                                               int pl, int cl) {
-  static_assert(kWideRows == 4 && kWideCols == 8, "weight record layout");
+                                               const float* sv, const float* rec, int n) {
+  static_assert(kWideRows == 4 && kWideCols == 8 && kWideRec == 12, "weight record layout");
   for (int s = 0; s < n; ++s) {
-    const int jr = jr0 + s;
-    const float val = st[(((jr >> 2) * 16 + pl) * 4 + (jr & 3)) * 2 + cl];
-    const float4 wr = *reinterpret_cast<const float4*>(rec + s * 16);
+    const float val = sv[s * kWideRowStride];
+    const float4 wr = *reinterpret_cast<const float4*>(rec + s * kWideRec);
     const float wrs[4] = {wr.x, wr.y, wr.z, wr.w};
-    const float4 wc0 = *reinterpret_cast<const float4*>(rec + s * 16 + 8);
-    const float4 wc1 = *reinterpret_cast<const float4*>(rec + s * 16 + 12);
+    const float4 wc0 = *reinterpret_cast<const float4*>(rec + s * kWideRec + 4);
+    const float4 wc1 = *reinterpret_cast<const float4*>(rec + s * kWideRec + 8);
     const unsigned long long wc[4] = {pack2(wc0.x, wc0.y), pack2(wc0.z, wc0.w),
                                       pack2(wc1.x, wc1.y), pack2(wc1.z, wc1.w)};
 #pragma unroll
@@ -864,28 +869,62 @@ __device__ __forceinline__ void wide_apply_run(unsigned long long (&acc)[kWideRo
   }
 }
 
+// The weights of every (run, sample) of the 16-pair work list, computed once
+// per work list: they depend on the geometry only.  Thread r takes run r of
+// sub-tile meta[r].y (tile index) and writes, for each of its samples, the 4
+// row and 8 column weights w(|u - row|), w(|v - col|) -- zero where a distance
+// exceeds L/2 -- at wts + meta[r].x * kWideRec, with positions formed as
+// grid_kernel forms them (FP64, relative to the enclosing 32 x 32 tile, moved
+// to the sub-tile by an integer).  It then replaces meta[r].y by the range of
+// column pairs some sample reaches, c2lo * 4 + c2hi, or kWideNoReach.
+__global__ void __launch_bounds__(128) wide_weights_kernel(GridArgs a, int n_runs, float* wts,
+                                                           int2* meta) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_runs) return;
+  const Run run = a.runs[r];
+  const int2 m = meta[r];
+  const int tu = m.y / a.tiles_v, tv = m.y - (m.y / a.tiles_v) * a.tiles_v;
+  const int p0 = tu * kWideRows, q0 = tv * kWideCols;
+  const double offu = (double)(a.M / 2 - (p0 & ~(kTile - 1))), subu = (double)(p0 & (kTile - 1));
+  const double offv = (double)(a.M / 2 - (q0 & ~(kTile - 1))), subv = (double)(q0 & (kTile - 1));
+  const double2 d = a.dir[run.dir];
+  const double L2d = a.L2, tsd = a.tblspcg;
+  float* w = wts + (size_t)m.x * kWideRec;
+  unsigned cols = 0;
+  for (int j = run.jlo; j <= run.jhi; ++j, w += kWideRec) {
+    const double u = fma((double)j, d.x, offu) - subu, v = fma((double)j, d.y, offv) - subv;
+    float4 o[3];
+    float* of = reinterpret_cast<float*>(o);
+#pragma unroll
+    for (int k = 0; k < kWideRows; ++k) {
+      const double dd = fabs(u - (double)k);
+      of[k] = dd <= L2d ? __ldg(&a.wtbl[min(table_index64(dd, tsd), a.ltbl)]) : 0.f;
+    }
+#pragma unroll
+    for (int k = 0; k < kWideCols; ++k) {
+      const double dd = fabs(v - (double)k);
+      of[kWideRows + k] = dd <= L2d ? __ldg(&a.wtbl[min(table_index64(dd, tsd), a.ltbl)]) : 0.f;
+      if (dd <= L2d) cols |= 1u << k;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) reinterpret_cast<float4*>(w)[k] = o[k];
+  }
+  meta[r].y = cols ? ((__ffs(cols) - 1) >> 1) * 4 + ((31 - __clz(cols)) >> 1) : kWideNoReach;
+}
+
 // kWideMinBlocks CTAs per SM (registers capped accordingly, no spills)
 __global__ void __launch_bounds__(kWideWarps * 32, kWideMinBlocks) grid_wide_kernel(GridArgs a) {
   constexpr int TR = kWideRows, TC = kWideCols;
   extern __shared__ float4 smw4[];
-  float* s_wtbl = reinterpret_cast<float*>(smw4);  // table: up to 1028 floats
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float* wbase = reinterpret_cast<float*>(smw4 + 257) + warp * kWideWarpFloats;
-  float* stage = wbase;                     // [2][kWideQuads][16][4][2]
-  float* rec = wbase + 2 * kWideStage;      // [kRunMaxW][16]: rows 0..7, columns 8..15
-  for (int i = threadIdx.x; i <= a.ltbl; i += blockDim.x) s_wtbl[i] = __ldg(&a.wtbl[i]);
-  __syncthreads();
-  const double L2d = a.L2, tsd = a.tblspcg;
-  const int ltbl = a.ltbl;
+  float* wbase = reinterpret_cast<float*>(smw4) + warp * kWideWarpFloats;
+  float* stage = wbase;                     // [kWideQuads][16][4][2] as copied
+  float* samp = wbase + kWideStage;         // [kWideQuads * 4][kWideRowStride]
+  float* recs = samp + kWideSamp;           // [2][kRunMaxW][kWideRec] weights, double-buffered
   const int groups = (a.pairs + kWidePairs - 1) / kWidePairs;
   const unsigned total = (unsigned)a.n_items * (unsigned)groups;
   const size_t per_dir = (size_t)(a.J >> 2) * 64;  // float2 per direction and group
   const size_t MM = (size_t)a.M * a.M;
-  // weight pass: lanes 0-15 serve sample s0, 16-31 sample s0 + 1; lane k & 15
-  // computes row k (k < 8) or column k - 8
-  const int w_s = lane >> 4, w_k = lane & 15;
-  const bool w_row = w_k < 8;
-  const double w_cell = (double)(w_k & 7);
   const int pl = lane >> 1, cl = lane & 1;
   for (;;) {
     unsigned w = 0;
@@ -899,90 +938,82 @@ __global__ void __launch_bounds__(kWideWarps * 32, kWideMinBlocks) grid_wide_ker
     const int tu = it.tile / a.tiles_v;
     const int tv = it.tile - tu * a.tiles_v;
     const int p0 = tu * TR, q0 = tv * TC;
-    // FP64 positions as grid_kernel forms them (relative to the enclosing
-    // 32 x 32 tile), then moved to the sub-tile by an integer (exact for every
-    // tap within L/2): both kernels see the same |d| and table indices
-    const double w_off = (double)(a.M / 2 - (w_row ? (p0 & ~(kTile - 1)) : (q0 & ~(kTile - 1))));
-    const double w_sub = (double)(w_row ? (p0 & (kTile - 1)) : (q0 & (kTile - 1)));
     const float2* specg = a.spec + (size_t)grp * 2 * a.n_ang * per_dir;
     unsigned long long acc[TR][TC / 2];  // (cell c, cell c + 1) of row r
 #pragma unroll
     for (int r = 0; r < TR; ++r)
 #pragma unroll
       for (int c = 0; c < TC / 2; ++c) acc[r][c] = 0ull;
-    // the quads of run rn -> staging buffer b
-    auto stage_run = [&](const Run& rn, int b) {
+    // run rn's quads -> the staging buffer, its weights -> weight buffer b
+    auto stage_run = [&](const Run& rn, int2 mn, int b) {
       const int nq = (rn.jhi >> 2) - (rn.jlo >> 2) + 1;
-      float* dst = stage + b * kWideStage;
       const float2* src = specg + (size_t)rn.dir * per_dir + (size_t)(rn.jlo >> 2) * 64;
-      for (int i = lane; i < nq * 32; i += 32) cp_async16(dst + i * 4, src + i * 2);
+      for (int i = lane; i < nq * 32; i += 32) cp_async16(stage + i * 4, src + i * 2);
+      const float* wsrc = a.wts + (size_t)mn.x * kWideRec;
+      float* wdst = recs + b * (kRunMaxW * kWideRec);
+      for (int i = lane; i < (rn.jhi - rn.jlo + 1) * (kWideRec / 4); i += 32)
+        cp_async16(wdst + i * 4, wsrc + i * 4);
     };
     // run records travel two runs ahead of their use, staging one run ahead;
     // a tile that no sample reaches has an empty item (rb == re, possibly one
     // past the last run): nothing is read and its cells are written as zeros
     const int rb = it.run_begin, re = it.run_end;
     Run run1{0, 1, 0, 1}, run2{0, 1, 0, 1};
-    double dir1 = 0.0, dir2 = 0.0;  // this lane's component of the run's direction
+    int2 meta1 = make_int2(0, kWideNoReach), meta2 = meta1;
     if (rb < re) {
       run1 = a.runs[rb];
-      dir1 = w_row ? __ldg(&a.dir[run1.dir].x) : __ldg(&a.dir[run1.dir].y);
+      meta1 = __ldg(&a.wmeta[rb]);
       run2 = run1;
-      dir2 = dir1;
-      stage_run(run1, 0);
+      meta2 = meta1;
+      stage_run(run1, meta1, 0);
     }
     if (rb + 1 < re) {
       run2 = a.runs[rb + 1];
-      dir2 = w_row ? __ldg(&a.dir[run2.dir].x) : __ldg(&a.dir[run2.dir].y);
+      meta2 = __ldg(&a.wmeta[rb + 1]);
     }
     cp_async_commit();
     for (int r = rb; r < re; ++r) {
       const Run run = run1;
-      const double d = dir1;
+      const int2 meta = meta1;
       const int b = (r - rb) & 1;
       run1 = run2;
-      dir1 = dir2;
-      if (r + 1 < re) stage_run(run1, b ^ 1);
-      cp_async_commit();  // possibly empty: keeps one group per run
+      meta1 = meta2;
       if (r + 2 < re) {
         run2 = a.runs[r + 2];
-        dir2 = w_row ? __ldg(&a.dir[run2.dir].x) : __ldg(&a.dir[run2.dir].y);
+        meta2 = __ldg(&a.wmeta[r + 2]);
       }
-      // row and column weights of this run's samples
-      const int n = run.jhi - run.jlo + 1;
-      bool touched = false;  // some sample of the run reaches this lane's row / column
-      for (int s0 = 0; s0 < n; s0 += 2) {
-        const int s = s0 + w_s;
-        if (s < n) {
-          const double pos = fma((double)(run.jlo + s), d, w_off) - w_sub;
-          const double dd = fabs(pos - w_cell);
-          const float wt = s_wtbl[min(table_index64(dd, tsd), ltbl)];
-          rec[s * 16 + w_k] = dd <= L2d ? wt : 0.f;
-          touched |= dd <= L2d;
-        }
-      }
-      cp_async_wait<1>();  // this run's values have landed (the next run's may be in flight)
+      cp_async_wait<0>();  // this run's values and weights have landed
       __syncwarp();
-      // the run's samples over the column pairs some sample reaches (column
-      // lanes 8-15 and 24-31 report nonzero weights); the other pairs would
-      // only add zero products
-      const unsigned reach = __ballot_sync(0xffffffffu, touched);
-      const unsigned cols = ((reach >> 8) | (reach >> 24)) & 0xFFu;
-      if (cols) {
-        const float* st = stage + b * kWideStage;
-        const int jr0 = run.jlo - (run.jlo & ~3);  // j relative to the first staged quad
-        const int c2lo = (__ffs(cols) - 1) >> 1, c2hi = (31 - __clz(cols)) >> 1;
-        switch (c2lo * 4 + c2hi) {
-          case 0: wide_apply_run<0, 0>(acc, st, rec, n, jr0, pl, cl); break;
-          case 1: wide_apply_run<0, 1>(acc, st, rec, n, jr0, pl, cl); break;
-          case 2: wide_apply_run<0, 2>(acc, st, rec, n, jr0, pl, cl); break;
-          case 3: wide_apply_run<0, 3>(acc, st, rec, n, jr0, pl, cl); break;
-          case 5: wide_apply_run<1, 1>(acc, st, rec, n, jr0, pl, cl); break;
-          case 6: wide_apply_run<1, 2>(acc, st, rec, n, jr0, pl, cl); break;
-          case 7: wide_apply_run<1, 3>(acc, st, rec, n, jr0, pl, cl); break;
-          case 10: wide_apply_run<2, 2>(acc, st, rec, n, jr0, pl, cl); break;
-          case 11: wide_apply_run<2, 3>(acc, st, rec, n, jr0, pl, cl); break;
-          default: wide_apply_run<3, 3>(acc, st, rec, n, jr0, pl, cl); break;
-        }
+      // sample-major rows: lane (p, h) moves its 16-byte piece of each quad --
+      // samples 2h and 2h + 1 of pair p, (re, im) each -- to rows 4q + 2h and
+      // 4q + 2h + 1, columns 2p and 2p + 1
+      const int nq = (run.jhi >> 2) - (run.jlo >> 2) + 1;
+      for (int q = 0; q < nq; ++q) {
+        const float4 c = *reinterpret_cast<const float4*>(stage + q * 128 + lane * 4);
+        float* dst = samp + (q * 4 + 2 * (lane & 1)) * kWideRowStride + pl * 2;
+        *reinterpret_cast<float2*>(dst) = make_float2(c.x, c.y);
+        *reinterpret_cast<float2*>(dst + kWideRowStride) = make_float2(c.z, c.w);
+      }
+      __syncwarp();  // staging read and rows written before the next copy lands
+      if (r + 1 < re) stage_run(run1, meta1, b ^ 1);  // overlaps this run's FMAs
+      cp_async_commit();  // possibly empty: keeps one group per run
+      // the run's samples over the column pairs some sample reaches (the
+      // other pairs would only add zero products)
+      const int n = run.jhi - run.jlo + 1;
+      const float* sv = samp + (run.jlo & 3) * kWideRowStride + lane;  // first sample's row
+      const float* rec = recs + b * (kRunMaxW * kWideRec);
+      switch (meta.y) {
+        case 0: wide_apply_run<0, 0>(acc, sv, rec, n); break;
+        case 1: wide_apply_run<0, 1>(acc, sv, rec, n); break;
+        case 2: wide_apply_run<0, 2>(acc, sv, rec, n); break;
+        case 3: wide_apply_run<0, 3>(acc, sv, rec, n); break;
+        case 5: wide_apply_run<1, 1>(acc, sv, rec, n); break;
+        case 6: wide_apply_run<1, 2>(acc, sv, rec, n); break;
+        case 7: wide_apply_run<1, 3>(acc, sv, rec, n); break;
+        case 10: wide_apply_run<2, 2>(acc, sv, rec, n); break;
+        case 11: wide_apply_run<2, 3>(acc, sv, rec, n); break;
+        case 15: wide_apply_run<3, 3>(acc, sv, rec, n); break;
+        default: break;  // kWideNoReach: no sample reaches the sub-tile
       }
       __syncwarp();
     }
@@ -1659,7 +1690,14 @@ cudaError_t launch_grid(const GridArgs& a, int ntaps, cudaStream_t s) {
 }
 
 static int grid_wide_smem_bytes() {
-  return 257 * (int)sizeof(float4) + kWideWarps * kWideWarpFloats * (int)sizeof(float);
+  return kWideWarps * kWideWarpFloats * (int)sizeof(float);
+}
+
+cudaError_t launch_wide_weights(const GridArgs& a, int n_runs, float* wts, int2* meta,
+                                cudaStream_t s) {
+  if (n_runs == 0) return cudaSuccess;
+  wide_weights_kernel<<<(n_runs + 127) / 128, 128, 0, s>>>(a, n_runs, wts, meta);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_grid_wide(const GridArgs& a, cudaStream_t s) {

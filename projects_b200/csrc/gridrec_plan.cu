@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -139,6 +140,8 @@ struct Plan {
   Run* d_w_runs = nullptr;
   int4* d_w_split_list = nullptr;
   float4* d_w_scratch = nullptr;    // [pair group of 16][slot][64 cells x 32 lanes] floats
+  float* d_w_wts = nullptr;         // [sample of the list][4 row + 8 column weights]
+  int2* d_w_meta = nullptr;         // per run: {first weight record, column-pair range}
   size_t w_scratch_cells = 0;
   int spec_pairs = 0;               // pairs the spectra workspace holds
   // tensor-core gridding (grid_tc_kernel, gr_params.wide_grid = 2): 16 x 8
@@ -408,13 +411,40 @@ int install_work_list_wide(Plan* p, int item_cap) {
   for (size_t t = 0; t < wl.splits.size(); ++t)
     if (wl.splits[t].nsplit > 1)
       split_list.push_back(make_int4((int)t, wl.splits[t].slot0, wl.splits[t].nsplit, 0));
+  // per run: its first weight record (samples of the runs before it) and its
+  // sub-tile, which the weights kernel replaces by the run's column-pair range
+  std::vector<int2> meta(wl.runs.size(), make_int2(0, 0));
+  for (const Item& it : wl.items)
+    for (int r = it.run_begin; r < it.run_end; ++r) meta[r].y = it.tile;
+  size_t n_rec = 0;
+  for (size_t r = 0; r < wl.runs.size(); ++r) {
+    meta[r].x = (int)n_rec;
+    n_rec += (size_t)(wl.runs[r].jhi - wl.runs[r].jlo + 1);
+  }
+  if (n_rec > (size_t)INT_MAX) return fail(GR_ERR_UNSUPPORTED, "work list too large");
   dev_free(p, &p->d_w_items);
   dev_free(p, &p->d_w_runs);
   dev_free(p, &p->d_w_split_list);
+  dev_free(p, &p->d_w_meta);
+  dev_free(p, &p->d_w_wts);
   int rc;
   if ((rc = upload(p, &p->d_w_items, wl.items)) || (rc = upload(p, &p->d_w_runs, wl.runs)) ||
-      (rc = upload(p, &p->d_w_split_list, split_list)))
+      (rc = upload(p, &p->d_w_split_list, split_list)) || (rc = upload(p, &p->d_w_meta, meta)) ||
+      (rc = dev_alloc(p, &p->d_w_wts, std::max<size_t>(n_rec, 1) * kWideRec)))
     return rc;
+  {
+    GridArgs g{};
+    g.runs = p->d_w_runs;
+    g.dir = p->d_dir;
+    g.wtbl = p->d_wtbl;
+    g.M = p->M;
+    g.tiles_v = wl.tiles_v;
+    g.ltbl = p->ltbl;
+    g.L2 = p->L / 2;
+    g.tblspcg = 2.0 * p->ltbl / p->L;
+    GR_CUDA(launch_wide_weights(g, (int)wl.runs.size(), p->d_w_wts, p->d_w_meta, 0));
+    GR_CUDA(cudaStreamSynchronize(0));
+  }
   // 64 cells x 32 lanes floats = 512 float4 per slot and group of 16 pairs
   const size_t groups = (size_t)(p->max_pairs + kWidePairs - 1) / kWidePairs;
   const size_t cells = groups * (size_t)std::max(wl.n_slots, 1) * (kWideRows * kWideCols * 32 / 4);
@@ -505,6 +535,10 @@ GridArgs grid_args(const Plan* p, int pairs, bool wide) {
                       p->d_split_list, p->n_split_tiles, p->d_dir, p->d_wtbl, p->n_items, pairs,
                       p->n_ang, p->J, p->M, p->tiles_v, p->n_slots, p->ltbl, p->L / 2,
                       2.0 * p->ltbl / p->L};
+  if (wide) {
+    g.wts = p->d_w_wts;
+    g.wmeta = p->d_w_meta;
+  }
   return g;
 }
 
