@@ -813,8 +813,10 @@ constexpr int kWideStage = kWideQuads * 16 * 4 * 2;  // floats of one staged run
 // writes at once (t and t + 2 of a quad) fall on disjoint banks
 constexpr int kWideRowStride = 40;
 constexpr int kWideSamp = kWideQuads * 4 * kWideRowStride;
-// per warp: staging [kWideStage] + sample rows [kWideSamp] + weights [2][kRunMaxW][kWideRec]
-constexpr int kWideWarpFloats = kWideStage + kWideSamp + 2 * kRunMaxW * kWideRec;
+// per warp: staging [2][kWideStage] + sample rows [kWideSamp] + weights [3][kRunMaxW][kWideRec]
+// (copies run two runs ahead: values of runs r+1, r+2 in flight or landed
+// while run r is applied)
+constexpr int kWideWarpFloats = 2 * kWideStage + kWideSamp + 3 * kRunMaxW * kWideRec;
 
 __device__ __forceinline__ void cp_async16(float* dst_smem, const void* src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
@@ -918,9 +920,9 @@ __global__ void __launch_bounds__(kWideWarps * 32, kWideMinBlocks) grid_wide_ker
   extern __shared__ float4 smw4[];
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   float* wbase = reinterpret_cast<float*>(smw4) + warp * kWideWarpFloats;
-  float* stage = wbase;                     // [kWideQuads][16][4][2] as copied
-  float* samp = wbase + kWideStage;         // [kWideQuads * 4][kWideRowStride]
-  float* recs = samp + kWideSamp;           // [2][kRunMaxW][kWideRec] weights, double-buffered
+  float* stages = wbase;                    // [2][kWideQuads][16][4][2] as copied
+  float* samp = wbase + 2 * kWideStage;     // [kWideQuads * 4][kWideRowStride]
+  float* recs = samp + kWideSamp;           // [3][kRunMaxW][kWideRec] weights
   const int groups = (a.pairs + kWidePairs - 1) / kWidePairs;
   const unsigned total = (unsigned)a.n_items * (unsigned)groups;
   const size_t per_dir = (size_t)(a.J >> 2) * 64;  // float2 per direction and group
@@ -944,49 +946,51 @@ __global__ void __launch_bounds__(kWideWarps * 32, kWideMinBlocks) grid_wide_ker
     for (int r = 0; r < TR; ++r)
 #pragma unroll
       for (int c = 0; c < TC / 2; ++c) acc[r][c] = 0ull;
-    // run rn's quads -> the staging buffer, its weights -> weight buffer b
-    auto stage_run = [&](const Run& rn, int2 mn, int b) {
+    // run rn's quads -> staging buffer vb, its weights -> weight buffer b
+    auto stage_run = [&](const Run& rn, int2 mn, int vb, int b) {
       const int nq = (rn.jhi >> 2) - (rn.jlo >> 2) + 1;
       const float2* src = specg + (size_t)rn.dir * per_dir + (size_t)(rn.jlo >> 2) * 64;
-      for (int i = lane; i < nq * 32; i += 32) cp_async16(stage + i * 4, src + i * 2);
+      float* vdst = stages + vb * kWideStage;
+      for (int i = lane; i < nq * 32; i += 32) cp_async16(vdst + i * 4, src + i * 2);
       const float* wsrc = a.wts + (size_t)mn.x * kWideRec;
       float* wdst = recs + b * (kRunMaxW * kWideRec);
       for (int i = lane; i < (rn.jhi - rn.jlo + 1) * (kWideRec / 4); i += 32)
         cp_async16(wdst + i * 4, wsrc + i * 4);
     };
-    // run records travel two runs ahead of their use, staging one run ahead;
-    // a tile that no sample reaches has an empty item (rb == re, possibly one
-    // past the last run): nothing is read and its cells are written as zeros
+    // copies run two runs ahead (one cp.async group per run); run records are
+    // read one run before their copies are issued.  A tile that no sample
+    // reaches has an empty item (rb == re, possibly one past the last run):
+    // nothing is read and its cells are written as zeros
     const int rb = it.run_begin, re = it.run_end;
-    Run run1{0, 1, 0, 1}, run2{0, 1, 0, 1};
-    int2 meta1 = make_int2(0, kWideNoReach), meta2 = meta1;
+    Run runA{0, 1, 0, 1}, runB = runA, runC = runA;  // runs r, r + 1, r + 2
+    int2 metaA = make_int2(0, kWideNoReach), metaB = metaA, metaC = metaA;
     if (rb < re) {
-      run1 = a.runs[rb];
-      meta1 = __ldg(&a.wmeta[rb]);
-      run2 = run1;
-      meta2 = meta1;
-      stage_run(run1, meta1, 0);
-    }
-    if (rb + 1 < re) {
-      run2 = a.runs[rb + 1];
-      meta2 = __ldg(&a.wmeta[rb + 1]);
+      runA = a.runs[rb];
+      metaA = __ldg(&a.wmeta[rb]);
+      stage_run(runA, metaA, 0, 0);
     }
     cp_async_commit();
+    if (rb + 1 < re) {
+      runB = a.runs[rb + 1];
+      metaB = __ldg(&a.wmeta[rb + 1]);
+      stage_run(runB, metaB, 1, 1);
+    }
+    cp_async_commit();
+    if (rb + 2 < re) {
+      runC = a.runs[rb + 2];
+      metaC = __ldg(&a.wmeta[rb + 2]);
+    }
+    int wb = 0;  // weight buffer of run r: (r - rb) % 3
     for (int r = rb; r < re; ++r) {
-      const Run run = run1;
-      const int2 meta = meta1;
-      const int b = (r - rb) & 1;
-      run1 = run2;
-      meta1 = meta2;
-      if (r + 2 < re) {
-        run2 = a.runs[r + 2];
-        meta2 = __ldg(&a.wmeta[r + 2]);
-      }
-      cp_async_wait<0>();  // this run's values and weights have landed
+      const Run run = runA;
+      const int2 meta = metaA;
+      const int vb = (r - rb) & 1;
+      cp_async_wait<1>();  // run r's group has landed (run r + 1's may be in flight)
       __syncwarp();
       // sample-major rows: lane (p, h) moves its 16-byte piece of each quad --
       // samples 2h and 2h + 1 of pair p, (re, im) each -- to rows 4q + 2h and
       // 4q + 2h + 1, columns 2p and 2p + 1
+      const float* stage = stages + vb * kWideStage;
       const int nq = (run.jhi >> 2) - (run.jlo >> 2) + 1;
       for (int q = 0; q < nq; ++q) {
         const float4 c = *reinterpret_cast<const float4*>(stage + q * 128 + lane * 4);
@@ -994,14 +998,23 @@ __global__ void __launch_bounds__(kWideWarps * 32, kWideMinBlocks) grid_wide_ker
         *reinterpret_cast<float2*>(dst) = make_float2(c.x, c.y);
         *reinterpret_cast<float2*>(dst + kWideRowStride) = make_float2(c.z, c.w);
       }
-      __syncwarp();  // staging read and rows written before the next copy lands
-      if (r + 1 < re) stage_run(run1, meta1, b ^ 1);  // overlaps this run's FMAs
+      __syncwarp();  // staging buffer read and rows written before it is refilled
+      const int wb2 = wb == 0 ? 2 : wb - 1;  // (r + 2 - rb) % 3
+      if (r + 2 < re) stage_run(runC, metaC, vb, wb2);  // overlaps runs r and r + 1
       cp_async_commit();  // possibly empty: keeps one group per run
+      runA = runB;
+      metaA = metaB;
+      runB = runC;
+      metaB = metaC;
+      if (r + 3 < re) {
+        runC = a.runs[r + 3];
+        metaC = __ldg(&a.wmeta[r + 3]);
+      }
       // the run's samples over the column pairs some sample reaches (the
       // other pairs would only add zero products)
       const int n = run.jhi - run.jlo + 1;
       const float* sv = samp + (run.jlo & 3) * kWideRowStride + lane;  // first sample's row
-      const float* rec = recs + b * (kRunMaxW * kWideRec);
+      const float* rec = recs + wb * (kRunMaxW * kWideRec);
       switch (meta.y) {
         case 0: wide_apply_run<0, 0>(acc, sv, rec, n); break;
         case 1: wide_apply_run<0, 1>(acc, sv, rec, n); break;
@@ -1015,6 +1028,7 @@ __global__ void __launch_bounds__(kWideWarps * 32, kWideMinBlocks) grid_wide_ker
         case 15: wide_apply_run<3, 3>(acc, sv, rec, n); break;
         default: break;  // kWideNoReach: no sample reaches the sub-tile
       }
+      wb = wb == 2 ? 0 : wb + 1;
       __syncwarp();
     }
     cp_async_wait<0>();
