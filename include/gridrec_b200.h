@@ -96,7 +96,7 @@ typedef struct {
                               (0 = 1) */
   float roi_x0, roi_y0;    /* ROI offset X0, Y0: C1 times exp(-i j (X0 cos + Y0 sin) pi),
                               C2 times its conjugate */
-  int wide_grid;           /* gridding kernel: 0 = 16-pair kernel for chunks of >= 11 pairs
+  int wide_grid;           /* gridding kernel: 0 = 16-pair kernel for chunks of >= 7 pairs
                               (default), 1 = for every chunk, -1 = never (2 pairs per warp
                               over 32 x 32 tiles), 2 = tensor-core kernel (tcgen05, 3xTF32)
                               for every chunk; same taps and weights, the sums differ only

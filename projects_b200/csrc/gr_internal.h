@@ -39,8 +39,9 @@ constexpr int kRunMaxW = 16;
 constexpr int kItemCapW = 1024;
 // Chunks of at least this many pairs use it when gr_params.wide_grid is 0: its
 // cost per launch does not depend on the pairs (idle lanes), the tile kernel's
-// grows with them; measured crossover 10.3 pairs at 2048 x 1500, 10.9 at 4096 x 3000.
-constexpr int kWideMinPairs = 11;
+// grows with them (two pairs per warp): 6 pairs 538 against 563 us per launch,
+// 7 pairs 681 against 571 at 2048 x 1500; the same step at 4096 x 3000.
+constexpr int kWideMinPairs = 7;
 
 // The tensor-core gridding kernel (grid_tc_kernel): a CTA accumulates a
 // kTcRows x kTcCols sub-tile (128 cells, the MMA M) for 16 pairs x (re, im)
