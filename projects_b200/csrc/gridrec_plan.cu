@@ -12,6 +12,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "gr_internal.h"
@@ -174,7 +175,7 @@ struct Plan {
   bool timing = false;
   std::vector<cudaEvent_t> events;
   size_t events_used = 0;
-  std::vector<void*> allocs;
+  std::vector<std::pair<void*, size_t>> allocs;  // device allocations and their bytes
   std::vector<double> h_winv, h_wtbl;
 };
 
@@ -191,7 +192,7 @@ int dev_alloc(Plan* p, T** ptr, size_t count) {
     return fail(GR_ERR_NOMEM, "cudaMalloc(%zu bytes) failed: %s", count * sizeof(T),
                 cudaGetErrorString(e));
   }
-  p->allocs.push_back(*ptr);
+  p->allocs.emplace_back((void*)*ptr, count * sizeof(T));
   p->device_bytes += count * sizeof(T);
   return GR_OK;
 }
@@ -207,8 +208,12 @@ int upload(Plan* p, T** dptr, const std::vector<T>& h) {
 template <typename T>
 void dev_free(Plan* p, T** ptr) {
   if (!*ptr) return;
-  auto it = std::find(p->allocs.begin(), p->allocs.end(), (void*)*ptr);
-  if (it != p->allocs.end()) p->allocs.erase(it);
+  auto it = std::find_if(p->allocs.begin(), p->allocs.end(),
+                         [&](const std::pair<void*, size_t>& x) { return x.first == (void*)*ptr; });
+  if (it != p->allocs.end()) {
+    p->device_bytes -= it->second;
+    p->allocs.erase(it);
+  }
   cudaFree(*ptr);
   *ptr = nullptr;
 }
@@ -790,7 +795,7 @@ int gr_plan_destroy(gr_plan* plan) {
     gg->dead = true;
     gg->plans.erase(std::find(gg->plans.begin(), gg->plans.end(), plan));
   }
-  for (void* ptr : plan->allocs) cudaFree(ptr);
+  for (const auto& x : plan->allocs) cudaFree(x.first);
   for (int b = 0; b < 2; ++b) {
     if (plan->h_in[b]) cudaFreeHost(plan->h_in[b]);
     if (plan->h_out[b]) cudaFreeHost(plan->h_out[b]);

@@ -413,6 +413,21 @@ def test_autotune_keeps_parity_and_caches():
             assert again.autotune() == t  # cached for the shape
 
 
+def test_device_bytes_after_autotune_count_live_buffers_only():
+    """Autotune reinstalls the 16-pair work list (and its precomputed weights) once
+    per item cap it times; the plan's device byte count follows the frees, so it
+    ends within the size differences of the lists, not at one list per cap tried."""
+    th = ph.angles_deg(360)
+    _, runs, _, _ = G.worklist(512, 360, th, wide=True)
+    weights = int((runs[:, 2] - runs[:, 1] + 1).sum()) * 48  # one list's weights
+    with G.Plan(512, 360, th, filter=G.FILTER_HANN, max_pairs=16) as plan:
+        assert plan.grid_kernel(16) == "wide"
+        before = plan.device_bytes()
+        plan.autotune()  # times 5 item caps
+        after = plan.device_bytes()
+    assert abs(after - before) < 2 * weights, (before, after, weights)
+
+
 def test_autotune_refused_while_a_graph_holds_the_plan():
     n, a = 64, 40
     th = ph.angles_deg(a)
