@@ -241,14 +241,15 @@ def test_gridrec_class_call_surface():
     assert np.all(r1[m:, :] == 0) and np.all(r1[:, m:] == 0)
 
 
-# With only a few angles most grid cells receive one or two taps and FP32
-# tap rounding shows more: the reference's own FP32 build is 1.0-1.7e-3 from
-# float64 on the 300-detector cases below, so they get a 3e-3 bound.
+# With only a few angles most grid cells receive one or two taps, so a tap
+# that FP32 positions move into the next table bin shows: the reference's own
+# FP32 build is 1.0-1.7e-3 from float64 on the 300-detector cases below.  With
+# FP64 tap positions they measure ~4e-6 and are held to the parity bound.
 @pytest.mark.parametrize("n,a,theta,tol", [
     (9, 1, None, TOL),                              # smallest supported width, one angle
     (33, 7, np.array([-40, 0, 10, 95, 180, 250, 359], np.float32), TOL),  # outside [0, 180)
-    (300, 3, None, 3e-3),
-    (300, 8, None, 3e-3),
+    (300, 3, None, TOL),
+    (300, 8, None, TOL),
 ])
 def test_edge_shapes(n, a, theta, tol):
     th = ph.angles_deg(a) if theta is None else theta
@@ -258,8 +259,9 @@ def test_edge_shapes(n, a, theta, tol):
     g1, g2 = _gpu_pair(s1, s2, th, filter=4)       # default centre n_det/2 (integer)
     o1, o2 = O.port_gridrec_pair(s1, s2, th, filter=4)
     m = g1.shape[0]
-    assert ph.rel_l2(g1, o1[:, :m]) < tol
-    assert ph.rel_l2(g2, o2[:, :m]) < tol
+    e1, e2 = ph.rel_l2(g1, o1[:, :m]), ph.rel_l2(g2, o2[:, :m])
+    print(f"edge shape {n}x{a}: relL2 vs float64 {e1:.2e} {e2:.2e}")
+    assert e1 < tol and e2 < tol
 
 
 def test_full_size_2048x1500_and_linearity():
