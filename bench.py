@@ -492,6 +492,11 @@ def run_b200(args, rank, world, local_rank):
     achieved = bytes_total / (stage_ms[dominant] / 1000.0) / 1e9
     peak, peak_src = peaks()
     traffic = traffic_from_profile(dominant, min(args.max_pairs, (S + 1) // 2), n, a)
+    traffic_note = ("ncu DRAM read + write of one launch (profiles/traffic_%dx%d.txt)" % (n, a))
+    if dominant == "grid" and plan.grid_kernel(args.max_pairs) == "wide":
+        traffic_note += ("; includes the 16-pair kernel's precomputed weights (48 bytes per "
+                         "sample and 4x8 sub-tile, read once per launch for its 16 pairs), "
+                         "which replace an in-kernel weight pass")
     per_launch_bytes = bytes_total / max(n_launch, 1)
     stages = {k: {"ms_per_pair": v / pairs_timed,
                   "gbs": bpp[k] * pairs_timed / max(v / 1000.0, 1e-12) / 1e9}
@@ -560,7 +565,8 @@ def run_b200(args, rank, world, local_rank):
                        "l2": f"inputs larger than L2 ({S * a * n * in_bytes / 1e9:.1f} GB/step)"},
             "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": achieved / peak, "peak_source": peak_src,
-                         "traffic": traffic, "algorithmic_bytes_per_launch": per_launch_bytes},
+                         "traffic": traffic, "traffic_note": traffic_note,
+                         "algorithmic_bytes_per_launch": per_launch_bytes},
             "stages": stages,
             "pipeline": {"algorithmic_bytes_per_slice": model_bytes_slice,
                          "frac_of_hbm": model_bytes_slice * value / world / 1e9 / peak,
