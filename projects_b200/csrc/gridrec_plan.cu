@@ -12,6 +12,7 @@
 #include <map>
 #include <mutex>
 #include <string>
+#include <thread>
 #include <utility>
 #include <vector>
 
@@ -271,7 +272,6 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
   const int n_dir = 2 * n_ang;
   struct TRun { int tile, dir, jlo, jhi; };
   std::vector<TRun> all;
-  all.reserve((size_t)n_dir * wl->tiles_u * 2);
   auto slab = [](double o, double dd, double lo, double hi, double& tmin, double& tmax) {
     if (std::fabs(dd) < 1e-12) return o >= lo && o <= hi;
     double t1 = (lo - o) / dd, t2 = (hi - o) / dd;
@@ -280,32 +280,66 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
     tmax = std::min(tmax, t2);
     return tmin <= tmax;
   };
-  for (int d = 0; d < n_dir; ++d) {
-    const double dx = dxy[2 * d], dy = dxy[2 * d + 1];
-    for (int tu = 0; tu < wl->tiles_u; ++tu) {
-      const double x0 = tu * Tu - L2, x1 = std::min(tu * Tu + Tu, M) - 1 + L2;
-      double ta = 1.0, tb = J - 1.0;
-      if (!slab(M2, dx, x0, x1, ta, tb)) continue;
-      // y extent of the samples in this x slab -> candidate tile columns
-      const double ya = M2 + ta * dy, yb = M2 + tb * dy;
-      const double ymin = std::min(ya, yb), ymax = std::max(ya, yb);
-      int tv0 = (int)std::floor((ymin - L2) / Tv) - 1;
-      int tv1 = (int)std::floor((ymax + L2) / Tv) + 1;
-      tv0 = std::max(tv0, 0);
-      tv1 = std::min(tv1, wl->tiles_v - 1);
-      for (int tv = tv0; tv <= tv1; ++tv) {
-        const double y0 = tv * Tv - L2, y1 = std::min(tv * Tv + Tv, M) - 1 + L2;
-        double sa = ta, sb = tb;
-        if (!slab(M2, dy, y0, y1, sa, sb)) continue;
-        const int jlo = std::max(1, (int)std::ceil(sa - 1e-6));
-        const int jhi = std::min(J - 1, (int)std::floor(sb + 1e-6));
-        for (int j0 = jlo; j0 <= jhi; j0 += run_max)  // runs of at most run_max samples
-          all.push_back({tu * wl->tiles_v + tv, d, j0, std::min(jhi, j0 + run_max - 1)});
+  // runs of directions [d0, d1) in (direction, tile row, tile column, j) order
+  auto enumerate_dirs = [&](int d0, int d1, std::vector<TRun>& out) {
+    for (int d = d0; d < d1; ++d) {
+      const double dx = dxy[2 * d], dy = dxy[2 * d + 1];
+      for (int tu = 0; tu < wl->tiles_u; ++tu) {
+        const double x0 = tu * Tu - L2, x1 = std::min(tu * Tu + Tu, M) - 1 + L2;
+        double ta = 1.0, tb = J - 1.0;
+        if (!slab(M2, dx, x0, x1, ta, tb)) continue;
+        // y extent of the samples in this x slab -> candidate tile columns
+        const double ya = M2 + ta * dy, yb = M2 + tb * dy;
+        const double ymin = std::min(ya, yb), ymax = std::max(ya, yb);
+        int tv0 = (int)std::floor((ymin - L2) / Tv) - 1;
+        int tv1 = (int)std::floor((ymax + L2) / Tv) + 1;
+        tv0 = std::max(tv0, 0);
+        tv1 = std::min(tv1, wl->tiles_v - 1);
+        for (int tv = tv0; tv <= tv1; ++tv) {
+          const double y0 = tv * Tv - L2, y1 = std::min(tv * Tv + Tv, M) - 1 + L2;
+          double sa = ta, sb = tb;
+          if (!slab(M2, dy, y0, y1, sa, sb)) continue;
+          const int jlo = std::max(1, (int)std::ceil(sa - 1e-6));
+          const int jhi = std::min(J - 1, (int)std::floor(sb + 1e-6));
+          for (int j0 = jlo; j0 <= jhi; j0 += run_max)  // runs of at most run_max samples
+            out.push_back({tu * wl->tiles_v + tv, d, j0, std::min(jhi, j0 + run_max - 1)});
+        }
       }
     }
+  };
+  // directions split over host threads in contiguous blocks, concatenated in
+  // direction order: the same list as one thread builds
+  const long work = (long)n_dir * wl->tiles_u;
+  const int n_thr = work < (1L << 16)
+                        ? 1
+                        : (int)std::min<long>(std::min<long>(16, n_dir),
+                                              std::max(1u, std::thread::hardware_concurrency()));
+  if (n_thr == 1) {
+    all.reserve((size_t)n_dir * wl->tiles_u * 2);
+    enumerate_dirs(0, n_dir, all);
+  } else {
+    std::vector<std::vector<TRun>> parts(n_thr);
+    std::vector<std::thread> pool;
+    for (int k = 0; k < n_thr; ++k)
+      pool.emplace_back([&, k] {
+        enumerate_dirs((int)((long)n_dir * k / n_thr), (int)((long)n_dir * (k + 1) / n_thr),
+                       parts[k]);
+      });
+    for (auto& th : pool) th.join();
+    size_t total_runs = 0;
+    for (const auto& part : parts) total_runs += part.size();
+    all.reserve(total_runs);
+    for (const auto& part : parts) all.insert(all.end(), part.begin(), part.end());
   }
-  std::stable_sort(all.begin(), all.end(),
-                   [](const TRun& a, const TRun& b) { return a.tile < b.tile; });
+  // stable counting sort by tile (runs of a tile keep their enumeration order)
+  {
+    std::vector<size_t> at(n_tiles + 1, 0);
+    for (const TRun& r : all) at[r.tile + 1]++;
+    for (int t = 0; t < n_tiles; ++t) at[t + 1] += at[t];
+    std::vector<TRun> sorted(all.size());
+    for (const TRun& r : all) sorted[at[r.tile]++] = r;
+    all.swap(sorted);
+  }
   wl->runs.resize(all.size());
   std::vector<long> run_cost(all.size());
   // the kernel's NT: footprint rows per sample (3 for L < 3, e.g. C = 4 at sampl = 1)
