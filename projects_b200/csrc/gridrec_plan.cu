@@ -320,16 +320,25 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
   } else {
     std::vector<std::vector<TRun>> parts(n_thr);
     std::vector<std::thread> pool;
-    for (int k = 0; k < n_thr; ++k)
-      pool.emplace_back([&, k] {
-        enumerate_dirs((int)((long)n_dir * k / n_thr), (int)((long)n_dir * (k + 1) / n_thr),
-                       parts[k]);
-      });
+    bool threaded = true;
+    try {
+      for (int k = 0; k < n_thr; ++k)
+        pool.emplace_back([&, k] {
+          enumerate_dirs((int)((long)n_dir * k / n_thr), (int)((long)n_dir * (k + 1) / n_thr),
+                         parts[k]);
+        });
+    } catch (...) {  // no thread to be had: the threads started finish, then one pass
+      threaded = false;
+    }
     for (auto& th : pool) th.join();
-    size_t total_runs = 0;
-    for (const auto& part : parts) total_runs += part.size();
-    all.reserve(total_runs);
-    for (const auto& part : parts) all.insert(all.end(), part.begin(), part.end());
+    if (threaded) {
+      size_t total_runs = 0;
+      for (const auto& part : parts) total_runs += part.size();
+      all.reserve(total_runs);
+      for (const auto& part : parts) all.insert(all.end(), part.begin(), part.end());
+    } else {
+      enumerate_dirs(0, n_dir, all);
+    }
   }
   // stable counting sort by tile (runs of a tile keep their enumeration order)
   {
