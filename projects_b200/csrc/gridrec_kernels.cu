@@ -800,7 +800,7 @@ __global__ void __launch_bounds__(256) split_reduce_kernel(GridArgs a) {
 // order (runs in work-list order, samples in j order; split sub-tiles by
 // slot): results are bitwise reproducible.  The run's values for the 16 pairs
 // are one contiguous range of the interleaved spectra layout
-// ([group][dir][j / 4][pair][j % 4]), staged by 16-byte cp.async one run ahead
+// ([group][dir][j / 4][pair][j % 4]), staged by 16-byte cp.async two runs ahead
 // and then moved sample-major (one 32-value row per sample) into a second
 // buffer, so the FMA loop reads a sample's values with one conflict-free load
 // at a fixed stride.
