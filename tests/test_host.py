@@ -267,3 +267,22 @@ def test_wide_worklist_random_geometries(seed):
     sampl = float(rng.choice([1.0, 1.2, 1.5]))
     C_ = float(rng.choice([4.0, 5.0, 6.0, 7.0]))
     assert _emulate_wide(n, a, th, sampl, C_) < 1e-14
+
+
+@pytest.mark.parametrize("n,a,sampl,C_", [(2048, 1500, 1.0, 6.0), (120, 72, 1.2, 7.0),
+                                          (64, 9, 1.0, 4.0)])
+def test_wide_worklist_runs_fit_the_precomputed_weights(n, a, sampl, C_):
+    """The 16-pair kernel's weights are computed once per list, one 48-byte
+    record per run sample, each run tagged with the sub-tile of its item: every
+    run belongs to exactly one item, runs hold 1..16 samples (the kernel's
+    staging and weight buffers), and the record count fits an int."""
+    items, runs, splits, tv = G.worklist(n, a, ph.angles_deg(a), sampl=sampl, pswf_c=C_,
+                                         wide=True)
+    owner = np.zeros(len(runs), np.int64)
+    for it in items:
+        owner[it[1]:it[2]] += 1
+    assert (owner == 1).all()
+    lens = runs[:, 2] - runs[:, 1] + 1
+    assert lens.min() >= 1 and lens.max() <= 16
+    assert (runs[:, 3] == 1).all()
+    assert int(lens.sum()) < 2**31 - 1
