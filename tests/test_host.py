@@ -286,3 +286,14 @@ def test_wide_worklist_runs_fit_the_precomputed_weights(n, a, sampl, C_):
     assert lens.min() >= 1 and lens.max() <= 16
     assert (runs[:, 3] == 1).all()
     assert int(lens.sum()) < 2**31 - 1
+
+
+def test_no_gpu_means_an_error_not_a_fallback():
+    """Without a usable GPU every compute entry point fails loudly: plan creation
+    returns GR_ERR_CUDA (there is no CPU path to fall back to)."""
+    torch = pytest.importorskip("torch")
+    if torch.cuda.is_available():
+        pytest.skip("a GPU is present")
+    with pytest.raises(G.GrError) as err:
+        G.Plan(64, 32, ph.angles_deg(32))
+    assert "GR_ERR_CUDA" in str(err.value)
