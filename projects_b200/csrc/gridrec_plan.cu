@@ -359,7 +359,7 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
   for (size_t i = 0; i < all.size(); ++i) {
     const int n = all[i].jhi - all[i].jlo + 1;
     if (wide) {
-      // one warp-uniform pass per sample; the run's staging and weight pass
+      // one pass per sample over the register tile; the run's copies, restaging and dispatch
       wl->runs[i] = {all[i].dir, all[i].jlo, all[i].jhi, 1};
       run_cost[i] = n + 6;
     } else {
