@@ -53,7 +53,7 @@ def parse():
     ap.add_argument("--n-ang", type=int, default=1500)
     ap.add_argument("--max-pairs", type=int, default=16)
     ap.add_argument("--dtype", default="f32", choices=["f32", "f16", "bf16"])
-    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-pipeline", action="store_true",
@@ -280,6 +280,24 @@ def cpu_reference(n_det, n_ang, seconds, threads=None, steps=None):
         pairs = sum(f.result() for f in futs)
     wall = time.perf_counter() - t0
     return 2.0 * pairs / wall, {"kind": kind, "cores": threads, "pairs": pairs, "wall_s": wall}
+
+
+def parity_check(sinos, outs, centers, th, M0):
+    """relL2 and max-abs of the first slice pair of the timed step's images against
+    float64 gridrec of the same sinograms (the oracle as the checker, after the
+    timed region)."""
+    from oracle import oracle as O
+    from projects_b200 import phantom as ph
+    s = sinos[:2].float().cpu().numpy()
+    got = outs[:2, :, :M0].cpu().numpy().astype(np.float64)
+    r1, r2 = O.port_gridrec_pair(s[0], s[1], th, center1=float(centers[0]),
+                                 center2=float(centers[1]), filter=2)
+    res = {"slices": [0, 1], "reference": "float64 gridrec (oracle/gridrec_oracle.c)",
+           "tolerance_rel_l2": 1e-3}
+    for k, r in ((0, r1[:, :M0]), (1, r2[:, :M0])):
+        res[f"slice{k}"] = {"rel_l2": ph.rel_l2(got[k], r), "max_abs": float(np.abs(got[k] - r).max()),
+                            "peak": float(np.abs(r).max())}
+    return res
 
 
 def measure_slice_pipeline(G, sinos, th, n, a, dev, stream, peak):
@@ -539,7 +557,11 @@ def run_b200(args, rank, world, local_rank):
         pipe = measure_slice_pipeline(G, sinos, th, n, a, dev, stream, peaks()[0])
 
     cpu = None
+    parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # the CPU leg: the oracle checks two of the timed images, then the reference's
+        # own CPU GridRec is timed on the host cores
+        parity = parity_check(sinos, outs, centers, th, plan.M0)
         v, info = cpu_reference(n, a, args.cpu_seconds)
         cpu = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
                "sample": f"{info['pairs']} slice pairs of {n}x{a} (Hann) over "
@@ -576,6 +598,7 @@ def run_b200(args, rank, world, local_rank):
             "clocks": clk.summary(),
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "parity": parity,
             "slice_pipeline": pipe,
             "learned": learned,
         }

@@ -171,24 +171,30 @@ int gr_reconstruct_batch(gr_plan* plan, const gr_batch_desc* batch, void* stream
  * overlap likewise).  Synchronises `stream` before returning. */
 int gr_reconstruct_host(gr_plan* plan, const gr_batch_desc* batch, void* stream);
 
-/* One slice pair, device pointers, exactly like gr_reconstruct_pair, but the
- * call allocates nothing: every intermediate of the pass (phase ramps,
- * filtered spectra, frequency grid, partial tiles of split tiles, work-queue
- * head) lives in a static 32 MiB device array that the library holds on each
- * GPU it runs on until the process exits, instead of in workspaces reached
- * through cudaMalloc.  It is for callers that must not allocate device memory
- * when they reconstruct: code that records the call into a CUDA graph by
- * stream capture (cudaMalloc is not permitted there), and applications whose
- * memory manager already owns the GPU's memory so that a further cudaMalloc
- * would fail or stall.  The plan itself is created beforehand (that step
- * allocates its tables).  Limits: plans whose intermediates need more than
- * 32 MiB are rejected with GR_ERR_UNSUPPORTED (for example 1024 x 1024 fits,
- * 2048 x 1500 does not).  The first call on a device looks up the array's
- * device address (cudaGetSymbolAddress); make that first call before any
- * stream capture.  All calls on a device share the array, so calls that can
- * overlap on the GPU (different streams, or different host threads) race;
- * serialise them.  No counterpart in the reference: its GridRec allocates
- * its grid in init() (gridrec/GPU/gridrec.cu:281). */
+/* One slice pair, device pointers, like gr_reconstruct_pair, but the call
+ * allocates nothing: every intermediate of the pass (phase ramps, filtered
+ * spectra, frequency grid, partial tiles of split tiles, work-queue head)
+ * lives in a static 32 MiB device array that the library holds on each GPU it
+ * runs on until the process exits, instead of in workspaces reached through
+ * cudaMalloc.  It is for callers that cannot call cudaMalloc while they
+ * reconstruct: an application whose own memory pool has already reserved the
+ * GPU's memory, so that a further cudaMalloc fails, and loops in which the
+ * device-wide synchronisation that cudaMalloc may imply is not acceptable.
+ * The plan itself is created beforehand (that step allocates its tables).
+ * Limits: the intermediates (about 8 (M^2 + n_ang pdim) bytes plus 16 KiB per
+ * split tile) must fit in 32 MiB, else GR_ERR_UNSUPPORTED: M <= 1024 with up
+ * to about 2500 angles fits (1024 x 1024 at sampl 1.0); 1024 x 1024 at
+ * sampl 1.2 (M = 2048) and 2048 x 1500 do not.  It always grids with the tile kernel (the plan's
+ * wide_grid choice does not apply), so its result equals gr_reconstruct_pair's
+ * bit for bit on plans with the default wide_grid = 0 and agrees within the
+ * usual tolerance otherwise.  A bounded-wait timeout of its column FFT is
+ * reported by gr_plan_device_status(plan), like the plan's own calls.  The
+ * first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress).  All calls on a device share the array and it keeps
+ * the last call's contents, so calls that can overlap on the GPU (different
+ * streams, or different host threads) race: serialise them.  No counterpart in
+ * the reference: its GridRec allocates its grid in init()
+ * (gridrec/GPU/gridrec.cu:281). */
 int gr_reconstruct_pair_noalloc(gr_plan* plan, const float* sino1, const float* sino2, float* out1,
                                 float* out2, long out_stride, void* stream);
 

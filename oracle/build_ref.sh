@@ -15,14 +15,19 @@
 # the reference is copied into this repository.  gridrec.cu is plain host C++
 # when USE_GRIDREC_GPU is undefined, so an empty tomo_recon_config.h suffices.
 #
-# Usage: oracle/build_ref.sh [REFERENCE_ROOT]   (default /root/reference)
+# Usage: oracle/build_ref.sh [--if-present] [REFERENCE_ROOT]
+#   REFERENCE_ROOT defaults to $GR_REFERENCE_ROOT, else /root/reference;
+#   --if-present: exit 0 without building when the reference tree is absent.
 set -euo pipefail
-REF="${1:-/root/reference}"
+IF_PRESENT=0
+if [ "${1:-}" = "--if-present" ]; then IF_PRESENT=1; shift; fi
+REF="${1:-${GR_REFERENCE_ROOT:-/root/reference}}"
 HERE="$(cd "$(dirname "$0")" && pwd)"
 OUT="$HERE/_ref"
 GPU="$REF/gridrec/GPU"
 CPP="$REF/gridrec/GridrecCPP/Gridrec5.2"
 if [ ! -f "$GPU/gridrec.cu" ]; then
+  [ "$IF_PRESENT" = 1 ] && exit 0
   echo "build_ref.sh: reference not found at $REF" >&2
   exit 1
 fi

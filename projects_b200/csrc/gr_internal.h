@@ -43,6 +43,15 @@ constexpr int kItemCapW = 1024;
 // 7 pairs 681 against 571 at 2048 x 1500; the same step at 4096 x 3000.
 constexpr int kWideMinPairs = 7;
 
+// The 32-pair gridding kernel (grid_w32_kernel): the 16-pair kernel's work list
+// (4 x 8 sub-tiles, runs of <= kRunMaxW samples), one complex value per lane for
+// 32 slice pairs; per (run, sample) 12 table indices of 16 bits, each run's
+// index block padded to 16 bytes.
+constexpr int kW32Pairs = 32;
+constexpr int kW32MinBlocks = 4;
+// Index of a zero weight (a tap beyond L/2) in the kernel's table copy.
+inline int w32_zero_index(int ltbl) { return ltbl + 1; }
+
 // The tensor-core gridding kernel (grid_tc_kernel): a CTA accumulates a
 // kTcRows x kTcCols sub-tile (128 cells, the MMA M) for 16 pairs x (re, im)
 // (the MMA N) in tensor memory, 8 samples (the MMA K) per step.
@@ -88,11 +97,14 @@ struct SpectraArgs {
   const float* dark;
   long flat_stride;
   const float4* pq;      // [pair][J] (P.re, P.im, Q.re, Q.im)
-  float2* spec;          // [pair][n_ang][2][J], or (wide) [pair / 16][2 n_ang][J / 4][16][4]
+  float2* spec;          // [pair][n_ang][2][J], or the wide layout below
   const float2* tw;      // two-level twiddle table for pdim (see gridrec_kernels.cu)
   int n_det, n_ang, pdim, J, pairs;
   const double* roi_off; // per angle (X0 cos + Y0 sin) pi of the ROI offset, or null
-  int wide = 0;          // spec in the 16-pair kernel's interleaved layout
+  // 0: plain [pair][dir][j]; 16 or 32: the 16- or 32-pair gridding kernel's
+  // interleaved layout [pair / G][dir][j / 4][pair % G][j % 4] (G = wide), for G = 32
+  // with position (j % 4) ^ ((pair / 4) % 4) inside each pair's 32-byte chunk
+  int wide = 0;
 };
 
 struct PhaseArgs {
@@ -127,6 +139,11 @@ struct GridArgs {
   // {first sample's record, column-pair range}, from launch_wide_weights
   const float* wts = nullptr;
   const int2* wmeta = nullptr;
+  // grid_w32_kernel: per run {quad of its first sample (direction * J/4 + jlo/4),
+  // index block (16-byte units), n | (jlo & 3) << 5 | quads << 8 | column-pair
+  // range << 12, 0}, and the 16-bit table indices (launch_w32_index)
+  const int4* xmeta = nullptr;
+  const unsigned short* xidx = nullptr;
 };
 
 struct ColArgs {
@@ -195,6 +212,11 @@ cudaError_t launch_grid_wide(const GridArgs& a, cudaStream_t s);
 cudaError_t launch_wide_weights(const GridArgs& a, int n_runs, float* wts, int2* meta,
                                 cudaStream_t s);
 cudaError_t launch_grid_tc(const GridArgs& a, cudaStream_t s);
+// 32-pair gridding: the index records of the 16-pair work list (once per list;
+// rinfo[r] = {index block in 16-byte units, sub-tile index}) and the kernel.
+cudaError_t launch_w32_index(const GridArgs& a, int n_runs, const int2* rinfo,
+                             unsigned short* idx, int4* xmeta, cudaStream_t s);
+cudaError_t launch_grid_w32(const GridArgs& a, cudaStream_t s);
 int cols_group(int M);
 cudaError_t launch_cols(const ColArgs& a, cudaStream_t s);
 cudaError_t launch_rows(const RowArgs& a, cudaStream_t s);

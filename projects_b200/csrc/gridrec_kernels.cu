@@ -493,8 +493,8 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
   extern __shared__ float2 sm[];
   float2* tw = sm;
   float2* buf = sm + kTwSlots;
-  // wide layout: pairs vary fastest, so the 16 pairs sharing each 512-byte span
-  // of the interleaved spectra write it at about the same time
+  // wide layouts: pairs vary fastest, so the 16 or 32 pairs sharing each 512- or
+  // 1024-byte span of the interleaved spectra write it at about the same time
   const int n = a.wide ? blockIdx.y : blockIdx.x, pair = a.wide ? blockIdx.x : blockIdx.y;
   const int tid = threadIdx.x, nthr = blockDim.x;
   load_twiddles(tw, a.tw, a.pdim);
@@ -527,26 +527,32 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
   for (int idx = 0; idx < 16; ++idx) buf[swz(tid + nthr * out_index(idx, Rl))] = v[idx];
   __syncthreads();
   const float4* pq = a.pq + (size_t)pair * a.J;
-  // plain: [pair][dir][j]; wide: [pair / 16][dir][j / 4][pair % 16][j % 4], so each
-  // pair still writes whole 32-byte sectors and the 16-pair gridding kernel
-  // stages a run of 16 pairs as one contiguous range
+  // plain: [pair][dir][j]; wide (G = 16 or 32 pairs): [pair / G][dir][j / 4][pair % G][j % 4],
+  // so each pair still writes whole 32-byte sectors and the gridding kernel stages a
+  // run of G pairs as one contiguous range.  For G = 32 sample j of pair p sits at
+  // position (j % 4) ^ ((p / 4) % 4) of p's chunk: the 16 lanes of a half-warp that
+  // read one sample of 16 pairs then hit 16 distinct bank pairs.
   float2* o1;
   float2* o2;
-  int qshift, qmask;
+  int qshift, qmask, qlog, rot = 0;
   if (a.wide) {
-    const size_t per_dir = (size_t)(a.J >> 2) * 64;
-    o1 = a.spec + ((size_t)(pair >> 4) * 2 * a.n_ang + 2 * n) * per_dir + (pair & 15) * 4;
+    const int G = a.wide;
+    qlog = G == 32 ? 7 : 6;  // float2 per quad: 4 samples x G pairs
+    const size_t per_dir = (size_t)(a.J >> 2) << qlog;
+    o1 = a.spec + ((size_t)(pair / G) * 2 * a.n_ang + 2 * n) * per_dir + (pair % G) * 4;
     o2 = o1 + per_dir;
     qshift = 2;
     qmask = 3;
+    if (G == 32) rot = (pair >> 2) & 3;
   } else {
     o1 = a.spec + ((size_t)pair * a.n_ang + n) * 2 * a.J;
     o2 = o1 + a.J;
     qshift = 30;
     qmask = 0x3fffffff;
+    qlog = 6;
   }
   for (int j = tid; j < a.J; j += nthr) {
-    const int oj = ((j >> qshift) << 6) + (j & qmask);
+    const int oj = ((j >> qshift) << qlog) + ((j & qmask) ^ rot);
     float2 c1 = make_float2(0.f, 0.f), c2 = make_float2(0.f, 0.f);
     if (j > 0) {
       const float2 F = buf[swz(j)];
@@ -1088,6 +1094,297 @@ __global__ void __launch_bounds__(256) split_reduce_wide_kernel(GridArgs a) {
     if (p == 0 || q == 0) sum = 0.f;
     float* Hf = reinterpret_cast<float*>(a.H + (size_t)(pg0 + (l >> 1)) * MM);
     Hf[((size_t)p * a.M + q) * 2 + (l & 1)] = sum;
+  }
+}
+
+// ------------------------------------------------------------------ gridding, 32 pairs per warp
+// The gather of grid_wide_kernel (same work list, taps, weights and positions)
+// with one complex value per lane: lane p carries (re, im) of pair p of a group
+// of kW32Pairs pairs, and each cell's accumulator is one packed (re, im) register
+// pair.  Per sample the row products x_r = w(|u - r|) value take one packed
+// multiply with the row weight doubled, and each cell adds w(|v - c|) x_r with
+// one packed FMA with the column weight doubled.  Per element that is the
+// rounding and the summation order of grid_wide_kernel, whose output this
+// kernel reproduces bit for bit from the same work list, for twice the pairs
+// per instruction and per unit of run and item bookkeeping.
+// Per run one lane issues two 1-D bulk copies (cp.async.bulk global -> shared,
+// completed on the buffer's mbarrier; no multicast): the run's spectra quads,
+// 1 KB each (4 samples x 32 pairs), and its 16-bit table indices.  The spectra
+// kernel rotates each pair's 4 samples inside its 32-byte chunk, so the 16 lanes
+// of a half-warp read one sample of 16 pairs from 16 distinct bank pairs with
+// one 8-byte load, in place.  Copies run one run ahead (two buffers per warp).
+// The lanes expand the run's indices once, through a shared copy of the table
+// with a zero entry appended, into doubled weights.  Every wait is bounded: on
+// a timeout the warp records it in the error word, waits a second bounded time
+// for its copies and returns.  At the end of an item the warp transposes its
+// 32 cells x 32 pairs through shared memory, so each store writes whole 64-byte
+// row segments of H.
+
+constexpr int kW32Bufs = 2;
+constexpr int kW32QuadBytes = 4 * kW32Pairs * 8;                      // 1 KB
+constexpr int kW32ValBytes = kWideQuads * kW32QuadBytes;              // a run spans <= 5 quads
+constexpr int kW32IdxBytes = (kRunMaxW * kWideRec * 2 + 15) & ~15;    // 384
+constexpr int kW32BufBytes = kW32ValBytes + kW32IdxBytes;
+constexpr int kW32DblBytes = kRunMaxW * kWideRec * 8;                 // doubled weights of a run
+constexpr int kW32RowBytes = (kWideRows * kWideCols + 2) * 8;         // transposition row per pair
+constexpr int kW32WarpBytes = kW32Bufs * kW32BufBytes + kW32DblBytes;
+static_assert(kW32Pairs * kW32RowBytes <= kW32WarpBytes, "the transposition fits the warp's buffers");
+static_assert(kW32WarpBytes % 16 == 0 && kW32BufBytes % 16 == 0 && kW32ValBytes % 16 == 0,
+              "bulk-copy destinations are 16-byte aligned");
+static_assert(kWideRows == 4 && kWideCols == 8 && kWideRec == 12, "index record layout");
+
+__host__ __device__ constexpr int w32_table_bytes(int ltbl) { return ((ltbl + 2) * 4 + 15) & ~15; }
+
+__device__ __forceinline__ unsigned long long fmul2(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+
+// Applies the n samples of one run to the 4 x 8 register tile over column pairs
+// C0..C1.  vb: the run's staged quads; sample s sits at quad (t0 + s) / 4,
+// position ((t0 + s) % 4) ^ rot of this lane's 32-byte chunk (lane_off = 32 lane,
+// rot8 = 8 rot); dbl: per sample 6 x 16 bytes of doubled weights, rows 0..3
+// then columns 0..7.
+template <int C0, int C1>
+__device__ __forceinline__ void w32_apply_run(unsigned long long (&acc)[kWideRows][kWideCols],
+                                              const unsigned char* vb, const ulonglong2* dbl,
+                                              int n, int t0, int lane_off, int rot8) {
+  for (int s = 0; s < n; ++s) {
+    const int t = t0 + s;
+    const unsigned long long v = *reinterpret_cast<const unsigned long long*>(
+        vb + ((t << 8) & ~1023) + lane_off + (((t & 3) << 3) ^ rot8));
+    const ulonglong2 r01 = dbl[s * 6], r23 = dbl[s * 6 + 1];
+    const unsigned long long x[kWideRows] = {fmul2(r01.x, v), fmul2(r01.y, v), fmul2(r23.x, v),
+                                             fmul2(r23.y, v)};  // wu * value, (re, im)
+#pragma unroll
+    for (int c2 = C0; c2 <= C1; ++c2) {
+      const ulonglong2 w = dbl[s * 6 + 2 + c2];  // (wv_c, wv_c), (wv_c+1, wv_c+1)
+#pragma unroll
+      for (int rr = 0; rr < kWideRows; ++rr) {
+        ffma2(acc[rr][2 * c2], w.x, x[rr]);
+        ffma2(acc[rr][2 * c2 + 1], w.y, x[rr]);
+      }
+    }
+  }
+}
+
+// The 16-bit table indices of every (run, sample) of the 16-pair work list, once
+// per list: min((int)(|u - r| tblspcg + 0.5), ltbl) for the 4 rows and 8 columns
+// of the run's sub-tile where the distance is within L/2, else the zero entry
+// ltbl + 1, at the positions grid_wide_kernel's weights use.  Thread r takes run
+// r (rinfo[r] = {index block in 16-byte units, sub-tile}) and writes its record
+// {first quad, index block, n | (jlo & 3) << 5 | quads << 8 | column-pair range << 12}.
+__global__ void __launch_bounds__(128) w32_index_kernel(GridArgs a, int n_runs, const int2* rinfo,
+                                                        unsigned short* idx, int4* xmeta) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= n_runs) return;
+  const Run run = a.runs[r];
+  const int2 ri = rinfo[r];
+  const int tu = ri.y / a.tiles_v, tv = ri.y - (ri.y / a.tiles_v) * a.tiles_v;
+  const int p0 = tu * kWideRows, q0 = tv * kWideCols;
+  const double offu = (double)(a.M / 2 - (p0 & ~(kTile - 1))), subu = (double)(p0 & (kTile - 1));
+  const double offv = (double)(a.M / 2 - (q0 & ~(kTile - 1))), subv = (double)(q0 & (kTile - 1));
+  const double2 d = a.dir[run.dir];
+  const double L2d = a.L2, tsd = a.tblspcg;
+  const unsigned short zero = (unsigned short)(a.ltbl + 1);
+  unsigned short* w = idx + (size_t)ri.x * 8;
+  unsigned cols = 0;
+  for (int j = run.jlo; j <= run.jhi; ++j, w += kWideRec) {
+    const double u = fma((double)j, d.x, offu) - subu, v = fma((double)j, d.y, offv) - subv;
+#pragma unroll
+    for (int k = 0; k < kWideRows; ++k) {
+      const double dd = fabs(u - (double)k);
+      w[k] = dd <= L2d ? (unsigned short)min(table_index64(dd, tsd), a.ltbl) : zero;
+    }
+#pragma unroll
+    for (int k = 0; k < kWideCols; ++k) {
+      const double dd = fabs(v - (double)k);
+      w[kWideRows + k] = dd <= L2d ? (unsigned short)min(table_index64(dd, tsd), a.ltbl) : zero;
+      if (dd <= L2d) cols |= 1u << k;
+    }
+  }
+  const int n = run.jhi - run.jlo + 1, nq = (run.jhi >> 2) - (run.jlo >> 2) + 1;
+  const int code = cols ? ((__ffs(cols) - 1) >> 1) * 4 + ((31 - __clz(cols)) >> 1) : kWideNoReach;
+  xmeta[r] = make_int4(run.dir * (a.J >> 2) + (run.jlo >> 2), ri.x,
+                       n | ((run.jlo & 3) << 5) | (nq << 8) | (code << 12), 0);
+}
+
+__global__ void __launch_bounds__(kWideWarps * 32, kW32MinBlocks) grid_w32_kernel(GridArgs a) {
+  extern __shared__ __align__(128) unsigned char smx[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const int tbl_bytes = w32_table_bytes(a.ltbl);
+  float* tbl = reinterpret_cast<float*>(smx);
+  uint64_t* bars = reinterpret_cast<uint64_t*>(smx + tbl_bytes) + warp * kW32Bufs;
+  unsigned char* wbuf = smx + tbl_bytes + kWideWarps * kW32Bufs * 8 + warp * kW32WarpBytes;
+  ulonglong2* dbl = reinterpret_cast<ulonglong2*>(wbuf + kW32Bufs * kW32BufBytes);
+  for (int i = threadIdx.x; i <= a.ltbl; i += blockDim.x) tbl[i] = __ldg(&a.wtbl[i]);
+  if (threadIdx.x == 0) tbl[a.ltbl + 1] = 0.f;
+  if (lane == 0) {
+    for (int b = 0; b < kW32Bufs; ++b) mbar_init(&bars[b], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();  // table and barriers ready before any use
+  const int groups = (a.pairs + kW32Pairs - 1) / kW32Pairs;
+  const unsigned total = (unsigned)a.n_items * (unsigned)groups;
+  const size_t group_bytes = (size_t)a.n_ang * 2 * a.J * kW32Pairs * 8;
+  const size_t MM = (size_t)a.M * a.M;
+  const int lane_off = lane * 32, rot8 = ((lane >> 2) & 3) << 3;
+  const unsigned char* idxb = reinterpret_cast<const unsigned char*>(a.xidx);
+  unsigned phase = 0;     // bit b: parity of bars[b]'s next phase
+  unsigned inflight = 0;  // bit b: a copy into buffer b is issued and not yet consumed
+  int cur = 0;            // buffer of the next run to consume
+  bool failed = false;
+  for (;;) {
+    unsigned w = 0;
+    if (lane == 0) w = atomicAdd(a.queue, 1u);
+    w = __shfl_sync(0xffffffffu, w, 0);
+    if (w >= total) break;
+    const int grp = (int)(w / (unsigned)a.n_items);
+    const Item it = a.items[w - (unsigned)grp * (unsigned)a.n_items];
+    const int pg0 = grp * kW32Pairs;
+    const int np = min(kW32Pairs, a.pairs - pg0);
+    const int tu = it.tile / a.tiles_v;
+    const int tv = it.tile - tu * a.tiles_v;
+    const int p0 = tu * kWideRows, q0 = tv * kWideCols;
+    const unsigned char* specg = reinterpret_cast<const unsigned char*>(a.spec) + (size_t)grp * group_bytes;
+    unsigned long long acc[kWideRows][kWideCols];
+#pragma unroll
+    for (int r = 0; r < kWideRows; ++r)
+#pragma unroll
+      for (int c = 0; c < kWideCols; ++c) acc[r][c] = 0ull;
+    // run m's quads and indices into buffer b (one lane issues, all lanes track)
+    auto issue = [&](const int4& m, int b) {
+      if (lane == 0) {
+        const unsigned n = (unsigned)m.z & 31u, nq = ((unsigned)m.z >> 8) & 7u;
+        const unsigned vbytes = nq * kW32QuadBytes, ibytes = (n * (kWideRec * 2) + 15u) & ~15u;
+        unsigned char* dst = wbuf + b * kW32BufBytes;
+        fence_proxy_async();  // this warp's earlier shared accesses before the copy's writes
+        mbar_expect_tx(&bars[b], vbytes + ibytes);
+        bulk_g2s(dst, specg + (size_t)m.x * kW32QuadBytes, vbytes, &bars[b]);
+        bulk_g2s(dst + kW32ValBytes, idxb + (size_t)m.y * 16, ibytes, &bars[b]);
+      }
+      inflight |= 1u << b;
+    };
+    // A sub-tile that no sample reaches has an empty item (rb == re): nothing is
+    // read and its cells are written as zeros.
+    const int rb = it.run_begin, re = it.run_end;
+    int4 mA = make_int4(0, 0, 0, 0), mB = mA;
+    if (rb < re) {
+      mA = __ldg(&a.xmeta[rb]);
+      issue(mA, cur);
+    }
+    if (rb + 1 < re) {
+      mB = __ldg(&a.xmeta[rb + 1]);
+      issue(mB, cur ^ 1);
+    }
+    for (int r = rb; r < re; ++r) {
+      int4 mC = mB;
+      if (r + 2 < re) mC = __ldg(&a.xmeta[r + 2]);  // read early: its copies follow run r
+      const int b = cur;
+      const bool ok = mbar_wait(&bars[b], (phase >> b) & 1u);
+      if (__any_sync(0xffffffffu, !ok)) {
+        failed = true;
+        break;
+      }
+      phase ^= 1u << b;
+      inflight &= ~(1u << b);
+      const unsigned char* vb = wbuf + b * kW32BufBytes;
+      const unsigned short* ib = reinterpret_cast<const unsigned short*>(vb + kW32ValBytes);
+      const int n = mA.z & 31;
+      float2* d2 = reinterpret_cast<float2*>(dbl);
+      for (int i = lane; i < n * kWideRec; i += 32) {
+        const float wv = tbl[ib[i]];
+        d2[i] = make_float2(wv, wv);
+      }
+      __syncwarp();
+      const int t0 = (mA.z >> 5) & 3;
+      // the run's samples over the column pairs some sample reaches (the other
+      // pairs would only add zero products)
+      switch ((mA.z >> 12) & 31) {
+        case 0: w32_apply_run<0, 0>(acc, vb, dbl, n, t0, lane_off, rot8); break;
+        case 1: w32_apply_run<0, 1>(acc, vb, dbl, n, t0, lane_off, rot8); break;
+        case 2: w32_apply_run<0, 2>(acc, vb, dbl, n, t0, lane_off, rot8); break;
+        case 3: w32_apply_run<0, 3>(acc, vb, dbl, n, t0, lane_off, rot8); break;
+        case 5: w32_apply_run<1, 1>(acc, vb, dbl, n, t0, lane_off, rot8); break;
+        case 6: w32_apply_run<1, 2>(acc, vb, dbl, n, t0, lane_off, rot8); break;
+        case 7: w32_apply_run<1, 3>(acc, vb, dbl, n, t0, lane_off, rot8); break;
+        case 10: w32_apply_run<2, 2>(acc, vb, dbl, n, t0, lane_off, rot8); break;
+        case 11: w32_apply_run<2, 3>(acc, vb, dbl, n, t0, lane_off, rot8); break;
+        case 15: w32_apply_run<3, 3>(acc, vb, dbl, n, t0, lane_off, rot8); break;
+        default: break;  // kWideNoReach: no sample reaches the sub-tile
+      }
+      __syncwarp();  // buffer b and the weights read by every lane before they are refilled
+      if (r + 2 < re) issue(mC, b);
+      mA = mB;
+      mB = mC;
+      cur ^= 1;
+    }
+    if (failed) break;
+    // no copy is in flight now: the transposition reuses the warp's buffers
+    if (it.slot < 0) {
+      unsigned char* tr = wbuf;
+#pragma unroll
+      for (int rr = 0; rr < kWideRows; ++rr)
+#pragma unroll
+        for (int c2 = 0; c2 < kWideCols / 2; ++c2)
+          *reinterpret_cast<ulonglong2*>(tr + lane * kW32RowBytes + (rr * kWideCols + 2 * c2) * 8) =
+              make_ulonglong2(acc[rr][2 * c2], acc[rr][2 * c2 + 1]);
+      __syncwarp();
+      // chunk k * 32 + lane: pair P, row rr, cells 2h and 2h + 1
+#pragma unroll 4
+      for (int k = 0; k < kW32Pairs * kWideRows * (kWideCols / 2) / 32; ++k) {
+        const int ch = k * 32 + lane;
+        const int P = ch >> 4, rr = (ch >> 2) & 3, h = ch & 3;
+        float4 v = *reinterpret_cast<const float4*>(tr + P * kW32RowBytes + (rr * kWideCols + 2 * h) * 8);
+        const int p = p0 + rr, q = q0 + 2 * h;
+        if (p == 0) v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (q == 0) v.x = v.y = 0.f;
+        if (P < np) *reinterpret_cast<float4*>(a.H + (size_t)(pg0 + P) * MM + (size_t)p * a.M + q) = v;
+      }
+      __syncwarp();  // the transposition area is read before copies land in it again
+    } else {
+      // partial sub-tile of a split sub-tile: [cell][lane] complex, summed by split_reduce_w32_kernel
+      unsigned long long* part = reinterpret_cast<unsigned long long*>(a.scratch) +
+                                 ((size_t)grp * a.n_slots + it.slot) * (kWideRows * kWideCols * 32);
+#pragma unroll
+      for (int rr = 0; rr < kWideRows; ++rr)
+#pragma unroll
+        for (int c = 0; c < kWideCols; ++c) part[(rr * kWideCols + c) * 32 + lane] = acc[rr][c];
+    }
+  }
+  if (failed) {
+    if (lane == 0) atomicExch(a.err, 1);
+    // let the copies in flight land before the CTA's shared memory is released
+    for (int b = 0; b < kW32Bufs; ++b)
+      if ((inflight >> b) & 1u) mbar_wait(&bars[b], (phase >> b) & 1u);
+  }
+}
+
+// Sums the partial sub-tiles of every split sub-tile in slot order and writes H.
+// Grid: (split sub-tiles, pair groups of 32); 256 threads over (cell, pair).
+__global__ void __launch_bounds__(256) split_reduce_w32_kernel(GridArgs a) {
+  const int4 sp = a.split_list[blockIdx.x];  // (tile, slot0, nsplit, -)
+  const int grp = blockIdx.y;
+  const int pg0 = grp * kW32Pairs;
+  const int np = min(kW32Pairs, a.pairs - pg0);
+  const int tu = sp.x / a.tiles_v, tv = sp.x - (sp.x / a.tiles_v) * a.tiles_v;
+  const int p0 = tu * kWideRows, q0 = tv * kWideCols;
+  const float2* base = reinterpret_cast<const float2*>(a.scratch) +
+                       ((size_t)grp * a.n_slots + sp.y) * (kWideRows * kWideCols * 32);
+  const size_t MM = (size_t)a.M * a.M;
+  for (int i = threadIdx.x; i < kWideRows * kWideCols * 32; i += blockDim.x) {
+    const int cell = i >> 5, l = i & 31;
+    if (l >= np) continue;
+    float2 sum = make_float2(0.f, 0.f);
+    for (int k = 0; k < sp.z; ++k) {
+      const float2 v = __ldg(&base[(size_t)k * (kWideRows * kWideCols * 32) + i]);
+      sum.x += v.x;
+      sum.y += v.y;
+    }
+    const int p = p0 + cell / kWideCols, q = q0 + cell % kWideCols;
+    if (p == 0 || q == 0) sum = make_float2(0.f, 0.f);
+    a.H[(size_t)(pg0 + l) * MM + (size_t)p * a.M + q] = sum;
   }
 }
 
@@ -1634,6 +1931,7 @@ cudaError_t init_kernel_attributes() {
   fns.push_back((const void*)grid_kernel<kMaxTaps>);
   fns.push_back((const void*)grid_wide_kernel);
   fns.push_back((const void*)grid_tc_kernel);
+  fns.push_back((const void*)grid_w32_kernel);
   for (const void* f : fns) {
     if (e != cudaSuccess) break;
     e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
@@ -1732,6 +2030,38 @@ cudaError_t launch_grid_wide(const GridArgs& a, cudaStream_t s) {
   if (e != cudaSuccess || a.n_split_tiles == 0) return e;
   dim3 rgrid(a.n_split_tiles, (unsigned)groups);
   split_reduce_wide_kernel<<<rgrid, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+static int grid_w32_smem_bytes(int ltbl) {
+  return w32_table_bytes(ltbl) + kWideWarps * kW32Bufs * 8 + kWideWarps * kW32WarpBytes;
+}
+
+cudaError_t launch_w32_index(const GridArgs& a, int n_runs, const int2* rinfo,
+                             unsigned short* idx, int4* xmeta, cudaStream_t s) {
+  if (n_runs == 0) return cudaSuccess;
+  w32_index_kernel<<<(n_runs + 127) / 128, 128, 0, s>>>(a, n_runs, rinfo, idx, xmeta);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_grid_w32(const GridArgs& a, cudaStream_t s) {
+  if (a.n_items == 0) return cudaSuccess;
+  cudaError_t e = cudaMemsetAsync(a.queue, 0, sizeof(unsigned), s);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int smem = grid_w32_smem_bytes(a.ltbl);
+  int per_sm = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_w32_kernel, kWideWarps * 32, smem);
+  const long groups = (a.pairs + kW32Pairs - 1) / kW32Pairs;
+  const long want = ((long)a.n_items * groups + kWideWarps - 1) / kWideWarps;
+  const int blocks = (int)std::min<long>(want, (long)std::max(per_sm, 1) * sms);
+  grid_w32_kernel<<<blocks, kWideWarps * 32, smem, s>>>(a);
+  e = cudaGetLastError();
+  if (e != cudaSuccess || a.n_split_tiles == 0) return e;
+  dim3 rgrid(a.n_split_tiles, (unsigned)groups);
+  split_reduce_w32_kernel<<<rgrid, 256, 0, s>>>(a);
   return cudaGetLastError();
 }
 

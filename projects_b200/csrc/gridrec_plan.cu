@@ -1439,7 +1439,7 @@ extern "C" int gr_reconstruct_pair_noalloc(gr_plan* p, const float* sino1, const
   const size_t off_part = align256(off_H + (size_t)p->M * p->M * sizeof(float2));
   const size_t off_queue =
       align256(off_part + (size_t)std::max(p->n_slots, 1) * kTile * kTile * sizeof(float4));
-  const size_t need = off_queue + 256;
+  const size_t need = off_queue + sizeof(unsigned);
   if (need > kNoallocBytes)
     return fail(GR_ERR_UNSUPPORTED,
                 "gr_reconstruct_pair_noalloc: %d x %d needs %zu bytes of scratch, the static "
@@ -1469,13 +1469,14 @@ extern "C" int gr_reconstruct_pair_noalloc(gr_plan* p, const float* sino1, const
               p->d_dir, p->d_wtbl, p->n_items, 1, p->n_ang, p->J, p->M, p->tiles_v, p->n_slots,
               p->ltbl, p->L / 2, 2.0 * p->ltbl / p->L};
   GR_CUDA(launch_grid(ga, p->ntaps, st));
-  int* err = reinterpret_cast<int*>(base + off_queue + 64);
-  GR_CUDA(cudaMemsetAsync(err, 0, sizeof(int), st));
-  ColArgs ca{H, p->d_tw_m, p->M, 1, err};
+  // the plan's own error word (allocated with the plan): a bounded-wait timeout of
+  // the column FFT is reported by gr_plan_device_status, as for the plan's other calls
+  ColArgs ca{H, p->d_tw_m, p->M, 1, p->d_err, p->cols_G};
   GR_CUDA(launch_cols(ca, st));
   RowArgs ra{H, p->d_tw_m, p->d_winv, out1, o2, 0, out_stride, n_valid, p->M, p->M0, p->M02, 1};
   GR_CUDA(launch_rows(ra, st));
-  p->launches += 5;
+  // phase, spectra, grid (+ split reduction when tiles are split), cols, rows
+  p->launches += 5 + (ga.n_items > 0 && ga.n_split_tiles > 0 ? 1 : 0);
   return GR_OK;
 }
 

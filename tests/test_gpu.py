@@ -287,6 +287,52 @@ def test_full_size_2048x1500_and_linearity():
     assert ph.rel_l2(gl[0], 2 * g[0] - g[1]) < TOL
 
 
+def _oracle_pairs_rel_l2(sinos, centers, th, got, filter):
+    """relL2 of every slice of `got` against float64 gridrec, pairs (2k, 2k+1) with
+    their own centres; the oracle runs on host threads (its C calls release the GIL)."""
+    import concurrent.futures as cf
+    M0 = got.shape[1]
+
+    def one(k):
+        r1, r2 = O.port_gridrec_pair(sinos[2 * k], sinos[2 * k + 1], th,
+                                     center1=float(centers[2 * k]),
+                                     center2=float(centers[2 * k + 1]), filter=filter)
+        return (ph.rel_l2(got[2 * k], r1[:, :M0]), ph.rel_l2(got[2 * k + 1], r2[:, :M0]))
+
+    with cf.ThreadPoolExecutor(8) as ex:
+        return [e for pair in ex.map(one, range(len(sinos) // 2)) for e in pair]
+
+
+@pytest.mark.parametrize("max_pairs", [16])
+def test_bench_chunk_2048x1500_against_float64(max_pairs):
+    """The benchmark's own configuration at full size: one chunk of max_pairs pairs
+    of 2048 x 1500 random-ellipse slices (seed = slice index, per-slice centres
+    1024 + U[-2, 2], Hann), autotuned plan, through the gridding kernel the
+    benchmark's chunks use; every slice against float64 gridrec."""
+    n, a = 2048, 1500
+    th = ph.angles_deg(a)
+    S = 2 * max_pairs
+    sinos = torch.empty((S, a, n), device="cuda")
+    centers = np.zeros(S, np.float32)
+    for i in range(S):
+        s, c = ph.random_ellipse_sinogram(i, n, a, device="cuda")
+        sinos[i].copy_(s)
+        centers[i] = c
+    with G.Plan(n, a, th, filter=G.FILTER_HANN, max_pairs=max_pairs) as plan:
+        assert plan.grid_kernel(max_pairs) == "wide"
+        plan.autotune()
+        o = torch.zeros((S, plan.M0, n), device="cuda")
+        plan.reconstruct_batch(sinos, o, centers=_dev(centers))
+        torch.cuda.synchronize()
+        plan.device_status()
+        got = o[:, :, :plan.M0].cpu().numpy()
+    del o
+    errs = _oracle_pairs_rel_l2(sinos.cpu().numpy(), centers, th, got, G.FILTER_HANN)
+    print(f"bench chunk {max_pairs} pairs 2048x1500: relL2 vs float64 worst {max(errs):.2e} "
+          f"median {float(np.median(errs)):.2e}")
+    assert max(errs) < FULL_SIZE_TOL
+
+
 def test_bounded_wait_timeout_is_reported():
     """Failure detection without a fault: a wait that nothing completes runs
     out, the kernel returns, and the host reads GR_ERR_TIMEOUT."""
