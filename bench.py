@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--slices", type=int, default=256)
     ap.add_argument("--n-det", type=int, default=2048)
     ap.add_argument("--n-ang", type=int, default=1500)
-    ap.add_argument("--max-pairs", type=int, default=16)
+    ap.add_argument("--max-pairs", type=int, default=32)
     ap.add_argument("--dtype", default="f32", choices=["f32", "f16", "bf16"])
     ap.add_argument("--e2e-steps", type=int, default=10)
     ap.add_argument("--no-e2e", action="store_true")
@@ -511,10 +511,13 @@ def run_b200(args, rank, world, local_rank):
     peak, peak_src = peaks()
     traffic = traffic_from_profile(dominant, min(args.max_pairs, (S + 1) // 2), n, a)
     traffic_note = ("ncu DRAM read + write of one launch (profiles/traffic_%dx%d.txt)" % (n, a))
-    if dominant == "grid" and plan.grid_kernel(args.max_pairs) == "wide":
+    gk = plan.grid_kernel(args.max_pairs)
+    if dominant == "grid" and gk == "wide32":
+        traffic_note += ("; includes the 32-pair kernel's table indices (24 bytes per sample "
+                         "and 4x8 sub-tile, read once per launch for its 32 pairs)")
+    elif dominant == "grid" and gk == "wide":
         traffic_note += ("; includes the 16-pair kernel's precomputed weights (48 bytes per "
-                         "sample and 4x8 sub-tile, read once per launch for its 16 pairs), "
-                         "which replace an in-kernel weight pass")
+                         "sample and 4x8 sub-tile, read once per launch for its 16 pairs)")
     per_launch_bytes = bytes_total / max(n_launch, 1)
     stages = {k: {"ms_per_pair": v / pairs_timed,
                   "gbs": bpp[k] * pairs_timed / max(v / 1000.0, 1e-12) / 1e9}
@@ -580,7 +583,8 @@ def run_b200(args, rank, world, local_rank):
                                    f"of {n} det x {a} angles per step, Hann, per-slice centres "
                                    f"{n // 2}+U[-2,2], output {plan.M0}^2 in {n}-stride f32",
                        "n_det": n, "n_ang": a, "slices_per_step": S,
-                       "pairs_per_launch": args.max_pairs, "parallelism": f"slices x{world}",
+                       "pairs_per_launch": args.max_pairs, "grid_kernel": gk,
+                       "parallelism": f"slices x{world}",
                        "launch": f"one CUDA graph per step ({launches // args.steps} kernels); "
                                  f"stage times from {stage_steps} eager steps with events",
                        "tuning": tuning,

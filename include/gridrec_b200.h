@@ -96,11 +96,14 @@ typedef struct {
                               (0 = 1) */
   float roi_x0, roi_y0;    /* ROI offset X0, Y0: C1 times exp(-i j (X0 cos + Y0 sin) pi),
                               C2 times its conjugate */
-  int wide_grid;           /* gridding kernel: 0 = 16-pair kernel for chunks of >= 7 pairs
-                              (default), 1 = for every chunk, -1 = never (2 pairs per warp
-                              over 32 x 32 tiles), 2 = tensor-core kernel (tcgen05, 3xTF32)
-                              for every chunk; same taps and weights, the sums differ only
-                              in order (and, for 2, in ~2^-22 relative rounding per term) */
+  int wide_grid;           /* gridding kernel: 0 (default) = 32-pair kernel for chunks of
+                              more than 16 pairs, 16-pair kernel for 7..16 pairs, else the
+                              tile kernel; 1 = 16-pair kernel for every chunk, -1 = never
+                              (2 pairs per warp over 32 x 32 tiles), 2 = tensor-core kernel
+                              (tcgen05, 3xTF32) for every chunk, 3 = 32-pair kernel for
+                              every chunk.  Same taps and weights; the sums differ only in
+                              order (the 32- and 16-pair kernels agree bit for bit) and, for
+                              2, in ~2^-22 relative rounding per term */
 } gr_params;
 
 typedef struct gr_plan gr_plan;
@@ -229,8 +232,8 @@ int gr_worklist_export(const gr_params* p, int* n_items, int* n_runs, int* tiles
  * splits then holds 2 * tiles_v * tiles_v records (M/4 tile rows of M/8 tiles). */
 int gr_worklist_export_wide(const gr_params* p, int* n_items, int* n_runs, int* tiles_v,
                             int* items, int* runs, int* splits, int cap_items, int cap_runs);
-/* *wide = 0 (tile kernel), 1 (16-pair kernel) or 2 (tensor-core kernel) for a chunk of
- * `pairs` pairs. */
+/* *wide = 0 (tile kernel), 1 (16-pair kernel), 2 (tensor-core kernel) or 3 (32-pair
+ * kernel) for a chunk of `pairs` pairs. */
 int gr_plan_grid_kernel(const gr_plan* plan, int pairs, int* wide);
 
 /* Text of the last error recorded on this thread (never NULL). */

@@ -102,8 +102,8 @@ struct SpectraArgs {
   int n_det, n_ang, pdim, J, pairs;
   const double* roi_off; // per angle (X0 cos + Y0 sin) pi of the ROI offset, or null
   // 0: plain [pair][dir][j]; 16 or 32: the 16- or 32-pair gridding kernel's
-  // interleaved layout [pair / G][dir][j / 4][pair % G][j % 4] (G = wide), for G = 32
-  // with position (j % 4) ^ ((pair / 4) % 4) inside each pair's 32-byte chunk
+  // [pair / G][dir][j / 4][pair % G][j % 4] (G = wide), for G = 32 with the two
+  // 16-byte halves of a pair's chunk swapped when (pair / 4) is odd
   int wide = 0;
 };
 
@@ -139,9 +139,9 @@ struct GridArgs {
   // {first sample's record, column-pair range}, from launch_wide_weights
   const float* wts = nullptr;
   const int2* wmeta = nullptr;
-  // grid_w32_kernel: per run {quad of its first sample (direction * J/4 + jlo/4),
-  // index block (16-byte units), n | (jlo & 3) << 5 | quads << 8 | column-pair
-  // range << 12, 0}, and the 16-bit table indices (launch_w32_index)
+  // grid_w32_kernel: per run {first quad (direction * J / 4 + jlo / 4), index
+  // block (16-byte units), n | (jlo % 4) << 5 | column-pair range << 12, 0}, and
+  // the 16-bit table indices (launch_w32_index)
   const int4* xmeta = nullptr;
   const unsigned short* xidx = nullptr;
 };

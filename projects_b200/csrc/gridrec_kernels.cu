@@ -529,9 +529,10 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
   const float4* pq = a.pq + (size_t)pair * a.J;
   // plain: [pair][dir][j]; wide (G = 16 or 32 pairs): [pair / G][dir][j / 4][pair % G][j % 4],
   // so each pair still writes whole 32-byte sectors and the gridding kernel stages a
-  // run of G pairs as one contiguous range.  For G = 32 sample j of pair p sits at
-  // position (j % 4) ^ ((p / 4) % 4) of p's chunk: the 16 lanes of a half-warp that
-  // read one sample of 16 pairs then hit 16 distinct bank pairs.
+  // run of G pairs as one contiguous range.  For G = 32 the two 16-byte halves of
+  // pair p's chunk are swapped when (p / 4) is odd (sample j at position
+  // (j % 4) ^ (2 ((p / 4) % 2))): the 32-pair kernel's lanes then read their chunks
+  // with two conflict-free 16-byte loads.
   float2* o1;
   float2* o2;
   int qshift, qmask, qlog, rot = 0;
@@ -543,7 +544,7 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
     o2 = o1 + per_dir;
     qshift = 2;
     qmask = 3;
-    if (G == 32) rot = (pair >> 2) & 3;
+    if (G == 32) rot = ((pair >> 2) & 1) << 1;
   } else {
     o1 = a.spec + ((size_t)pair * a.n_ang + n) * 2 * a.J;
     o2 = o1 + a.J;
@@ -1109,10 +1110,11 @@ __global__ void __launch_bounds__(256) split_reduce_wide_kernel(GridArgs a) {
 // per instruction and per unit of run and item bookkeeping.
 // Per run one lane issues two 1-D bulk copies (cp.async.bulk global -> shared,
 // completed on the buffer's mbarrier; no multicast): the run's spectra quads,
-// 1 KB each (4 samples x 32 pairs), and its 16-bit table indices.  The spectra
-// kernel rotates each pair's 4 samples inside its 32-byte chunk, so the 16 lanes
-// of a half-warp read one sample of 16 pairs from 16 distinct bank pairs with
-// one 8-byte load, in place.  Copies run one run ahead (two buffers per warp).
+// 1 KB each (4 samples x 32 pairs, each pair's 4 samples one 32-byte chunk whose
+// halves the spectra kernel swaps for every other group of 4 pairs), and its
+// 16-bit table indices.  Each lane then loads its pair's 4 samples of a quad with
+// two conflict-free 16-byte loads and applies them from registers.  Copies run
+// kW32Bufs - 1 runs ahead (kW32Bufs buffers per warp).
 // The lanes expand the run's indices once, through a shared copy of the table
 // with a zero entry appended, into doubled weights.  Every wait is bounded: on
 // a timeout the warp records it in the error word, waits a second bounded time
@@ -1141,30 +1143,43 @@ __device__ __forceinline__ unsigned long long fmul2(unsigned long long a, unsign
   return r;
 }
 
-// Applies the n samples of one run to the 4 x 8 register tile over column pairs
-// C0..C1.  vb: the run's staged quads; sample s sits at quad (t0 + s) / 4,
-// position ((t0 + s) % 4) ^ rot of this lane's 32-byte chunk (lane_off = 32 lane,
-// rot8 = 8 rot); dbl: per sample 6 x 16 bytes of doubled weights, rows 0..3
-// then columns 0..7.
+// One sample: x_r = w_r * value (packed (re, im)), then every cell of column pairs
+// C0..C1 adds w_c * x_r; d: the sample's 6 x 16 bytes of doubled weights, rows
+// 0..3 then columns 0..7.
+template <int C0, int C1>
+__device__ __forceinline__ void w32_apply_sample(unsigned long long (&acc)[kWideRows][kWideCols],
+                                                 unsigned long long v, const ulonglong2* d) {
+  const ulonglong2 r01 = d[0], r23 = d[1];
+  const unsigned long long x[kWideRows] = {fmul2(r01.x, v), fmul2(r01.y, v), fmul2(r23.x, v),
+                                           fmul2(r23.y, v)};  // wu * value, (re, im)
+#pragma unroll
+  for (int c2 = C0; c2 <= C1; ++c2) {
+    const ulonglong2 w = d[2 + c2];  // (wv_c, wv_c), (wv_c+1, wv_c+1)
+#pragma unroll
+    for (int rr = 0; rr < kWideRows; ++rr) {
+      ffma2(acc[rr][2 * c2], w.x, x[rr]);
+      ffma2(acc[rr][2 * c2 + 1], w.y, x[rr]);
+    }
+  }
+}
+
+// Applies the n samples of one run, at positions t0 .. t0 + n - 1 of its staged
+// quads, to the 4 x 8 register tile over column pairs C0..C1.  qa, qb: this
+// lane's 16-byte halves with samples (0, 1) and (2, 3) of the run's first quad
+// (quads 64 x 16 bytes apart); dbl: the run's doubled weights, 6 x 16 bytes per
+// sample.
 template <int C0, int C1>
 __device__ __forceinline__ void w32_apply_run(unsigned long long (&acc)[kWideRows][kWideCols],
-                                              const unsigned char* vb, const ulonglong2* dbl,
-                                              int n, int t0, int lane_off, int rot8) {
-  for (int s = 0; s < n; ++s) {
-    const int t = t0 + s;
-    const unsigned long long v = *reinterpret_cast<const unsigned long long*>(
-        vb + ((t << 8) & ~1023) + lane_off + (((t & 3) << 3) ^ rot8));
-    const ulonglong2 r01 = dbl[s * 6], r23 = dbl[s * 6 + 1];
-    const unsigned long long x[kWideRows] = {fmul2(r01.x, v), fmul2(r01.y, v), fmul2(r23.x, v),
-                                             fmul2(r23.y, v)};  // wu * value, (re, im)
+                                              const ulonglong2* qa, const ulonglong2* qb,
+                                              const ulonglong2* dbl, int n, int t0) {
+  const int tend = t0 + n;
+  for (int q = 0; 4 * q < tend; ++q) {
+    const ulonglong2 va = qa[q * 64], vb = qb[q * 64];
+    const unsigned long long v[4] = {va.x, va.y, vb.x, vb.y};
 #pragma unroll
-    for (int c2 = C0; c2 <= C1; ++c2) {
-      const ulonglong2 w = dbl[s * 6 + 2 + c2];  // (wv_c, wv_c), (wv_c+1, wv_c+1)
-#pragma unroll
-      for (int rr = 0; rr < kWideRows; ++rr) {
-        ffma2(acc[rr][2 * c2], w.x, x[rr]);
-        ffma2(acc[rr][2 * c2 + 1], w.y, x[rr]);
-      }
+    for (int k = 0; k < 4; ++k) {
+      const int t = 4 * q + k;
+      if (t >= t0 && t < tend) w32_apply_sample<C0, C1>(acc, v[k], dbl + (t - t0) * 6);
     }
   }
 }
@@ -1174,7 +1189,8 @@ __device__ __forceinline__ void w32_apply_run(unsigned long long (&acc)[kWideRow
 // of the run's sub-tile where the distance is within L/2, else the zero entry
 // ltbl + 1, at the positions grid_wide_kernel's weights use.  Thread r takes run
 // r (rinfo[r] = {index block in 16-byte units, sub-tile}) and writes its record
-// {first quad, index block, n | (jlo & 3) << 5 | quads << 8 | column-pair range << 12}.
+// {first quad (direction * J / 4 + jlo / 4), index block, n | (jlo % 4) << 5 |
+// column-pair range << 12}.
 __global__ void __launch_bounds__(128) w32_index_kernel(GridArgs a, int n_runs, const int2* rinfo,
                                                         unsigned short* idx, int4* xmeta) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1204,10 +1220,10 @@ __global__ void __launch_bounds__(128) w32_index_kernel(GridArgs a, int n_runs, 
       if (dd <= L2d) cols |= 1u << k;
     }
   }
-  const int n = run.jhi - run.jlo + 1, nq = (run.jhi >> 2) - (run.jlo >> 2) + 1;
+  const int n = run.jhi - run.jlo + 1;
   const int code = cols ? ((__ffs(cols) - 1) >> 1) * 4 + ((31 - __clz(cols)) >> 1) : kWideNoReach;
   xmeta[r] = make_int4(run.dir * (a.J >> 2) + (run.jlo >> 2), ri.x,
-                       n | ((run.jlo & 3) << 5) | (nq << 8) | (code << 12), 0);
+                       n | ((run.jlo & 3) << 5) | (code << 12), 0);
 }
 
 __global__ void __launch_bounds__(kWideWarps * 32, kW32MinBlocks) grid_w32_kernel(GridArgs a) {
@@ -1228,8 +1244,10 @@ __global__ void __launch_bounds__(kWideWarps * 32, kW32MinBlocks) grid_w32_kerne
   const int groups = (a.pairs + kW32Pairs - 1) / kW32Pairs;
   const unsigned total = (unsigned)a.n_items * (unsigned)groups;
   const size_t group_bytes = (size_t)a.n_ang * 2 * a.J * kW32Pairs * 8;
+  // this lane's halves of its pair's 32-byte chunk: samples (0, 1), then (2, 3)
+  const int swap16 = ((lane >> 2) & 1) * 16;
+  const int off_a = lane * 32 + swap16, off_b = lane * 32 + (16 - swap16);
   const size_t MM = (size_t)a.M * a.M;
-  const int lane_off = lane * 32, rot8 = ((lane >> 2) & 3) << 3;
   const unsigned char* idxb = reinterpret_cast<const unsigned char*>(a.xidx);
   unsigned phase = 0;     // bit b: parity of bars[b]'s next phase
   unsigned inflight = 0;  // bit b: a copy into buffer b is issued and not yet consumed
@@ -1256,8 +1274,9 @@ __global__ void __launch_bounds__(kWideWarps * 32, kW32MinBlocks) grid_w32_kerne
     // run m's quads and indices into buffer b (one lane issues, all lanes track)
     auto issue = [&](const int4& m, int b) {
       if (lane == 0) {
-        const unsigned n = (unsigned)m.z & 31u, nq = ((unsigned)m.z >> 8) & 7u;
-        const unsigned vbytes = nq * kW32QuadBytes, ibytes = (n * (kWideRec * 2) + 15u) & ~15u;
+        const unsigned n = (unsigned)m.z & 31u, t0 = ((unsigned)m.z >> 5) & 3u;
+        const unsigned vbytes = ((t0 + n + 3u) >> 2) * kW32QuadBytes;
+        const unsigned ibytes = (n * (kWideRec * 2) + 15u) & ~15u;
         unsigned char* dst = wbuf + b * kW32BufBytes;
         fence_proxy_async();  // this warp's earlier shared accesses before the copy's writes
         mbar_expect_tx(&bars[b], vbytes + ibytes);
@@ -1269,18 +1288,19 @@ __global__ void __launch_bounds__(kWideWarps * 32, kW32MinBlocks) grid_w32_kerne
     // A sub-tile that no sample reaches has an empty item (rb == re): nothing is
     // read and its cells are written as zeros.
     const int rb = it.run_begin, re = it.run_end;
-    int4 mA = make_int4(0, 0, 0, 0), mB = mA;
-    if (rb < re) {
-      mA = __ldg(&a.xmeta[rb]);
-      issue(mA, cur);
-    }
-    if (rb + 1 < re) {
-      mB = __ldg(&a.xmeta[rb + 1]);
-      issue(mB, cur ^ 1);
+    int4 mq[kW32Bufs];  // records of runs r .. r + kW32Bufs - 1 (the runs in flight)
+#pragma unroll
+    for (int k = 0; k < kW32Bufs; ++k) {
+      mq[k] = make_int4(0, 0, 0, 0);
+      if (rb + k < re) {
+        mq[k] = __ldg(&a.xmeta[rb + k]);
+        issue(mq[k], cur + k < kW32Bufs ? cur + k : cur + k - kW32Bufs);
+      }
     }
     for (int r = rb; r < re; ++r) {
-      int4 mC = mB;
-      if (r + 2 < re) mC = __ldg(&a.xmeta[r + 2]);  // read early: its copies follow run r
+      int4 mn = make_int4(0, 0, 0, 0);
+      if (r + kW32Bufs < re) mn = __ldg(&a.xmeta[r + kW32Bufs]);  // read early: issued after run r
+      const int4 mA = mq[0];
       const int b = cur;
       const bool ok = mbar_wait(&bars[b], (phase >> b) & 1u);
       if (__any_sync(0xffffffffu, !ok)) {
@@ -1298,27 +1318,25 @@ __global__ void __launch_bounds__(kWideWarps * 32, kW32MinBlocks) grid_w32_kerne
         d2[i] = make_float2(wv, wv);
       }
       __syncwarp();
+      const ulonglong2* qa = reinterpret_cast<const ulonglong2*>(vb + off_a);
+      const ulonglong2* qb = reinterpret_cast<const ulonglong2*>(vb + off_b);
       const int t0 = (mA.z >> 5) & 3;
-      // the run's samples over the column pairs some sample reaches (the other
-      // pairs would only add zero products)
+      // the run's samples over the column pairs some sample reaches (the other pairs
+      // would only add zero products): runs within columns 0..3 or 4..7 get their own
+      // loops, the rest take all four column pairs -- few loop bodies keep the
+      // instruction fetch warm
       switch ((mA.z >> 12) & 31) {
-        case 0: w32_apply_run<0, 0>(acc, vb, dbl, n, t0, lane_off, rot8); break;
-        case 1: w32_apply_run<0, 1>(acc, vb, dbl, n, t0, lane_off, rot8); break;
-        case 2: w32_apply_run<0, 2>(acc, vb, dbl, n, t0, lane_off, rot8); break;
-        case 3: w32_apply_run<0, 3>(acc, vb, dbl, n, t0, lane_off, rot8); break;
-        case 5: w32_apply_run<1, 1>(acc, vb, dbl, n, t0, lane_off, rot8); break;
-        case 6: w32_apply_run<1, 2>(acc, vb, dbl, n, t0, lane_off, rot8); break;
-        case 7: w32_apply_run<1, 3>(acc, vb, dbl, n, t0, lane_off, rot8); break;
-        case 10: w32_apply_run<2, 2>(acc, vb, dbl, n, t0, lane_off, rot8); break;
-        case 11: w32_apply_run<2, 3>(acc, vb, dbl, n, t0, lane_off, rot8); break;
-        case 15: w32_apply_run<3, 3>(acc, vb, dbl, n, t0, lane_off, rot8); break;
-        default: break;  // kWideNoReach: no sample reaches the sub-tile
+        case 0: case 1: case 5: w32_apply_run<0, 1>(acc, qa, qb, dbl, n, t0); break;
+        case 10: case 11: case 15: w32_apply_run<2, 3>(acc, qa, qb, dbl, n, t0); break;
+        case kWideNoReach: break;  // no sample reaches the sub-tile
+        default: w32_apply_run<0, 3>(acc, qa, qb, dbl, n, t0); break;
       }
       __syncwarp();  // buffer b and the weights read by every lane before they are refilled
-      if (r + 2 < re) issue(mC, b);
-      mA = mB;
-      mB = mC;
-      cur ^= 1;
+      if (r + kW32Bufs < re) issue(mn, b);
+#pragma unroll
+      for (int k = 0; k + 1 < kW32Bufs; ++k) mq[k] = mq[k + 1];
+      mq[kW32Bufs - 1] = mn;
+      cur = cur + 1 == kW32Bufs ? 0 : cur + 1;
     }
     if (failed) break;
     // no copy is in flight now: the transposition reuses the warp's buffers

@@ -154,6 +154,12 @@ struct Plan {
   int4* d_t_split_list = nullptr;
   float4* d_t_scratch = nullptr;    // [group of 16][slot][128 cells][32 values] floats
   size_t t_scratch_cells = 0;
+  // 32-pair gridding (grid_w32_kernel): the 16-pair list's runs as index records
+  unsigned short* d_x_idx = nullptr;  // per run: 12 16-bit table indices per sample, 16-byte blocks
+  int4* d_x_meta = nullptr;           // per run: {first quad, index block, packed n/offset/quads/range}
+  float4* d_x_scratch = nullptr;      // [pair group of 32][slot][32 cells x 32 pairs] complex
+  size_t x_scratch_cells = 0;
+  bool x_ready = false;
   int cols_G = 0;                   // column-FFT group width (0 = cols_group(M); autotuned)
   std::vector<gr_graph*> graphs;    // live CUDA graphs replaying this plan's buffers
   float4* d_pq = nullptr;
@@ -451,7 +457,17 @@ int install_work_list(Plan* p, int item_cap) {
   return GR_OK;
 }
 
-// The 16-pair kernel's work list (8 x 8 sub-tiles), placed on the device.
+// Whether chunks of this plan can use the 16-pair kernel (its weights) or the
+// 32-pair kernel (its index records); both run on the 4 x 8 work list.
+bool wide16_possible(const Plan* p) {
+  return p->wide_mode == 1 || (p->wide_mode == 0 && p->max_pairs >= kWideMinPairs);
+}
+bool w32_possible(const Plan* p) {
+  return p->wide_mode == 3 || (p->wide_mode == 0 && p->max_pairs > kWidePairs);
+}
+
+// The 16- and 32-pair kernels' work list (4 x 8 sub-tiles), placed on the device
+// with the records of whichever of the two kernels the plan can use.
 int install_work_list_wide(Plan* p, int item_cap) {
   WorkList wl;
   build_work_list(p->M, p->J, p->L, p->n_ang, p->dxy, &wl, item_cap, kListWide);
@@ -470,33 +486,73 @@ int install_work_list_wide(Plan* p, int item_cap) {
     n_rec += (size_t)(wl.runs[r].jhi - wl.runs[r].jlo + 1);
   }
   if (n_rec > (size_t)INT_MAX) return fail(GR_ERR_UNSUPPORTED, "work list too large");
+  // the 32-pair kernel's records: per run an index block of n * 12 16-bit indices,
+  // padded to whole 16-byte units (its bulk copies move whole units)
+  const bool need16 = wide16_possible(p), need32 = w32_possible(p);
+  std::vector<int2> rinfo;
+  size_t n_units = 0;
+  if (need32) {
+    rinfo.resize(wl.runs.size());
+    for (size_t r = 0; r < wl.runs.size(); ++r) {
+      rinfo[r] = make_int2((int)n_units, meta[r].y);
+      n_units += ((size_t)(wl.runs[r].jhi - wl.runs[r].jlo + 1) * kWideRec * 2 + 15) / 16;
+    }
+    if (n_units > (size_t)INT_MAX) return fail(GR_ERR_UNSUPPORTED, "work list too large");
+  }
   dev_free(p, &p->d_w_items);
   dev_free(p, &p->d_w_runs);
   dev_free(p, &p->d_w_split_list);
   dev_free(p, &p->d_w_meta);
   dev_free(p, &p->d_w_wts);
+  dev_free(p, &p->d_x_idx);
+  dev_free(p, &p->d_x_meta);
+  p->x_ready = false;
   int rc;
   if ((rc = upload(p, &p->d_w_items, wl.items)) || (rc = upload(p, &p->d_w_runs, wl.runs)) ||
-      (rc = upload(p, &p->d_w_split_list, split_list)) || (rc = upload(p, &p->d_w_meta, meta)) ||
-      (rc = dev_alloc(p, &p->d_w_wts, std::max<size_t>(n_rec, 1) * kWideRec)))
+      (rc = upload(p, &p->d_w_split_list, split_list)) ||
+      (need16 && ((rc = upload(p, &p->d_w_meta, meta)) ||
+                  (rc = dev_alloc(p, &p->d_w_wts, std::max<size_t>(n_rec, 1) * kWideRec)))))
     return rc;
-  {
-    GridArgs g{};
-    g.runs = p->d_w_runs;
-    g.dir = p->d_dir;
-    g.wtbl = p->d_wtbl;
-    g.M = p->M;
-    g.tiles_v = wl.tiles_v;
-    g.ltbl = p->ltbl;
-    g.L2 = p->L / 2;
-    g.tblspcg = 2.0 * p->ltbl / p->L;
-    GR_CUDA(launch_wide_weights(g, (int)wl.runs.size(), p->d_w_wts, p->d_w_meta, 0));
-    GR_CUDA(cudaStreamSynchronize(0));
+  GridArgs g{};
+  g.runs = p->d_w_runs;
+  g.dir = p->d_dir;
+  g.wtbl = p->d_wtbl;
+  g.M = p->M;
+  g.J = p->J;
+  g.tiles_v = wl.tiles_v;
+  g.ltbl = p->ltbl;
+  g.L2 = p->L / 2;
+  g.tblspcg = 2.0 * p->ltbl / p->L;
+  if (need16) GR_CUDA(launch_wide_weights(g, (int)wl.runs.size(), p->d_w_wts, p->d_w_meta, 0));
+  if (need32) {
+    int2* d_rinfo = nullptr;
+    if ((rc = upload(p, &d_rinfo, rinfo)) ||
+        (rc = dev_alloc(p, &p->d_x_idx, std::max<size_t>(n_units, 1) * 8)) ||
+        (rc = dev_alloc(p, &p->d_x_meta, std::max<size_t>(wl.runs.size(), 1)))) {
+      dev_free(p, &d_rinfo);
+      return rc;
+    }
+    cudaError_t e = cudaMemsetAsync(p->d_x_idx, 0, std::max<size_t>(n_units, 1) * 16, 0);
+    if (e == cudaSuccess)
+      e = launch_w32_index(g, (int)wl.runs.size(), d_rinfo, p->d_x_idx, p->d_x_meta, 0);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(0);
+    dev_free(p, &d_rinfo);
+    if (e != cudaSuccess) return fail(GR_ERR_CUDA, "32-pair index records: %s", cudaGetErrorString(e));
+    // 32 cells x 32 pairs complex = 512 float4 per slot and group of 32 pairs
+    const size_t groups32 = (size_t)(p->max_pairs + kW32Pairs - 1) / kW32Pairs;
+    const size_t xcells = groups32 * (size_t)std::max(wl.n_slots, 1) * (kWideRows * kWideCols * 32 / 2);
+    if (xcells > p->x_scratch_cells) {
+      dev_free(p, &p->d_x_scratch);
+      if ((rc = dev_alloc(p, &p->d_x_scratch, xcells))) return rc;
+      p->x_scratch_cells = xcells;
+    }
+    p->x_ready = true;
   }
+  GR_CUDA(cudaStreamSynchronize(0));
   // 64 cells x 32 lanes floats = 512 float4 per slot and group of 16 pairs
   const size_t groups = (size_t)(p->max_pairs + kWidePairs - 1) / kWidePairs;
   const size_t cells = groups * (size_t)std::max(wl.n_slots, 1) * (kWideRows * kWideCols * 32 / 4);
-  if (cells > p->w_scratch_cells) {
+  if (need16 && cells > p->w_scratch_cells) {
     dev_free(p, &p->d_w_scratch);
     if ((rc = dev_alloc(p, &p->d_w_scratch, cells))) return rc;
     p->w_scratch_cells = cells;
@@ -559,10 +615,20 @@ bool use_tc(const Plan* p, int pairs) {
   return p->t_items > 0 && p->wide_mode == 2;
 }
 
+// Whether a chunk of `pairs` pairs grids with grid_w32_kernel: always in mode 3;
+// by default for chunks of more than 16 pairs.  Its cost per launch does not
+// depend on the live pairs (idle lanes): one launch for 17..32 pairs costs less
+// than the 16-pair kernel's two groups (2048 x 1500: 32.1 against 2 x 39.3 us per
+// group pair-slot), while up to 16 pairs the 16-pair kernel's launch is cheaper.
+bool use_w32(const Plan* p, int pairs) {
+  if (!p->x_ready || p->w_items == 0) return false;
+  return p->wide_mode == 3 || (p->wide_mode == 0 && pairs > kWidePairs);
+}
+
 // Whether a chunk of `pairs` pairs grids with grid_wide_kernel.
 bool use_wide(const Plan* p, int pairs) {
-  if (p->w_items == 0 || p->wide_mode < 0 || use_tc(p, pairs)) return false;
-  return p->wide_mode > 0 || pairs >= kWideMinPairs;
+  if (p->w_items == 0 || p->wide_mode < 0 || use_tc(p, pairs) || use_w32(p, pairs)) return false;
+  return p->wide_mode == 1 || pairs >= kWideMinPairs;
 }
 
 GridArgs grid_args_tc(const Plan* p, int pairs) {
@@ -587,6 +653,17 @@ GridArgs grid_args(const Plan* p, int pairs, bool wide) {
     g.wts = p->d_w_wts;
     g.wmeta = p->d_w_meta;
   }
+  return g;
+}
+
+GridArgs grid_args_w32(const Plan* p, int pairs) {
+  GridArgs g{p->d_spec, p->d_H, p->d_x_scratch, p->d_queue, p->d_w_items, p->d_w_runs,
+             p->d_w_split_list, p->w_split_tiles, p->d_dir, p->d_wtbl, p->w_items, pairs,
+             p->n_ang, p->J, p->M, p->w_tiles_v, p->w_slots, p->ltbl, p->L / 2,
+             2.0 * p->ltbl / p->L};
+  g.err = p->d_err;
+  g.xmeta = p->d_x_meta;
+  g.xidx = p->d_x_idx;
   return g;
 }
 
@@ -632,8 +709,8 @@ int check_params(const gr_params* prm, const Pswf** pw) {
   if (!(prm->sampl >= 1.0f) || prm->sampl > 4.0f)
     return fail(GR_ERR_ARG, "sampl must be in [1, 4]");
   if (prm->max_pairs < 1) return fail(GR_ERR_ARG, "max_pairs must be >= 1");
-  if (prm->wide_grid < -1 || prm->wide_grid > 2)
-    return fail(GR_ERR_ARG, "wide_grid must be -1, 0, 1 or 2");
+  if (prm->wide_grid < -1 || prm->wide_grid > 3)
+    return fail(GR_ERR_ARG, "wide_grid must be -1, 0, 1, 2 or 3");
   if (prm->roi_size < 0.f || prm->roi_size > 4.f || prm->pixel_size < 0.f || prm->pixel_size > 16.f)
     return fail(GR_ERR_ARG, "roi_size in [0, 4] and pixel_size in [0, 16] (0 = 1)");
   *pw = find_pswf(prm->pswf_c);
@@ -706,16 +783,19 @@ int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1
   GR_CUDA(launch_phase(ph, st));
   GR_MARK();
   const bool tc = use_tc(p, pairs);
+  const bool w32 = use_w32(p, pairs);
   const bool wide = use_wide(p, pairs);
   SpectraArgs sa{s1, s2, in_pair_stride, n_valid, slice_base, flat, dark, flat_stride, p->d_pq,
                  p->d_spec,
                  p->d_tw_p, p->n_det, p->n_ang, p->pdim, p->J, pairs, p->d_roi_off,
-                 (wide || tc) ? 1 : 0};
+                 w32 ? kW32Pairs : ((wide || tc) ? kWidePairs : 0)};
   GR_CUDA(launch_spectra(sa, dt, st));
   GR_MARK();
-  const GridArgs ga = tc ? grid_args_tc(p, pairs) : grid_args(p, pairs, wide);
+  const GridArgs ga = tc ? grid_args_tc(p, pairs)
+                         : (w32 ? grid_args_w32(p, pairs) : grid_args(p, pairs, wide));
   GR_CUDA(tc ? launch_grid_tc(ga, st)
-             : (wide ? launch_grid_wide(ga, st) : launch_grid(ga, p->ntaps, st)));
+             : (w32 ? launch_grid_w32(ga, st)
+                    : (wide ? launch_grid_wide(ga, st) : launch_grid(ga, p->ntaps, st))));
   GR_MARK();
   ColArgs ca{p->d_H, p->d_tw_m, p->M, pairs, p->d_err, p->cols_G};
   GR_CUDA(launch_cols(ca, st));
@@ -949,15 +1029,14 @@ int gr_plan_create(const gr_params* prm, gr_plan** out) {
       (rc = upload(p, &p->d_tw_m, twiddles((int)M))) || (rc = upload(p, &p->d_dir, dirs)) ||
       (rc = install_work_list(p, kItemCap)) ||
       (p->wide_mode == 2 && (rc = install_work_list_tc(p, kItemCapT))) ||
-      ((p->wide_mode == 1 || (p->wide_mode == 0 && p->max_pairs >= kWideMinPairs)) &&
-       (rc = install_work_list_wide(p, kItemCapW)))) {
+      ((wide16_possible(p) || w32_possible(p)) && (rc = install_work_list_wide(p, kItemCapW)))) {
     gr_plan_destroy(p);
     return rc;
   }
   const size_t P = (size_t)p->max_pairs;
-  // the 16-pair kernel's spectra layout holds whole groups of 16 pairs
-  const size_t P_spec =
-      (p->w_items || p->t_items) ? (P + kWidePairs - 1) / kWidePairs * kWidePairs : P;
+  // the 16- and 32-pair kernels' spectra layouts hold whole groups of pairs
+  const size_t G_spec = p->x_ready ? kW32Pairs : ((p->w_items || p->t_items) ? kWidePairs : 1);
+  const size_t P_spec = (P + G_spec - 1) / G_spec * G_spec;
   p->spec_pairs = (int)P_spec;
   if ((rc = dev_alloc(p, &p->d_spec, P_spec * p->n_ang * 2 * p->J)) ||
       (rc = dev_alloc(p, &p->d_H, P * (size_t)M * M)) ||
@@ -1015,7 +1094,7 @@ int gr_worklist_export_wide(const gr_params* prm, int* n_items, int* n_runs, int
 int gr_plan_grid_kernel(const gr_plan* p, int pairs, int* wide) {
   if (!p || !wide) return gr::fail(GR_ERR_ARG, "null argument");
   const int pr = std::min(std::max(pairs, 1), p->max_pairs);
-  *wide = gr::use_tc(p, pr) ? 2 : (gr::use_wide(p, pr) ? 1 : 0);
+  *wide = gr::use_tc(p, pr) ? 2 : (gr::use_w32(p, pr) ? 3 : (gr::use_wide(p, pr) ? 1 : 0));
   return GR_OK;
 }
 
@@ -1116,7 +1195,8 @@ int gr_plan_autotune(gr_plan* p, void* stream) {
   static std::mutex mu;
   struct Tuned { int cap, G; };  // cap: item cap of the kernel a full chunk uses
   static std::map<unsigned long long, Tuned> cache;
-  const bool wide = use_wide(p, p->max_pairs);
+  const bool w32 = use_w32(p, p->max_pairs);
+  const bool wide = use_wide(p, p->max_pairs) || w32;  // both use the 4 x 8 work list
   auto install = [&](int cap) {
     if (wide) return cap == p->w_item_cap ? GR_OK : install_work_list_wide(p, cap);
     return cap == p->item_cap ? GR_OK : install_work_list(p, cap);
@@ -1154,9 +1234,10 @@ int gr_plan_autotune(gr_plan* p, void* stream) {
                                      : std::vector<int>{512, 1024, 2048, 4096, 8192};
   for (int cap : caps) {
     if ((rc = install(cap))) break;
-    const GridArgs ga = grid_args(p, pairs, wide);
+    const GridArgs ga = w32 ? grid_args_w32(p, pairs) : grid_args(p, pairs, wide);
     const float t = time_ms([&] {
-      if (wide) launch_grid_wide(ga, st);
+      if (w32) launch_grid_w32(ga, st);
+      else if (wide) launch_grid_wide(ga, st);
       else launch_grid(ga, p->ntaps, st);
     });
     if (t < best_t) {
@@ -1192,7 +1273,8 @@ int gr_plan_autotune(gr_plan* p, void* stream) {
 
 int gr_plan_tuning(const gr_plan* p, int* item_cap, int* cols_group_width) {
   if (!p) return gr::fail(GR_ERR_ARG, "null plan");
-  if (item_cap) *item_cap = gr::use_wide(p, p->max_pairs) ? p->w_item_cap : p->item_cap;
+  const bool wl4x8 = gr::use_wide(p, p->max_pairs) || gr::use_w32(p, p->max_pairs);
+  if (item_cap) *item_cap = wl4x8 ? p->w_item_cap : p->item_cap;
   if (cols_group_width) *cols_group_width = p->cols_G > 0 ? p->cols_G : gr::cols_group(p->M);
   return GR_OK;
 }

@@ -258,12 +258,12 @@ class Plan:
         return self._h
 
     def grid_kernel(self, pairs=None) -> str:
-        """'tensor' (tcgen05), 'wide' (16 pairs per warp) or 'tiles' for a chunk of
-        `pairs` pairs."""
+        """'wide32' (32 pairs per warp), 'wide' (16 pairs per warp), 'tensor'
+        (tcgen05) or 'tiles' for a chunk of `pairs` pairs."""
         w = C.c_int()
         _check(lib().gr_plan_grid_kernel(self._h, int(pairs or self.max_pairs), C.byref(w)),
                "gr_plan_grid_kernel")
-        return ("tiles", "wide", "tensor")[w.value]
+        return ("tiles", "wide", "tensor", "wide32")[w.value]
 
     def device_bytes(self) -> int:
         b = C.c_size_t()

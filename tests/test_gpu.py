@@ -27,7 +27,8 @@ def _dev(a):
 def _gpu_pair(s1, s2, theta, **kw):
     n_ang, n_det = s1.shape
     with G.Plan(n_det, n_ang, theta, **kw) as plan:
-        assert plan.grid_kernel(1) == ("tiles", "wide", "tensor")[max(kw.get("wide_grid", 0), 0)]
+        assert plan.grid_kernel(1) == ("tiles", "wide", "tensor", "wide32")[
+            max(kw.get("wide_grid", 0), 0)]
         o1 = torch.zeros((plan.M0, max(plan.M0, n_det)), device="cuda")
         o2 = torch.zeros_like(o1)
         plan.reconstruct_pair(_dev(s1), _dev(s2), o1, o2)
@@ -37,7 +38,7 @@ def _gpu_pair(s1, s2, theta, **kw):
         return o1.cpu().numpy()[:, :plan.M0], o2.cpu().numpy()[:, :plan.M0]
 
 
-@pytest.mark.parametrize("grid", ["tiles", "wide", "tensor"])
+@pytest.mark.parametrize("grid", ["tiles", "wide", "tensor", "wide32"])
 @pytest.mark.parametrize("case", CASES, ids=[c["name"] for c in CASES])
 def test_pair_against_goldens(case, grid):
     """Every golden case through the three gridding kernels (the 16-pair and
@@ -46,7 +47,7 @@ def test_pair_against_goldens(case, grid):
     g1, g2 = _gpu_pair(case["sino1"], case["sino2"], case["theta"], center=case["center"],
                        filter=case["filter"], pswf_c=case["C"], sampl=case["sampl"],
                        geom=case["geom"], roi_size=R, pixel_size=pix, roi_x0=x0, roi_y0=y0,
-                       wide_grid={"tiles": -1, "wide": 1, "tensor": 2}[grid])
+                       wide_grid={"tiles": -1, "wide": 1, "tensor": 2, "wide32": 3}[grid])
     m = case["M0"]
     assert g1.shape == (m, m)
     o1, o2 = O.port_gridrec_pair(case["sino1"], case["sino2"], case["theta"],
@@ -303,7 +304,7 @@ def _oracle_pairs_rel_l2(sinos, centers, th, got, filter):
         return [e for pair in ex.map(one, range(len(sinos) // 2)) for e in pair]
 
 
-@pytest.mark.parametrize("max_pairs", [16])
+@pytest.mark.parametrize("max_pairs", [16, 32])
 def test_bench_chunk_2048x1500_against_float64(max_pairs):
     """The benchmark's own configuration at full size: one chunk of max_pairs pairs
     of 2048 x 1500 random-ellipse slices (seed = slice index, per-slice centres
@@ -319,7 +320,7 @@ def test_bench_chunk_2048x1500_against_float64(max_pairs):
         sinos[i].copy_(s)
         centers[i] = c
     with G.Plan(n, a, th, filter=G.FILTER_HANN, max_pairs=max_pairs) as plan:
-        assert plan.grid_kernel(max_pairs) == "wide"
+        assert plan.grid_kernel(max_pairs) == {16: "wide", 32: "wide32"}[max_pairs]
         plan.autotune()
         o = torch.zeros((S, plan.M0, n), device="cuda")
         plan.reconstruct_batch(sinos, o, centers=_dev(centers))
@@ -585,6 +586,74 @@ def test_wide_kernel_mixed_chunks_and_reproducible():
         assert ph.rel_l2(got[i], refs[i]) < TOL, i
 
 
+def test_w32_kernel_mixed_chunks_against_16_pair_kernel_and_oracle():
+    """45 pairs and an odd slice with max_pairs 40 (a 32-pair-kernel chunk of 40 pairs,
+    then a tile-kernel chunk of 5.5): every slice within the parity bound of float64;
+    the 40-pair chunk equals, bit for bit, the 16-pair kernel's images of the same
+    slices (same taps, weights and summation order); three runs bitwise identical."""
+    n, a = 80, 60
+    th = ph.angles_deg(a)
+    S = 91
+    sinos, centers = _ellipse_batch(n, a, S, seed=11)
+    outs = {}
+    for mode in (0, 1):
+        with G.Plan(n, a, th, filter=G.FILTER_HANN, max_pairs=40, wide_grid=mode) as plan:
+            want = {0: ("wide32", "wide", "tiles"), 1: ("wide", "wide", "wide")}[mode]
+            assert (plan.grid_kernel(40), plan.grid_kernel(16), plan.grid_kernel(5)) == want
+            o = [torch.zeros((S, plan.M0, max(plan.M0, n)), device="cuda")
+                 for _ in range(3 if mode == 0 else 1)]
+            for k in range(len(o)):
+                plan.reconstruct_batch(_dev(sinos), o[k], centers=_dev(centers))
+            torch.cuda.synchronize()
+            plan.device_status()
+            M0 = plan.M0
+            if mode == 0:
+                assert torch.equal(o[0], o[1]) and torch.equal(o[0], o[2])
+            outs[mode] = o[0].cpu().numpy()[:, :, :M0]
+    np.testing.assert_array_equal(outs[0][:80], outs[1][:80])
+    ext_s = np.concatenate([sinos, np.zeros_like(sinos[:1])])
+    ext_c = np.concatenate([centers, centers[-1:]])
+    refs = _oracle_batch(ext_s, ext_c, th, M0, filter=2)
+    for i in range(S):
+        assert ph.rel_l2(outs[0][i], refs[i]) < TOL, i
+
+
+@pytest.mark.parametrize("dtype", ["float16", "u16raw"])
+def test_w32_kernel_input_types_and_host_streaming(dtype):
+    """Reduced-precision and raw-count inputs through the 32-pair kernel (a chunk of
+    32 pairs), on the device and streamed from pinned host memory: the same bits
+    as the 16-pair kernel on the same input, and the host path equal to the device
+    path."""
+    n, a = 96, 64
+    th = ph.angles_deg(a)
+    S = 64
+    if dtype == "u16raw":
+        p = [ph.line_integrals(ph.random_ellipses(s), n, th, 48.0) / (n / 2) for s in range(S)]
+        raws, flats, darks = zip(*[ph.raw_counts(p[s], seed=s) for s in range(S)])
+        host = np.stack(raws).view(np.int16)
+        kw = dict(flat=np.stack(flats), dark=np.stack(darks), dtype=G.DTYPE_U16_RAW)
+    else:
+        host = np.stack([ph.random_ellipse_sinogram(s, n, a, center=48.0)[0]
+                         for s in range(S)]).astype(np.float16)
+        kw = dict(dtype=G.DTYPE_F16)
+    dkw = {k: (_dev(v) if isinstance(v, np.ndarray) else v) for k, v in kw.items()}
+    outs = {}
+    for mode in (3, 1):
+        with G.Plan(n, a, th, center=48.0, filter=G.FILTER_HANN, max_pairs=32,
+                    wide_grid=mode) as plan:
+            o = torch.zeros((S, plan.M0, 128), device="cuda")
+            plan.reconstruct_batch(_dev(host), o, **dkw)
+            torch.cuda.synchronize()
+            plan.device_status()
+            outs[mode] = o.cpu().numpy()
+            if mode == 3:
+                h_in = torch.from_numpy(host).pin_memory()
+                h_out = torch.zeros((S, plan.M0, 128)).pin_memory()
+                plan.reconstruct_host(h_in, h_out, **kw)
+                np.testing.assert_array_equal(h_out.numpy(), outs[3])
+    np.testing.assert_array_equal(outs[3], outs[1])
+
+
 def test_wide_kernel_split_subtiles_2048x1500():
     """Full-size geometry: the centre sub-tiles are split over many items and
     summed by the split reduction; a 16-pair chunk matches the tile kernel on the
@@ -669,11 +738,12 @@ def test_wide_kernel_host_streaming_and_graph():
 
 
 @pytest.mark.parametrize("seed", [21, 22, 23])
-@pytest.mark.parametrize("mode", [-1, 0, 2])
+@pytest.mark.parametrize("mode", [-1, 0, 2, 3])
 def test_wide_and_tensor_random_geometries(seed, mode):
     """Seeded random widths, irregular angle lists, oversampling, PSWF parameter,
-    filter and centres through the 32 x 32 tile (mode -1), 16-pair (mode 0) and
-    tensor-core (mode 2) gridding kernels: every slice of a 16-pair chunk within
+    filter and centres through the 32 x 32 tile (mode -1), 16-pair (mode 0),
+    tensor-core (mode 2) and 32-pair (mode 3) gridding kernels: every slice of a
+    16-pair chunk within
     the parity bound of float64, and the worst slice no further from float64 than
     the reference's own FP32 build's worst slice (GridrecCPP, one centre per pair).
     Tap positions and table indices are FP64 in every kernel; FP32 positions move
@@ -692,7 +762,7 @@ def test_wide_and_tensor_random_geometries(seed, mode):
                       / (n / 2) for s, c in enumerate(centers)]).astype(np.float32)
     with G.Plan(n, a, th, filter=filt, pswf_c=C_, sampl=sampl, max_pairs=16,
                 wide_grid=mode) as plan:
-        assert plan.grid_kernel() == {-1: "tiles", 0: "wide", 2: "tensor"}[mode]
+        assert plan.grid_kernel() == {-1: "tiles", 0: "wide", 2: "tensor", 3: "wide32"}[mode]
         o = torch.zeros((S, plan.M0, max(plan.M0, n)), device="cuda")
         plan.reconstruct_batch(_dev(sinos), o, centers=_dev(centers))
         torch.cuda.synchronize()
