@@ -14,6 +14,12 @@ in 2048-stride float32 images.  Inputs (3.1 GB per step) are larger than L2.
          measured copy bandwidth
   cpu_baseline  the reference's own CPU GridRec (compiled from its sources into
          oracle/_ref) on the host cores, bounded sample
+  parity relL2 / max-abs of two timed images against float64 gridrec (CPU leg)
+  uneven the 512-slice uneven batch (1024x720, 2048x1500, 4096x3000 at 3:2:1), raw
+         uint16 with flat/dark fused on load, one CUDA-graph launch per step, plus
+         f32 and f16 storage; their error against float64 in the CPU leg
+  stream 128 slices of 4096x3000 raw uint16 streamed from pinned host memory and back,
+         end to end next to kernel-only
 
 python bench.py [--gpus N --steps K --warmup W] [--impl reference]
 Under torchrun each rank reconstructs its own 256 slices (weak scaling, no
@@ -54,6 +60,8 @@ def parse():
     ap.add_argument("--max-pairs", type=int, default=32)
     ap.add_argument("--dtype", default="f32", choices=["f32", "f16", "bf16"])
     ap.add_argument("--e2e-steps", type=int, default=10)
+    ap.add_argument("--e2e-max-pairs", type=int, default=8,
+                    help="pairs per streamed chunk of the end-to-end (host buffer) measurement")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-pipeline", action="store_true",
@@ -69,6 +77,8 @@ def parse():
                          "4096 x 3000 raw uint16 slices streamed from pinned host memory "
                          "(--stream-slices, cycling a 64-slice host ring)")
     ap.add_argument("--stream-slices", type=int, default=2048)
+    ap.add_argument("--no-configs", action="store_true",
+                    help="skip the uneven-batch and streaming keys of the default run")
     return ap.parse_args()
 
 
@@ -535,20 +545,29 @@ def run_b200(args, rank, world, local_rank):
             h_in = torch.empty(sinos.shape, dtype=sinos.dtype).pin_memory()
             h_out = torch.empty(outs.shape, dtype=torch.float32).pin_memory()
         h_in.copy_(sinos.cpu())
-        plan.reconstruct_host(h_in, h_out, centers=centers, stream=int(stream.cuda_stream))
+        # the host path is bound by the PCIe links: its own plan streams smaller chunks,
+        # so that less of the first copy-in and the last copy-out is left without overlap
+        plan_h = G.Plan(n, a, th, filter=G.FILTER_HANN, max_pairs=args.e2e_max_pairs,
+                        device=local_rank)
+        if not args.no_autotune:
+            plan_h.autotune()
+        plan_h.reconstruct_host(h_in, h_out, centers=centers, stream=int(stream.cuda_stream))
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         for _ in range(args.e2e_steps):
-            plan.reconstruct_host(h_in, h_out, centers=centers, stream=int(stream.cuda_stream))
-            float(h_out[0, plan.M0 // 2, plan.M0 // 2])   # read the result on the host
+            plan_h.reconstruct_host(h_in, h_out, centers=centers, stream=int(stream.cuda_stream))
+            float(h_out[0, plan_h.M0 // 2, plan_h.M0 // 2])   # read the result on the host
         te = max_over_ranks(time.perf_counter() - t0, dev, world)
         e2e = {"value": S * args.e2e_steps * world / te, "unit": UNIT,
                "h2d_bytes_per_step": int(h_in.numel() * h_in.element_size()),
                "d2h_bytes_per_step": int(h_out.numel() * h_out.element_size()),
                "steps": args.e2e_steps, "path": "gr_reconstruct_host, pinned host buffers",
+               "pairs_per_chunk": args.e2e_max_pairs,
+               "grid_kernel": plan_h.grid_kernel(args.e2e_max_pairs),
                "host_buffers_on_cpus": host_node.cpus}
+        plan_h.close()
         del h_in, h_out
 
     learned = None
@@ -559,12 +578,21 @@ def run_b200(args, rank, world, local_rank):
     if rank == 0 and not args.no_pipeline:
         pipe = measure_slice_pipeline(G, sinos, th, n, a, dev, stream, peaks()[0])
 
+    # BASELINE configs 3 and 5 on the same box (one GPU): the uneven batch (one graph
+    # launch per step, raw u16 / f32 / f16 storage) and 128 slices of the streaming volume
+    uneven = stream_cfg = uneven_checks = None
+    if world == 1 and not args.no_configs:
+        uneven, _, _, uneven_checks = measure_uneven(args, rank, world, local_rank, steps=2)
+        stream_cfg, _ = measure_stream(args, rank, world, local_rank, total=128)
+
     cpu = None
     parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         # the CPU leg: the oracle checks two of the timed images, then the reference's
         # own CPU GridRec is timed on the host cores
         parity = parity_check(sinos, outs, centers, th, plan.M0)
+        if uneven_checks is not None:
+            uneven["float64_check"] = uneven_float64_check(uneven_checks)
         v, info = cpu_reference(n, a, args.cpu_seconds)
         cpu = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
                "sample": f"{info['pairs']} slice pairs of {n}x{a} (Hann) over "
@@ -605,6 +633,8 @@ def run_b200(args, rank, world, local_rank):
             "parity": parity,
             "slice_pipeline": pipe,
             "learned": learned,
+            "uneven": uneven,
+            "stream": stream_cfg,
         }
         print(json.dumps(out), flush=True)
     plan.close()
@@ -613,19 +643,19 @@ def run_b200(args, rank, world, local_rank):
 UNEVEN_SHAPES = ((1024, 720, 256), (2048, 1500, 171), (4096, 3000, 85))
 
 
-def run_uneven(args, rank, world, local_rank):
+def measure_uneven(args, rank, world, local_rank, steps):
     """512 slices of three shapes (3:2:1), raw uint16 counts with per-slice flat/dark
     rows fused on load, reconstructed by one CUDA-graph launch per step; plus the
-    same slices pre-normalised and stored as f32 and as f16."""
+    same slices pre-normalised and stored as f32 and as f16.  Returns (result,
+    clocks, launches, checks); checks holds the first 1024 x 720 pair's f32
+    sinograms and its images from the three paths, for the float64 check."""
     import torch
     import torch.distributed as dist
 
     from projects_b200 import gridrec as G
     from projects_b200 import phantom as ph
-    torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     stream = torch.cuda.current_stream()
-    pairs_by_n = {1024: 32, 2048: 16, 4096: 16}
     groups = []
     seed0 = rank * 100000
     for n, a, S in UNEVEN_SHAPES:
@@ -633,22 +663,24 @@ def run_uneven(args, rank, world, local_rank):
         raw = torch.empty((S, a, n), dtype=torch.int16, device=dev)
         flat = torch.empty((S, n), dtype=torch.float32, device=dev)
         dark = torch.empty((S, n), dtype=torch.float32, device=dev)
+        centers = np.zeros(S, np.float32)
         for i in range(S):
-            r, f, d, _ = ph.random_ellipse_raw(seed0 + n + i, n, a, dev)
+            r, f, d, c = ph.random_ellipse_raw(seed0 + n + i, n, a, dev)
             raw[i].copy_(r)
             flat[i].copy_(f)
             dark[i].copy_(d)
-        plan = G.Plan(n, a, th, filter=G.FILTER_HANN, max_pairs=pairs_by_n[n], device=local_rank)
+            centers[i] = c
+        plan = G.Plan(n, a, th, filter=G.FILTER_HANN, max_pairs=32, device=local_rank)
         tuning = plan.autotune() if not args.no_autotune else plan.tuning()
         outs = torch.empty((S, plan.M0, plan.M0), dtype=torch.float32, device=dev)
         # the same slices normalised once (log, as the fused load) for the f32/f16 variants
         v = raw.to(torch.int32).remainder(65536).to(torch.float32) - dark[:, None, :]
         rr = (flat - dark)[:, None, :] / v
         norm = torch.where((v > 0) & (rr > 0), torch.log(rr), torch.zeros_like(v))
-        groups.append({"n": n, "a": a, "S": S, "plan": plan, "tuning": tuning, "raw": raw,
-                       "flat": flat,
-                       "dark": dark, "outs": outs, "f32": norm.contiguous(),
-                       "f16": norm.half().contiguous()})
+        groups.append({"n": n, "a": a, "S": S, "th": th, "plan": plan, "tuning": tuning,
+                       "raw": raw, "flat": flat, "dark": dark, "centers": centers,
+                       "centers_d": torch.from_numpy(centers).to(dev), "outs": outs,
+                       "f32": norm.contiguous(), "f16": norm.half().contiguous()})
         del v, rr, norm
 
     def graph_for(kind):
@@ -656,15 +688,15 @@ def run_uneven(args, rank, world, local_rank):
         for g in groups:
             p = g["plan"]
             if kind == "raw":
-                b = p.batch_desc(g["raw"], g["outs"], flat=g["flat"], dark=g["dark"],
-                                 dtype=G.DTYPE_U16_RAW)
+                b = p.batch_desc(g["raw"], g["outs"], centers=g["centers_d"], flat=g["flat"],
+                                 dark=g["dark"], dtype=G.DTYPE_U16_RAW)
             else:
-                b = p.batch_desc(g[kind], g["outs"])
+                b = p.batch_desc(g[kind], g["outs"], centers=g["centers_d"])
             items.append((p, b))
         return G.Graph(items)
 
-    def timed(graph, steps):
-        for _ in range(args.warmup):
+    def timed(graph):
+        for _ in range(max(args.warmup, 1)):
             graph.launch(stream)
         torch.cuda.synchronize()
         if world > 1:
@@ -678,17 +710,19 @@ def run_uneven(args, rank, world, local_rank):
         return max_over_ranks(e0.elapsed_time(e1) / 1000.0, dev, world)
 
     total = sum(g["S"] for g in groups)
-    steps = max(1, min(args.steps, 10))
     g_raw = graph_for("raw")
     with ClockSampler(local_rank) as clk:
-        t_raw = timed(g_raw, steps)
+        t_raw = timed(g_raw)
     launches = g_raw.launches() * steps
     g_raw.close()
     ref = [g["outs"][:4].clone() for g in groups]  # raw-path images of 4 slices per shape
-    res = {}
+    g0 = groups[0]
+    checks = {"n": g0["n"], "a": g0["a"], "th": g0["th"], "centers": g0["centers"][:2].copy(),
+              "sinos": g0["f32"][:2].cpu().numpy(), "raw": ref[0][:2].cpu().numpy()}
+    res = {"raw_u16": {"slices_per_s": total * steps * world / t_raw}}
     for kind in ("f32", "f16"):
         gk = graph_for(kind)
-        t = timed(gk, steps)
+        t = timed(gk)
         gk.close()
         errs = {}
         for g, r in zip(groups, ref):
@@ -697,48 +731,86 @@ def run_uneven(args, rank, world, local_rank):
                                              / torch.linalg.vector_norm(r))
         res[kind] = {"slices_per_s": total * steps * world / t,
                      "rel_l2_vs_raw_path_images": errs}
-    in_bytes = sum(g["raw"].numel() * 2 for g in groups)
+        checks[kind] = groups[0]["outs"][:2].cpu().numpy()
+    result = {
+        "value": total * steps * world / t_raw, "unit": UNIT, "steps": steps,
+        "ms_per_step": 1000.0 * t_raw / steps,
+        "workload": "uneven batch: " + ", ".join(
+            f"{g['S']} x {g['n']} det x {g['a']} angles" for g in groups) +
+            "; raw uint16 with per-slice flat/dark fused on load (log); Hann; per-slice "
+            "centres; one CUDA-graph launch of all three shapes per step",
+        "slices_per_step": total,
+        "grid_kernels": {f"{g['n']}x{g['a']}": g["plan"].grid_kernel() for g in groups},
+        "tuning": {f"{g['n']}x{g['a']}": g["tuning"] for g in groups},
+        "storage_variants": res,
+        "l2": f"inputs larger than L2 ({sum(g['raw'].numel() * 2 for g in groups) / 1e9:.1f} "
+              "GB/step)"}
+    for g in groups:
+        g["plan"].close()
+    del groups
+    torch.cuda.empty_cache()
+    return result, clk.summary(), launches, checks
+
+
+def uneven_float64_check(checks):
+    """relL2 of the first 1024 x 720 pair's images from the raw-u16, f32 and f16 paths
+    against float64 gridrec of the f32-normalised sinograms (the oracle as the checker)."""
+    from oracle import oracle as O
+    from projects_b200 import phantom as ph
+    s, c = checks["sinos"], checks["centers"]
+    r1, r2 = O.port_gridrec_pair(s[0], s[1], checks["th"], center1=float(c[0]),
+                                 center2=float(c[1]), filter=2)
+    M0 = checks["raw"].shape[1]
+    out = {}
+    for kind in ("raw", "f32", "f16"):
+        g = checks[kind]
+        out[kind] = max(ph.rel_l2(g[0], r1[:, :M0]), ph.rel_l2(g[1], r2[:, :M0]))
+    return {"pair": f"first {checks['n']}x{checks['a']} pair", "worst_rel_l2": out,
+            "reference": "float64 gridrec of the f32-normalised sinograms"}
+
+
+def run_uneven(args, rank, world, local_rank):
+    """--config uneven: the uneven batch as its own JSON line."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    steps = max(1, min(args.steps, 10))
+    result, clocks, launches, checks = measure_uneven(args, rank, world, local_rank, steps)
     if rank == 0:
         out = {
-            "metric": METRIC, "value": total * steps * world / t_raw, "unit": UNIT,
+            "metric": METRIC, "value": result["value"], "unit": UNIT,
             "n_gpus": world, "steps": steps, "warmup": args.warmup,
-            "ms_per_step": 1000.0 * t_raw / steps, "higher_is_better": True,
+            "ms_per_step": result["ms_per_step"], "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u16 raw in, f32 compute",
             "data": "synthetic (seeded random-ellipse phantoms, Poisson counts, per-slice "
                     "flat/dark rows)",
-            "config": {"workload": "uneven batch: " + ", ".join(
-                f"{g['S']} x {g['n']} det x {g['a']} angles" for g in groups) +
-                "; raw uint16 with fused flat/dark + log; Hann; one CUDA-graph launch of "
-                "all three shapes per step",
-                "slices_per_step": total, "parallelism": f"slices x{world}",
-                "tuning": {f"{g['n']}x{g['a']}": g["tuning"] for g in groups},
-                "l2": f"inputs larger than L2 ({in_bytes / 1e9:.1f} GB/step)"},
+            "config": {"workload": result["workload"], "slices_per_step": result["slices_per_step"],
+                       "parallelism": f"slices x{world}", "tuning": result["tuning"],
+                       "grid_kernels": result["grid_kernels"], "l2": result["l2"]},
             "gpu_launches": launches,
-            "storage_variants": res,
-            "clocks": clk.summary(),
+            "storage_variants": result["storage_variants"],
+            "clocks": clocks,
         }
+        if world == 1 and not args.no_cpu_baseline:
+            out["float64_check"] = uneven_float64_check(checks)
         print(json.dumps(out), flush=True)
-    for g in groups:
-        g["plan"].close()
 
 
-def run_stream(args, rank, world, local_rank):
+def measure_stream(args, rank, world, local_rank, total, ring=64):
     """Streaming volume: 4096 x 3000 raw uint16 slices with per-slice flat/dark rows,
     streamed from pinned host memory through gr_reconstruct_host (double-buffered
     chunks of 8 pairs, H2D and D2H on their own streams beside the kernels), the
-    4095^2 float32 images streamed back into pinned host memory.  A 64-slice host
-    ring is cycled to move --stream-slices slices (2048 = 50 GB in, 137 GB out);
-    kernel-only slices/s is measured on the same slices resident in HBM."""
+    4095^2 float32 images streamed back into pinned host memory.  A host ring of
+    `ring` slices is cycled to move `total` slices; kernel-only slices/s is measured
+    on the same slices resident in HBM."""
     import torch
     import torch.distributed as dist
 
     from projects_b200 import gridrec as G
     from projects_b200 import phantom as ph
-    torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
     stream = torch.cuda.current_stream()
-    n, a, K = 4096, 3000, 64
-    total = max(K, (args.stream_slices // K) * K)
+    n, a, K = 4096, 3000, ring
+    total = max(K, (total // K) * K)
     th = ph.angles_deg(a)
     raw = torch.empty((K, a, n), dtype=torch.int16, device=dev)
     flat = torch.empty((K, n), dtype=torch.float32, device=dev)
@@ -749,7 +821,7 @@ def run_stream(args, rank, world, local_rank):
         flat[i].copy_(f)
         dark[i].copy_(d)
     plan = G.Plan(n, a, th, filter=G.FILTER_HANN, max_pairs=8, device=local_rank)
-    tuning = plan.autotune()
+    tuning = plan.autotune() if not args.no_autotune else plan.tuning()
     outs = torch.empty((K, plan.M0, plan.M0), dtype=torch.float32, device=dev)
     # kernel-only: resident in HBM
     for _ in range(2):
@@ -785,29 +857,50 @@ def run_stream(args, rank, world, local_rank):
     te = max_over_ranks(te, dev, world)
     in_b = int(h_in.numel() * 2) * (total // K)
     out_b = int(h_out.numel() * 4) * (total // K)
+    result = {
+        "value": total * world / te, "unit": UNIT, "slices": total, "ring_slices": K,
+        "ms_per_ring": 1000.0 * te / (total // K),
+        "workload": f"streaming volume: {total} slices of {n} det x {a} angles raw uint16 from "
+                    f"pinned host memory, images {plan.M0}^2 f32 streamed back (host ring of {K} "
+                    f"slices cycled)",
+        "e2e": {"value": total * world / te, "unit": UNIT,
+                "h2d_bytes_per_step": in_b // (total // K),
+                "d2h_bytes_per_step": out_b // (total // K),
+                "path": "gr_reconstruct_host, double-buffered, separate H2D/D2H streams",
+                "host_buffers_on_cpus": host_node.cpus},
+        "kernel_only_slices_per_s": kernel_only,
+        "pcie_gbs": {"h2d": in_b / te / 1e9, "d2h": out_b / te / 1e9},
+        "tuning": tuning,
+        "path": "plain gridrec (the learned path falls back to it)"}
+    plan.close()
+    del h_in, h_out
+    return result, clk.summary()
+
+
+def run_stream(args, rank, world, local_rank):
+    """--config stream: the streaming volume as its own JSON line."""
+    import torch
+    torch.cuda.set_device(local_rank)
+    result, clocks = measure_stream(args, rank, world, local_rank, args.stream_slices)
     if rank == 0:
+        K = result["ring_slices"]
+        steps = result["slices"] // K
         out = {
-            "metric": METRIC, "value": total * world / te, "unit": UNIT, "n_gpus": world,
-            "steps": total // K, "warmup": 1, "ms_per_step": 1000.0 * te / (total // K),
+            "metric": METRIC, "value": result["value"], "unit": UNIT, "n_gpus": world,
+            "steps": steps, "warmup": 1, "ms_per_step": result["ms_per_ring"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "u16 raw in, f32 compute, f32 out",
             "data": "synthetic (seeded random-ellipse phantoms, Poisson counts, per-slice "
                     "flat/dark rows)",
-            "config": {"workload": f"streaming volume: {total} slices of {n} det x {a} angles "
-                                   f"raw uint16 from pinned host memory, images {plan.M0}^2 "
-                                   f"f32 streamed back (host ring of {K} slices cycled)",
-                       "slices": total, "parallelism": f"slices x{world}", "tuning": tuning,
-                       "path": "plain gridrec (the learned path falls back to it)"},
-            "e2e": {"value": total * world / te, "unit": UNIT, "h2d_bytes_per_step":
-                    in_b // (total // K), "d2h_bytes_per_step": out_b // (total // K),
-                    "path": "gr_reconstruct_host, double-buffered, separate H2D/D2H streams",
-                    "host_buffers_on_cpus": host_node.cpus},
-            "kernel_only_slices_per_s": kernel_only,
-            "pcie_gbs": {"h2d": in_b / te / 1e9, "d2h": out_b / te / 1e9},
-            "clocks": clk.summary(),
+            "config": {"workload": result["workload"], "slices": result["slices"],
+                       "parallelism": f"slices x{world}", "tuning": result["tuning"],
+                       "path": result["path"]},
+            "e2e": result["e2e"],
+            "kernel_only_slices_per_s": result["kernel_only_slices_per_s"],
+            "pcie_gbs": result["pcie_gbs"],
+            "clocks": clocks,
         }
         print(json.dumps(out), flush=True)
-    plan.close()
 
 
 def main():
