@@ -137,6 +137,18 @@ int gr_plan_device_bytes(const gr_plan* plan, size_t* bytes);
 int gr_reconstruct_pair(gr_plan* plan, const float* sino1, const float* sino2, float* out1,
                         float* out2, long out_stride, void* stream);
 
+/* One slice pair from HOST buffers, synchronous: the GridRec::reconstruct call of
+ * the reference's callers (gridrec/GPU/gridrec.cu:314-369 with the buffers of
+ * setSinoAndReconBuffers, :174-212), which keep sinograms and images in host
+ * memory.  sino1/sino2: n_ang x n_det float32 (pageable or pinned; sino2 may be
+ * NULL = zeros); out1/out2: M0 rows of out_stride floats (out2 may be NULL);
+ * only the M0 x M0 block is written.  The copies go straight between the
+ * caller's buffers and the plan's device buffers (allocated on first use), with
+ * no host-side staging.  Returns after the images are in place; a bounded-wait
+ * timeout is reported as by gr_plan_device_status. */
+int gr_reconstruct_pair_host(gr_plan* plan, const float* sino1, const float* sino2, float* out1,
+                             float* out2, long out_stride, void* stream);
+
 /* A batch of n_slices slices (n_slices even, or odd with the last slice
  * paired with zeros), device pointers:
  *   sinos      n_slices sinograms, each n_ang x n_det of `dtype`, contiguous

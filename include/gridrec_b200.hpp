@@ -8,8 +8,9 @@
 // n_ang x n_det float, reconstruction n_det rows of n_det floats with the
 // leading M0 x M0 block written) and the two-slices-per-call contract stay.
 // Differences, all additive: setCenter() (GridRec::init fixes n_det/2,
-// gridrec.cu:227), lastStatus() instead of exit(2) on bad parameters, and no
-// cuFFT or cutil dependency.
+// gridrec.cu:227), setCenterShift() of find_shift's GridRec (centre = n_det/2 +
+// shift, find_shift/src/main/gridrec.cu:229, 809-813), lastStatus() instead of
+// exit(2) on bad parameters, and no cuFFT or cutil dependency.
 #ifndef GRIDREC_B200_HPP
 #define GRIDREC_B200_HPP
 
@@ -49,13 +50,23 @@ class GridRec {
   int getFilter() const { return filter_; }
   void setGPUDeviceID(int id) { device_ = id; }
   int getGPUDeviceID() const { return device_; }
-  void setCenter(float center) { center_ = center; }
+  void setCenter(float center) {
+    center_ = center;
+    shift_set_ = false;
+  }
+  // find_shift's GridRec: the centre is n_det / 2 (integer division) + shift,
+  // applied at init() (find_shift/src/main/gridrec.cu:229, 809-813)
+  void setCenterShift(float shift) {
+    shift_ = shift;
+    shift_set_ = true;
+  }
+  float getCenter() const { return shift_set_ ? (float)(n_det_ / 2) + shift_ : center_; }
 
   void init() {
     destroy();
     gr_params p;
     gr_params_default(&p, n_det_, n_ang_, theta_);
-    p.center = center_;
+    p.center = getCenter();
     p.filter = filter_;
     p.device = device_;
     status_ = gr_plan_create(&p, &plan_);
@@ -79,6 +90,14 @@ class GridRec {
       status_ = GR_ERR_ARG;
       return;
     }
+    if (m0_ <= n_det_) {  // the caller's buffers directly (power-of-two widths: M0 = n_det - 1)
+      status_ = gr_reconstruct_pair_host(plan_, sino_[0], sino_[1], recon_[0], recon_[1], n_det_,
+                                         nullptr);
+      return;
+    }
+    // M0 > n_det (other widths): the reference's rows of stride n_det overlap
+    // (gridrec.cu:196-197); here the images go through a staging buffer and each
+    // row keeps its first n_det values
     const size_t slice = (size_t)n_ang_ * n_det_;
     in_.resize(2 * slice);
     std::memcpy(in_.data(), sino_[0], slice * sizeof(float));
@@ -115,7 +134,8 @@ class GridRec {
 
  private:
   int n_det_ = 0, n_ang_ = 0, n_theta_ = 0, filter_ = GR_FILTER_NONE, device_ = 0, m0_ = 0;
-  float center_ = -1.f;
+  float center_ = -1.f, shift_ = 0.f;
+  bool shift_set_ = false;
   float* theta_ = nullptr;
   float* sino_[2] = {nullptr, nullptr};
   float* recon_[2] = {nullptr, nullptr};

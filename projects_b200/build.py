@@ -17,7 +17,7 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgridrec_b200.so")
 SOURCES = ["gridrec_kernels.cu", "gridrec_plan.cu", "gridrec_prep.cu", "gridrec_fbp.cu",
-           "gridrec_cnn.cu"]
+           "gridrec_cnn.cu", "gridrec_cpp.cu"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 
@@ -33,7 +33,8 @@ def _stale() -> bool:
         return True
     t = os.path.getmtime(LIB)
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)]
-    deps.append(os.path.join(ROOT, "include", "gridrec_b200.h"))
+    inc = os.path.join(ROOT, "include")
+    deps += [os.path.join(inc, f) for f in os.listdir(inc)]
     return any(os.path.getmtime(d) > t for d in deps)
 
 

@@ -180,6 +180,24 @@ cudaError_t launch_fbp_filter(const FbpFilterArgs& a, cudaStream_t s);
 // Records a formatted message for gr_last_error() and returns code (gridrec_plan.cu).
 int fail(int code, const char* fmt, ...);
 
+// A prolate spheroidal wave function record: C, eigenvalue, Legendre degree and
+// the even-order Legendre coefficients (the layout of gridrec/GPU/gridrec.h:60-68,
+// in double).
+struct Pswf {
+  double C, lmbda;
+  int nt;
+  double coefs[11];
+};
+// The PSWF database entry within 0.01 of C, or null (gridrec_plan.cu).
+const Pswf* find_pswf(double C);
+// Filter value at x = j / pdim for a ReconAlgorithm filter code (gridrec_plan.cu).
+double filter_value(int code, double x);
+// Plan creation (gr_plan_create) with two GridrecCPP extras: the PSWF from a record
+// instead of the database lookup by p->pswf_c (null: the lookup), and the filter as
+// a caller's function of the frequency j / pdim (null: p->filter's formula).
+int plan_create_ex(const gr_params* p, const Pswf* pswf, float (*filter_fn)(float),
+                   gr_plan** plan);
+
 // Shape of a plan, for the pre/post-processing entry points (gridrec_plan.cu).
 int plan_shape(const gr_plan* p, int* n_det, int* n_ang, int* M0, int* max_pairs, int* device);
 // Grow-only device scratch owned by the plan (the slice-pipeline entry points).

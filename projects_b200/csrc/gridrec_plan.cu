@@ -44,11 +44,6 @@ namespace {
 
 // PSWF database: the numerical table of gridrec/GPU/gridrec.cu:21-114 (C,
 // eigenvalue, Legendre degree, even-order Legendre coefficients).
-struct Pswf {
-  double C, lmbda;
-  int nt;
-  double coefs[11];
-};
 const Pswf kPswfDb[5] = {
     {4.0, 0.99588549, 16,
      {0.5239891E+01, -0.5308499E+01, 0.1184591E+01, -0.1230763E-00, 0.7371623E-02,
@@ -67,6 +62,8 @@ const Pswf kPswfDb[5] = {
       -0.1780527E-00, 0.1372983E-01, -0.7963169E-03, 0.3593372E-04, -0.1295941E-05,
       0.3817796E-07}},
 };
+
+}  // namespace
 
 const Pswf* find_pswf(double C) {
   for (const Pswf& p : kPswfDb)
@@ -97,8 +94,6 @@ double filter_value(int code, double x) {
     default: return x;
   }
 }
-
-}  // namespace
 
 // ------------------------------------------------------------------ the plan
 
@@ -170,6 +165,8 @@ struct Plan {
   float* d_out[2] = {nullptr, nullptr};
   size_t in_bytes = 0, out_bytes = 0;  // per staging buffer
   long out_stride_staged = 0;
+  float* d_pair_in = nullptr;          // gr_reconstruct_pair_host: one pair of sinograms
+  float* d_pair_out = nullptr;         //   and its two M0 x M0 images
   cudaStream_t copy_stream = nullptr;   // host->device copies
   cudaStream_t d2h_stream = nullptr;    // device->host copies (runs beside the H2D ones)
   cudaEvent_t ev_h2d[2] = {}, ev_comp[2] = {}, ev_d2h[2] = {};
@@ -700,7 +697,7 @@ int geometry(const gr_params* prm, const Pswf* pw, Geometry* g) {
   return GR_OK;
 }
 
-int check_params(const gr_params* prm, const Pswf** pw) {
+int check_params(const gr_params* prm, const Pswf** pw, const Pswf* pswf_override = nullptr) {
   if (!prm) return fail(GR_ERR_ARG, "null argument");
   if (prm->geom < 0 || prm->geom > 2) return fail(GR_ERR_ARG, "geom must be 0, 1 or 2");
   if (prm->n_det < 9 || prm->n_ang < 1 || (prm->geom == 0 && !prm->theta_deg))
@@ -713,6 +710,13 @@ int check_params(const gr_params* prm, const Pswf** pw) {
     return fail(GR_ERR_ARG, "wide_grid must be -1, 0, 1, 2 or 3");
   if (prm->roi_size < 0.f || prm->roi_size > 4.f || prm->pixel_size < 0.f || prm->pixel_size > 16.f)
     return fail(GR_ERR_ARG, "roi_size in [0, 4] and pixel_size in [0, 16] (0 = 1)");
+  if (pswf_override) {
+    if (pswf_override->nt < 0 || pswf_override->nt > 20 || !(pswf_override->C > 0.0) ||
+        !(pswf_override->lmbda > 0.0))
+      return fail(GR_ERR_PSWF, "PSWF record: C > 0, eigenvalue > 0 and degree 0..20 required");
+    *pw = pswf_override;
+    return GR_OK;
+  }
   *pw = find_pswf(prm->pswf_c);
   if (!*pw) return fail(GR_ERR_PSWF, "Prolate parameter C = %f not in data base", prm->pswf_c);
   return GR_OK;
@@ -937,11 +941,18 @@ int gr_plan_destroy(gr_plan* plan) {
 }
 
 int gr_plan_create(const gr_params* prm, gr_plan** out) {
+  return gr::plan_create_ex(prm, nullptr, nullptr, out);
+}
+
+}  // extern "C"
+
+int gr::plan_create_ex(const gr_params* prm, const Pswf* pswf, float (*filter_fn)(float),
+                       gr_plan** out) {
   using namespace gr;
   if (!out) return fail(GR_ERR_ARG, "null argument");
   *out = nullptr;
   const Pswf* pw = nullptr;
-  int rc = check_params(prm, &pw);
+  int rc = check_params(prm, &pw, pswf);
   if (rc) return rc;
   Geometry geo;
   if ((rc = geometry(prm, pw, &geo))) return rc;
@@ -993,7 +1004,10 @@ int gr_plan_create(const gr_params* prm, gr_plan** out) {
   // filter x normalisation (filphase_su magnitude, gridrec.cu:789-797)
   std::vector<float> filt(p->J);
   const double norm = M_PI / pdim / prm->n_ang;
-  for (int j = 0; j < p->J; ++j) filt[j] = (float)(filter_value(prm->filter, (double)j / pdim) * norm);
+  for (int j = 0; j < p->J; ++j)
+    filt[j] = filter_fn  // a caller's filter function, sampled as filphase_su does (grid.cpp:437-461)
+                  ? (float)((double)filter_fn((float)j / (float)pdim) * norm)
+                  : (float)(filter_value(prm->filter, (double)j / pdim) * norm);
   // two-level twiddle table of exp(+2 pi i e/N): lo[e] for e < 64, then
   // hi[f] = exp(+2 pi i 64 f/N) for f < max(1, N/64); FP64, rounded once
   auto twiddles = [](int N) {
@@ -1054,6 +1068,8 @@ int gr_plan_create(const gr_params* prm, gr_plan** out) {
   *out = p;
   return GR_OK;
 }
+
+extern "C" {
 
 static int worklist_export(const gr_params* prm, bool wide, int* n_items, int* n_runs,
                            int* tiles_v, int* items, int* runs, int* splits, int cap_items,
@@ -1299,6 +1315,37 @@ int gr_reconstruct_pair(gr_plan* p, const float* sino1, const float* sino2, floa
   return launch_chunk(p, 1, n_valid, 0, sino1, sino2 ? sino2 : sino1, 0, GR_DTYPE_F32, nullptr,
                       nullptr, nullptr, 0, out1, out2 ? out2 : out1, 0, out_stride,
                       (cudaStream_t)stream);
+}
+
+int gr_reconstruct_pair_host(gr_plan* p, const float* sino1, const float* sino2, float* out1,
+                             float* out2, long out_stride, void* stream) {
+  using namespace gr;
+  if (!p || !sino1 || !out1) return fail(GR_ERR_ARG, "null argument");
+  if (out_stride < p->M0) return fail(GR_ERR_ARG, "out_stride %ld < M0 %d", out_stride, p->M0);
+  DeviceGuard g(p->device);
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t slice = (size_t)p->n_ang * p->n_det, img = (size_t)p->M0 * p->M0;
+  int rc;
+  if (!p->d_pair_in && ((rc = dev_alloc(p, &p->d_pair_in, 2 * slice)) ||
+                        (rc = dev_alloc(p, &p->d_pair_out, 2 * img))))
+    return rc;
+  // the caller's buffers straight to and from the device (pageable or pinned),
+  // the images with the caller's row stride: no host-side staging copies
+  GR_CUDA(cudaMemcpyAsync(p->d_pair_in, sino1, slice * sizeof(float), cudaMemcpyHostToDevice, st));
+  if (sino2)
+    GR_CUDA(cudaMemcpyAsync(p->d_pair_in + slice, sino2, slice * sizeof(float),
+                            cudaMemcpyHostToDevice, st));
+  const int n_valid = (sino2 && out2) ? 2 : 1;
+  rc = launch_chunk(p, 1, n_valid, 0, p->d_pair_in, p->d_pair_in + slice, 0, GR_DTYPE_F32, nullptr,
+                    nullptr, nullptr, 0, p->d_pair_out, p->d_pair_out + img, 0, p->M0, st);
+  if (rc) return rc;
+  const size_t row = (size_t)p->M0 * sizeof(float);
+  GR_CUDA(cudaMemcpy2DAsync(out1, (size_t)out_stride * sizeof(float), p->d_pair_out, row, row,
+                            p->M0, cudaMemcpyDeviceToHost, st));
+  if (out2 && n_valid == 2)
+    GR_CUDA(cudaMemcpy2DAsync(out2, (size_t)out_stride * sizeof(float), p->d_pair_out + img, row,
+                              row, p->M0, cudaMemcpyDeviceToHost, st));
+  return gr_plan_device_status(p, stream);  // synchronises the stream
 }
 
 int gr_reconstruct_batch(gr_plan* p, const gr_batch_desc* b, void* stream) {

@@ -30,6 +30,7 @@ EXPORTS = ("gr_params_default", "gr_filter_code", "gr_plan_create", "gr_plan_des
            "gr_plan_launch_count", "gr_plan_work_stats", "gr_worklist_export",
            "gr_worklist_export_wide", "gr_plan_grid_kernel",
            "gr_plan_set_timing", "gr_plan_stage_times", "gr_reconstruct_pair_noalloc",
+           "gr_reconstruct_pair_host",
            "gr_plan_device_status", "gr_selftest_wait_timeout", "gr_ring_workspace_bytes",
            "gr_ring_removal", "gr_shift_pad", "gr_crop_center", "gr_entropy_workspace_bytes",
            "gr_entropy", "gr_reconstruct_padded", "gr_center_search", "gr_graph_create",
@@ -90,6 +91,7 @@ def lib():
                                           C.c_void_p, C.c_long, C.c_void_p]
         L.gr_reconstruct_pair_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p,
                                                   C.c_void_p, C.c_void_p, C.c_long, C.c_void_p]
+        L.gr_reconstruct_pair_host.argtypes = L.gr_reconstruct_pair.argtypes
         L.gr_reconstruct_batch.argtypes = [C.c_void_p, C.POINTER(GrBatch), C.c_void_p]
         L.gr_reconstruct_host.argtypes = [C.c_void_p, C.POINTER(GrBatch), C.c_void_p]
         L.gr_last_error.restype = C.c_char_p
@@ -412,7 +414,8 @@ class GridRec:
     (sinogram n_ang x n_det float32; reconstruction n_det x n_det float32, the
     leading M0 x M0 block written with row stride n_det as in gridrec.cu:196-197),
     then reconstruct().  setCenter() adds the rotation centre that GridRec::init
-    fixes at n_det/2 (gridrec.cu:227) and find_shift's copy exposes.
+    fixes at n_det/2 (gridrec.cu:227); setCenterShift() is find_shift's form of it
+    (centre = n_det // 2 + shift at init, find_shift/src/main/gridrec.cu:229, 809-813).
     """
 
     def __init__(self):
@@ -421,6 +424,7 @@ class GridRec:
         self._filter = FILTER_NONE
         self._device = 0
         self._center = None
+        self._shift = None
         self._bufs = {}
         self._plan = None
 
@@ -459,11 +463,23 @@ class GridRec:
 
     def setCenter(self, center: float):
         self._center = float(center)
+        self._shift = None
+
+    def setCenterShift(self, shift: float):
+        self._shift = float(shift)
+
+    def getThetaList(self):
+        return self._theta
+
+    def getCenter(self):
+        if self._shift is not None:
+            return float(np.float32(self._dims[0] // 2) + np.float32(self._shift))
+        return self._center
 
     def init(self):
         n_det, n_ang = self._dims
-        self._plan = Plan(n_det, n_ang, self._theta, center=self._center, filter=self._filter,
-                          device=self._device, max_pairs=1)
+        self._plan = Plan(n_det, n_ang, self._theta, center=self.getCenter(),
+                          filter=self._filter, device=self._device, max_pairs=1)
         self.M0 = self._plan.M0
 
     def setSinoAndReconBuffers(self, number: int, sinogram, reconstruction):
@@ -473,14 +489,36 @@ class GridRec:
     def reconstruct(self):
         n_det, n_ang = self._dims
         s1, r1 = self._bufs[1]
-        s2, r2 = self._bufs.get(2, (np.zeros_like(s1), np.zeros_like(r1)))
-        sinos = np.stack([np.asarray(s1, np.float32).reshape(n_ang, n_det),
-                          np.asarray(s2, np.float32).reshape(n_ang, n_det)])
-        outs = np.zeros((2, self.M0, n_det), np.float32)
-        self._plan.reconstruct_host(sinos, outs)
+        s2, r2 = self._bufs.get(2, (None, None))
+        m0 = self.M0
+
+        def host_f32(x, shape):
+            a = np.asarray(x)
+            ok = a.dtype == np.float32 and a.flags.c_contiguous and a.size == shape[0] * shape[1]
+            return a if ok else np.ascontiguousarray(a, np.float32).reshape(shape)
+        in1 = host_f32(s1, (n_ang, n_det))
+        in2 = host_f32(s2, (n_ang, n_det)) if s2 is not None else None
+        direct = m0 <= n_det and all(
+            r is None or (isinstance(r, np.ndarray) and r.dtype == np.float32 and
+                          r.flags.c_contiguous and r.size >= m0 * n_det) for r in (r1, r2))
+        if direct:  # the caller's host arrays in and out, rows of stride n_det
+            _check(lib().gr_reconstruct_pair_host(
+                self._plan.handle, in1.ctypes.data, in2.ctypes.data if in2 is not None else None,
+                r1.ctypes.data, r2.ctypes.data if r2 is not None else None, n_det, None),
+                "gr_reconstruct_pair_host")
+            return
+        stride = max(m0, n_det)
+        outs = np.zeros((2, m0, stride), np.float32)
+        _check(lib().gr_reconstruct_pair_host(
+            self._plan.handle, in1.ctypes.data, in2.ctypes.data if in2 is not None else None,
+            outs[0].ctypes.data, outs[1].ctypes.data, stride, None), "gr_reconstruct_pair_host")
         for r, o in ((r1, outs[0]), (r2, outs[1])):
+            if r is None:
+                continue
             rv = np.asarray(r).reshape(-1, n_det)
-            rv[:self.M0, :self.M0] = o[:, :self.M0]
+            k = min(m0, n_det)
+            rows = min(m0, rv.shape[0])
+            rv[:rows, :k] = o[:rows, :k]
 
     def destroy(self):
         if self._plan is not None:

@@ -242,6 +242,35 @@ def test_gridrec_class_call_surface():
     assert np.all(r1[m:, :] == 0) and np.all(r1[:, m:] == 0)
 
 
+def test_gridrec_class_centre_shift_and_getters():
+    """find_shift's setter sequence: setCenterShift before init (centre n_det // 2 +
+    shift), the ReconAlgorithm getters, and images against float64 at that centre."""
+    n, a, shift = 128, 100, -1.3
+    th = ph.angles_deg(a)
+    c = float(np.float32(n // 2) + np.float32(shift))
+    s1 = ph.random_ellipse_sinogram(11, n, a, center=c)[0]
+    s2 = ph.random_ellipse_sinogram(12, n, a, center=c)[0]
+    g = G.GridRec()
+    g.setSinogramDimensions(n, a)
+    g.setThetaList(th, a)
+    g.setFilter(G.FILTER_HANN)
+    g.setCenterShift(shift)
+    assert (g.getSinogramXDimension(), g.getSinogramYDimension(), g.getThetaListSize(),
+            g.getFilter(), g.numberOfReconstructions()) == (n, a, a, G.FILTER_HANN, 2)
+    assert g.getCenter() == c
+    g.init()
+    r1 = np.zeros((n, n), np.float32)
+    r2 = np.zeros((n, n), np.float32)
+    g.setSinoAndReconBuffers(1, s1, r1)
+    g.setSinoAndReconBuffers(2, s2, r2)
+    g.reconstruct()
+    g.destroy()
+    o1, o2 = O.port_gridrec_pair(s1, s2, th, center1=c, filter=2)
+    m = o1.shape[0]
+    assert ph.rel_l2(r1[:m, :m], o1[:, :m]) < TOL
+    assert ph.rel_l2(r2[:m, :m], o2[:, :m]) < TOL
+
+
 # With only a few angles most grid cells receive one or two taps, so a tap
 # that FP32 positions move into the next table bin shows: the reference's own
 # FP32 build is 1.0-1.7e-3 from float64 on the 300-detector cases below.  With

@@ -225,6 +225,70 @@ def _build_shim(tmp_path):
     return exe
 
 
+def _build_demo(tmp_path, name):
+    """Builds tests/cxx/<name> (C or C++) against include/ and the library."""
+    import shutil
+    import subprocess
+    src = os.path.join(ROOT, "tests", "cxx", name)
+    cc = "gcc" if name.endswith(".c") else "g++"
+    if shutil.which(cc) is None:
+        pytest.skip(f"{cc} not available")
+    exe = str(tmp_path / name.split(".")[0])
+    lib_dir = os.path.join(ROOT, "projects_b200")
+    std = ["-std=c11"] if cc == "gcc" else ["-std=c++17"]
+    subprocess.run([cc, "-O2", *std, "-Wall", "-Werror", "-I", os.path.join(ROOT, "include"), src,
+                    "-L", lib_dir, "-lgridrec_b200", f"-Wl,-rpath,{lib_dir}", "-lm", "-o", exe],
+                   check=True)
+    return exe
+
+
+def test_gridrec_cpp_api_exports_and_callers_build(tmp_path):
+    """The GridrecCPP calling sequence (include/gridrec_cpp_b200.h): its functions and
+    row-pointer globals are exported, and a C caller and a find_shift-style C++
+    caller build against include/ and the library."""
+    lib = G.lib()
+    for name in ("recon_init", "do_recon", "recon_free", "get_pswf", "get_filter",
+                 "gr_gridrec_cpp_status", "gr_gridrec_cpp_set_device"):
+        assert hasattr(lib, name), name
+    for name in ("G1", "G2", "S1", "S2"):
+        assert C.c_void_p.in_dll(lib, name).value is None  # null until a caller sets them
+    assert C.c_long.in_dll(lib, "imgsiz").value == 0
+    assert os.path.exists(_build_demo(tmp_path, "gridrec_cpp_demo.c"))
+    assert os.path.exists(_build_demo(tmp_path, "find_shift_demo.cpp"))
+
+
+class _PswfStruct(C.Structure):
+    _fields_ = [("C", C.c_float), ("nt", C.c_int), ("lmbda", C.c_float),
+                ("coefs", C.c_float * 15)]
+
+
+def test_gridrec_cpp_pswf_and_filters_host():
+    """get_pswf / get_filter (Gridrec5.2/pswf.cpp:36-47, filters.cpp:26-48): database
+    entries by C, an unknown C reported instead of exit(2); the filter formulas,
+    and an unknown name giving Shepp-Logan with the name overwritten."""
+    lib = G.lib()
+    lib.get_pswf.argtypes = [C.c_float, C.POINTER(C.POINTER(_PswfStruct))]
+    ptr = C.POINTER(_PswfStruct)()
+    lib.get_pswf(6.0, C.byref(ptr))
+    assert lib.gr_gridrec_cpp_status() == 0
+    assert ptr.contents.nt == 18 and abs(ptr.contents.lmbda - 0.9990188) < 1e-7
+    assert abs(ptr.contents.coefs[0] - 24.95593) < 1e-4
+    lib.get_pswf(5.5, C.byref(ptr))
+    assert not ptr and lib.gr_gridrec_cpp_status() == -2
+    FN = C.CFUNCTYPE(C.c_float, C.c_float)
+    lib.get_filter.restype = FN
+    lib.get_filter.argtypes = [C.c_char_p]
+    x = 0.3
+    want = {"shlo": abs(np.sin(np.pi * x) / np.pi), "hann": x * 0.5 * (1 + np.cos(2 * np.pi * x)),
+            "hamming": x * (0.54 + 0.46 * np.cos(2 * np.pi * x)), "ramlak": x}
+    for name, v in want.items():
+        buf = C.create_string_buffer(name.encode(), 16)
+        assert abs(lib.get_filter(buf)(x) - v) < 1e-7, name
+    buf = C.create_string_buffer(b"bogus", 16)
+    assert abs(lib.get_filter(buf)(x) - want["shlo"]) < 1e-7
+    assert buf.value == b"shlo"
+
+
 def test_cxx_shim_compiles_against_the_c_abi(tmp_path):
     """include/gridrec_b200.hpp (the GridRec-compatible class) builds and links."""
     assert os.path.exists(_build_shim(tmp_path))
