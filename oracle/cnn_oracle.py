@@ -39,15 +39,17 @@ def _shift(a, dy, dx):
 TAPS = [(t // 3 - 1, t % 3 - 1) for t in range(9)]
 
 
-def forward(p, x, bf16=False):
+def forward(p, x, bf16=False, x_conv1=None):
     """x (N, H, W) -> dict of h1, h2 (N, H, W, 16), y (N, H, W).  bf16=True rounds the
-    stored hidden activations to bfloat16 as the device does."""
+    stored hidden activations to bfloat16 as the device does; x_conv1 (optional) is
+    conv1's input in place of x (a rounded copy of it), the residual still adds x."""
     w1, b1, w2, b2, w3, b3 = unpack(p)
     x = np.asarray(x, np.float64)
+    xc = x if x_conv1 is None else np.asarray(x_conv1, np.float64)
     rnd = _bf16 if bf16 else (lambda a: a)
     z1 = np.broadcast_to(b1, x.shape + (C,)).copy()
     for t, (dy, dx) in enumerate(TAPS):
-        z1 += _shift(x, dy, dx)[..., None] * w1[t]
+        z1 += _shift(xc, dy, dx)[..., None] * w1[t]
     h1 = rnd(np.maximum(z1, 0.0))
     z2 = np.broadcast_to(b2, x.shape + (C,)).copy()
     for t, (dy, dx) in enumerate(TAPS):

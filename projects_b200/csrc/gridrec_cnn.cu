@@ -18,6 +18,7 @@
 
 #include <algorithm>
 
+#include "gr_device.cuh"
 #include "gr_internal.h"
 
 namespace gr {
@@ -356,6 +357,337 @@ __global__ void cnn_adam_kernel(float* params, const float* grads, float* m, flo
   params[k] -= lr * (mk / c1) / (sqrtf(vk / c2) + eps);
 }
 
+// ---------------------------------------------------------------- fused inference, tcgen05
+// One CTA (8 warps) computes output tiles of kFTh x kFTw pixels.  The tile's x region
+// ((kFTh + 6) x (kFTw + 6) pixels), its h1 and h2 and conv3's per-tap partials stay in
+// shared memory; only x is read from HBM and y written.  Positions of the x region are
+// flattened with row stride kFWt, so a 3x3 tap (dy, dx) is the constant offset
+// dy kFWt + dx: conv2 on a block of 128 consecutive positions is nine tcgen05 MMAs whose
+// A operand is the same activation plane started dy kFWt + dx positions later -- no
+// im2col copy.  The layers:
+//  * conv1 (1 -> 16): a tcgen05 MMA per block of 128 positions on a 16-wide im2col of x
+//    (the nine taps and seven zeros, BF16) built in shared memory, against w1 in BF16,
+//    on the rows conv2 reads (rows 1..kFTh+4 of the x region); the im2col is dead once
+//    the MMAs are done, and h1 = relu(conv1 + b1) in BF16 is written over it;
+//  * conv2 (16 -> 16): tcgen05.mma kind::f16, BF16 operands from shared memory (A: 128
+//    positions x 16 input channels, K-major, two 8-channel planes; B: the tap's 16 x 16
+//    weights), FP32 accumulator in tensor memory (M = 128, N = 16, K = 16; one MMA per
+//    tap), then bias, ReLU and BF16 on the way back to shared memory;
+//  * conv3 (16 -> 1): a 1x1 tcgen05 MMA to the nine per-tap partials
+//    Z[p][tap] = sum_ci w3[tap][ci] h2[p][ci] (w3 in BF16; N = 16, taps 9..15 zero), then
+//    y[p] = x[p] + (b3 + sum_tap Z[p + (dy, dx)][tap]) in FP32 on the CUDA cores.
+// Positions outside the image hold zero x, h1 and h2 (the network's zero padding); the
+// wrap-around columns of the flattened rows produce values only at positions that no
+// kept output reads.  One thread issues the MMAs; completion is a tcgen05.commit on an
+// mbarrier with bounded waits (timeout: error word, early exit).  Each CTA holds 256
+// tensor-memory columns; its dynamic shared memory (kFSmemLaunch) admits at most two CTAs
+// per SM, so an allocation never waits on a third.
+
+constexpr int kFTh = 16, kFTw = 64;
+constexpr int kFWt = kFTw + 6;                                 // flattened row stride
+constexpr int kFRows = kFTh + 6;
+constexpr int kFPos = kFRows * kFWt;                           // positions of the x region
+constexpr int kFPlane = 1536;                                  // positions per activation plane
+constexpr int kFQ1 = kFWt, kFQ1e = (kFTh + 5) * kFWt;          // conv1: rows 1..kFTh+4
+constexpr int kFQ2 = 2 * kFWt;                                 // first conv2 / conv3 position
+constexpr int kFBlocks = ((kFTh + 4) * kFWt - kFQ2 + 127) / 128;  // 128-position blocks
+constexpr int kFBlocks1 = (kFQ1e - kFQ1 + 127) / 128;           // conv1's blocks from kFQ1
+constexpr int kFZ = 128 * kFBlocks;                            // partials per tap
+constexpr int kFThreads = 256;
+constexpr int kFXOff = 72;                                     // x buffer: reads at q - 71 .. q + 71
+constexpr int kFXLen = kFPos + 2 * kFXOff;
+constexpr int kFTmemCols = 256;
+constexpr int kFParams = 177;                                  // w1, b1, b2, b3 in FP32
+// shared memory: activation planes | B2 (9 taps) | B3 | B1 | x | FP32 params | mbarrier, tmem slot
+constexpr int kFSmAct = 0, kFSmB2 = 2 * kFPlane * 16, kFSmB3 = kFSmB2 + 9 * 512;
+constexpr int kFSmB1 = kFSmB3 + 512;
+constexpr int kFSmX = kFSmB1 + 512, kFSmP = kFSmX + kFXLen * 4;
+constexpr int kFSmBar = (kFSmP + kFParams * 4 + 15) & ~15;
+constexpr int kFSmUsed = kFSmBar + 16;
+constexpr int kFSmemLaunch = 100 * 1024;
+static_assert(kFQ2 + kFZ + kFWt + 1 <= kFPlane, "conv2's shifted reads stay inside the planes");
+static_assert(kFQ1 + 128 * kFBlocks1 <= kFPlane, "conv1's blocks fit the planes");
+static_assert(16 * kFBlocks1 <= kFTmemCols, "conv1's accumulators fit the allocation");
+static_assert(9 * kFZ * 4 <= 2 * kFPlane * 16, "conv3's partials fit the activation buffer");
+static_assert(16 * kFBlocks <= kFTmemCols, "accumulators fit the tensor-memory allocation");
+static_assert(kFSmUsed <= kFSmemLaunch && 3 * (kFSmemLaunch + 1024) > 228 * 1024,
+              "at most two CTAs per SM");
+
+__device__ __forceinline__ uint64_t cnn_smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  // start >> 4 [0,14), leading-dimension offset >> 4 [16,30), stride offset >> 4
+  // [32,46), version 1 [46,48); no swizzle, base offset 0 (K-major core matrices of
+  // 8 rows x 16 bytes)
+  return (uint64_t)((saddr >> 4) & 0x3FFF) | ((uint64_t)((lbo >> 4) & 0x3FFF) << 16) |
+         ((uint64_t)((sbo >> 4) & 0x3FFF) << 32) | (1ull << 46);
+}
+// instruction descriptor: D f32 [4,6) = 1, A bf16 [7,10) = 1, B bf16 [10,13) = 1, both
+// K-major, N = 16 [17,23) = 16 >> 3, M = 128 [24,29) = 128 >> 4
+constexpr uint32_t kCnnIdesc = (1u << 4) | (1u << 7) | (1u << 10) | ((16u >> 3) << 17) |
+                               ((128u >> 4) << 24);
+
+__device__ __forceinline__ void cnn_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t acc) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem),
+      "l"(da), "l"(db), "r"(kCnnIdesc), "r"(acc));
+}
+__device__ __forceinline__ void cnn_commit(uint64_t* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                   smem_u32(bar))
+               : "memory");
+}
+// 16 accumulator columns of this warp's 32 lanes
+__device__ __forceinline__ void cnn_tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+      "%14,%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
+}
+
+__global__ void __launch_bounds__(kFThreads, 2) cnn_fused_kernel(const float* params, const float* x,
+                                                                  float* y, int n_img, int h, int w,
+                                                                  int* err) {
+  extern __shared__ __align__(1024) unsigned char smf[];
+  uint4* act = reinterpret_cast<uint4*>(smf + kFSmAct);  // plane g: act[g kFPlane + q] = 8 BF16 channels
+  unsigned short* b2s = reinterpret_cast<unsigned short*>(smf + kFSmB2);
+  unsigned short* b3s = reinterpret_cast<unsigned short*>(smf + kFSmB3);
+  unsigned short* b1s = reinterpret_cast<unsigned short*>(smf + kFSmB1);
+  float* xs = reinterpret_cast<float*>(smf + kFSmX) + kFXOff;
+  float* pw = reinterpret_cast<float*>(smf + kFSmP);
+  uint64_t* bar = reinterpret_cast<uint64_t*>(smf + kFSmBar);
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(smf + kFSmBar + 8);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // B operands in BF16, K-major core matrices [ci / 8][n][ci % 8]: conv2's taps (n = co)
+  // and conv3's 1x1 matrix (n = tap, taps 9..15 zero); FP32 w1, b1, b2, b3
+  for (int e = tid; e < 9 * 256; e += kFThreads) {
+    const int t = e >> 8, g = (e >> 7) & 1, co = (e >> 3) & 15, k8 = e & 7;
+    const __nv_bfloat16 v = __float2bfloat16_rn(params[kW2 + (t * kC + co) * kC + g * 8 + k8]);
+    b2s[e] = *reinterpret_cast<const unsigned short*>(&v);
+  }
+  for (int e = tid; e < 256; e += kFThreads) {
+    const int g = e >> 7, n = (e >> 3) & 15, k8 = e & 7;
+    const __nv_bfloat16 v = __float2bfloat16_rn(n < 9 ? params[kW3 + n * kC + g * 8 + k8] : 0.f);
+    b3s[e] = *reinterpret_cast<const unsigned short*>(&v);
+  }
+  for (int e = tid; e < 256; e += kFThreads) {  // conv1: n = co, k = tap (taps 9..15 zero)
+    const int g = e >> 7, co = (e >> 3) & 15, k = g * 8 + (e & 7);
+    const __nv_bfloat16 v = __float2bfloat16_rn(k < 9 ? params[kW1 + k * kC + co] : 0.f);
+    b1s[e] = *reinterpret_cast<const unsigned short*>(&v);
+  }
+  for (int i = tid; i < kFParams; i += kFThreads)
+    pw[i] = i < kB1 + kC ? params[i] : (i < kB1 + 2 * kC ? params[kB2 + i - kB1 - kC] : params[kB3]);
+  for (int i = tid; i < kFXLen; i += kFThreads) xs[i - kFXOff] = 0.f;
+  for (int i = tid; i < 2 * kFPlane; i += kFThreads) act[i] = make_uint4(0u, 0u, 0u, 0u);
+  if (tid == 0) {
+    mbar_init(bar, 1);
+    fence_mbar_init();
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                     smem_u32(tslot)), "n"(kFTmemCols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  fence_proxy_async();  // the B operands and zeroed planes, before the tensor core reads them
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const uint32_t a0 = smem_u32(act), b2a = smem_u32(b2s), b3a = smem_u32(b3s), b1a = smem_u32(b1s);
+  const int tiles_x = (w + kFTw - 1) / kFTw, tiles_y = (h + kFTh - 1) / kFTh;
+  const long n_tiles = (long)n_img * tiles_x * tiles_y;
+  const int lq = warp & 3;  // this warp's quarter of the tensor-memory lanes
+  unsigned phase = 0;
+  bool ok = true;
+  // the x region of a tile (zero outside the image), this thread's positions
+  // tid + k kFThreads; loaded one tile ahead into registers, so that the loads' latency
+  // passes during the previous tile's work
+  constexpr int kXPer = (kFPos + kFThreads - 1) / kFThreads;
+  float xr[kXPer];
+  auto load_x = [&](long t) {
+    const int im = (int)(t / ((long)tiles_x * tiles_y));
+    const int rem = (int)(t - (long)im * tiles_x * tiles_y);
+    const int ty0 = (rem / tiles_x) * kFTh, tx0 = (rem % tiles_x) * kFTw;
+    const float* xm = x + (size_t)im * h * w;
+#pragma unroll
+    for (int k = 0; k < kXPer; ++k) {
+      const int q = tid + k * kFThreads;
+      const int r = q / kFWt, c = q - r * kFWt;
+      const int iy = ty0 - 3 + r, ix = tx0 - 3 + c;
+      xr[k] = (q < kFPos && t < n_tiles && iy >= 0 && iy < h && ix >= 0 && ix < w)
+                  ? __ldg(&xm[(size_t)iy * w + ix])
+                  : 0.f;
+    }
+  };
+  load_x(blockIdx.x);
+  for (long tile = blockIdx.x; tile < n_tiles; tile += gridDim.x) {
+    const int im = (int)(tile / ((long)tiles_x * tiles_y));
+    const int rem = (int)(tile - (long)im * tiles_x * tiles_y);
+    const int y0 = (rem / tiles_x) * kFTh, x0 = (rem % tiles_x) * kFTw;
+    auto inside = [&](int q) {
+      const int r = q / kFWt, c = q - (q / kFWt) * kFWt;
+      const int iy = y0 - 3 + r, ix = x0 - 3 + c;
+      return iy >= 0 && iy < h && ix >= 0 && ix < w;
+    };
+#pragma unroll
+    for (int k = 0; k < kXPer; ++k)
+      if (tid + k * kFThreads < kFPos) xs[tid + k * kFThreads] = xr[k];
+    __syncthreads();
+    load_x(tile + gridDim.x);  // the next tile's x, in flight during this tile
+    // conv1's im2col (BF16): plane 0 holds taps 0..7 of position q, plane 1 tap 8 and
+    // zeros; conv1's blocks cover [kFQ1, kFQ1 + 128 kFBlocks1)
+    for (int q = kFQ1 + tid; q < kFQ1 + 128 * kFBlocks1; q += kFThreads) {
+      float in[9];
+#pragma unroll
+      for (int tap = 0; tap < 9; ++tap) in[tap] = xs[q + tap_dy(tap) * kFWt + tap_dx(tap)];
+      act[q] = make_uint4(pack_bf16(in[0], in[1]), pack_bf16(in[2], in[3]),
+                          pack_bf16(in[4], in[5]), pack_bf16(in[6], in[7]));
+      act[kFPlane + q] = make_uint4(pack_bf16(in[8], 0.f), 0u, 0u, 0u);
+    }
+    fence_proxy_async();
+    __syncthreads();
+    if (tid == 0) {
+      tc_fence_after();
+      for (int b = 0; b < kFBlocks1; ++b)
+        cnn_mma(tmem + 16 * b, cnn_smem_desc(a0 + (kFQ1 + 128 * b) * 16, kFPlane * 16, 128),
+                cnn_smem_desc(b1a, 256, 128), 0u);
+      cnn_commit(bar);
+    }
+    bool got = warp == 0 ? mbar_wait(bar, phase) : true;
+    if (__syncthreads_or(!got)) {
+      ok = false;
+      break;
+    }
+    phase ^= 1u;
+    tc_fence_after();
+    // h1 = relu(conv1 + b1) in BF16 over the im2col (every MMA reading it is done); zero
+    // outside the image and beyond conv1's rows; the planes' other positions are
+    // cleared of the previous tile's values
+    for (int b = warp >> 2; b < kFBlocks1; b += 2) {
+      float v[16];
+      cnn_tmem_ld16(tmem + ((uint32_t)(32 * lq) << 16) + 16 * b, v);
+      const int q = kFQ1 + 128 * b + 32 * lq + lane;
+      uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
+      if (q < kFQ1e && inside(q)) {
+        unsigned o[kC / 2];
+#pragma unroll
+        for (int c = 0; c < kC; c += 2)
+          o[c / 2] = pack_bf16(fmaxf(v[c] + pw[kB1 + c], 0.f), fmaxf(v[c + 1] + pw[kB1 + c + 1], 0.f));
+        lo = make_uint4(o[0], o[1], o[2], o[3]);
+        hi = make_uint4(o[4], o[5], o[6], o[7]);
+      }
+      act[q] = lo;
+      act[kFPlane + q] = hi;
+    }
+    for (int i = tid; i < kFPlane - 128 * kFBlocks1; i += kFThreads) {
+      const int q = i < kFQ1 ? i : i + 128 * kFBlocks1;
+      act[q] = act[kFPlane + q] = make_uint4(0u, 0u, 0u, 0u);
+    }
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    // conv2: nine MMAs per block of 128 positions, A shifted by the tap's offset
+    if (tid == 0) {
+      tc_fence_after();
+      for (int b = 0; b < kFBlocks; ++b)
+#pragma unroll
+        for (int t = 0; t < 9; ++t) {
+          const uint32_t q = kFQ2 + 128 * b + tap_dy(t) * kFWt + tap_dx(t);
+          cnn_mma(tmem + 16 * b, cnn_smem_desc(a0 + q * 16, kFPlane * 16, 128),
+                  cnn_smem_desc(b2a + t * 512, 256, 128), t > 0 ? 1u : 0u);
+        }
+      cnn_commit(bar);
+    }
+    // one warp polls the barrier; the others wait at the CTA barrier (no issue slots)
+    got = warp == 0 ? mbar_wait(bar, phase) : true;
+    if (__syncthreads_or(!got)) {
+      ok = false;
+      break;
+    }
+    phase ^= 1u;
+    tc_fence_after();
+    // h2 = relu(conv2 + b2) in BF16 over h1's planes (every MMA reading h1 is done);
+    // warps 0-3 take the even blocks, 4-7 the odd ones
+    for (int b = warp >> 2; b < kFBlocks; b += 2) {
+      float v[16];
+      cnn_tmem_ld16(tmem + ((uint32_t)(32 * lq) << 16) + 16 * b, v);
+      const int q = kFQ2 + 128 * b + 32 * lq + lane;
+      uint4 lo = make_uint4(0u, 0u, 0u, 0u), hi = lo;
+      if (inside(q)) {
+        unsigned o[kC / 2];
+#pragma unroll
+        for (int c = 0; c < kC; c += 2)
+          o[c / 2] = pack_bf16(fmaxf(v[c] + pw[kB1 + kC + c], 0.f),
+                               fmaxf(v[c + 1] + pw[kB1 + kC + c + 1], 0.f));
+        lo = make_uint4(o[0], o[1], o[2], o[3]);
+        hi = make_uint4(o[4], o[5], o[6], o[7]);
+      }
+      act[q] = lo;
+      act[kFPlane + q] = hi;
+    }
+    fence_proxy_async();
+    tc_fence_before();
+    __syncthreads();
+    // conv3's 1x1 MMA: Z[q][tap] for every block
+    if (tid == 0) {
+      tc_fence_after();
+      for (int b = 0; b < kFBlocks; ++b)
+        cnn_mma(tmem + 16 * b, cnn_smem_desc(a0 + (kFQ2 + 128 * b) * 16, kFPlane * 16, 128),
+                cnn_smem_desc(b3a, 256, 128), 0u);
+      cnn_commit(bar);
+    }
+    got = warp == 0 ? mbar_wait(bar, phase) : true;
+    if (__syncthreads_or(!got)) {
+      ok = false;
+      break;
+    }
+    phase ^= 1u;
+    tc_fence_after();
+    // partials into the activation buffer (h2 is consumed): z_s[tap][q - kFQ2]
+    float* zs = reinterpret_cast<float*>(smf + kFSmAct);
+    for (int b = warp >> 2; b < kFBlocks; b += 2) {
+      float v[16];
+      cnn_tmem_ld16(tmem + ((uint32_t)(32 * lq) << 16) + 16 * b, v);
+      const int qi = 128 * b + 32 * lq + lane;
+#pragma unroll
+      for (int t = 0; t < 9; ++t) zs[t * kFZ + qi] = v[t];
+    }
+    tc_fence_before();
+    __syncthreads();
+    // y = x + (b3 + sum_tap Z[p + (dy, dx)][tap])
+    float* ym = y + (size_t)im * h * w;
+    for (int k = tid; k < kFTh * kFTw; k += kFThreads) {
+      const int ry = k / kFTw, rx = k - ry * kFTw;
+      const int iy = y0 + ry, ix = x0 + rx;
+      if (iy >= h || ix >= w) continue;
+      const int q = (ry + 3) * kFWt + rx + 3;
+      float z = pw[kB1 + 2 * kC];
+#pragma unroll
+      for (int t = 0; t < 9; ++t) z += zs[t * kFZ + q + tap_dy(t) * kFWt + tap_dx(t) - kFQ2];
+      ym[(size_t)iy * w + ix] = xs[q] + z;
+    }
+    __syncthreads();  // x and the partials are read before the next tile overwrites them
+  }
+  if (!ok) {
+    if (tid == 0) atomicExch(err, 1);
+    // the MMAs in flight finish before the tensor memory is released
+    if (warp == 0) mbar_wait(bar, phase);
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem),
+                 "n"(kFTmemCols)
+                 : "memory");
+}
+
 int cnn_check(int n_img, int h, int w) {
   if (n_img < 1 || h < 1 || w < 1 || n_img > 65535 || h > 65535)
     return fail(GR_ERR_ARG, "cnn: need 1 <= n_img, h <= 65535 and w >= 1");
@@ -441,6 +773,40 @@ int gr_cnn_backward(const float* params, const float* x, const float* y, const f
   }
   e = cudaGetLastError();
   return e == cudaSuccess ? GR_OK : fail(GR_ERR_CUDA, "cnn backward: %s", cudaGetErrorString(e));
+}
+
+size_t gr_cnn_infer_workspace_bytes(void) { return 256; }
+
+int gr_cnn_infer(const float* params, const float* x, float* y, int n_img, int h, int w,
+                 void* workspace, void* stream) {
+  int rc = cnn_check(n_img, h, w);
+  if (rc) return rc;
+  if (!params || !x || !y || !workspace) return fail(GR_ERR_ARG, "cnn infer: null pointer");
+  cudaStream_t st = (cudaStream_t)stream;
+  int dev = 0, sms = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e == cudaSuccess) e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(cnn_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             kFSmemLaunch);
+  if (e != cudaSuccess) return fail(GR_ERR_CUDA, "cnn infer: %s", cudaGetErrorString(e));
+  const long tiles = (long)n_img * ((h + kFTh - 1) / kFTh) * ((w + kFTw - 1) / kFTw);
+  const int blocks = (int)std::min<long>(tiles, 2L * sms);
+  cnn_fused_kernel<<<blocks, kFThreads, kFSmemLaunch, st>>>(params, x, y, n_img, h, w,
+                                                            static_cast<int*>(workspace));
+  e = cudaGetLastError();
+  return e == cudaSuccess ? GR_OK : fail(GR_ERR_CUDA, "cnn infer: %s", cudaGetErrorString(e));
+}
+
+int gr_cnn_infer_status(void* workspace, void* stream) {
+  if (!workspace) return fail(GR_ERR_ARG, "cnn infer status: null workspace");
+  cudaStream_t st = (cudaStream_t)stream;
+  int flag = 0;
+  cudaError_t e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess) e = cudaMemcpy(&flag, workspace, sizeof(int), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && flag) e = cudaMemset(workspace, 0, sizeof(int));
+  if (e != cudaSuccess) return fail(GR_ERR_CUDA, "cnn infer status: %s", cudaGetErrorString(e));
+  return flag ? fail(GR_ERR_TIMEOUT, "cnn infer: a bounded device wait ran out") : GR_OK;
 }
 
 int gr_cnn_adam(float* params, const float* grads, float* m, float* v, int step, float lr,

@@ -25,6 +25,7 @@
 #include <mutex>
 #include <vector>
 
+#include "gr_device.cuh"
 #include "gr_internal.h"
 
 namespace gr {
@@ -360,41 +361,8 @@ __device__ __forceinline__ void load_twiddles(float2* dst, const float2* src, in
 constexpr int kTwSlots = 64 + 128;  // table slots reserved in shared memory (N <= 8192)
 
 // ------------------------------------------------------------------ bulk copies + mbarriers
-// One-dimensional TMA bulk copies (global -> shared) completed on an
-// mbarrier.  Every wait is bounded: after kWaitLimit polls the kernel records
-// a timeout in the plan's device error word and stops.
+// (the 1-D bulk copy, mbarrier and tcgen05 fence helpers are in gr_device.cuh)
 
-constexpr int kWaitLimit = 1 << 22;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-__device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
-               : "memory");
-}
-// makes an mbarrier initialisation visible to the async proxy (bulk copies)
-__device__ __forceinline__ void fence_mbar_init() {
-  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-// orders this thread's generic-proxy shared accesses before later async-proxy ones
-__device__ __forceinline__ void fence_proxy_async() {
-  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-}
-__device__ __forceinline__ void mbar_expect_tx(uint64_t* bar, unsigned bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, unsigned bytes,
-                                         uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-          smem_u32(dst)),
-      "l"(src), "r"(bytes), "r"(smem_u32(bar))
-      : "memory");
-}
 // Tiled 2-D TMA load of one box at (x, y) (x: innermost, in elements) into
 // shared memory, completed on `bar`.  x * element size must be a multiple of 16.
 __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
@@ -405,23 +373,6 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
       "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(smem_u32(bar))
       : "memory");
 }
-__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, unsigned parity) {
-  uint32_t ok;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}"
-      : "=r"(ok)
-      : "r"(smem_u32(bar)), "r"(parity)
-      : "memory");
-  return ok != 0;
-}
-// Bounded wait for phase `parity` of `bar`; false when the limit ran out.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, unsigned parity) {
-  for (int it = 0; it < kWaitLimit; ++it)
-    if (mbar_try_wait(bar, parity)) return true;
-  return false;
-}
-
 // ------------------------------------------------------------------ phase ramps
 
 __global__ void phase_kernel(PhaseArgs a) {
@@ -1451,12 +1402,6 @@ __device__ __forceinline__ void tc_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                    smem_u32(bar))
                : "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
 }
 __device__ __forceinline__ float tf32_hi(float x) { return __uint_as_float(__float_as_uint(x) & 0xFFFFE000u); }
 

@@ -39,7 +39,8 @@ EXPORTS = ("gr_params_default", "gr_filter_code", "gr_plan_create", "gr_plan_des
            "gr_threshold_workspace_bytes", "gr_threshold_range", "gr_to_u8",
            "gr_fbp_destroy", "gr_cnn_param_count", "gr_cnn_workspace_bytes",
            "gr_cnn_forward_workspace_bytes", "gr_cnn_forward",
-           "gr_cnn_backward", "gr_cnn_adam")
+           "gr_cnn_backward", "gr_cnn_adam", "gr_cnn_infer_workspace_bytes", "gr_cnn_infer",
+           "gr_cnn_infer_status")
 STAGES = ("phase", "spectra", "grid", "cols", "rows_deapod")
 
 

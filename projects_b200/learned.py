@@ -4,9 +4,10 @@ reference's table (C = 4, 3 x 3 taps instead of 4 x 4 at C = 6) followed by a
 gridrec.  Plain gridrec stays the fallback and the judge: a batch whose held-out
 error against the full kernel exceeds the tolerance is recomputed with it.
 
-The network runs on this library's own kernels (projects_b200/csrc/gridrec_cnn.cu:
-BF16 tensor-core 16 -> 16 layer, FP32 accumulation), trained on the GPU by its own
-forward, backward and Adam kernels.
+The network runs on this library's own kernels (projects_b200/csrc/gridrec_cnn.cu):
+inference is one fused kernel per launch (tcgen05 BF16 MMAs for the 16 -> 16 layer
+and conv3's 1x1 partials, FP32 accumulation in tensor memory, activations kept in
+shared memory); training runs its own forward, backward and Adam kernels.
 """
 from __future__ import annotations
 
@@ -34,6 +35,9 @@ def _lib():
         L.gr_cnn_backward.argtypes = [vp, vp, vp, vp, i_, i_, i_, vp, C.POINTER(C.c_double), vp,
                                       vp]
         L.gr_cnn_adam.argtypes = [vp, vp, vp, vp, i_, f_, f_, f_, f_, vp]
+        L.gr_cnn_infer_workspace_bytes.restype = C.c_size_t
+        L.gr_cnn_infer.argtypes = [vp, vp, vp, i_, i_, i_, vp, vp]
+        L.gr_cnn_infer_status.argtypes = [vp, vp]
         L._cnn_bound = True
     return L
 
@@ -63,6 +67,9 @@ class CorrectionNet:
         self.step = 0
         self._ws = None
         self._ws_shape = None
+        # the fused inference kernel's error word (zeroed; gr_cnn_infer_status clears it)
+        self._iws = torch.zeros(int(_lib().gr_cnn_infer_workspace_bytes()), dtype=torch.uint8,
+                                device=self.params.device)
 
     def _workspace(self, n, h, w, train=False):
         """Forward-only workspace (the activations) unless training needs the
@@ -88,6 +95,22 @@ class CorrectionNet:
         G._check(_lib().gr_cnn_forward(G._ptr(self.params), G._ptr(x), G._ptr(y), n, h, w,
                                        G._ptr(ws), G._stream_ptr(stream)), "gr_cnn_forward")
         return y
+
+    def infer(self, x, y=None, stream=None):
+        """x: (N, H, W) float32 CUDA tensor -> y = x + correction, by the fused
+        tcgen05 inference kernel (conv3's weights in BF16; no activation workspace)."""
+        import torch
+        n, h, w = x.shape
+        if y is None:
+            y = torch.empty_like(x)
+        G._check(_lib().gr_cnn_infer(G._ptr(self.params), G._ptr(x), G._ptr(y), n, h, w,
+                                     G._ptr(self._iws), G._stream_ptr(stream)), "gr_cnn_infer")
+        return y
+
+    def infer_status(self, stream=None):
+        """Synchronises; raises if a bounded wait of the fused kernel ran out."""
+        G._check(_lib().gr_cnn_infer_status(G._ptr(self._iws), G._stream_ptr(stream)),
+                 "gr_cnn_infer_status")
 
     def loss_and_grads(self, x, target, stream=None):
         """Forward + backward; fills self.grads, returns the mean-squared loss."""
@@ -143,9 +166,9 @@ class LearnedGridrec:
         return torch.sqrt(torch.mean(images * images, dim=(1, 2), keepdim=True)).clamp_min(1e-30)
 
     def correct(self, raw, stream=None):
-        """s * net(raw / s) per slice."""
+        """s * net(raw / s) per slice (the fused inference kernel)."""
         s = self.scales(raw)
-        return self.net.forward((raw / s).contiguous(), stream=stream) * s
+        return self.net.infer((raw / s).contiguous(), stream=stream) * s
 
     def corrected(self, sinos, centers=None, stream=None):
         """Narrow-kernel images corrected by the network, (S, M0, M0)."""
@@ -156,17 +179,23 @@ class LearnedGridrec:
         return self.correct(raw, stream=stream)
 
     def reconstruct_batch(self, sinos, centers=None, stream=None):
-        """Returns (images, info): info = {"held_out_rel_l2", "fallback"}."""
+        """Returns (images, info): info = {"held_out_rel_l2", "fallback"}.  The first
+        pair is judged before the rest is reconstructed, so a batch that falls back
+        runs the narrow kernel and the network on two slices only."""
         import torch
-        out = self.corrected(sinos, centers, stream)
         k = min(2, sinos.shape[0])
+        ck = None if centers is None else centers[:k]
         ref = torch.empty((k, self.M0, self.M0), dtype=torch.float32, device=sinos.device)
-        self.full.reconstruct_batch(sinos[:k], ref, centers=None if centers is None
-                                    else centers[:k], stream=stream)
-        err = float(torch.linalg.vector_norm(out[:k] - ref) / torch.linalg.vector_norm(ref))
+        self.full.reconstruct_batch(sinos[:k], ref, centers=ck, stream=stream)
+        probe = self.corrected(sinos[:k], ck, stream)
+        err = float(torch.linalg.vector_norm(probe - ref) / torch.linalg.vector_norm(ref))
         fallback = err > self.tol
+        out = torch.empty((sinos.shape[0], self.M0, self.M0), dtype=torch.float32,
+                          device=sinos.device)
         if fallback:
             self.full.reconstruct_batch(sinos, out, centers=centers, stream=stream)
+        else:
+            out.copy_(self.corrected(sinos, centers, stream))
         return out, {"held_out_rel_l2": err, "fallback": fallback}
 
     def close(self):

@@ -45,6 +45,47 @@ def test_forward_matches_oracle():
     assert np.linalg.norm(y - ref) / np.linalg.norm(ref - x) < 2e-3
 
 
+def _bf16_fused(p):
+    """The fused kernel's BF16 weights: w1, w2 and w3 rounded."""
+    q = _bf16_w2(p)
+    q[0:144] = CO._bf16(q[0:144])
+    q[2480:2624] = CO._bf16(q[2480:2624])
+    return q
+
+
+@pytest.mark.parametrize("shape", [(1, 16, 64), (3, 37, 150), (2, 70, 200), (1, 5, 9)])
+def test_fused_inference_matches_oracle(shape):
+    """The fused tcgen05 inference kernel (gr_cnn_infer) on shapes of one tile, several
+    tiles with partial edges and less than a tile: against the float64 oracle with the
+    kernel's BF16 rounding of the weights, of conv1's input and of h1, h2 mirrored."""
+    p = _params(5)
+    rng = np.random.default_rng(6)
+    x = rng.normal(0, 1, shape).astype(np.float32)
+    net = Lrn.CorrectionNet(p)
+    y = net.infer(torch.tensor(x, device="cuda")).cpu().numpy()
+    net.infer_status()
+    ref = CO.forward(_bf16_fused(p), x, bf16=True, x_conv1=CO._bf16(x))["y"]
+    err = np.linalg.norm(y - ref) / np.linalg.norm(ref - x)
+    print(f"fused inference {shape}: error / correction {err:.2e}")
+    assert np.isfinite(y).all() and err < 2e-3
+
+
+def test_fused_inference_matches_unfused_forward_2048():
+    """At the held-out slice size (2048 x 2048, the trained parameters) the fused kernel
+    agrees with the three-kernel forward to within its BF16 rounding of conv1's input
+    and weights and of conv3's weights (input rounding alone is 2^-9 of each x value,
+    about 6e-3 of the correction on unit-variance inputs)."""
+    net = Lrn.CorrectionNet(np.load(Lrn.PARAMS_FILE))
+    rng = np.random.default_rng(7)
+    x = torch.tensor(rng.normal(0, 1, (2, 2048, 2048)).astype(np.float32), device="cuda")
+    y_f = net.infer(x)
+    y_u = net.forward(x)
+    net.infer_status()
+    d = float(torch.linalg.vector_norm(y_f - y_u) / torch.linalg.vector_norm(y_u - x))
+    print(f"fused vs unfused at 2048^2: {d:.2e} of the correction")
+    assert d < 1e-2
+
+
 def test_gradients_match_oracle():
     p = _params(2)
     rng = np.random.default_rng(3)
