@@ -358,7 +358,7 @@ __global__ void cnn_adam_kernel(float* params, const float* grads, float* m, flo
 }
 
 // ---------------------------------------------------------------- fused inference, tcgen05
-// One CTA (8 warps) computes output tiles of kFTh x kFTw pixels.  The tile's x region
+// One CTA (kFThreads / 32 warps) computes output tiles of kFTh x kFTw pixels.  The tile's x region
 // ((kFTh + 6) x (kFTw + 6) pixels), its h1 and h2 and conv3's per-tap partials stay in
 // shared memory; only x is read from HBM and y written.  Positions of the x region are
 // flattened with row stride kFWt, so a 3x3 tap (dy, dx) is the constant offset
@@ -375,28 +375,37 @@ __global__ void cnn_adam_kernel(float* params, const float* grads, float* m, flo
 //    tap), then bias, ReLU and BF16 on the way back to shared memory;
 //  * conv3 (16 -> 1): a 1x1 tcgen05 MMA to the nine per-tap partials
 //    Z[p][tap] = sum_ci w3[tap][ci] h2[p][ci] (w3 in BF16; N = 16, taps 9..15 zero), then
-//    y[p] = x[p] + (b3 + sum_tap Z[p + (dy, dx)][tap]) in FP32 on the CUDA cores.
+//    y[p] = x[p] + (b3 + sum_tap Z[p + (dy, dx)][tap]) in FP32 on the CUDA cores.  (Nine
+//    shifted MMAs into one column would drop the partials, but every N = 16 MMA reads its
+//    4 KB A operand from shared memory, about 30 cycles of the SM's shared-memory
+//    bandwidth: eight more of them per block cost more than the partials' stores and loads.)
 // Positions outside the image hold zero x, h1 and h2 (the network's zero padding); the
 // wrap-around columns of the flattened rows produce values only at positions that no
 // kept output reads.  One thread issues the MMAs; completion is a tcgen05.commit on an
-// mbarrier with bounded waits (timeout: error word, early exit).  Each CTA holds 256
-// tensor-memory columns; its dynamic shared memory (kFSmemLaunch) admits at most two CTAs
-// per SM, so an allocation never waits on a third.
+// mbarrier with bounded waits (timeout: error word, early exit).  Each CTA holds
+// kFTmemCols tensor-memory columns; its dynamic shared memory (kFSmemLaunch) admits at
+// most kFCtas CTAs per SM, whose allocations fit the SM's 512 columns together, so an
+// allocation never waits on another CTA.
 
-constexpr int kFTh = 16, kFTw = 64;
+constexpr int kFTh = 8, kFTw = 64;
+constexpr int kFThreads = 128, kFCtas = 4;                     // 4 warps, 4 CTAs per SM
+constexpr int kFGroups = kFThreads / 128;                      // warp groups sharing the blocks
 constexpr int kFWt = kFTw + 6;                                 // flattened row stride
 constexpr int kFRows = kFTh + 6;
 constexpr int kFPos = kFRows * kFWt;                           // positions of the x region
-constexpr int kFPlane = 1536;                                  // positions per activation plane
 constexpr int kFQ1 = kFWt, kFQ1e = (kFTh + 5) * kFWt;          // conv1: rows 1..kFTh+4
 constexpr int kFQ2 = 2 * kFWt;                                 // first conv2 / conv3 position
 constexpr int kFBlocks = ((kFTh + 4) * kFWt - kFQ2 + 127) / 128;  // 128-position blocks
 constexpr int kFBlocks1 = (kFQ1e - kFQ1 + 127) / 128;           // conv1's blocks from kFQ1
 constexpr int kFZ = 128 * kFBlocks;                            // partials per tap
-constexpr int kFThreads = 256;
+constexpr int kFPlane = ((kFQ1 + 128 * kFBlocks1 > kFQ2 + kFZ + kFWt + 1 ? kFQ1 + 128 * kFBlocks1
+                                                                         : kFQ2 + kFZ + kFWt + 1) +
+                         127) / 128 * 128;                     // positions per activation plane
 constexpr int kFXOff = 72;                                     // x buffer: reads at q - 71 .. q + 71
 constexpr int kFXLen = kFPos + 2 * kFXOff;
-constexpr int kFTmemCols = 256;
+constexpr int kFTmemNeed = 16 * (kFBlocks1 > kFBlocks ? kFBlocks1 : kFBlocks);
+constexpr int kFTmemCols = kFTmemNeed <= 32 ? 32 : kFTmemNeed <= 64 ? 64 : kFTmemNeed <= 128 ? 128
+                                                                                                : 256;
 constexpr int kFParams = 177;                                  // w1, b1, b2, b3 in FP32
 // shared memory: activation planes | B2 (9 taps) | B3 | B1 | x | FP32 params | mbarrier, tmem slot
 constexpr int kFSmAct = 0, kFSmB2 = 2 * kFPlane * 16, kFSmB3 = kFSmB2 + 9 * 512;
@@ -404,14 +413,14 @@ constexpr int kFSmB1 = kFSmB3 + 512;
 constexpr int kFSmX = kFSmB1 + 512, kFSmP = kFSmX + kFXLen * 4;
 constexpr int kFSmBar = (kFSmP + kFParams * 4 + 15) & ~15;
 constexpr int kFSmUsed = kFSmBar + 16;
-constexpr int kFSmemLaunch = 100 * 1024;
+constexpr int kFSmemLaunch = (228 * 1024 / kFCtas - 1024) & ~1023;
 static_assert(kFQ2 + kFZ + kFWt + 1 <= kFPlane, "conv2's shifted reads stay inside the planes");
 static_assert(kFQ1 + 128 * kFBlocks1 <= kFPlane, "conv1's blocks fit the planes");
-static_assert(16 * kFBlocks1 <= kFTmemCols, "conv1's accumulators fit the allocation");
+static_assert(kFTmemNeed <= kFTmemCols && kFCtas * kFTmemCols <= 512,
+              "accumulators fit the tensor-memory allocation, and every CTA of an SM gets one");
 static_assert(9 * kFZ * 4 <= 2 * kFPlane * 16, "conv3's partials fit the activation buffer");
-static_assert(16 * kFBlocks <= kFTmemCols, "accumulators fit the tensor-memory allocation");
-static_assert(kFSmUsed <= kFSmemLaunch && 3 * (kFSmemLaunch + 1024) > 228 * 1024,
-              "at most two CTAs per SM");
+static_assert(kFSmUsed <= kFSmemLaunch && (kFCtas + 1) * (kFSmemLaunch + 1024) > 228 * 1024,
+              "at most kFCtas CTAs per SM");
 
 __device__ __forceinline__ uint64_t cnn_smem_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
   // start >> 4 [0,14), leading-dimension offset >> 4 [16,30), stride offset >> 4
@@ -436,6 +445,16 @@ __device__ __forceinline__ void cnn_commit(uint64_t* bar) {
                    smem_u32(bar))
                : "memory");
 }
+// relu(v + b) of two channels in BF16 (packed FP32 add, then one converting relu)
+__device__ __forceinline__ unsigned relu_bias_pack(float v0, float v1, float b0, float b1) {
+  unsigned long long s;
+  asm("{\n .reg .b64 x, y;\n mov.b64 x, {%1, %2};\n mov.b64 y, {%3, %4};\n"
+      " add.rn.f32x2 %0, x, y;\n}" : "=l"(s) : "f"(v0), "f"(v1), "f"(b0), "f"(b1));
+  unsigned r;
+  asm("{\n .reg .f32 lo, hi;\n mov.b64 {lo, hi}, %1;\n cvt.rn.relu.bf16x2.f32 %0, hi, lo;\n}"
+      : "=r"(r) : "l"(s));
+  return r;
+}
 // 16 accumulator columns of this warp's 32 lanes
 __device__ __forceinline__ void cnn_tmem_ld16(uint32_t taddr, float (&v)[16]) {
   uint32_t r[16];
@@ -451,7 +470,7 @@ __device__ __forceinline__ void cnn_tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int k = 0; k < 16; ++k) v[k] = __uint_as_float(r[k]);
 }
 
-__global__ void __launch_bounds__(kFThreads, 2) cnn_fused_kernel(const float* params, const float* x,
+__global__ void __launch_bounds__(kFThreads, kFCtas) cnn_fused_kernel(const float* params, const float* x,
                                                                   float* y, int n_img, int h, int w,
                                                                   int* err) {
   extern __shared__ __align__(1024) unsigned char smf[];
@@ -500,7 +519,18 @@ __global__ void __launch_bounds__(kFThreads, 2) cnn_fused_kernel(const float* pa
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tslot;
-  const uint32_t a0 = smem_u32(act), b2a = smem_u32(b2s), b3a = smem_u32(b3s), b1a = smem_u32(b1s);
+  // descriptors: a position offset q adds q to the start-address field (16-byte units)
+  const uint64_t da = cnn_smem_desc(smem_u32(act), kFPlane * 16, 128);
+  const uint64_t db1 = cnn_smem_desc(smem_u32(b1s), 256, 128);
+  const uint64_t db2 = cnn_smem_desc(smem_u32(b2s), 256, 128);
+  const uint64_t db3 = cnn_smem_desc(smem_u32(b3s), 256, 128);
+  const float b3 = pw[kB1 + 2 * kC];
+  float bias1[kC], bias2[kC];
+#pragma unroll
+  for (int c = 0; c < kC; ++c) {
+    bias1[c] = pw[kB1 + c];
+    bias2[c] = pw[kB1 + kC + c];
+  }
   const int tiles_x = (w + kFTw - 1) / kFTw, tiles_y = (h + kFTh - 1) / kFTh;
   const long n_tiles = (long)n_img * tiles_x * tiles_y;
   const int lq = warp & 3;  // this warp's quarter of the tensor-memory lanes
@@ -511,19 +541,27 @@ __global__ void __launch_bounds__(kFThreads, 2) cnn_fused_kernel(const float* pa
   // passes during the previous tile's work
   constexpr int kXPer = (kFPos + kFThreads - 1) / kFThreads;
   float xr[kXPer];
+  const int r_tid = tid / kFWt, c_tid = tid - r_tid * kFWt;
   auto load_x = [&](long t) {
     const int im = (int)(t / ((long)tiles_x * tiles_y));
     const int rem = (int)(t - (long)im * tiles_x * tiles_y);
     const int ty0 = (rem / tiles_x) * kFTh, tx0 = (rem % tiles_x) * kFTw;
+    const bool all_in = t < n_tiles && ty0 >= 3 && tx0 >= 3 && ty0 + kFTh + 3 <= h &&
+                        tx0 + kFTw + 3 <= w;
     const float* xm = x + (size_t)im * h * w;
+    int r = r_tid, c = c_tid;  // position tid + k kFThreads = (r, c)
 #pragma unroll
     for (int k = 0; k < kXPer; ++k) {
-      const int q = tid + k * kFThreads;
-      const int r = q / kFWt, c = q - r * kFWt;
       const int iy = ty0 - 3 + r, ix = tx0 - 3 + c;
-      xr[k] = (q < kFPos && t < n_tiles && iy >= 0 && iy < h && ix >= 0 && ix < w)
-                  ? __ldg(&xm[(size_t)iy * w + ix])
-                  : 0.f;
+      const bool in = tid + k * kFThreads < kFPos &&
+                      (all_in || (t < n_tiles && iy >= 0 && iy < h && ix >= 0 && ix < w));
+      xr[k] = in ? __ldg(&xm[(size_t)iy * w + ix]) : 0.f;
+      r += kFThreads / kFWt;
+      c += kFThreads % kFWt;
+      if (c >= kFWt) {
+        c -= kFWt;
+        ++r;
+      }
     }
   };
   load_x(blockIdx.x);
@@ -531,7 +569,10 @@ __global__ void __launch_bounds__(kFThreads, 2) cnn_fused_kernel(const float* pa
     const int im = (int)(tile / ((long)tiles_x * tiles_y));
     const int rem = (int)(tile - (long)im * tiles_x * tiles_y);
     const int y0 = (rem / tiles_x) * kFTh, x0 = (rem % tiles_x) * kFTw;
+    // a tile whose x region lies inside the image needs no zero padding
+    const bool all_in = y0 >= 3 && x0 >= 3 && y0 + kFTh + 3 <= h && x0 + kFTw + 3 <= w;
     auto inside = [&](int q) {
+      if (all_in) return true;
       const int r = q / kFWt, c = q - (q / kFWt) * kFWt;
       const int iy = y0 - 3 + r, ix = x0 - 3 + c;
       return iy >= 0 && iy < h && ix >= 0 && ix < w;
@@ -555,9 +596,8 @@ __global__ void __launch_bounds__(kFThreads, 2) cnn_fused_kernel(const float* pa
     __syncthreads();
     if (tid == 0) {
       tc_fence_after();
-      for (int b = 0; b < kFBlocks1; ++b)
-        cnn_mma(tmem + 16 * b, cnn_smem_desc(a0 + (kFQ1 + 128 * b) * 16, kFPlane * 16, 128),
-                cnn_smem_desc(b1a, 256, 128), 0u);
+#pragma unroll
+      for (int b = 0; b < kFBlocks1; ++b) cnn_mma(tmem + 16 * b, da + (kFQ1 + 128 * b), db1, 0u);
       cnn_commit(bar);
     }
     bool got = warp == 0 ? mbar_wait(bar, phase) : true;
@@ -570,7 +610,7 @@ __global__ void __launch_bounds__(kFThreads, 2) cnn_fused_kernel(const float* pa
     // h1 = relu(conv1 + b1) in BF16 over the im2col (every MMA reading it is done); zero
     // outside the image and beyond conv1's rows; the planes' other positions are
     // cleared of the previous tile's values
-    for (int b = warp >> 2; b < kFBlocks1; b += 2) {
+    for (int b = warp >> 2; b < kFBlocks1; b += kFGroups) {
       float v[16];
       cnn_tmem_ld16(tmem + ((uint32_t)(32 * lq) << 16) + 16 * b, v);
       const int q = kFQ1 + 128 * b + 32 * lq + lane;
@@ -578,8 +618,7 @@ __global__ void __launch_bounds__(kFThreads, 2) cnn_fused_kernel(const float* pa
       if (q < kFQ1e && inside(q)) {
         unsigned o[kC / 2];
 #pragma unroll
-        for (int c = 0; c < kC; c += 2)
-          o[c / 2] = pack_bf16(fmaxf(v[c] + pw[kB1 + c], 0.f), fmaxf(v[c + 1] + pw[kB1 + c + 1], 0.f));
+        for (int c = 0; c < kC; c += 2) o[c / 2] = relu_bias_pack(v[c], v[c + 1], bias1[c], bias1[c + 1]);
         lo = make_uint4(o[0], o[1], o[2], o[3]);
         hi = make_uint4(o[4], o[5], o[6], o[7]);
       }
@@ -596,13 +635,12 @@ __global__ void __launch_bounds__(kFThreads, 2) cnn_fused_kernel(const float* pa
     // conv2: nine MMAs per block of 128 positions, A shifted by the tap's offset
     if (tid == 0) {
       tc_fence_after();
+#pragma unroll 2
       for (int b = 0; b < kFBlocks; ++b)
 #pragma unroll
-        for (int t = 0; t < 9; ++t) {
-          const uint32_t q = kFQ2 + 128 * b + tap_dy(t) * kFWt + tap_dx(t);
-          cnn_mma(tmem + 16 * b, cnn_smem_desc(a0 + q * 16, kFPlane * 16, 128),
-                  cnn_smem_desc(b2a + t * 512, 256, 128), t > 0 ? 1u : 0u);
-        }
+        for (int t = 0; t < 9; ++t)
+          cnn_mma(tmem + 16 * b, da + (kFQ2 + 128 * b + tap_dy(t) * kFWt + tap_dx(t)),
+                  db2 + 32 * t, t > 0 ? 1u : 0u);
       cnn_commit(bar);
     }
     // one warp polls the barrier; the others wait at the CTA barrier (no issue slots)
@@ -614,8 +652,8 @@ __global__ void __launch_bounds__(kFThreads, 2) cnn_fused_kernel(const float* pa
     phase ^= 1u;
     tc_fence_after();
     // h2 = relu(conv2 + b2) in BF16 over h1's planes (every MMA reading h1 is done);
-    // warps 0-3 take the even blocks, 4-7 the odd ones
-    for (int b = warp >> 2; b < kFBlocks; b += 2) {
+    // warp group g (4 warps, one per quarter of the lanes) takes blocks g, g + kFGroups, ...
+    for (int b = warp >> 2; b < kFBlocks; b += kFGroups) {
       float v[16];
       cnn_tmem_ld16(tmem + ((uint32_t)(32 * lq) << 16) + 16 * b, v);
       const int q = kFQ2 + 128 * b + 32 * lq + lane;
@@ -623,9 +661,7 @@ __global__ void __launch_bounds__(kFThreads, 2) cnn_fused_kernel(const float* pa
       if (inside(q)) {
         unsigned o[kC / 2];
 #pragma unroll
-        for (int c = 0; c < kC; c += 2)
-          o[c / 2] = pack_bf16(fmaxf(v[c] + pw[kB1 + kC + c], 0.f),
-                               fmaxf(v[c + 1] + pw[kB1 + kC + c + 1], 0.f));
+        for (int c = 0; c < kC; c += 2) o[c / 2] = relu_bias_pack(v[c], v[c + 1], bias2[c], bias2[c + 1]);
         lo = make_uint4(o[0], o[1], o[2], o[3]);
         hi = make_uint4(o[4], o[5], o[6], o[7]);
       }
@@ -638,9 +674,8 @@ __global__ void __launch_bounds__(kFThreads, 2) cnn_fused_kernel(const float* pa
     // conv3's 1x1 MMA: Z[q][tap] for every block
     if (tid == 0) {
       tc_fence_after();
-      for (int b = 0; b < kFBlocks; ++b)
-        cnn_mma(tmem + 16 * b, cnn_smem_desc(a0 + (kFQ2 + 128 * b) * 16, kFPlane * 16, 128),
-                cnn_smem_desc(b3a, 256, 128), 0u);
+#pragma unroll
+      for (int b = 0; b < kFBlocks; ++b) cnn_mma(tmem + 16 * b, da + (kFQ2 + 128 * b), db3, 0u);
       cnn_commit(bar);
     }
     got = warp == 0 ? mbar_wait(bar, phase) : true;
@@ -652,7 +687,7 @@ __global__ void __launch_bounds__(kFThreads, 2) cnn_fused_kernel(const float* pa
     tc_fence_after();
     // partials into the activation buffer (h2 is consumed): z_s[tap][q - kFQ2]
     float* zs = reinterpret_cast<float*>(smf + kFSmAct);
-    for (int b = warp >> 2; b < kFBlocks; b += 2) {
+    for (int b = warp >> 2; b < kFBlocks; b += kFGroups) {
       float v[16];
       cnn_tmem_ld16(tmem + ((uint32_t)(32 * lq) << 16) + 16 * b, v);
       const int qi = 128 * b + 32 * lq + lane;
@@ -668,7 +703,7 @@ __global__ void __launch_bounds__(kFThreads, 2) cnn_fused_kernel(const float* pa
       const int iy = y0 + ry, ix = x0 + rx;
       if (iy >= h || ix >= w) continue;
       const int q = (ry + 3) * kFWt + rx + 3;
-      float z = pw[kB1 + 2 * kC];
+      float z = b3;
 #pragma unroll
       for (int t = 0; t < 9; ++t) z += zs[t * kFZ + q + tap_dy(t) * kFWt + tap_dx(t) - kFQ2];
       ym[(size_t)iy * w + ix] = xs[q] + z;
@@ -791,7 +826,7 @@ int gr_cnn_infer(const float* params, const float* x, float* y, int n_img, int h
                              kFSmemLaunch);
   if (e != cudaSuccess) return fail(GR_ERR_CUDA, "cnn infer: %s", cudaGetErrorString(e));
   const long tiles = (long)n_img * ((h + kFTh - 1) / kFTh) * ((w + kFTw - 1) / kFTw);
-  const int blocks = (int)std::min<long>(tiles, 2L * sms);
+  const int blocks = (int)std::min<long>(tiles, (long)kFCtas * sms);
   cnn_fused_kernel<<<blocks, kFThreads, kFSmemLaunch, st>>>(params, x, y, n_img, h, w,
                                                             static_cast<int*>(workspace));
   e = cudaGetLastError();
