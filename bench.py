@@ -93,6 +93,15 @@ def peaks():
     return FALLBACK_HBM_GBS, "fallback 6.65 TB/s"
 
 
+def bf16_sustained_tflops():
+    """Sustained dense BF16 TFLOP/s of MEASURED_PEAKS.json, else the 1.4 PFLOP/s fallback."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f).get("bf16_tflops_sustained", 1400.0))
+    return 1400.0
+
+
 class ClockSampler:
     """nvidia-smi samples of SM clock and throttle reasons during a region."""
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
@@ -378,51 +387,71 @@ def measure_slice_pipeline(G, sinos, th, n, a, dev, stream, peak):
 
 
 def measure_learned(sinos, th, n, a, dev, stream, args, centers_d):
-    """The learned narrow-kernel path on the same resident slices: narrow (C = 4)
-    gridrec + the trained correction network (projects_b200/correction_c4.npy),
-    timed with CUDA events; its held-out error against full-width gridrec on two
-    slices decides the fallback (tolerance 1e-3), as LearnedGridrec does."""
+    """The learned narrow-kernel path on the same resident slices, one row per narrow
+    width (PSWF C = 4 and 5, networks projects_b200/correction_c4.npy and _c5.npy):
+    narrow gridrec alone and narrow + the fused correction network, timed with CUDA
+    events; their relative L2 against full-width gridrec on two held-out slices decides
+    the fallback (tolerance 1e-3), as LearnedGridrec does.  The network's own cost is
+    the fused inference kernel (gr_cnn_infer) on S resident normalised images, with its
+    fractions of the HBM roof (x read, y written: 8 bytes per pixel) and of the
+    sustained BF16 tensor roof (5184 useful FLOP per pixel: 2 (9 x 16 + 9 x 16 x 16 +
+    16 x 9))."""
     import torch
 
     from projects_b200 import learned as Lrn
     if sinos.dtype != torch.float32:
         return None
     S = min(64, sinos.shape[0])
-    lg = Lrn.LearnedGridrec(n, a, th, max_pairs=args.max_pairs, device=dev.index or 0)
     x = sinos[:S]
     c = centers_d[:S]
-    for _ in range(2):
-        lg.corrected(x, centers=c, stream=stream)
-    torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(3):
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / 1000.0 / reps
+
+    rows, cnn = [], None
+    for C in (4.0, 5.0):
+        lg = Lrn.LearnedGridrec(n, a, th, max_pairs=args.max_pairs, device=dev.index or 0,
+                                pswf_c=C)
         raw = torch.empty((S, lg.M0, lg.M0), device=dev)
-        lg.narrow.reconstruct_batch(x, raw, centers=c, stream=stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t_narrow = e0.elapsed_time(e1) / 3000.0
-    e0.record(stream)
-    for _ in range(3):
-        y = lg.corrected(x, centers=c, stream=stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    t_learned = e0.elapsed_time(e1) / 3000.0
-    out, info = lg.reconstruct_batch(x[:4], centers=c[:4], stream=stream)
-    raw = torch.empty((2, lg.M0, lg.M0), device=dev)
-    lg.narrow.reconstruct_batch(x[:2], raw, centers=c[:2], stream=stream)
-    ref = torch.empty_like(raw)
-    lg.full.reconstruct_batch(x[:2], ref, centers=c[:2], stream=stream)
-    e_narrow = float(torch.linalg.vector_norm(raw - ref) / torch.linalg.vector_norm(ref))
-    lg.close()
-    return {"narrow_kernel": "PSWF C = 4 (3 x 3 taps), same grid and image size",
-            "narrow_slices_per_s": S / t_narrow,
-            "narrow_plus_cnn_slices_per_s": S / t_learned,
-            "held_out_rel_l2_vs_full_width": {"narrow": e_narrow,
-                                              "narrow_plus_cnn": info["held_out_rel_l2"]},
-            "tolerance": 1e-3, "fallback_to_full_width": info["fallback"],
-            "network": "3-layer 16-channel 3x3 residual CNN, BF16 tensor-core conv2, trained "
-                       "on 4096 slices of 1024 x 900 (projects_b200/train_correction.py)"}
+        t_narrow = timed(lambda: lg.narrow.reconstruct_batch(x, raw, centers=c, stream=stream))
+        t_learned = timed(lambda: lg.corrected(x, centers=c, stream=stream))
+        if cnn is None:
+            xn = (raw / Lrn.LearnedGridrec.scales(raw)).contiguous()
+            t_cnn = timed(lambda: lg.net.infer(xn, stream=stream), reps=5) / S
+            lg.net.infer_status(stream)
+            px = lg.M0 * lg.M0
+            hbm, _ = peaks()
+            tf = bf16_sustained_tflops()
+            cnn = {"kernel": "cnn_fused_kernel (conv1, conv2, conv3's partials as tcgen05 MMAs)",
+                   "us_per_slice": t_cnn * 1e6,
+                   "hbm_frac": 8.0 * px / t_cnn / (hbm * 1e9),
+                   "bf16_sustained_frac": 5184.0 * px / t_cnn / (tf * 1e12),
+                   "bound": "shared-memory bandwidth: every N = 16 MMA reads a 4 KB A tile "
+                            "(54 conv2 MMAs per 8 x 64 tile)"}
+            del xn
+        _, info = lg.reconstruct_batch(x[:4], centers=c[:4], stream=stream)
+        ref = torch.empty((2, lg.M0, lg.M0), device=dev)
+        lg.full.reconstruct_batch(x[:2], ref, centers=c[:2], stream=stream)
+        e_narrow = float(torch.linalg.vector_norm(raw[:2] - ref) / torch.linalg.vector_norm(ref))
+        rows.append({"pswf_c": C, "narrow_slices_per_s": S / t_narrow,
+                     "narrow_plus_cnn_slices_per_s": S / t_learned,
+                     "held_out_rel_l2_vs_full_width": {"narrow": e_narrow,
+                                                       "narrow_plus_cnn": info["held_out_rel_l2"]},
+                     "fallback_to_full_width": info["fallback"]})
+        del raw, ref
+        lg.close()
+    return {"widths": rows, "cnn": cnn, "tolerance": 1e-3,
+            "network": "3-layer 16-channel 3x3 residual CNN, BF16 tensor-core layers with FP32 "
+                       "accumulators, trained on 4096 slices of 1024 x 900 per narrow width "
+                       "(projects_b200/train_correction.py)"}
 
 
 # ------------------------------------------------------------------ arms

@@ -417,17 +417,19 @@ int gr_cnn_backward(const float* params, const float* x, const float* y, const f
 int gr_cnn_adam(float* params, const float* grads, float* m, float* v, int step, float lr,
                 float beta1, float beta2, float eps, void* stream);
 /* Fused inference: the same network in one kernel per call, for inference only.
- * conv1 in FP32 on the CUDA cores; conv2 and conv3 (as a 1x1 product to its nine
- * per-tap partials, then a shifted FP32 sum) on tcgen05 BF16 MMAs with FP32
+ * conv1 (on a BF16 im2col of x), conv2 and conv3 (as a 1x1 product to its nine
+ * per-tap partials, then a shifted FP32 sum) run as tcgen05 BF16 MMAs with FP32
  * accumulators in tensor memory; h1, h2 and the partials stay in shared memory, so
- * only x and y cross HBM.  Differs from gr_cnn_forward by conv3's weights rounded to
- * BF16 and the tensor core's summation order.  workspace: gr_cnn_infer_workspace_bytes()
- * device bytes, zeroed once by the caller (it holds the error word of the kernel's
- * bounded waits); gr_cnn_infer_status synchronises `stream`, reports GR_ERR_TIMEOUT if
- * a wait ran out and clears the word. */
+ * only x and y cross HBM.  Differs from gr_cnn_forward by conv1's input and conv1's
+ * and conv3's weights rounded to BF16 and the tensor core's summation order.
+ * scale (device, n_img floats, or NULL for 1): image i is corrected at unit scale,
+ * y = s_i * net(x / s_i), the scaling fused into the x loads and y stores.
+ * workspace: gr_cnn_infer_workspace_bytes() device bytes, zeroed once by the caller
+ * (it holds the error word of the kernel's bounded waits); gr_cnn_infer_status
+ * synchronises `stream`, reports GR_ERR_TIMEOUT if a wait ran out and clears the word. */
 size_t gr_cnn_infer_workspace_bytes(void);
-int gr_cnn_infer(const float* params, const float* x, float* y, int n_img, int h, int w,
-                 void* workspace, void* stream);
+int gr_cnn_infer(const float* params, const float* x, float* y, const float* scale, int n_img,
+                 int h, int w, void* workspace, void* stream);
 int gr_cnn_infer_status(void* workspace, void* stream);
 
 #ifdef __cplusplus

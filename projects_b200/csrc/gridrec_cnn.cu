@@ -471,8 +471,9 @@ __device__ __forceinline__ void cnn_tmem_ld16(uint32_t taddr, float (&v)[16]) {
 }
 
 __global__ void __launch_bounds__(kFThreads, kFCtas) cnn_fused_kernel(const float* params, const float* x,
-                                                                  float* y, int n_img, int h, int w,
-                                                                  int* err) {
+                                                                       float* y, const float* scale,
+                                                                       int n_img, int h, int w,
+                                                                       int* err) {
   extern __shared__ __align__(1024) unsigned char smf[];
   uint4* act = reinterpret_cast<uint4*>(smf + kFSmAct);  // plane g: act[g kFPlane + q] = 8 BF16 channels
   unsigned short* b2s = reinterpret_cast<unsigned short*>(smf + kFSmB2);
@@ -540,7 +541,7 @@ __global__ void __launch_bounds__(kFThreads, kFCtas) cnn_fused_kernel(const floa
   // tid + k kFThreads; loaded one tile ahead into registers, so that the loads' latency
   // passes during the previous tile's work
   constexpr int kXPer = (kFPos + kFThreads - 1) / kFThreads;
-  float xr[kXPer];
+  float xr[kXPer], x_inv = 1.f;
   const int r_tid = tid / kFWt, c_tid = tid - r_tid * kFWt;
   auto load_x = [&](long t) {
     const int im = (int)(t / ((long)tiles_x * tiles_y));
@@ -549,6 +550,9 @@ __global__ void __launch_bounds__(kFThreads, kFCtas) cnn_fused_kernel(const floa
     const bool all_in = t < n_tiles && ty0 >= 3 && tx0 >= 3 && ty0 + kFTh + 3 <= h &&
                         tx0 + kFTw + 3 <= w;
     const float* xm = x + (size_t)im * h * w;
+    // the image's 1 / scale, applied when the values are stored to shared memory (a
+    // product here would wait on the loads)
+    x_inv = scale && t < n_tiles ? 1.f / __ldg(&scale[im]) : 1.f;
     int r = r_tid, c = c_tid;  // position tid + k kFThreads = (r, c)
 #pragma unroll
     for (int k = 0; k < kXPer; ++k) {
@@ -579,7 +583,7 @@ __global__ void __launch_bounds__(kFThreads, kFCtas) cnn_fused_kernel(const floa
     };
 #pragma unroll
     for (int k = 0; k < kXPer; ++k)
-      if (tid + k * kFThreads < kFPos) xs[tid + k * kFThreads] = xr[k];
+      if (tid + k * kFThreads < kFPos) xs[tid + k * kFThreads] = xr[k] * x_inv;
     __syncthreads();
     load_x(tile + gridDim.x);  // the next tile's x, in flight during this tile
     // conv1's im2col (BF16): plane 0 holds taps 0..7 of position q, plane 1 tap 8 and
@@ -698,6 +702,7 @@ __global__ void __launch_bounds__(kFThreads, kFCtas) cnn_fused_kernel(const floa
     __syncthreads();
     // y = x + (b3 + sum_tap Z[p + (dy, dx)][tap])
     float* ym = y + (size_t)im * h * w;
+    const float sc = scale ? __ldg(&scale[im]) : 1.f;
     for (int k = tid; k < kFTh * kFTw; k += kFThreads) {
       const int ry = k / kFTw, rx = k - ry * kFTw;
       const int iy = y0 + ry, ix = x0 + rx;
@@ -706,7 +711,7 @@ __global__ void __launch_bounds__(kFThreads, kFCtas) cnn_fused_kernel(const floa
       float z = b3;
 #pragma unroll
       for (int t = 0; t < 9; ++t) z += zs[t * kFZ + q + tap_dy(t) * kFWt + tap_dx(t) - kFQ2];
-      ym[(size_t)iy * w + ix] = xs[q] + z;
+      ym[(size_t)iy * w + ix] = (xs[q] + z) * sc;
     }
     __syncthreads();  // x and the partials are read before the next tile overwrites them
   }
@@ -812,8 +817,8 @@ int gr_cnn_backward(const float* params, const float* x, const float* y, const f
 
 size_t gr_cnn_infer_workspace_bytes(void) { return 256; }
 
-int gr_cnn_infer(const float* params, const float* x, float* y, int n_img, int h, int w,
-                 void* workspace, void* stream) {
+int gr_cnn_infer(const float* params, const float* x, float* y, const float* scale, int n_img,
+                 int h, int w, void* workspace, void* stream) {
   int rc = cnn_check(n_img, h, w);
   if (rc) return rc;
   if (!params || !x || !y || !workspace) return fail(GR_ERR_ARG, "cnn infer: null pointer");
@@ -827,7 +832,7 @@ int gr_cnn_infer(const float* params, const float* x, float* y, int n_img, int h
   if (e != cudaSuccess) return fail(GR_ERR_CUDA, "cnn infer: %s", cudaGetErrorString(e));
   const long tiles = (long)n_img * ((h + kFTh - 1) / kFTh) * ((w + kFTw - 1) / kFTw);
   const int blocks = (int)std::min<long>(tiles, (long)kFCtas * sms);
-  cnn_fused_kernel<<<blocks, kFThreads, kFSmemLaunch, st>>>(params, x, y, n_img, h, w,
+  cnn_fused_kernel<<<blocks, kFThreads, kFSmemLaunch, st>>>(params, x, y, scale, n_img, h, w,
                                                             static_cast<int*>(workspace));
   e = cudaGetLastError();
   return e == cudaSuccess ? GR_OK : fail(GR_ERR_CUDA, "cnn infer: %s", cudaGetErrorString(e));

@@ -12,6 +12,7 @@ shared memory); training runs its own forward, backward and Adam kernels.
 from __future__ import annotations
 
 import ctypes as C
+import math
 import os
 
 import numpy as np
@@ -19,7 +20,12 @@ import numpy as np
 from . import gridrec as G
 
 N_PARAMS = 2625
-PARAMS_FILE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "correction_c4.npy")
+def params_file(pswf_c=4.0):
+    """Trained parameters of the network for the narrow kernel of PSWF parameter C."""
+    return os.path.join(os.path.dirname(os.path.abspath(__file__)), f"correction_c{pswf_c:g}.npy")
+
+
+PARAMS_FILE = params_file(4.0)
 
 
 def _lib():
@@ -36,7 +42,7 @@ def _lib():
                                       vp]
         L.gr_cnn_adam.argtypes = [vp, vp, vp, vp, i_, f_, f_, f_, f_, vp]
         L.gr_cnn_infer_workspace_bytes.restype = C.c_size_t
-        L.gr_cnn_infer.argtypes = [vp, vp, vp, i_, i_, i_, vp, vp]
+        L.gr_cnn_infer.argtypes = [vp, vp, vp, vp, i_, i_, i_, vp, vp]
         L.gr_cnn_infer_status.argtypes = [vp, vp]
         L._cnn_bound = True
     return L
@@ -96,14 +102,22 @@ class CorrectionNet:
                                        G._ptr(ws), G._stream_ptr(stream)), "gr_cnn_forward")
         return y
 
-    def infer(self, x, y=None, stream=None):
+    def infer(self, x, y=None, stream=None, scale=None):
         """x: (N, H, W) float32 CUDA tensor -> y = x + correction, by the fused
-        tcgen05 inference kernel (conv3's weights in BF16; no activation workspace)."""
+        tcgen05 inference kernel (weights and conv1's input in BF16, FP32
+        accumulators; no activation workspace).  scale (N floats on the device):
+        y_i = s_i * net(x_i / s_i), the scaling done inside the kernel."""
         import torch
         n, h, w = x.shape
         if y is None:
             y = torch.empty_like(x)
-        G._check(_lib().gr_cnn_infer(G._ptr(self.params), G._ptr(x), G._ptr(y), n, h, w,
+        sp = None
+        if scale is not None:
+            scale = scale.reshape(-1).contiguous()
+            if scale.numel() != n or scale.dtype != torch.float32 or scale.device != x.device:
+                raise ValueError("scale: one float32 per image, on the images' device")
+            sp = G._ptr(scale)
+        G._check(_lib().gr_cnn_infer(G._ptr(self.params), G._ptr(x), G._ptr(y), sp, n, h, w,
                                      G._ptr(self._iws), G._stream_ptr(stream)), "gr_cnn_infer")
         return y
 
@@ -136,7 +150,8 @@ class CorrectionNet:
 
 
 class LearnedGridrec:
-    """Narrow-kernel (C = 4) gridrec + correction CNN, with full-width fallback.
+    """Narrow-kernel (C = 4 by default, or 5) gridrec + correction CNN, with
+    full-width (C = 6) fallback.
 
     reconstruct_batch() reconstructs with the narrow plan, corrects with the
     network, then reconstructs the first pair with the full plan and compares:
@@ -144,15 +159,15 @@ class LearnedGridrec:
     the full plan (the result is then plain gridrec)."""
 
     def __init__(self, n_det, n_ang, theta_deg, params=None, tol=1e-3, max_pairs=8,
-                 filter=G.FILTER_HANN, device=0):
-        self.narrow = G.Plan(n_det, n_ang, theta_deg, filter=filter, pswf_c=4.0,
+                 filter=G.FILTER_HANN, device=0, pswf_c=4.0):
+        self.narrow = G.Plan(n_det, n_ang, theta_deg, filter=filter, pswf_c=pswf_c,
                              max_pairs=max_pairs, device=device)
         self.full = G.Plan(n_det, n_ang, theta_deg, filter=filter, pswf_c=6.0,
                            max_pairs=max_pairs, device=device)
         if self.narrow.M0 != self.full.M0:
             raise ValueError("narrow and full plans disagree on the image size")
-        if params is None and os.path.exists(PARAMS_FILE):
-            params = np.load(PARAMS_FILE)
+        if params is None and os.path.exists(params_file(pswf_c)):
+            params = np.load(params_file(pswf_c))
         self.net = CorrectionNet(params, device=f"cuda:{device}")
         self.tol = tol
         self.M0 = self.full.M0
@@ -163,12 +178,13 @@ class LearnedGridrec:
         its correction does not depend on the absolute scale of the values (which
         follows the pixel size, i.e. the detector width)."""
         import torch
-        return torch.sqrt(torch.mean(images * images, dim=(1, 2), keepdim=True)).clamp_min(1e-30)
+        n = images.shape[1] * images.shape[2]
+        rms = torch.linalg.vector_norm(images, dim=(1, 2), keepdim=True) / math.sqrt(n)
+        return rms.clamp_min(1e-30)
 
     def correct(self, raw, stream=None):
-        """s * net(raw / s) per slice (the fused inference kernel)."""
-        s = self.scales(raw)
-        return self.net.infer((raw / s).contiguous(), stream=stream) * s
+        """s * net(raw / s) per slice (the fused inference kernel, which applies s)."""
+        return self.net.infer(raw.contiguous(), stream=stream, scale=self.scales(raw))
 
     def corrected(self, sinos, centers=None, stream=None):
         """Narrow-kernel images corrected by the network, (S, M0, M0)."""

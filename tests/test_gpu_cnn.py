@@ -86,6 +86,21 @@ def test_fused_inference_matches_unfused_forward_2048():
     assert d < 1e-2
 
 
+def test_fused_inference_scale_per_image():
+    """infer(x, scale=s) corrects each image at unit scale: s_i * net(x_i / s_i), against
+    the unscaled kernel on x / s (FP32 scaling round-off only)."""
+    net = Lrn.CorrectionNet(np.load(Lrn.PARAMS_FILE))
+    rng = np.random.default_rng(8)
+    x = torch.tensor(rng.normal(0, 1, (3, 100, 130)).astype(np.float32), device="cuda")
+    s = torch.tensor([0.5, 3.0, 1e-3], device="cuda")
+    y = net.infer(x, scale=s)
+    ref = net.infer((x / s[:, None, None]).contiguous()) * s[:, None, None]
+    net.infer_status()
+    for i in range(3):
+        d = float(torch.linalg.vector_norm(y[i] - ref[i]) / torch.linalg.vector_norm(ref[i] - x[i]))
+        assert d < 1e-4, (i, d)
+
+
 def test_gradients_match_oracle():
     p = _params(2)
     rng = np.random.default_rng(3)
