@@ -539,7 +539,7 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
 // Cells in row 0 or column 0 stay zero (the reference clamps taps to [1, M-1]).
 //
 // Execution: a persistent grid of warps pulls (work item, pair group) entries
-// from a queue.  A warp accumulates the tile of kGridPairs slice pairs (their
+// from a queue.  A warp accumulates the tile of PG slice pairs (their
 // cells interleaved as float4) in a private shared-memory tile, NT lanes per
 // sample (lane t owns footprint row t; column weights are exchanged by
 // shuffles), so the geometry -- positions, table lookups -- is computed once
@@ -556,7 +556,6 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
 
 constexpr int kTileStride = kTile + 1;
 constexpr int kGridWarps = 4;
-constexpr int kGridPairs = 2;   // slice pairs gridded together from one set of weights
 
 // (int)(d * ts + 0.5) for d >= 0 -- the nearest-neighbour table index of
 // gridrec.h:53 -- in FP64 with the product and the sum rounded separately, as
@@ -566,25 +565,68 @@ __device__ __forceinline__ int table_index64(double d, double ts) {
   return (int)fmin(__dadd_rn(__dmul_rn(d, ts), 0.5), 2.0e9);
 }
 
-template <int NT>
+// A cell of PG pairs gridded together: float4 (C_A, C_B) for two, float2 for one.
+template <int PG>
+struct GridCell;
+template <>
+struct GridCell<2> {
+  using T = float4;
+  static __device__ __forceinline__ float4 zero() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+  static __device__ __forceinline__ float4 make(float2 A, float2 B) {
+    return make_float4(A.x, A.y, B.x, B.y);
+  }
+  static __device__ __forceinline__ float4 scale(float w, float4 c) {
+    return make_float4(w * c.x, w * c.y, w * c.z, w * c.w);
+  }
+  static __device__ __forceinline__ void fma(float w, float4 c, float4& h) {
+    h.x = fmaf(w, c.x, h.x);
+    h.y = fmaf(w, c.y, h.y);
+    h.z = fmaf(w, c.z, h.z);
+    h.w = fmaf(w, c.w, h.w);
+  }
+  static __device__ __forceinline__ float2 pairA(float4 c) { return make_float2(c.x, c.y); }
+  static __device__ __forceinline__ float2 pairB(float4 c) { return make_float2(c.z, c.w); }
+};
+template <>
+struct GridCell<1> {
+  using T = float2;
+  static __device__ __forceinline__ float2 zero() { return make_float2(0.f, 0.f); }
+  static __device__ __forceinline__ float2 make(float2 A, float2) { return A; }
+  static __device__ __forceinline__ float2 scale(float w, float2 c) {
+    return make_float2(w * c.x, w * c.y);
+  }
+  static __device__ __forceinline__ void fma(float w, float2 c, float2& h) {
+    h.x = fmaf(w, c.x, h.x);
+    h.y = fmaf(w, c.y, h.y);
+  }
+  static __device__ __forceinline__ float2 pairA(float2 c) { return c; }
+  static __device__ __forceinline__ float2 pairB(float2) { return make_float2(0.f, 0.f); }
+};
+
+// PG = 2: two pairs per warp from one set of weights (chunks of two or more pairs);
+// PG = 1: a lone pair, with half the tile memory and read-modify-write traffic.  Pair
+// A's arithmetic is the same in both, so a pair's cells are bitwise equal.
+template <int NT, int PG>
 __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
+  using CellOps = GridCell<PG>;
+  using Cell = typename CellOps::T;
   constexpr int SPW = 32 / NT;  // samples per step
   extern __shared__ float4 smem4[];
   float* s_wtbl = reinterpret_cast<float*>(smem4);
-  float4* tiles = smem4 + 257;  // table: up to 1028 floats
+  Cell* tiles = reinterpret_cast<Cell*>(smem4 + 257);  // table: up to 1028 floats
   for (int i = threadIdx.x; i <= a.ltbl; i += blockDim.x) s_wtbl[i] = __ldg(&a.wtbl[i]);
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  float4* tile = tiles + warp * (kTile * kTileStride);
-  // the current run's samples of both pairs: stage[j - jlo] = (C_A, C_B)
-  float4* stage = tiles + kGridWarps * (kTile * kTileStride) + warp * kRunMax;
+  Cell* tile = tiles + warp * (kTile * kTileStride);
+  // the current run's samples of the PG pairs: stage[j - jlo] = (C_A[, C_B])
+  Cell* stage = tiles + kGridWarps * (kTile * kTileStride) + warp * kRunMax;
   const int slot_k = lane / NT;          // sample slot of this lane
   const int t = lane - slot_k * NT;      // footprint row of this lane
   const int lane0 = slot_k * NT;         // first lane of this sample
   const bool lane_used = slot_k < SPW;
   const double L2d = a.L2, tsd = a.tblspcg;
   const int ltbl = a.ltbl;
-  const int groups = (a.pairs + kGridPairs - 1) / kGridPairs;
+  const int groups = (a.pairs + PG - 1) / PG;
   const unsigned total = (unsigned)a.n_items * (unsigned)groups;
   const size_t spec_pair = (size_t)a.n_ang * 2 * a.J;
   for (;;) {
@@ -594,12 +636,12 @@ __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
     if (w >= total) break;
     const int grp = (int)(w / (unsigned)a.n_items);
     const Item it = a.items[w - (unsigned)grp * (unsigned)a.n_items];
-    const int pA = grp * kGridPairs;
-    const bool hasB = pA + 1 < a.pairs;
+    const int pA = grp * PG;
+    const bool hasB = PG == 2 && pA + 1 < a.pairs;
     const int tu = it.tile / a.tiles_v;
     const int tv = it.tile - tu * a.tiles_v;
     const int p0 = tu * kTile, q0 = tv * kTile;
-    for (int i = lane; i < kTile * kTileStride; i += 32) tile[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int i = lane; i < kTile * kTileStride; i += 32) tile[i] = CellOps::zero();
     __syncwarp();
     const double offu = (double)(a.M / 2 - p0), offv = (double)(a.M / 2 - q0);
     const float2* specA = a.spec + (size_t)pA * spec_pair;
@@ -620,19 +662,19 @@ __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
       const float2* pb = specB + (size_t)nrun.dir * a.J;
       if (nrun.jlo + lane <= nrun.jhi) {
         nA0 = __ldg(&pa[nrun.jlo + lane]);
-        nB0 = __ldg(&pb[nrun.jlo + lane]);
+        if (PG == 2) nB0 = __ldg(&pb[nrun.jlo + lane]);
       }
       if (nrun.jlo + 32 + lane <= nrun.jhi) {
         nA1 = __ldg(&pa[nrun.jlo + 32 + lane]);
-        nB1 = __ldg(&pb[nrun.jlo + 32 + lane]);
+        if (PG == 2) nB1 = __ldg(&pb[nrun.jlo + 32 + lane]);
       }
     };
     prefetch(it.run_begin);
     for (int r = it.run_begin; r < it.run_end; ++r) {
       const Run run = nrun;
       const double2 d = ndir;
-      stage[lane] = make_float4(nA0.x, nA0.y, nB0.x, nB0.y);
-      stage[32 + lane] = make_float4(nA1.x, nA1.y, nB1.x, nB1.y);
+      stage[lane] = CellOps::make(nA0, nB0);
+      stage[32 + lane] = CellOps::make(nA1, nB1);
       __syncwarp();
       prefetch(r + 1);
       // run.P: samples P apart never share a valid tap (P * max(|du|,|dv|)
@@ -655,24 +697,19 @@ __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
           const float wtv = s_wtbl[min(table_index64(dv, tsd), ltbl)];
           const float wu = (active && du <= L2d && (unsigned)row < (unsigned)kTile) ? wtu : 0.f;
           const float wvt = (active && dv <= L2d && (unsigned)col < (unsigned)kTile) ? wtv : 0.f;
-          float4 cc = make_float4(0.f, 0.f, 0.f, 0.f);
+          Cell cc = CellOps::zero();
           if (wu != 0.f) cc = stage[j - run.jlo];
-          const float4 c4 = make_float4(wu * cc.x, wu * cc.y, wu * cc.z, wu * cc.w);
+          const Cell c4 = CellOps::scale(wu, cc);
           float wv[NT];
 #pragma unroll
           for (int s2 = 0; s2 < NT; ++s2) wv[s2] = __shfl_sync(0xffffffffu, wvt, lane0 + s2);
-          float4* cell = tile + row * kTileStride + iv0;
-          float4 h[NT];
+          Cell* cell = tile + row * kTileStride + iv0;
+          Cell h[NT];
 #pragma unroll
           for (int s2 = 0; s2 < NT; ++s2)
             if (wu != 0.f && wv[s2] != 0.f) h[s2] = cell[s2];
 #pragma unroll
-          for (int s2 = 0; s2 < NT; ++s2) {
-            h[s2].x = fmaf(wv[s2], c4.x, h[s2].x);
-            h[s2].y = fmaf(wv[s2], c4.y, h[s2].y);
-            h[s2].z = fmaf(wv[s2], c4.z, h[s2].z);
-            h[s2].w = fmaf(wv[s2], c4.w, h[s2].w);
-          }
+          for (int s2 = 0; s2 < NT; ++s2) CellOps::fma(wv[s2], c4, h[s2]);
 #pragma unroll
           for (int s2 = 0; s2 < NT; ++s2)
             if (wu != 0.f && wv[s2] != 0.f) cell[s2] = h[s2];
@@ -689,15 +726,15 @@ __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
         const int q = q0 + lane;
         for (int pr = 0; pr < np; ++pr) {
           const int p = p0 + pr;
-          float4 val = tile[pr * kTileStride + lane];
-          if (p == 0 || q == 0) val = make_float4(0.f, 0.f, 0.f, 0.f);
-          HA[(size_t)p * a.M + q] = make_float2(val.x, val.y);
-          if (hasB) HB[(size_t)p * a.M + q] = make_float2(val.z, val.w);
+          Cell val = tile[pr * kTileStride + lane];
+          if (p == 0 || q == 0) val = CellOps::zero();
+          HA[(size_t)p * a.M + q] = CellOps::pairA(val);
+          if (hasB) HB[(size_t)p * a.M + q] = CellOps::pairB(val);
         }
       }
     } else {
       // partial tile of a split tile: summed later by split_reduce_kernel
-      float4* part = a.scratch + ((size_t)grp * a.n_slots + it.slot) * (kTile * kTile);
+      Cell* part = reinterpret_cast<Cell*>(a.scratch) + ((size_t)grp * a.n_slots + it.slot) * (kTile * kTile);
       for (int pr = 0; pr < kTile; ++pr) part[pr * kTile + lane] = tile[pr * kTileStride + lane];
     }
     __syncwarp();
@@ -706,33 +743,30 @@ __global__ void __launch_bounds__(kGridWarps * 32) grid_kernel(GridArgs a) {
 
 // Sums the partial tiles of every split tile in slot order and writes H.
 // Grid: (split tiles, pair groups); 256 threads over the tile's cells.
+template <int PG>
 __global__ void __launch_bounds__(256) split_reduce_kernel(GridArgs a) {
+  using CellOps = GridCell<PG>;
+  using Cell = typename CellOps::T;
   const int4 sp = a.split_list[blockIdx.x];  // (tile, slot0, nsplit, -)
   const int grp = blockIdx.y;
-  const int pA = grp * kGridPairs;
-  const bool hasB = pA + 1 < a.pairs;
+  const int pA = grp * PG;
+  const bool hasB = PG == 2 && pA + 1 < a.pairs;
   const int tu = sp.x / a.tiles_v, tv = sp.x - (sp.x / a.tiles_v) * a.tiles_v;
   const int p0 = tu * kTile, q0 = tv * kTile;
   const int np = min(kTile, a.M - p0), nq = min(kTile, a.M - q0);
-  const float4* base = a.scratch + ((size_t)grp * a.n_slots + sp.y) * (kTile * kTile);
+  const Cell* base = reinterpret_cast<const Cell*>(a.scratch) + ((size_t)grp * a.n_slots + sp.y) * (kTile * kTile);
   const size_t MM = (size_t)a.M * a.M;
   float2* HA = a.H + (size_t)pA * MM;
   float2* HB = HA + MM;
   for (int i = threadIdx.x; i < kTile * kTile; i += blockDim.x) {
     const int pr = i / kTile, qc = i - (i / kTile) * kTile;
     if (pr >= np || qc >= nq) continue;
-    float4 sum = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int k = 0; k < sp.z; ++k) {
-      const float4 v4 = __ldg(&base[(size_t)k * (kTile * kTile) + i]);
-      sum.x += v4.x;
-      sum.y += v4.y;
-      sum.z += v4.z;
-      sum.w += v4.w;
-    }
+    Cell sum = CellOps::zero();
+    for (int k = 0; k < sp.z; ++k) CellOps::fma(1.f, __ldg(&base[(size_t)k * (kTile * kTile) + i]), sum);
     const int p = p0 + pr, q = q0 + qc;
-    if (p == 0 || q == 0) sum = make_float4(0.f, 0.f, 0.f, 0.f);
-    HA[(size_t)p * a.M + q] = make_float2(sum.x, sum.y);
-    if (hasB) HB[(size_t)p * a.M + q] = make_float2(sum.z, sum.w);
+    if (p == 0 || q == 0) sum = CellOps::zero();
+    HA[(size_t)p * a.M + q] = CellOps::pairA(sum);
+    if (hasB) HB[(size_t)p * a.M + q] = CellOps::pairB(sum);
   }
 }
 
@@ -1889,9 +1923,12 @@ cudaError_t init_kernel_attributes() {
   add_fft_kernels<2048>(fns);
   add_fft_kernels<4096>(fns);
   add_fft_kernels<8192>(fns);
-  fns.push_back((const void*)grid_kernel<3>);
-  fns.push_back((const void*)grid_kernel<4>);
-  fns.push_back((const void*)grid_kernel<kMaxTaps>);
+  fns.push_back((const void*)grid_kernel<3, 2>);
+  fns.push_back((const void*)grid_kernel<4, 2>);
+  fns.push_back((const void*)grid_kernel<kMaxTaps, 2>);
+  fns.push_back((const void*)grid_kernel<3, 1>);
+  fns.push_back((const void*)grid_kernel<4, 1>);
+  fns.push_back((const void*)grid_kernel<kMaxTaps, 1>);
   fns.push_back((const void*)grid_wide_kernel);
   fns.push_back((const void*)grid_tc_kernel);
   fns.push_back((const void*)grid_w32_kernel);
@@ -1931,37 +1968,44 @@ cudaError_t launch_spectra(const SpectraArgs& a, gr_dtype dt, cudaStream_t s) {
   return cudaErrorInvalidValue;
 }
 
-static int grid_smem_bytes() {
-  return (257 + kGridWarps * (kTile * kTileStride + kRunMax)) * (int)sizeof(float4);
+static int grid_smem_bytes(int pg) {
+  return 257 * (int)sizeof(float4) + kGridWarps * (kTile * kTileStride + kRunMax) * pg * (int)sizeof(float2);
 }
 
+template <int PG>
+static cudaError_t launch_grid_pg(const GridArgs& a, int ntaps, cudaStream_t s) {
+  int dev = 0, sms = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int smem = grid_smem_bytes(PG);
+  int per_sm = 0;
+  if (ntaps <= 3) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_kernel<3, PG>, kGridWarps * 32, smem);
+  } else if (ntaps <= 4) {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_kernel<4, PG>, kGridWarps * 32, smem);
+  } else {
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_kernel<kMaxTaps, PG>, kGridWarps * 32,
+                                                  smem);
+  }
+  const long groups = (a.pairs + PG - 1) / PG;
+  const long want = ((long)a.n_items * groups + kGridWarps - 1) / kGridWarps;
+  const int blocks = (int)std::min<long>(want, (long)std::max(per_sm, 1) * sms);
+  if (ntaps <= 3) grid_kernel<3, PG><<<blocks, kGridWarps * 32, smem, s>>>(a);
+  else if (ntaps <= 4) grid_kernel<4, PG><<<blocks, kGridWarps * 32, smem, s>>>(a);
+  else grid_kernel<kMaxTaps, PG><<<blocks, kGridWarps * 32, smem, s>>>(a);
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess || a.n_split_tiles == 0) return e;
+  dim3 rgrid(a.n_split_tiles, (unsigned)groups);
+  split_reduce_kernel<PG><<<rgrid, 256, 0, s>>>(a);
+  return cudaGetLastError();
+}
+
+// A chunk of one pair runs the one-pair variant; larger chunks grid two pairs per warp.
 cudaError_t launch_grid(const GridArgs& a, int ntaps, cudaStream_t s) {
   if (a.n_items == 0) return cudaSuccess;
   cudaError_t e = cudaMemsetAsync(a.queue, 0, sizeof(unsigned), s);
   if (e != cudaSuccess) return e;
-  int dev = 0, sms = 0;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int smem = grid_smem_bytes();
-  int per_sm = 0;
-  if (ntaps <= 3) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_kernel<3>, kGridWarps * 32, smem);
-  } else if (ntaps <= 4) {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_kernel<4>, kGridWarps * 32, smem);
-  } else {
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, grid_kernel<kMaxTaps>, kGridWarps * 32, smem);
-  }
-  const long groups = (a.pairs + kGridPairs - 1) / kGridPairs;
-  const long want = ((long)a.n_items * groups + kGridWarps - 1) / kGridWarps;
-  const int blocks = (int)std::min<long>(want, (long)std::max(per_sm, 1) * sms);
-  if (ntaps <= 3) grid_kernel<3><<<blocks, kGridWarps * 32, smem, s>>>(a);
-  else if (ntaps <= 4) grid_kernel<4><<<blocks, kGridWarps * 32, smem, s>>>(a);
-  else grid_kernel<kMaxTaps><<<blocks, kGridWarps * 32, smem, s>>>(a);
-  e = cudaGetLastError();
-  if (e != cudaSuccess || a.n_split_tiles == 0) return e;
-  dim3 rgrid(a.n_split_tiles, (unsigned)groups);
-  split_reduce_kernel<<<rgrid, 256, 0, s>>>(a);
-  return cudaGetLastError();
+  return a.pairs == 1 ? launch_grid_pg<1>(a, ntaps, s) : launch_grid_pg<2>(a, ntaps, s);
 }
 
 static int grid_wide_smem_bytes() {

@@ -158,6 +158,11 @@ struct Plan {
   int cols_G = 0;                   // column-FFT group width (0 = cols_group(M); autotuned)
   std::vector<gr_graph*> graphs;    // live CUDA graphs replaying this plan's buffers
   float4* d_pq = nullptr;
+  // pair slots of d_pq holding the ramps of the plan's own centre (no per-slice
+  // centres): such calls skip the phase kernel.  Off for good once a call is
+  // captured into a graph, whose replays may rewrite d_pq at any time.
+  int pq_default = 0;
+  bool pq_cache_off = false;
   // host streaming (gr_reconstruct_host)
   void* h_in[2] = {nullptr, nullptr};
   float* h_out[2] = {nullptr, nullptr};
@@ -783,8 +788,16 @@ int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1
                  const float* flat, const float* dark, long flat_stride, float* o1, float* o2,
                  long out_pair_stride, long out_stride, cudaStream_t st) {
   GR_MARK();
-  PhaseArgs ph{centers, p->center, slice_base, n_valid, p->d_filt, p->d_pq, p->J, p->pdim, pairs};
-  GR_CUDA(launch_phase(ph, st));
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess || cap != cudaStreamCaptureStatusNone) {
+    cudaGetLastError();
+    p->pq_cache_off = true;
+  }
+  if (centers || p->pq_cache_off || p->pq_default < pairs) {
+    PhaseArgs ph{centers, p->center, slice_base, n_valid, p->d_filt, p->d_pq, p->J, p->pdim, pairs};
+    GR_CUDA(launch_phase(ph, st));
+    p->pq_default = (centers || p->pq_cache_off) ? 0 : pairs;
+  }
   GR_MARK();
   const bool tc = use_tc(p, pairs);
   const bool w32 = use_w32(p, pairs);
