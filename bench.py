@@ -386,6 +386,63 @@ def measure_slice_pipeline(G, sinos, th, n, a, dev, stream, peak):
     return out
 
 
+def measure_single_pair(G, sinos, th, n, a, dev, stream):
+    """The reference's own call pattern: one slice pair per call.  Device time of
+    gr_reconstruct_pair on resident buffers (a one-pair plan, CUDA events over 20
+    calls, with its stage split), and host-to-host time of GridRec.reconstruct()
+    -- the GridRec call surface over gr_reconstruct_pair_host -- on the caller's
+    pageable float32 arrays (wall clock over 10 calls; each call synchronises)."""
+    import torch
+    if sinos.dtype != torch.float32:
+        return None
+    s1, s2 = sinos[0].contiguous(), sinos[1].contiguous()
+    with G.Plan(n, a, th, filter=G.FILTER_HANN, max_pairs=1, device=dev.index or 0) as plan:
+        o = torch.empty((2, plan.M0, plan.M0), device=dev)
+        for _ in range(3):
+            plan.reconstruct_pair(s1, s2, o[0], o[1], stream=stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(20):
+            plan.reconstruct_pair(s1, s2, o[0], o[1], stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dev_us = e0.elapsed_time(e1) / 20 * 1000.0
+        plan.set_timing(True)
+        for _ in range(10):
+            plan.reconstruct_pair(s1, s2, o[0], o[1], stream=stream)
+        st, nch = plan.stage_times()
+        plan.set_timing(False)
+        kernel = plan.grid_kernel(1)
+    gr = G.GridRec()
+    gr.setSinogramDimensions(n, a)
+    gr.setThetaList(np.asarray(th, np.float32), a)
+    gr.setFilter(G.FILTER_HANN)
+    gr.setGPUDeviceID(dev.index or 0)
+    gr.init()
+    h1, h2 = s1.cpu().numpy(), s2.cpu().numpy()
+    r1 = np.zeros((n, n), np.float32)
+    r2 = np.zeros((n, n), np.float32)
+    gr.setSinoAndReconBuffers(1, h1, r1)
+    gr.setSinoAndReconBuffers(2, h2, r2)
+    for _ in range(2):
+        gr.reconstruct()
+    t0 = time.perf_counter()
+    for _ in range(10):
+        gr.reconstruct()
+    h2h_ms = (time.perf_counter() - t0) / 10 * 1000.0
+    gr.destroy()
+    return {"device_us_per_pair": dev_us,
+            "stages_us": {k: 1000.0 * v / max(nch, 1) for k, v in st.items()},
+            "grid_kernel": kernel,
+            "host_to_host_ms_per_call": h2h_ms,
+            "host_bytes_per_call": {"in": 2 * a * n * 4, "out": 2 * n * n * 4},
+            "call": "GridRec.setSinoAndReconBuffers(1|2, sinogram, reconstruction); reconstruct() "
+                    "on pageable float32 arrays (gr_reconstruct_pair_host)",
+            "note": "stage times are taken with events between the stages (eager); the phase "
+                    "stage is host time when its ramps are cached"}
+
+
 def measure_learned(sinos, th, n, a, dev, stream, args, centers_d):
     """The learned narrow-kernel path on the same resident slices, one row per narrow
     width (PSWF C = 4 and 5, networks projects_b200/correction_c4.npy and _c5.npy):
@@ -603,9 +660,10 @@ def run_b200(args, rank, world, local_rank):
     if rank == 0 and not args.no_pipeline:
         learned = measure_learned(sinos, th, n, a, dev, stream, args, centers_d)
 
-    pipe = None
+    pipe = single = None
     if rank == 0 and not args.no_pipeline:
         pipe = measure_slice_pipeline(G, sinos, th, n, a, dev, stream, peaks()[0])
+        single = measure_single_pair(G, sinos, th, n, a, dev, stream)
 
     # BASELINE configs 3 and 5 on the same box (one GPU): the uneven batch (one graph
     # launch per step, raw u16 / f32 / f16 storage) and 128 slices of the streaming volume
@@ -661,6 +719,7 @@ def run_b200(args, rank, world, local_rank):
             "cpu_baseline": cpu,
             "parity": parity,
             "slice_pipeline": pipe,
+            "single_pair": single,
             "learned": learned,
             "uneven": uneven,
             "stream": stream_cfg,
