@@ -254,16 +254,30 @@ const char* gr_last_error(void);
 /* Number of kernel launches the plan has issued since creation. */
 int gr_plan_launch_count(const gr_plan* plan, long* launches);
 
-/* Autotuner: times the gridding work-item cost cap (512..8192 sample slots per
- * item: load balance against split-tile overhead) and the column-FFT group width
- * (1..8 columns per CTA) on the plan's own workspaces, and keeps the fastest.
- * Choices are cached per shape in the process, so later plans of the same shape
- * tune instantly.  Synchronises `stream`; not for use inside stream capture.
- * Results stay within the same tolerance; bitwise reproducibility holds per
- * tuning (the item cap sets the gridding's summation order).  No reference
+/* Autotuner: on the plan's own workspaces, times
+ *  - the gridding kernel of a full chunk (max_pairs pairs), in the default mode
+ *    (wide_grid = 0) among every kernel the plan holds records for: the 32 x 32
+ *    shared-memory tile kernel, and the 4 x 8 register sub-tile kernels at 16 and 32
+ *    pairs per warp (each sub-tile shape and tile size has one compiled instance);
+ *  - for each, the work-item cost cap (512..8192 sample slots per item on the tile
+ *    list, 256..4096 on the 4 x 8 list: load balance against split-tile overhead);
+ *  - the column-FFT group width (1..8 columns per CTA);
+ * and keeps the fastest (gr_plan_grid_kernel then reports the kernel chosen for a
+ * full chunk; smaller chunks keep the choice by chunk size).  The FFTs have one
+ * radix sequence per length, so there is nothing to choose there.  Choices are
+ * cached per shape in the process, so later plans of the same shape tune
+ * instantly.  Synchronises `stream`; not for use inside stream capture.  Results
+ * stay within the same tolerance; bitwise reproducibility holds per tuning (the
+ * kernel and item cap set the gridding's summation order).  No reference
  * counterpart (the reference has fixed launch shapes). */
 int gr_plan_autotune(gr_plan* plan, void* stream);  /* GR_ERR_ARG while a gr_graph holds the plan */
 int gr_plan_tuning(const gr_plan* plan, int* item_cap, int* cols_group);
+/* Pins a tuning instead of timing one: grid_kernel for full chunks (0 tiles, 1
+ * 16-pair, 3 32-pair, as gr_plan_grid_kernel reports; -1: by chunk size; only in the
+ * default mode and among the kernels the plan holds records for), item_cap of that
+ * kernel's work list (0: keep) and cols_group (1, 2, 4, 8; 0: keep).  GR_ERR_ARG for
+ * an option the plan cannot run, or while a gr_graph holds the plan. */
+int gr_plan_set_tuning(gr_plan* plan, int grid_kernel, int item_cap, int cols_group);
 
 /* Shape of the gridding work list: work items (CTAs per pair), sample runs,
  * scratch slots of split tiles, and samples visited per pair (with halo). */

@@ -156,6 +156,9 @@ struct Plan {
   size_t x_scratch_cells = 0;
   bool x_ready = false;
   int cols_G = 0;                   // column-FFT group width (0 = cols_group(M); autotuned)
+  // gridding kernel of full chunks (max_pairs pairs) in the default mode, chosen by the
+  // autotuner or gr_plan_set_tuning: 0 tiles, 1 16-pair, 3 32-pair (-1: by chunk size)
+  int tuned_kernel = -1;
   std::vector<gr_graph*> graphs;    // live CUDA graphs replaying this plan's buffers
   float4* d_pq = nullptr;
   // pair slots of d_pq holding the ramps of the plan's own centre (no per-slice
@@ -442,7 +445,7 @@ int install_work_list(Plan* p, int item_cap) {
     return rc;
   const size_t cells =
       ((size_t)(p->max_pairs + 1) / 2) * (size_t)std::max(wl.n_slots, 1) * kTile * kTile;
-  if (cells > p->scratch_cells) {
+  if (cells != p->scratch_cells) {  // exact: a reinstall with fewer splits gives memory back
     dev_free(p, &p->d_scratch);
     if ((rc = dev_alloc(p, &p->d_scratch, cells))) return rc;
     p->scratch_cells = cells;
@@ -543,7 +546,7 @@ int install_work_list_wide(Plan* p, int item_cap) {
     // 32 cells x 32 pairs complex = 512 float4 per slot and group of 32 pairs
     const size_t groups32 = (size_t)(p->max_pairs + kW32Pairs - 1) / kW32Pairs;
     const size_t xcells = groups32 * (size_t)std::max(wl.n_slots, 1) * (kWideRows * kWideCols * 32 / 2);
-    if (xcells > p->x_scratch_cells) {
+    if (xcells != p->x_scratch_cells) {
       dev_free(p, &p->d_x_scratch);
       if ((rc = dev_alloc(p, &p->d_x_scratch, xcells))) return rc;
       p->x_scratch_cells = xcells;
@@ -554,7 +557,7 @@ int install_work_list_wide(Plan* p, int item_cap) {
   // 64 cells x 32 lanes floats = 512 float4 per slot and group of 16 pairs
   const size_t groups = (size_t)(p->max_pairs + kWidePairs - 1) / kWidePairs;
   const size_t cells = groups * (size_t)std::max(wl.n_slots, 1) * (kWideRows * kWideCols * 32 / 4);
-  if (need16 && cells > p->w_scratch_cells) {
+  if (need16 && cells != p->w_scratch_cells) {
     dev_free(p, &p->d_w_scratch);
     if ((rc = dev_alloc(p, &p->d_w_scratch, cells))) return rc;
     p->w_scratch_cells = cells;
@@ -599,7 +602,7 @@ int install_work_list_tc(Plan* p, int item_cap) {
     return rc;
   const size_t groups = (size_t)(p->max_pairs + kWidePairs - 1) / kWidePairs;
   const size_t cells = groups * (size_t)std::max(wl.n_slots, 1) * (kTcRows * kTcCols * 32 / 4);
-  if (cells > p->t_scratch_cells) {
+  if (cells != p->t_scratch_cells) {
     dev_free(p, &p->d_t_scratch);
     if ((rc = dev_alloc(p, &p->d_t_scratch, cells))) return rc;
     p->t_scratch_cells = cells;
@@ -624,12 +627,14 @@ bool use_tc(const Plan* p, int pairs) {
 // group pair-slot), while up to 16 pairs the 16-pair kernel's launch is cheaper.
 bool use_w32(const Plan* p, int pairs) {
   if (!p->x_ready || p->w_items == 0) return false;
+  if (p->wide_mode == 0 && p->tuned_kernel >= 0 && pairs == p->max_pairs) return p->tuned_kernel == 3;
   return p->wide_mode == 3 || (p->wide_mode == 0 && pairs > kWidePairs);
 }
 
 // Whether a chunk of `pairs` pairs grids with grid_wide_kernel.
 bool use_wide(const Plan* p, int pairs) {
   if (p->w_items == 0 || p->wide_mode < 0 || use_tc(p, pairs) || use_w32(p, pairs)) return false;
+  if (p->wide_mode == 0 && p->tuned_kernel >= 0 && pairs == p->max_pairs) return p->tuned_kernel == 1;
   return p->wide_mode == 1 || pairs >= kWideMinPairs;
 }
 
@@ -1222,21 +1227,40 @@ int gr_plan_autotune(gr_plan* p, void* stream) {
   mix((unsigned long long)std::llround(p->L * 1e6));
   for (double d : p->dxy) mix((unsigned long long)std::llround(d * 1e9));
   static std::mutex mu;
-  struct Tuned { int cap, G; };  // cap: item cap of the kernel a full chunk uses
+  // kernel: gridding kernel of full chunks (-1: the mode's fixed choice); cap_t / cap_w:
+  // item caps of the tile and 4 x 8 work lists
+  struct Tuned { int kernel, cap_t, cap_w, G; };
   static std::map<unsigned long long, Tuned> cache;
-  const bool w32 = use_w32(p, p->max_pairs);
-  const bool wide = use_wide(p, p->max_pairs) || w32;  // both use the 4 x 8 work list
-  auto install = [&](int cap) {
-    if (wide) return cap == p->w_item_cap ? GR_OK : install_work_list_wide(p, cap);
+  const int pairs = p->max_pairs;
+  // the gridding kernels a full chunk can run: in the default mode every kernel the
+  // plan holds records for; in a forced mode the forced one
+  std::vector<int> kernels;
+  if (p->wide_mode == 0) {
+    kernels.push_back(0);
+    if (wide16_possible(p) && p->w_items) kernels.push_back(1);
+    if (w32_possible(p) && p->x_ready && p->w_items) kernels.push_back(3);
+  } else {
+    kernels.push_back(use_tc(p, pairs) ? 2 : (use_w32(p, pairs) ? 3 : (use_wide(p, pairs) ? 1 : 0)));
+  }
+  auto install = [&](int kernel, int cap) -> int {
+    if (kernel == 2) return GR_OK;  // the tensor-core list keeps its cap
+    if (kernel == 1 || kernel == 3)
+      return cap == p->w_item_cap ? GR_OK : install_work_list_wide(p, cap);
     return cap == p->item_cap ? GR_OK : install_work_list(p, cap);
+  };
+  auto apply = [&](const Tuned& t) -> int {
+    int rc = install(0, t.cap_t);
+    if (rc == GR_OK && p->w_items) rc = install(1, t.cap_w);
+    if (rc == GR_OK) {
+      p->cols_G = t.G;
+      p->tuned_kernel = p->wide_mode == 0 && kernels.size() > 1 ? t.kernel : -1;
+    }
+    return rc;
   };
   {
     std::lock_guard<std::mutex> lk(mu);
     auto it = cache.find(h);
-    if (it != cache.end()) {
-      p->cols_G = it->second.G;
-      return install(it->second.cap);
-    }
+    if (it != cache.end()) return apply(it->second);
   }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   GR_CUDA(cudaEventCreate(&e0));
@@ -1254,27 +1278,49 @@ int gr_plan_autotune(gr_plan* p, void* stream) {
     }
     return best;
   };
-  const int pairs = p->max_pairs;
   cudaMemsetAsync(p->d_spec, 0, (size_t)p->spec_pairs * p->n_ang * 2 * p->J * sizeof(float2), st);
   cudaMemsetAsync(p->d_H, 0, (size_t)pairs * p->M * p->M * sizeof(float2), st);
-  int best_cap = wide ? p->w_item_cap : p->item_cap, rc = GR_OK;
+  Tuned best{kernels[0], p->item_cap, p->w_item_cap, 0};
   float best_t = 1e30f;
-  const std::vector<int> caps = wide ? std::vector<int>{256, 512, 1024, 2048, 4096}
-                                     : std::vector<int>{512, 1024, 2048, 4096, 8192};
-  for (int cap : caps) {
-    if ((rc = install(cap))) break;
-    const GridArgs ga = w32 ? grid_args_w32(p, pairs) : grid_args(p, pairs, wide);
-    const float t = time_ms([&] {
-      if (w32) launch_grid_w32(ga, st);
-      else if (wide) launch_grid_wide(ga, st);
-      else launch_grid(ga, p->ntaps, st);
-    });
-    if (t < best_t) {
-      best_t = t;
-      best_cap = cap;
+  int best_cap_t = p->item_cap, best_cap_w = p->w_item_cap, rc = GR_OK;
+  float best_tt = 1e30f, best_tw = 1e30f;
+  const int saved = p->tuned_kernel;
+  for (int kernel : kernels) {
+    if (kernel == 2) {  // forced tensor-core mode: nothing to choose in the gridding
+      best.kernel = 2;
+      break;
     }
+    const bool wl4x8 = kernel != 0;
+    const std::vector<int> caps = wl4x8 ? std::vector<int>{256, 512, 1024, 2048, 4096}
+                                        : std::vector<int>{512, 1024, 2048, 4096, 8192};
+    for (int cap : caps) {
+      if ((rc = install(kernel, cap))) break;
+      const GridArgs ga =
+          kernel == 3 ? grid_args_w32(p, pairs) : grid_args(p, pairs, kernel == 1);
+      const float t = time_ms([&] {
+        if (kernel == 3) launch_grid_w32(ga, st);
+        else if (kernel == 1) launch_grid_wide(ga, st);
+        else launch_grid(ga, p->ntaps, st);
+      });
+      if (wl4x8 && t < best_tw) {
+        best_tw = t;
+        best_cap_w = cap;
+      }
+      if (!wl4x8 && t < best_tt) {
+        best_tt = t;
+        best_cap_t = cap;
+      }
+      if (t < best_t) {
+        best_t = t;
+        best.kernel = kernel;
+      }
+    }
+    if (rc) break;
   }
-  if (rc == GR_OK) rc = install(best_cap);
+  p->tuned_kernel = saved;
+  best.cap_t = best_cap_t;
+  best.cap_w = best_cap_w;
+  if (rc == GR_OK) rc = apply(best);
   int best_G = 0;
   float best_c = 1e30f;
   for (int G = 1; G <= 8 && rc == GR_OK; G *= 2) {
@@ -1293,15 +1339,51 @@ int gr_plan_autotune(gr_plan* p, void* stream) {
   cudaError_t e = cudaGetLastError();
   if (rc == GR_OK && e != cudaSuccess) rc = fail(GR_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
   if (rc == GR_OK) {
+    best.G = best_G;
     p->cols_G = best_G;
     std::lock_guard<std::mutex> lk(mu);
-    cache[h] = {best_cap, best_G};
+    cache[h] = best;
   }
+  return rc;
+}
+
+int gr_plan_set_tuning(gr_plan* p, int grid_kernel, int item_cap, int cols_group) {
+  using namespace gr;
+  if (!p) return fail(GR_ERR_ARG, "null plan");
+  if (!p->graphs.empty())
+    return fail(GR_ERR_ARG, "set_tuning replaces buffers that %d live graph(s) replay",
+                (int)p->graphs.size());
+  const bool ok_kernel =
+      grid_kernel < 0 ||
+      (p->wide_mode == 0 &&
+       (grid_kernel == 0 || (grid_kernel == 1 && wide16_possible(p) && p->w_items) ||
+        (grid_kernel == 3 && w32_possible(p) && p->x_ready && p->w_items)));
+  if (!ok_kernel)
+    return fail(GR_ERR_ARG, "grid kernel %d is not available on this plan (wide_grid %d, "
+                "max_pairs %d)", grid_kernel, p->wide_mode, p->max_pairs);
+  if (item_cap != 0 && (item_cap < 64 || item_cap > (1 << 20)))
+    return fail(GR_ERR_ARG, "item cap %d outside 64 .. 2^20 (0: keep)", item_cap);
+  if (cols_group != 0) {
+    const int threads = cols_group * (p->M / 16);
+    if (cols_group < 1 || (cols_group & (cols_group - 1)) || cols_group > 8 || threads < 32 ||
+        threads > 1024 || p->M % cols_group)
+      return fail(GR_ERR_ARG, "column group %d not valid for M = %d", cols_group, p->M);
+  }
+  DeviceGuard g(p->device);
+  p->tuned_kernel = grid_kernel;
+  const int k = grid_kernel >= 0 ? grid_kernel : (use_w32(p, p->max_pairs) ? 3 : (use_wide(p, p->max_pairs) ? 1 : 0));
+  int rc = GR_OK;
+  if (item_cap > 0) {
+    if (k == 0 && item_cap != p->item_cap) rc = install_work_list(p, item_cap);
+    if ((k == 1 || k == 3) && item_cap != p->w_item_cap) rc = install_work_list_wide(p, item_cap);
+  }
+  if (rc == GR_OK && cols_group > 0) p->cols_G = cols_group;
   return rc;
 }
 
 int gr_plan_tuning(const gr_plan* p, int* item_cap, int* cols_group_width) {
   if (!p) return gr::fail(GR_ERR_ARG, "null plan");
+  // the item cap of the work list a full chunk grids with
   const bool wl4x8 = gr::use_wide(p, p->max_pairs) || gr::use_w32(p, p->max_pairs);
   if (item_cap) *item_cap = wl4x8 ? p->w_item_cap : p->item_cap;
   if (cols_group_width) *cols_group_width = p->cols_G > 0 ? p->cols_G : gr::cols_group(p->M);

@@ -35,7 +35,7 @@ EXPORTS = ("gr_params_default", "gr_filter_code", "gr_plan_create", "gr_plan_des
            "gr_ring_removal", "gr_shift_pad", "gr_crop_center", "gr_entropy_workspace_bytes",
            "gr_entropy", "gr_reconstruct_padded", "gr_center_search", "gr_graph_create",
            "gr_graph_launch", "gr_graph_launch_count", "gr_graph_destroy", "gr_plan_autotune",
-           "gr_plan_tuning", "gr_xcorr_scores", "gr_fbp_create", "gr_fbp_reconstruct",
+           "gr_plan_tuning", "gr_plan_set_tuning", "gr_xcorr_scores", "gr_fbp_create", "gr_fbp_reconstruct",
            "gr_threshold_workspace_bytes", "gr_threshold_range", "gr_to_u8",
            "gr_fbp_destroy", "gr_cnn_param_count", "gr_cnn_workspace_bytes",
            "gr_cnn_forward_workspace_bytes", "gr_cnn_forward",
@@ -135,6 +135,7 @@ def lib():
         L.gr_xcorr_scores.argtypes = [vp, vp] + [i_] * 6 + [d_] * 4 + [i_, i_,
                                                                          C.POINTER(d_), vp]
         L.gr_plan_tuning.argtypes = [vp, C.POINTER(i_), C.POINTER(i_)]
+        L.gr_plan_set_tuning.argtypes = [vp, i_, i_, i_]
         _lib = L
     return _lib
 
@@ -293,14 +294,28 @@ class Plan:
         return dict(zip(STAGES, list(ms))), n.value
 
     def autotune(self, stream=None):
-        """Times the gridding item cap and column-FFT group width; returns the choice."""
+        """Times the gridding kernel of a full chunk, its item cap and the column-FFT
+        group width; returns the choice (tuning())."""
         _check(lib().gr_plan_autotune(self._h, _stream_ptr(stream)), "gr_plan_autotune")
+        return self.tuning()
+
+    GRID_KERNEL_CODES = {"tiles": 0, "wide": 1, "wide32": 3}
+
+    def set_tuning(self, grid_kernel=None, item_cap=0, cols_group=0):
+        """Pins a tuning: grid_kernel ('tiles', 'wide', 'wide32' or None for the
+        choice by chunk size) for full chunks, its work list's item cap (0: keep)
+        and the column-FFT group width (0: keep)."""
+        k = -1 if grid_kernel is None else self.GRID_KERNEL_CODES[grid_kernel]
+        _check(lib().gr_plan_set_tuning(self._h, k, int(item_cap), int(cols_group)),
+               "gr_plan_set_tuning")
         return self.tuning()
 
     def tuning(self):
         cap, g = C.c_int(), C.c_int()
         _check(lib().gr_plan_tuning(self._h, C.byref(cap), C.byref(g)), "gr_plan_tuning")
-        return {"item_cap": cap.value, "cols_group": g.value}
+        return {"grid_kernel": self.grid_kernel(self.max_pairs), "item_cap": cap.value,
+                "cols_group": g.value, "tile": "32 x 32 (tile kernel) / 4 x 8 (register "
+                "sub-tile kernels): one compiled instance each"}
 
     def work_stats(self):
         a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_long()

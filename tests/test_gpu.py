@@ -491,19 +491,69 @@ def test_autotune_keeps_parity_and_caches():
             assert again.autotune() == t  # cached for the shape
 
 
+def test_every_tuning_option_keeps_parity():
+    """Every choice the autotuner can make on a 32-pair plan -- the gridding kernel of
+    a full chunk (32 x 32 tiles, 4 x 8 sub-tiles at 16 and 32 pairs per warp), each
+    kernel's item caps, and the column-FFT group widths -- pinned with set_tuning,
+    reconstructs a 64-slice batch within the float64 tolerance; autotune picks one of
+    them and grid_kernel reports it."""
+    n, a = 128, 90
+    th = ph.angles_deg(a)
+    sin = np.stack([ph.random_ellipse_sinogram(k, n, a, center=64.0)[0] for k in range(64)])
+    ref = [O.port_gridrec_pair(sin[2 * i], sin[2 * i + 1], th, center1=64.0, filter=2)
+           for i in (0, 31)]
+    caps = {"tiles": (512, 1024, 2048, 4096, 8192), "wide": (256, 512, 1024, 2048, 4096),
+            "wide32": (256, 512, 1024, 2048, 4096)}
+    with G.Plan(n, a, th, center=64.0, filter=G.FILTER_HANN, max_pairs=32) as plan:
+        x = _dev(sin)
+        outs = torch.zeros((64, plan.M0, n), device="cuda")
+
+        def check(label):
+            outs.zero_()
+            plan.reconstruct_batch(x, outs)
+            torch.cuda.synchronize()
+            plan.device_status()
+            o = outs.cpu().numpy()
+            for k, (r1, r2) in zip((0, 31), ref):
+                m = r1.shape[0]
+                assert ph.rel_l2(o[2 * k, :m, :m], r1[:, :m]) < TOL, label
+                assert ph.rel_l2(o[2 * k + 1, :m, :m], r2[:, :m]) < TOL, label
+
+        for kernel, cl in caps.items():
+            for cap in cl:
+                t = plan.set_tuning(kernel, cap, 0)
+                assert t["grid_kernel"] == kernel and t["item_cap"] == cap
+                check((kernel, cap))
+        for g in (1, 2, 4, 8):
+            if g * (plan.M // 16) < 32 or g * (plan.M // 16) > 1024:
+                continue
+            assert plan.set_tuning(None, 0, g)["cols_group"] == g
+            check(("cols_group", g))
+        with pytest.raises(G.GrError):
+            plan.set_tuning("wide", 0, 3)  # not a power of two
+        t = plan.autotune()
+        assert t["grid_kernel"] in caps and t["item_cap"] in caps[t["grid_kernel"]]
+        assert plan.grid_kernel(32) == t["grid_kernel"]
+        check("autotuned")
+    with G.Plan(n, a, th, center=64.0, max_pairs=2) as small:
+        with pytest.raises(G.GrError):
+            small.set_tuning("wide32")  # no 32-pair records on a 2-pair plan
+
+
 def test_device_bytes_after_autotune_count_live_buffers_only():
-    """Autotune reinstalls the 16-pair work list (and its precomputed weights) once
-    per item cap it times; the plan's device byte count follows the frees, so it
-    ends within the size differences of the lists, not at one list per cap tried."""
+    """Autotune reinstalls the tile and 16-pair work lists (with the 16-pair
+    kernel's precomputed weights and the split-tile scratch) once per item cap it
+    times.  The plan's device byte count follows the frees and each scratch is sized
+    to the list kept: a plan tuned by trial ends at exactly the bytes of a plan of
+    the same shape that takes the cached choice without trying anything."""
     th = ph.angles_deg(360)
-    _, runs, _, _ = G.worklist(512, 360, th, wide=True)
-    weights = int((runs[:, 2] - runs[:, 1] + 1).sum()) * 48  # one list's weights
     with G.Plan(512, 360, th, filter=G.FILTER_HANN, max_pairs=16) as plan:
         assert plan.grid_kernel(16) == "wide"
-        before = plan.device_bytes()
-        plan.autotune()  # times 5 item caps
-        after = plan.device_bytes()
-    assert abs(after - before) < 2 * weights, (before, after, weights)
+        t = plan.autotune()  # times 5 item caps per kernel
+        tried = plan.device_bytes()
+        with G.Plan(512, 360, th, filter=G.FILTER_HANN, max_pairs=16) as again:
+            assert again.autotune() == t  # cached: installs the choice directly
+            assert again.device_bytes() == tried, (tried, again.device_bytes())
 
 
 def test_autotune_refused_while_a_graph_holds_the_plan():
