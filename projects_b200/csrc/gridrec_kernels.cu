@@ -146,6 +146,11 @@ __device__ __forceinline__ void dftR(float2* v) {
 // of exp(+2 pi i e/N) in shared memory.
 
 __device__ __forceinline__ int swz(int i) { return i ^ ((i >> 4) & 15); }
+// swz(x + d) = swz_at(x, d) + d for d a multiple of 16: the XOR mask of the low 4 bits
+// moves by d / 16 (mod 16), the rest of d passes through.  With d a compile-time
+// multiple of 16 the mask takes few distinct values across a pass's r (one when d is
+// a multiple of 256), so the bases are computed once and d becomes an immediate offset.
+__device__ __forceinline__ int swz_at(int x, int d) { return x ^ (((x >> 4) + (d >> 4)) & 15); }
 
 template <int S>
 __device__ __forceinline__ float2 twiddle(const float2* lo, const float2* hi, int e) {
@@ -255,11 +260,12 @@ template <int R, int S, int N, int Ns, bool LAST>
 __device__ __forceinline__ void fft_pass_t(float2 (&v)[16], float2* buf, int tid, const float2* lo,
                                            const float2* hi) {
   constexpr int B = 16 / R, NR = N / R, nthr = N / 16, tstep = N / (Ns * R);
+  static_assert(NR % 16 == 0 && Ns % 16 == 0, "offsets that keep the swizzle's low bits");
 #pragma unroll
   for (int i = 0; i < B; ++i) {
     const int j = tid + i * nthr;
 #pragma unroll
-    for (int r = 0; r < R; ++r) v[i * R + r] = buf[swz(j + r * NR)];
+    for (int r = 0; r < R; ++r) v[i * R + r] = buf[swz_at(j, r * NR) + r * NR];
   }
 #pragma unroll
   for (int i = 0; i < B; ++i) {
@@ -303,7 +309,7 @@ __device__ __forceinline__ void fft_pass_t(float2 (&v)[16], float2* buf, int tid
       const int k = j & (Ns - 1);
       const int base = (j - k) * R + k;
 #pragma unroll
-      for (int r = 0; r < R; ++r) buf[swz(base + r * Ns)] = v[i * R + r];
+      for (int r = 0; r < R; ++r) buf[swz_at(base, r * Ns) + r * Ns] = v[i * R + r];
     }
     __syncthreads();
   }
@@ -474,8 +480,14 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
   // F[j] and F[pdim - j] meet through shared memory
   const int Rl = line_last_radix<NT>(a.pdim);
   __syncthreads();
+  // offsets d = multiples of nthr = pdim / 16: when nthr is a multiple of 16 (pdim >=
+  // 256, always for the compile-time lengths) swz(tid + d) = swz_at(tid, d) + d
+  const bool d16 = NT > 0 || (nthr & 15) == 0;
 #pragma unroll
-  for (int idx = 0; idx < 16; ++idx) buf[swz(tid + nthr * out_index(idx, Rl))] = v[idx];
+  for (int idx = 0; idx < 16; ++idx) {
+    const int d = nthr * out_index(idx, Rl);
+    buf[d16 ? swz_at(tid, d) + d : swz(tid + d)] = v[idx];
+  }
   __syncthreads();
   const float4* pq = a.pq + (size_t)pair * a.J;
   // plain: [pair][dir][j]; wide (G = 16 or 32 pairs): [pair / G][dir][j / 4][pair % G][j % 4],
@@ -503,12 +515,18 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
     qmask = 0x3fffffff;
     qlog = 6;
   }
-  for (int j = tid; j < a.J; j += nthr) {
+  // J = pdim / 2 = 8 nthr: thread tid takes j = tid + i nthr, i < 8; the swizzled
+  // addresses of j and pdim - j follow from tid and pdim - tid by swz_at
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    const int j = tid + i * nthr;
+    if (j >= a.J) break;
     const int oj = ((j >> qshift) << qlog) + ((j & qmask) ^ rot);
     float2 c1 = make_float2(0.f, 0.f), c2 = make_float2(0.f, 0.f);
     if (j > 0) {
-      const float2 F = buf[swz(j)];
-      const float2 G = buf[swz(a.pdim - j)];
+      const int d = i * nthr;
+      const float2 F = buf[d16 ? swz_at(tid, d) + d : swz(j)];
+      const float2 G = buf[d16 ? swz_at(a.pdim - tid, -d) - d : swz(a.pdim - j)];
       const float4 q = __ldg(&pq[j]);  // P = (x, y), Q = (z, w)
       // C1 = P F + Q conj(G);  C2 = conj(P) G + conj(Q) conj(F)
       c1.x = q.x * F.x - q.y * F.y + q.z * G.x + q.w * G.y;
