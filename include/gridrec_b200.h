@@ -261,7 +261,8 @@ int gr_plan_launch_count(const gr_plan* plan, long* launches);
  *    pairs per warp (each sub-tile shape and tile size has one compiled instance);
  *  - for each, the work-item cost cap (512..8192 sample slots per item on the tile
  *    list, 256..4096 on the 4 x 8 list: load balance against split-tile overhead);
- *  - the column-FFT group width (1..8 columns per CTA);
+ *  - the column-FFT group width (1..8 columns per CTA), each with one strip per
+ *    CTA and with persistent CTAs that double-buffer their strips;
  * and keeps the fastest (gr_plan_grid_kernel then reports the kernel chosen for a
  * full chunk; smaller chunks keep the choice by chunk size).  The FFTs have one
  * radix sequence per length, so there is nothing to choose there.  Choices are
@@ -275,9 +276,16 @@ int gr_plan_tuning(const gr_plan* plan, int* item_cap, int* cols_group);
 /* Pins a tuning instead of timing one: grid_kernel for full chunks (0 tiles, 1
  * 16-pair, 3 32-pair, as gr_plan_grid_kernel reports; -1: by chunk size; only in the
  * default mode and among the kernels the plan holds records for), item_cap of that
- * kernel's work list (0: keep) and cols_group (1, 2, 4, 8; 0: keep).  GR_ERR_ARG for
- * an option the plan cannot run, or while a gr_graph holds the plan. */
-int gr_plan_set_tuning(gr_plan* plan, int grid_kernel, int item_cap, int cols_group);
+ * kernel's work list (0: keep), cols_group (1, 2, 4, 8; 0: keep) and cols_ring (1:
+ * the persistent double-buffered column FFT where its two landing buffers fit in
+ * shared memory, 0: one strip per CTA, -1: keep).  GR_ERR_ARG for an option the plan
+ * cannot run, or while a gr_graph holds the plan. */
+int gr_plan_set_tuning(gr_plan* plan, int grid_kernel, int item_cap, int cols_group,
+                       int cols_ring);
+/* The full tuning: gridding kernel of a full chunk, its item cap, column group width
+ * and whether the column FFT runs persistent and double-buffered. */
+int gr_plan_tuning_ex(const gr_plan* plan, int* grid_kernel, int* item_cap, int* cols_group,
+                      int* cols_ring);
 
 /* Shape of the gridding work list: work items (CTAs per pair), sample runs,
  * scratch slots of split tiles, and samples visited per pair (with halo). */

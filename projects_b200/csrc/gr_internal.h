@@ -152,6 +152,7 @@ struct ColArgs {
   int M, pairs;
   int* err;              // device error word for bounded-wait timeouts (null: plain loads)
   int G = 0;             // columns per CTA (0: cols_group(M))
+  int ring = 0;          // 1: persistent CTAs with two landing buffers (cols_ring_kernel)
 };
 
 struct RowArgs {

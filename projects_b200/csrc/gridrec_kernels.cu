@@ -1765,6 +1765,75 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT)
   for (int idx = 0; idx < 16; ++idx) Hp[(size_t)(tid + nthr * out_index(idx, Rl)) * M] = v[idx];
 }
 
+// The column FFT with persistent CTAs (as many as fit per SM): strip s = blockIdx.x + i gridDim.x
+// of G columns lands by TMA in buffer i % 2 while the previous strip is transformed
+// from the other, so the copy latency that the one-strip kernel waits out is hidden.
+// A buffer is refilled once every thread is done with it (its FFT exchange writes are
+// ordered before the copy by a proxy fence and a barrier).  Waits are bounded: on a
+// timeout the CTA records the error word, waits (bounded) for its copies in flight and
+// leaves.  Same transform, same results as cols_tma_kernel.
+template <int MAXT, int NT>
+__global__ void __launch_bounds__(MAXT, 512 / MAXT > 0 ? 512 / MAXT : 1)
+    cols_ring_kernel(const __grid_constant__ CUtensorMap tmap, ColArgs a, int G, int box_rows) {
+  extern __shared__ __align__(128) float2 sm[];
+  const int M = NT ? NT : a.M;
+  const int nthr = M >> 4;
+  const int per_pair = M / G, total = per_pair * a.pairs;
+  const int lstride = G * M + 16;  // landing buffer: [row][g], + 16 for the exchange stride
+  float2* tw = sm;
+  float2* land0 = sm + kTwSlots;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(land0 + 2 * lstride);
+  const int g = threadIdx.x % G, tid = threadIdx.x / G;
+  const unsigned bytes = (unsigned)(G * M) * (unsigned)sizeof(float2);
+  auto issue = [&](int s, int b) {  // one thread
+    const int pair = s / per_pair, q0 = (s - pair * per_pair) * G;
+    mbar_expect_tx(&bar[b], bytes);
+    for (int r = 0; r < M; r += box_rows)
+      tma_load_2d(land0 + (size_t)b * lstride + (size_t)r * G, &tmap, 2 * q0, pair * M + r, &bar[b]);
+  };
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();  // the barriers are initialised before any thread polls them
+  if (threadIdx.x == 0) {
+    if ((int)blockIdx.x < total) issue(blockIdx.x, 0);
+    if ((int)(blockIdx.x + gridDim.x) < total) issue(blockIdx.x + gridDim.x, 1);
+  }
+  load_twiddles(tw, a.tw, M);
+  const int Rl = line_last_radix<NT>(M);
+  int i = 0;
+  for (int s = blockIdx.x; s < total; s += gridDim.x, ++i) {
+    const int b = i & 1;
+    const unsigned ph = (unsigned)(i >> 1) & 1u;
+    float2* land = land0 + (size_t)b * lstride;
+    const bool ok = mbar_wait(&bar[b], ph);
+    if (__syncthreads_or(!ok)) {
+      if (threadIdx.x == 0) {
+        atomicExch(a.err, 1);
+        mbar_wait(&bar[b], ph);  // this strip's copy
+        if (s + (int)gridDim.x < total) mbar_wait(&bar[b ^ 1], (unsigned)((i + 1) >> 1) & 1u);
+      }
+      __syncthreads();
+      return;
+    }
+    float2 v[16];
+#pragma unroll
+    for (int r = 0; r < 16; ++r) v[r] = land[(tid + r * nthr) * G + g];
+    __syncthreads();  // inputs read before the landing buffer becomes the exchange buffer
+    fft_line<-1, NT>(v, land + g * (M + 16 / G), M, tid, nthr, tw, tw + 64);
+    const int pair = s / per_pair, q0 = (s - pair * per_pair) * G;
+    float2* Hp = a.H + (size_t)pair * M * M + q0 + g;
+#pragma unroll
+    for (int idx = 0; idx < 16; ++idx) Hp[(size_t)(tid + nthr * out_index(idx, Rl)) * M] = v[idx];
+    // every thread's exchange accesses of this buffer come before the copy that refills it
+    fence_proxy_async();
+    __syncthreads();
+    if (threadIdx.x == 0 && s + 2 * (int)gridDim.x < total) issue(s + 2 * gridDim.x, b);
+  }
+}
+
 // ------------------------------------------------------------------ second axis + deapod (K4)
 
 template <int MAXT, int NT>
@@ -1920,6 +1989,9 @@ void add_fft_kernels(std::vector<const void*>& f) {
   f.push_back((const void*)cols_tma_kernel<256, NT>);
   f.push_back((const void*)cols_tma_kernel<512, NT>);
   f.push_back((const void*)cols_tma_kernel<1024, NT>);
+  f.push_back((const void*)cols_ring_kernel<256, NT>);
+  f.push_back((const void*)cols_ring_kernel<512, NT>);
+  f.push_back((const void*)cols_ring_kernel<1024, NT>);
   f.push_back((const void*)rows_kernel<256, NT>);
   f.push_back((const void*)rows_kernel<512, NT>);
   f.push_back((const void*)fbp_filter_kernel<256, NT>);
@@ -2150,6 +2222,30 @@ cudaError_t launch_cols(const ColArgs& a, cudaStream_t s) {
     CUresult r = encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)a.H, dims, strides, box,
                         estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
                         CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    int optin = 0, dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const int ring_smem = (kTwSlots + 2 * (G * a.M + 16)) * (int)sizeof(float2) + 2 * (int)sizeof(uint64_t);
+    if (r == CUDA_SUCCESS && a.ring && ring_smem <= optin) {
+      const int total = (a.M / G) * a.pairs;
+      // persistent: as many CTAs as fit on the SMs at once
+#define GR_COLR(NT)                                                                              \
+  {                                                                                              \
+    const void* fn = threads <= 256 ? (const void*)cols_ring_kernel<256, NT>                     \
+                     : threads <= 512 ? (const void*)cols_ring_kernel<512, NT>                   \
+                                      : (const void*)cols_ring_kernel<1024, NT>;                 \
+    int per_sm = 0;                                                                              \
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, threads, ring_smem);              \
+    const int blocks = std::min(total, std::max(per_sm, 1) * std::max(sms, 1));                  \
+    if (threads <= 256) cols_ring_kernel<256, NT><<<blocks, threads, ring_smem, s>>>(map, a, G, box_rows); \
+    else if (threads <= 512) cols_ring_kernel<512, NT><<<blocks, threads, ring_smem, s>>>(map, a, G, box_rows); \
+    else cols_ring_kernel<1024, NT><<<blocks, threads, ring_smem, s>>>(map, a, G, box_rows);      \
+  }
+      GR_DISPATCH_N(a.M, GR_COLR)
+#undef GR_COLR
+      return cudaGetLastError();
+    }
     if (r == CUDA_SUCCESS) {
       const int smem = (kTwSlots + G * a.M + 16) * (int)sizeof(float2) + (int)sizeof(uint64_t);
       dim3 grid(a.M / G, a.pairs);

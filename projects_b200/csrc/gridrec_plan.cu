@@ -156,6 +156,7 @@ struct Plan {
   size_t x_scratch_cells = 0;
   bool x_ready = false;
   int cols_G = 0;                   // column-FFT group width (0 = cols_group(M); autotuned)
+  int cols_ring = 0;                // 1: persistent double-buffered column FFT (autotuned)
   // gridding kernel of full chunks (max_pairs pairs) in the default mode, chosen by the
   // autotuner or gr_plan_set_tuning: 0 tiles, 1 16-pair, 3 32-pair (-1: by chunk size)
   int tuned_kernel = -1;
@@ -819,7 +820,7 @@ int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1
              : (w32 ? launch_grid_w32(ga, st)
                     : (wide ? launch_grid_wide(ga, st) : launch_grid(ga, p->ntaps, st))));
   GR_MARK();
-  ColArgs ca{p->d_H, p->d_tw_m, p->M, pairs, p->d_err, p->cols_G};
+  ColArgs ca{p->d_H, p->d_tw_m, p->M, pairs, p->d_err, p->cols_G, p->cols_ring};
   GR_CUDA(launch_cols(ca, st));
   GR_MARK();
   RowArgs ra{p->d_H, p->d_tw_m, p->d_winv, o1, o2, out_pair_stride, out_stride, n_valid,
@@ -1229,7 +1230,7 @@ int gr_plan_autotune(gr_plan* p, void* stream) {
   static std::mutex mu;
   // kernel: gridding kernel of full chunks (-1: the mode's fixed choice); cap_t / cap_w:
   // item caps of the tile and 4 x 8 work lists
-  struct Tuned { int kernel, cap_t, cap_w, G; };
+  struct Tuned { int kernel, cap_t, cap_w, G, ring; };
   static std::map<unsigned long long, Tuned> cache;
   const int pairs = p->max_pairs;
   // the gridding kernels a full chunk can run: in the default mode every kernel the
@@ -1253,6 +1254,7 @@ int gr_plan_autotune(gr_plan* p, void* stream) {
     if (rc == GR_OK && p->w_items) rc = install(1, t.cap_w);
     if (rc == GR_OK) {
       p->cols_G = t.G;
+      p->cols_ring = t.ring;
       p->tuned_kernel = p->wide_mode == 0 && kernels.size() > 1 ? t.kernel : -1;
     }
     return rc;
@@ -1280,7 +1282,7 @@ int gr_plan_autotune(gr_plan* p, void* stream) {
   };
   cudaMemsetAsync(p->d_spec, 0, (size_t)p->spec_pairs * p->n_ang * 2 * p->J * sizeof(float2), st);
   cudaMemsetAsync(p->d_H, 0, (size_t)pairs * p->M * p->M * sizeof(float2), st);
-  Tuned best{kernels[0], p->item_cap, p->w_item_cap, 0};
+  Tuned best{kernels[0], p->item_cap, p->w_item_cap, 0, 0};
   float best_t = 1e30f;
   int best_cap_t = p->item_cap, best_cap_w = p->w_item_cap, rc = GR_OK;
   float best_tt = 1e30f, best_tw = 1e30f;
@@ -1321,17 +1323,20 @@ int gr_plan_autotune(gr_plan* p, void* stream) {
   best.cap_t = best_cap_t;
   best.cap_w = best_cap_w;
   if (rc == GR_OK) rc = apply(best);
-  int best_G = 0;
+  int best_G = 0, best_ring = 0;
   float best_c = 1e30f;
   for (int G = 1; G <= 8 && rc == GR_OK; G *= 2) {
     const int threads = G * (p->M / 16);
     // up to 1024 threads (the TMA-fed kernel); the plain one stops at 512
     if (threads < 32 || threads > 1024 || p->M % G) continue;
-    ColArgs ca{p->d_H, p->d_tw_m, p->M, pairs, p->d_err, G};
-    const float t = time_ms([&] { launch_cols(ca, st); });
-    if (t < best_c) {
-      best_c = t;
-      best_G = G;
+    for (int ring = 0; ring < 2; ++ring) {
+      ColArgs ca{p->d_H, p->d_tw_m, p->M, pairs, p->d_err, G, ring};
+      const float t = time_ms([&] { launch_cols(ca, st); });
+      if (t < best_c) {
+        best_c = t;
+        best_G = G;
+        best_ring = ring;
+      }
     }
   }
   cudaEventDestroy(e0);
@@ -1340,14 +1345,16 @@ int gr_plan_autotune(gr_plan* p, void* stream) {
   if (rc == GR_OK && e != cudaSuccess) rc = fail(GR_ERR_CUDA, "autotune: %s", cudaGetErrorString(e));
   if (rc == GR_OK) {
     best.G = best_G;
+    best.ring = best_ring;
     p->cols_G = best_G;
+    p->cols_ring = best_ring;
     std::lock_guard<std::mutex> lk(mu);
     cache[h] = best;
   }
   return rc;
 }
 
-int gr_plan_set_tuning(gr_plan* p, int grid_kernel, int item_cap, int cols_group) {
+int gr_plan_set_tuning(gr_plan* p, int grid_kernel, int item_cap, int cols_group, int cols_ring) {
   using namespace gr;
   if (!p) return fail(GR_ERR_ARG, "null plan");
   if (!p->graphs.empty())
@@ -1378,7 +1385,19 @@ int gr_plan_set_tuning(gr_plan* p, int grid_kernel, int item_cap, int cols_group
     if ((k == 1 || k == 3) && item_cap != p->w_item_cap) rc = install_work_list_wide(p, item_cap);
   }
   if (rc == GR_OK && cols_group > 0) p->cols_G = cols_group;
+  if (rc == GR_OK && cols_ring >= 0) p->cols_ring = cols_ring ? 1 : 0;
   return rc;
+}
+
+int gr_plan_tuning_ex(const gr_plan* p, int* grid_kernel, int* item_cap, int* cols_group,
+                      int* cols_ring) {
+  if (!p) return gr::fail(GR_ERR_ARG, "null plan");
+  if (grid_kernel) {
+    const int pr = p->max_pairs;
+    *grid_kernel = gr::use_tc(p, pr) ? 2 : (gr::use_w32(p, pr) ? 3 : (gr::use_wide(p, pr) ? 1 : 0));
+  }
+  if (cols_ring) *cols_ring = p->cols_ring;
+  return gr_plan_tuning(p, item_cap, cols_group);
 }
 
 int gr_plan_tuning(const gr_plan* p, int* item_cap, int* cols_group_width) {
@@ -1695,7 +1714,7 @@ extern "C" int gr_reconstruct_pair_noalloc(gr_plan* p, const float* sino1, const
   GR_CUDA(launch_grid(ga, p->ntaps, st));
   // the plan's own error word (allocated with the plan): a bounded-wait timeout of
   // the column FFT is reported by gr_plan_device_status, as for the plan's other calls
-  ColArgs ca{H, p->d_tw_m, p->M, 1, p->d_err, p->cols_G};
+  ColArgs ca{H, p->d_tw_m, p->M, 1, p->d_err, p->cols_G, p->cols_ring};
   GR_CUDA(launch_cols(ca, st));
   RowArgs ra{H, p->d_tw_m, p->d_winv, out1, o2, 0, out_stride, n_valid, p->M, p->M0, p->M02, 1};
   GR_CUDA(launch_rows(ra, st));

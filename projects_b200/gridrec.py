@@ -35,7 +35,7 @@ EXPORTS = ("gr_params_default", "gr_filter_code", "gr_plan_create", "gr_plan_des
            "gr_ring_removal", "gr_shift_pad", "gr_crop_center", "gr_entropy_workspace_bytes",
            "gr_entropy", "gr_reconstruct_padded", "gr_center_search", "gr_graph_create",
            "gr_graph_launch", "gr_graph_launch_count", "gr_graph_destroy", "gr_plan_autotune",
-           "gr_plan_tuning", "gr_plan_set_tuning", "gr_xcorr_scores", "gr_fbp_create", "gr_fbp_reconstruct",
+           "gr_plan_tuning", "gr_plan_set_tuning", "gr_plan_tuning_ex", "gr_xcorr_scores", "gr_fbp_create", "gr_fbp_reconstruct",
            "gr_threshold_workspace_bytes", "gr_threshold_range", "gr_to_u8",
            "gr_fbp_destroy", "gr_cnn_param_count", "gr_cnn_workspace_bytes",
            "gr_cnn_forward_workspace_bytes", "gr_cnn_forward",
@@ -135,7 +135,8 @@ def lib():
         L.gr_xcorr_scores.argtypes = [vp, vp] + [i_] * 6 + [d_] * 4 + [i_, i_,
                                                                          C.POINTER(d_), vp]
         L.gr_plan_tuning.argtypes = [vp, C.POINTER(i_), C.POINTER(i_)]
-        L.gr_plan_set_tuning.argtypes = [vp, i_, i_, i_]
+        L.gr_plan_set_tuning.argtypes = [vp, i_, i_, i_, i_]
+        L.gr_plan_tuning_ex.argtypes = [vp] + [C.POINTER(i_)] * 4
         _lib = L
     return _lib
 
@@ -301,21 +302,25 @@ class Plan:
 
     GRID_KERNEL_CODES = {"tiles": 0, "wide": 1, "wide32": 3}
 
-    def set_tuning(self, grid_kernel=None, item_cap=0, cols_group=0):
+    def set_tuning(self, grid_kernel=None, item_cap=0, cols_group=0, cols_ring=None):
         """Pins a tuning: grid_kernel ('tiles', 'wide', 'wide32' or None for the
-        choice by chunk size) for full chunks, its work list's item cap (0: keep)
-        and the column-FFT group width (0: keep)."""
+        choice by chunk size) for full chunks, its work list's item cap (0: keep),
+        the column-FFT group width (0: keep) and cols_ring (True: persistent
+        double-buffered column FFT, False: one strip per CTA, None: keep)."""
         k = -1 if grid_kernel is None else self.GRID_KERNEL_CODES[grid_kernel]
-        _check(lib().gr_plan_set_tuning(self._h, k, int(item_cap), int(cols_group)),
+        ring = -1 if cols_ring is None else int(bool(cols_ring))
+        _check(lib().gr_plan_set_tuning(self._h, k, int(item_cap), int(cols_group), ring),
                "gr_plan_set_tuning")
         return self.tuning()
 
     def tuning(self):
-        cap, g = C.c_int(), C.c_int()
-        _check(lib().gr_plan_tuning(self._h, C.byref(cap), C.byref(g)), "gr_plan_tuning")
-        return {"grid_kernel": self.grid_kernel(self.max_pairs), "item_cap": cap.value,
-                "cols_group": g.value, "tile": "32 x 32 (tile kernel) / 4 x 8 (register "
-                "sub-tile kernels): one compiled instance each"}
+        k, cap, g, ring = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(lib().gr_plan_tuning_ex(self._h, C.byref(k), C.byref(cap), C.byref(g),
+                                       C.byref(ring)), "gr_plan_tuning_ex")
+        return {"grid_kernel": ("tiles", "wide", "tensor", "wide32")[k.value],
+                "item_cap": cap.value, "cols_group": g.value, "cols_ring": bool(ring.value),
+                "tile": "32 x 32 (tile kernel) / 4 x 8 (register sub-tile kernels): one "
+                        "compiled instance each"}
 
     def work_stats(self):
         a, b, c, d = C.c_int(), C.c_int(), C.c_int(), C.c_long()

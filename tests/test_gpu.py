@@ -494,7 +494,8 @@ def test_autotune_keeps_parity_and_caches():
 def test_every_tuning_option_keeps_parity():
     """Every choice the autotuner can make on a 32-pair plan -- the gridding kernel of
     a full chunk (32 x 32 tiles, 4 x 8 sub-tiles at 16 and 32 pairs per warp), each
-    kernel's item caps, and the column-FFT group widths -- pinned with set_tuning,
+    kernel's item caps, the column-FFT group widths with one strip per CTA and with
+    persistent double-buffered CTAs -- pinned with set_tuning,
     reconstructs a 64-slice batch within the float64 tolerance; autotune picks one of
     them and grid_kernel reports it."""
     n, a = 128, 90
@@ -527,8 +528,10 @@ def test_every_tuning_option_keeps_parity():
         for g in (1, 2, 4, 8):
             if g * (plan.M // 16) < 32 or g * (plan.M // 16) > 1024:
                 continue
-            assert plan.set_tuning(None, 0, g)["cols_group"] == g
-            check(("cols_group", g))
+            for ring in (False, True):
+                t = plan.set_tuning(None, 0, g, ring)
+                assert t["cols_group"] == g and t["cols_ring"] == ring
+                check(("cols_group", g, ring))
         with pytest.raises(G.GrError):
             plan.set_tuning("wide", 0, 3)  # not a power of two
         t = plan.autotune()
