@@ -142,10 +142,15 @@ int gr_reconstruct_pair(gr_plan* plan, const float* sino1, const float* sino2, f
  * setSinoAndReconBuffers, :174-212), which keep sinograms and images in host
  * memory.  sino1/sino2: n_ang x n_det float32 (pageable or pinned; sino2 may be
  * NULL = zeros); out1/out2: M0 rows of out_stride floats (out2 may be NULL);
- * only the M0 x M0 block is written.  The copies go straight between the
- * caller's buffers and the plan's device buffers (allocated on first use), with
- * no host-side staging.  Returns after the images are in place; a bounded-wait
- * timeout is reported as by gr_plan_device_status. */
+ * only the M0 x M0 block is written.  Pinned (page-locked or registered) caller
+ * buffers are copied straight to and from the plan's device buffers (allocated on
+ * first use).  Pageable ones go through the plan's pinned staging (allocated on
+ * first use: 8 (n_ang n_det + M0^2) bytes): up to 8 host threads copy 4 MiB chunks,
+ * each chunk's DMA queued as soon as it is staged and each image chunk copied out
+ * as soon as its DMA completes, so host copies overlap the transfers (2048 x 1500:
+ * 2.8 ms per call against 4.4 ms through cudaMemcpy of pageable memory).  Returns
+ * after the images are in place; a bounded-wait timeout is reported as by
+ * gr_plan_device_status. */
 int gr_reconstruct_pair_host(gr_plan* plan, const float* sino1, const float* sino2, float* out1,
                              float* out2, long out_stride, void* stream);
 

@@ -4,7 +4,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <climits>
+#include <condition_variable>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -176,6 +178,9 @@ struct Plan {
   long out_stride_staged = 0;
   float* d_pair_in = nullptr;          // gr_reconstruct_pair_host: one pair of sinograms
   float* d_pair_out = nullptr;         //   and its two M0 x M0 images
+  float* h_pair_in = nullptr;          // pinned staging of the pair for pageable callers
+  float* h_pair_out = nullptr;
+  std::vector<cudaEvent_t> pair_events;  // one per staged image chunk
   cudaStream_t copy_stream = nullptr;   // host->device copies
   cudaStream_t d2h_stream = nullptr;    // device->host copies (runs beside the H2D ones)
   cudaEvent_t ev_h2d[2] = {}, ev_comp[2] = {}, ev_d2h[2] = {};
@@ -856,6 +861,157 @@ int validate_batch(const Plan* p, const gr_batch_desc* b) {
   return GR_OK;
 }
 
+// Whether [ptr, ptr + bytes) lies in page-locked (or registered) host memory: both ends
+// are checked.
+bool is_pinned(const void* ptr, size_t bytes) {
+  for (const void* q : {ptr, (const void*)((const char*)ptr + (bytes ? bytes - 1 : 0))}) {
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, q) != cudaSuccess) {
+      cudaGetLastError();
+      return false;
+    }
+    if (at.type != cudaMemoryTypeHost) return false;
+  }
+  return true;
+}
+
+// gr_reconstruct_pair_host on pageable caller buffers.  cudaMemcpy from pageable
+// memory goes through the driver's small bounce buffers at a fraction of the link
+// rate; here host threads copy the sinograms into the plan's pinned staging in
+// chunks, each chunk's H2D copy queued as soon as it is staged (copies of later
+// chunks overlap the DMA of earlier ones), and the images come back in row chunks
+// whose host copies into the caller's rows (stride out_stride) start as each
+// chunk's DMA completes (one event per chunk).  The calling thread is worker 0 and
+// queues the reconstruction between the two phases.
+int pair_host_staged(Plan* p, const float* sino1, const float* sino2, float* out1, float* out2,
+                     long out_stride, cudaStream_t st, int n_valid) {
+  const size_t slice = (size_t)p->n_ang * p->n_det, img = (size_t)p->M0 * p->M0;
+  if (!p->h_pair_in) {
+    if (cudaHostAlloc((void**)&p->h_pair_in, 2 * slice * sizeof(float), cudaHostAllocDefault) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      p->h_pair_in = nullptr;
+      return fail(GR_ERR_NOMEM, "pinned staging of %zu bytes", 2 * slice * sizeof(float));
+    }
+  }
+  if (!p->h_pair_out) {
+    if (cudaHostAlloc((void**)&p->h_pair_out, 2 * img * sizeof(float), cudaHostAllocDefault) !=
+        cudaSuccess) {
+      cudaGetLastError();
+      p->h_pair_out = nullptr;
+      return fail(GR_ERR_NOMEM, "pinned staging of %zu bytes", 2 * img * sizeof(float));
+    }
+  }
+  constexpr size_t kChunk = (size_t)4 << 20;  // bytes per staged copy
+  struct InChunk {
+    const char* src;
+    char* pin;
+    char* dev;
+    size_t n;
+  };
+  std::vector<InChunk> in;
+  auto add_in = [&](const float* src, size_t off) {
+    const size_t bytes = slice * sizeof(float);
+    for (size_t b = 0; b < bytes; b += kChunk)
+      in.push_back({reinterpret_cast<const char*>(src) + b,
+                    reinterpret_cast<char*>(p->h_pair_in + off) + b,
+                    reinterpret_cast<char*>(p->d_pair_in + off) + b, std::min(kChunk, bytes - b)});
+  };
+  add_in(sino1, 0);
+  if (sino2) add_in(sino2, slice);
+  struct OutChunk {
+    int image, r0, r1;
+  };
+  std::vector<OutChunk> out;
+  const int rows_per = (int)std::max<size_t>(1, kChunk / ((size_t)p->M0 * sizeof(float)));
+  for (int i = 0; i < n_valid; ++i)
+    for (int r = 0; r < p->M0; r += rows_per) out.push_back({i, r, std::min(p->M0, r + rows_per)});
+  while (p->pair_events.size() < out.size()) {
+    cudaEvent_t e = nullptr;
+    GR_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    p->pair_events.push_back(e);
+  }
+  const int hw = (int)std::max(1u, std::thread::hardware_concurrency());
+  const int T = std::max(1, std::min({8, hw / 2, (int)std::max(in.size(), out.size())}));
+  std::mutex mu;
+  std::condition_variable cv;
+  int h2d_left = T, stage = 0;  // stage 1: images queued; -1: give up
+  std::atomic<int> cuda_err{0};
+  float* outs[2] = {out1, out2};
+  auto h2d = [&](int t) {
+    for (size_t k = (size_t)t; k < in.size(); k += (size_t)T) {
+      std::memcpy(in[k].pin, in[k].src, in[k].n);
+      if (cudaMemcpyAsync(in[k].dev, in[k].pin, in[k].n, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        cuda_err = 1;
+    }
+    std::lock_guard<std::mutex> lk(mu);
+    if (--h2d_left == 0) cv.notify_all();
+  };
+  auto d2h = [&](int t) {
+    for (size_t k = (size_t)t; k < out.size(); k += (size_t)T) {
+      if (cudaEventSynchronize(p->pair_events[k]) != cudaSuccess) {
+        cuda_err = 1;
+        continue;
+      }
+      const OutChunk& c = out[k];
+      const float* src = p->h_pair_out + (size_t)c.image * img;
+      for (int r = c.r0; r < c.r1; ++r)
+        std::memcpy(outs[c.image] + (size_t)r * out_stride, src + (size_t)r * p->M0,
+                    (size_t)p->M0 * sizeof(float));
+    }
+  };
+  std::vector<std::thread> pool;
+  try {
+    for (int t = 1; t < T; ++t)
+      pool.emplace_back([&, t] {
+        cudaSetDevice(p->device);
+        h2d(t);
+        std::unique_lock<std::mutex> lk(mu);
+        cv.wait(lk, [&] { return stage != 0; });
+        const bool go = stage > 0;
+        lk.unlock();
+        if (go) d2h(t);
+      });
+  } catch (...) {  // no threads to be had: the calling thread takes every chunk
+    {
+      std::lock_guard<std::mutex> lk(mu);
+      stage = -1;
+      h2d_left -= T - 1 - (int)pool.size();
+    }
+    cv.notify_all();
+    for (auto& th : pool) th.join();
+    return fail(GR_ERR_CUDA, "host threads for the pair's staged copies could not be started");
+  }
+  h2d(0);
+  int rc = GR_OK;
+  {
+    std::unique_lock<std::mutex> lk(mu);
+    cv.wait(lk, [&] { return h2d_left == 0; });
+  }
+  if (cuda_err) rc = fail(GR_ERR_CUDA, "staged host-to-device copy failed");
+  if (rc == GR_OK)
+    rc = launch_chunk(p, 1, n_valid, 0, p->d_pair_in, p->d_pair_in + slice, 0, GR_DTYPE_F32,
+                      nullptr, nullptr, nullptr, 0, p->d_pair_out, p->d_pair_out + img, 0, p->M0, st);
+  for (size_t k = 0; k < out.size() && rc == GR_OK; ++k) {
+    const OutChunk& c = out[k];
+    const size_t off = (size_t)c.image * img + (size_t)c.r0 * p->M0;
+    const size_t n = (size_t)(c.r1 - c.r0) * p->M0 * sizeof(float);
+    if (cudaMemcpyAsync(p->h_pair_out + off, p->d_pair_out + off, n, cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess ||
+        cudaEventRecord(p->pair_events[k], st) != cudaSuccess)
+      rc = fail(GR_ERR_CUDA, "staged device-to-host copy: %s", cudaGetErrorString(cudaGetLastError()));
+  }
+  {
+    std::lock_guard<std::mutex> lk(mu);
+    stage = rc == GR_OK ? 1 : -1;
+  }
+  cv.notify_all();
+  if (rc == GR_OK) d2h(0);
+  for (auto& th : pool) th.join();
+  if (rc == GR_OK && cuda_err) rc = fail(GR_ERR_CUDA, "staged device-to-host copy failed");
+  return rc;
+}
+
 }  // namespace
 }  // namespace gr
 
@@ -951,6 +1107,9 @@ int gr_plan_destroy(gr_plan* plan) {
     if (plan->ev_comp[b]) cudaEventDestroy(plan->ev_comp[b]);
     if (plan->ev_d2h[b]) cudaEventDestroy(plan->ev_d2h[b]);
   }
+  if (plan->h_pair_in) cudaFreeHost(plan->h_pair_in);
+  if (plan->h_pair_out) cudaFreeHost(plan->h_pair_out);
+  for (cudaEvent_t e : plan->pair_events) cudaEventDestroy(e);
   if (plan->copy_stream) cudaStreamDestroy(plan->copy_stream);
   if (plan->d2h_stream) cudaStreamDestroy(plan->d2h_stream);
   for (cudaEvent_t e : plan->events) cudaEventDestroy(e);
@@ -1443,23 +1602,33 @@ int gr_reconstruct_pair_host(gr_plan* p, const float* sino1, const float* sino2,
   if (!p->d_pair_in && ((rc = dev_alloc(p, &p->d_pair_in, 2 * slice)) ||
                         (rc = dev_alloc(p, &p->d_pair_out, 2 * img))))
     return rc;
-  // the caller's buffers straight to and from the device (pageable or pinned),
-  // the images with the caller's row stride: no host-side staging copies
-  GR_CUDA(cudaMemcpyAsync(p->d_pair_in, sino1, slice * sizeof(float), cudaMemcpyHostToDevice, st));
-  if (sino2)
-    GR_CUDA(cudaMemcpyAsync(p->d_pair_in + slice, sino2, slice * sizeof(float),
-                            cudaMemcpyHostToDevice, st));
   const int n_valid = (sino2 && out2) ? 2 : 1;
-  rc = launch_chunk(p, 1, n_valid, 0, p->d_pair_in, p->d_pair_in + slice, 0, GR_DTYPE_F32, nullptr,
-                    nullptr, nullptr, 0, p->d_pair_out, p->d_pair_out + img, 0, p->M0, st);
-  if (rc) return rc;
-  const size_t row = (size_t)p->M0 * sizeof(float);
-  GR_CUDA(cudaMemcpy2DAsync(out1, (size_t)out_stride * sizeof(float), p->d_pair_out, row, row,
-                            p->M0, cudaMemcpyDeviceToHost, st));
-  if (out2 && n_valid == 2)
-    GR_CUDA(cudaMemcpy2DAsync(out2, (size_t)out_stride * sizeof(float), p->d_pair_out + img, row,
-                              row, p->M0, cudaMemcpyDeviceToHost, st));
-  return gr_plan_device_status(p, stream);  // synchronises the stream
+  const size_t out_span = ((size_t)(p->M0 - 1) * out_stride + p->M0) * sizeof(float);
+  if (is_pinned(sino1, slice * sizeof(float)) && (!sino2 || is_pinned(sino2, slice * sizeof(float))) &&
+      is_pinned(out1, out_span) && (!out2 || is_pinned(out2, out_span))) {
+    // pinned caller buffers: straight to and from the device, the images with the
+    // caller's row stride
+    GR_CUDA(cudaMemcpyAsync(p->d_pair_in, sino1, slice * sizeof(float), cudaMemcpyHostToDevice, st));
+    if (sino2)
+      GR_CUDA(cudaMemcpyAsync(p->d_pair_in + slice, sino2, slice * sizeof(float),
+                              cudaMemcpyHostToDevice, st));
+    rc = launch_chunk(p, 1, n_valid, 0, p->d_pair_in, p->d_pair_in + slice, 0, GR_DTYPE_F32, nullptr,
+                      nullptr, nullptr, 0, p->d_pair_out, p->d_pair_out + img, 0, p->M0, st);
+    if (rc) return rc;
+    const size_t row = (size_t)p->M0 * sizeof(float);
+    GR_CUDA(cudaMemcpy2DAsync(out1, (size_t)out_stride * sizeof(float), p->d_pair_out, row, row,
+                              p->M0, cudaMemcpyDeviceToHost, st));
+    if (out2 && n_valid == 2)
+      GR_CUDA(cudaMemcpy2DAsync(out2, (size_t)out_stride * sizeof(float), p->d_pair_out + img, row,
+                                row, p->M0, cudaMemcpyDeviceToHost, st));
+    return gr_plan_device_status(p, stream);  // synchronises the stream
+  }
+  rc = pair_host_staged(p, sino1, sino2, out1, out2, out_stride, st, n_valid);
+  if (rc) {
+    cudaStreamSynchronize(st);
+    return rc;
+  }
+  return gr_plan_device_status(p, stream);
 }
 
 int gr_reconstruct_batch(gr_plan* p, const gr_batch_desc* b, void* stream) {
