@@ -117,3 +117,37 @@ def test_reconstruct_pair_host_equals_device_pair():
         assert rc == 0, G.last_error()
     np.testing.assert_array_equal(h[:, :, :m], o.cpu().numpy()[:, :, :m])
     assert np.all(h[:, :, m:] == -7.0)
+
+
+def test_reconstruct_pair_host_pinned_and_pageable_agree():
+    """Pinned caller buffers (direct copies) and pageable ones (staged through the plan's
+    pinned memory by host threads, in chunks) give the device call's images bit for bit,
+    with one slice only (sino2 / out2 NULL) too, and leave the rows' extra columns alone."""
+    n, a = 512, 360
+    th = ph.angles_deg(a)
+    s1 = ph.random_ellipse_sinogram(11, n, a, center=256.0)[0].astype(np.float32)
+    s2 = ph.random_ellipse_sinogram(12, n, a, center=256.0)[0].astype(np.float32)
+    lib = G.lib()
+    with G.Plan(n, a, th, filter=G.FILTER_HANN) as plan:
+        m = plan.M0
+        o = torch.zeros((2, m, m), device="cuda")
+        plan.reconstruct_pair(torch.from_numpy(s1).cuda(), torch.from_numpy(s2).cuda(), o[0], o[1])
+        torch.cuda.synchronize()
+        ref = o.cpu().numpy()
+        ps1, ps2 = torch.from_numpy(s1).pin_memory(), torch.from_numpy(s2).pin_memory()
+        pout = torch.full((2, m, m + 5), -3.0).pin_memory()
+        rc = lib.gr_reconstruct_pair_host(plan.handle, ps1.data_ptr(), ps2.data_ptr(),
+                                          pout[0].data_ptr(), pout[1].data_ptr(), m + 5, None)
+        assert rc == 0, G.last_error()
+        np.testing.assert_array_equal(pout[:, :, :m].numpy(), ref)
+        assert np.all(pout[:, :, m:].numpy() == -3.0)
+        one = np.full((m, m + 3), -1.0, np.float32)
+        rc = lib.gr_reconstruct_pair_host(plan.handle, s1.ctypes.data, None, one.ctypes.data, None,
+                                          m + 3, None)
+        assert rc == 0, G.last_error()
+        o1 = torch.zeros((m, m), device="cuda")
+        plan.reconstruct_pair(torch.from_numpy(s1).cuda(), None, o1, None)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(one[:, :m], o1.cpu().numpy())
+        assert np.all(one[:, m:] == -1.0)
+
