@@ -972,11 +972,10 @@ int pair_host_staged(Plan* p, const float* sino1, const float* sino2, float* out
         lk.unlock();
         if (go) d2h(t);
       });
-  } catch (...) {  // no threads to be had: the calling thread takes every chunk
-    {
+  } catch (...) {  // no thread to be had: the started ones stop after their copies in
+    {               // (the caller synchronises the stream on the error)
       std::lock_guard<std::mutex> lk(mu);
       stage = -1;
-      h2d_left -= T - 1 - (int)pool.size();
     }
     cv.notify_all();
     for (auto& th : pool) th.join();
