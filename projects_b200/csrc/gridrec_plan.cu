@@ -422,9 +422,29 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
       start = cut.first;
     }
   }
-  // heaviest items first so that the long ones start early
-  std::stable_sort(items.begin(), items.end(),
-                   [](const CItem& a, const CItem& b) { return a.cost > b.cost; });
+  if (kind == kListWide) {
+    // 4 x 8 sub-tiles in Morton order of (tile row, tile column): the warps running at
+    // once take neighbouring sub-tiles, which share the spectra quads of the rays that
+    // cross them, so a quad is read from DRAM about once
+    auto spread = [](unsigned x) {
+      x &= 0xffffu;
+      x = (x | (x << 8)) & 0x00ff00ffu;
+      x = (x | (x << 4)) & 0x0f0f0f0fu;
+      x = (x | (x << 2)) & 0x33333333u;
+      x = (x | (x << 1)) & 0x55555555u;
+      return x;
+    };
+    const int tv_n = wl->tiles_v;
+    std::stable_sort(items.begin(), items.end(), [&](const CItem& a, const CItem& b) {
+      const unsigned ma = spread((unsigned)(a.it.tile / tv_n)) | spread((unsigned)(a.it.tile % tv_n)) << 1;
+      const unsigned mb = spread((unsigned)(b.it.tile / tv_n)) | spread((unsigned)(b.it.tile % tv_n)) << 1;
+      return ma < mb;
+    });
+  } else {
+    // heaviest items first so that the long ones start early
+    std::stable_sort(items.begin(), items.end(),
+                     [](const CItem& a, const CItem& b) { return a.cost > b.cost; });
+  }
   wl->items.resize(items.size());
   for (size_t i = 0; i < items.size(); ++i) wl->items[i] = items[i].it;
   wl->n_slots = n_slots;
