@@ -1316,9 +1316,19 @@ __global__ void __launch_bounds__(kWideWarps * 32, kW32MinBlocks) grid_w32_kerne
       const unsigned short* ib = reinterpret_cast<const unsigned short*>(vb + kW32ValBytes);
       const int n = mA.z & 31;
       float2* d2 = reinterpret_cast<float2*>(dbl);
-      for (int i = lane; i < n * kWideRec; i += 32) {
-        const float wv = tbl[ib[i]];
-        d2[i] = make_float2(wv, wv);
+      {  // up to kRunMaxW * kWideRec = 192 entries, 6 per lane: all index loads, then
+         // all table loads, then all stores, so the six chains overlap
+        constexpr int kE = (kRunMaxW * kWideRec + 31) / 32;
+        const int ne = n * kWideRec;
+        unsigned short ix[kE];
+#pragma unroll
+        for (int e = 0; e < kE; ++e) ix[e] = lane + 32 * e < ne ? ib[lane + 32 * e] : (unsigned short)0;
+        float wv[kE];
+#pragma unroll
+        for (int e = 0; e < kE; ++e) wv[e] = tbl[ix[e]];
+#pragma unroll
+        for (int e = 0; e < kE; ++e)
+          if (lane + 32 * e < ne) d2[lane + 32 * e] = make_float2(wv[e], wv[e]);
       }
       __syncwarp();
       const ulonglong2* qa = reinterpret_cast<const ulonglong2*>(vb + off_a);
