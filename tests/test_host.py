@@ -189,6 +189,34 @@ def test_worklist_splits_heavy_tiles():
     assert np.all(runs[:, 3] * step > 2 * 6.0 * (2048 / 2047) / np.pi)
 
 
+def _morton(u, v):
+    """Interleaved bits of (u, v), u in the even bits."""
+    key = np.zeros_like(u, dtype=np.int64)
+    for b in range(16):
+        key |= ((u >> b) & 1).astype(np.int64) << (2 * b)
+        key |= ((v >> b) & 1).astype(np.int64) << (2 * b + 1)
+    return key
+
+
+def test_wide_worklist_items_in_morton_order():
+    """The 4 x 8 list is queued in Morton order of the sub-tiles (neighbours run at
+    the same time and share the spectra quads of the rays crossing them); every
+    sub-tile that some run reaches appears, and a split sub-tile's items are
+    consecutive, with their slots in order."""
+    items, runs, splits, tiles_v = G.worklist(2048, 1500, ph.angles_deg(1500), wide=True)
+    tu, tv = items[:, 0] // tiles_v, items[:, 0] % tiles_v
+    key = _morton(tu, tv)
+    assert np.all(np.diff(key) >= 0)
+    whole = items[items[:, 3] < 0, 0]
+    assert len(np.unique(whole)) == len(whole)  # an unsplit sub-tile is one item
+    assert items[:, 2].max() == len(runs) and np.all(items[:, 1] <= items[:, 2])
+    split = items[items[:, 3] >= 0]
+    for t in np.unique(split[:, 0])[:50]:
+        rows = np.nonzero(items[:, 0] == t)[0]
+        assert np.all(np.diff(rows) == 1) and np.all(np.diff(items[rows, 3]) == 1)
+        assert np.all(items[rows[:-1], 2] == items[rows[1:], 1])  # runs continue in order
+
+
 def test_phantom_line_integrals():
     # a centred disk of radius r: p(t) = 2 sqrt(r^2 - t^2) (in units of n/2)
     e = np.array([[1.0, 0.5, 0.5, 0.0, 0.0, 0.0]])
