@@ -434,8 +434,15 @@ void build_work_list(int M, int J, double L, int n_ang, const std::vector<double
       x = (x | (x << 1)) & 0x55555555u;
       return x;
     };
+    // in eight cost classes, heaviest first, so that no heavy item starts late and holds
+    // up the launch's tail; Morton order within a class
     const int tv_n = wl->tiles_v;
+    long cmax = 1;
+    for (const CItem& c : items) cmax = std::max(cmax, c.cost);
+    auto cls = [&](const CItem& c) { return (int)std::min<long>(7, c.cost * 8 / (cmax + 1)); };
     std::stable_sort(items.begin(), items.end(), [&](const CItem& a, const CItem& b) {
+      const int ca = cls(a), cb = cls(b);
+      if (ca != cb) return ca > cb;
       const unsigned ma = spread((unsigned)(a.it.tile / tv_n)) | spread((unsigned)(a.it.tile % tv_n)) << 1;
       const unsigned mb = spread((unsigned)(b.it.tile / tv_n)) | spread((unsigned)(b.it.tile % tv_n)) << 1;
       return ma < mb;

@@ -199,22 +199,30 @@ def _morton(u, v):
 
 
 def test_wide_worklist_items_in_morton_order():
-    """The 4 x 8 list is queued in Morton order of the sub-tiles (neighbours run at
-    the same time and share the spectra quads of the rays crossing them); every
-    sub-tile that some run reaches appears, and a split sub-tile's items are
-    consecutive, with their slots in order."""
+    """The 4 x 8 list is queued in eight cost classes, heaviest first (no heavy item
+    starts late), and in Morton order of the sub-tiles within a class (neighbours run
+    at the same time and share the spectra quads of the rays crossing them); an
+    unsplit sub-tile is one item, and a split sub-tile's items, taken in slot order,
+    cover its runs in order.  An item's cost: its samples plus 6 per run."""
     items, runs, splits, tiles_v = G.worklist(2048, 1500, ph.angles_deg(1500), wide=True)
+    per_run = runs[:, 2] - runs[:, 1] + 1 + 6
+    cum = np.concatenate([[0], np.cumsum(per_run)])
+    cost = cum[items[:, 2]] - cum[items[:, 1]]
+    cls = np.minimum(7, cost * 8 // (cost.max() + 1))
+    assert np.all(np.diff(cls) <= 0) and len(np.unique(cls)) > 1
     tu, tv = items[:, 0] // tiles_v, items[:, 0] % tiles_v
     key = _morton(tu, tv)
-    assert np.all(np.diff(key) >= 0)
+    same = np.diff(cls) == 0
+    assert np.all(np.diff(key)[same] >= 0)
     whole = items[items[:, 3] < 0, 0]
     assert len(np.unique(whole)) == len(whole)  # an unsplit sub-tile is one item
     assert items[:, 2].max() == len(runs) and np.all(items[:, 1] <= items[:, 2])
     split = items[items[:, 3] >= 0]
     for t in np.unique(split[:, 0])[:50]:
         rows = np.nonzero(items[:, 0] == t)[0]
-        assert np.all(np.diff(rows) == 1) and np.all(np.diff(items[rows, 3]) == 1)
-        assert np.all(items[rows[:-1], 2] == items[rows[1:], 1])  # runs continue in order
+        part = items[rows[np.argsort(items[rows, 3])]]  # in slot order
+        assert np.all(np.diff(part[:, 3]) == 1)
+        assert np.all(part[:-1, 2] == part[1:, 1])  # the parts cover the tile's runs in order
 
 
 def test_phantom_line_integrals():
