@@ -214,7 +214,9 @@ class gpu_local_cpus:
     device's local_cpulist in sysfs), so that pinned host buffers, placed on first
     touch, sit on the GPU's NUMA node: host<->device copies then avoid the
     inter-socket link.  The previous affinity is restored on exit; where the
-    information is missing nothing changes.  `self.cpus` records what was used."""
+    information is missing nothing changes.  `self.cpus` records what was found:
+    the local CPU list and whether the process was narrowed to it, was on it
+    already, or has no CPU on it; or why the list could not be read."""
 
     def __init__(self, device):
         self.device, self.cpus, self._old = device, None, None
@@ -234,9 +236,13 @@ class gpu_local_cpus:
             use = cpus & old
             if use and use != old:
                 os.sched_setaffinity(0, use)
-                self._old, self.cpus = old, spec
-        except (OSError, ValueError, AttributeError, RuntimeError):
-            pass
+                self._old, self.cpus = old, f"{spec} (process narrowed to them)"
+            elif use:
+                self.cpus = f"{spec} (process already on them)"
+            else:
+                self.cpus = f"{spec} (no process CPU among them: placement unchanged)"
+        except (OSError, ValueError, AttributeError, RuntimeError) as e:
+            self.cpus = f"GPU-local CPU list unavailable ({type(e).__name__})"
         return self
 
     def __exit__(self, *exc):
