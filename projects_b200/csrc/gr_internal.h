@@ -105,6 +105,9 @@ struct SpectraArgs {
   // [pair / G][dir][j / 4][pair % G][j % 4] (G = wide), for G = 32 with the two
   // 16-byte halves of a pair's chunk swapped when (pair / 4) is odd
   int wide = 0;
+  // device error word for the bounded wait of the staged input (null: the rows are
+  // loaded element by element, with no wait)
+  int* err = nullptr;
 };
 
 struct PhaseArgs {

@@ -843,7 +843,7 @@ int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1
   SpectraArgs sa{s1, s2, in_pair_stride, n_valid, slice_base, flat, dark, flat_stride, p->d_pq,
                  p->d_spec,
                  p->d_tw_p, p->n_det, p->n_ang, p->pdim, p->J, pairs, p->d_roi_off,
-                 w32 ? kW32Pairs : ((wide || tc) ? kWidePairs : 0)};
+                 w32 ? kW32Pairs : ((wide || tc) ? kWidePairs : 0), p->d_err};
   GR_CUDA(launch_spectra(sa, dt, st));
   GR_MARK();
   const GridArgs ga = tc ? grid_args_tc(p, pairs)
