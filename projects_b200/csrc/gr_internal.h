@@ -108,6 +108,10 @@ struct SpectraArgs {
   // device error word for the bounded wait of the staged input (null: the rows are
   // loaded element by element, with no wait)
   int* err = nullptr;
+  // u16 raw only: per slice of the chunk, {dark, log(flat - dark) or NaN} per detector
+  // (launch_dark_log), so that a sample costs one load and one logarithm; null: the
+  // flat and dark rows above are read per sample
+  const float2* dl = nullptr;
 };
 
 struct PhaseArgs {
@@ -238,6 +242,8 @@ cudaError_t launch_grid_tc(const GridArgs& a, cudaStream_t s);
 // rinfo[r] = {index block in 16-byte units, sub-tile index}) and the kernel.
 cudaError_t launch_w32_index(const GridArgs& a, int n_runs, const int2* rinfo,
                              unsigned short* idx, int4* xmeta, cudaStream_t s);
+cudaError_t launch_dark_log(const float* flat, const float* dark, long flat_stride, int slice_base,
+                            int n_valid, int n_det, float2* out, cudaStream_t s);
 cudaError_t launch_grid_w32(const GridArgs& a, cudaStream_t s);
 int cols_group(int M);
 cudaError_t launch_cols(const ColArgs& a, cudaStream_t s);

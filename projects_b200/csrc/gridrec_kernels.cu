@@ -22,6 +22,7 @@
 #include <cuda_fp16.h>
 
 #include <algorithm>
+#include <type_traits>
 #include <mutex>
 #include <vector>
 
@@ -451,6 +452,35 @@ __device__ __forceinline__ float load_sino<U16Linear>(const U16Linear* row, int 
 
 // Lines of up to 4096 points run 64-register variants (several CTAs per SM);
 // 8192-point lines need 512 threads and use the MAXT = 512 variants.
+// Raw u16 counts with the slice's precomputed {dark, log(flat - dark) or NaN}: the
+// value of load_sino<uint16_t> (same operations, same order) from one 8-byte load and
+// one logarithm.
+__device__ __forceinline__ float raw_log(unsigned short raw, const float2* dl, int k) {
+  const float2 q = __ldg(&dl[k]);
+  const float v = (float)raw - q.x;
+  return (v > 0.f && q.y == q.y) ? q.y - __logf(v) : 0.f;
+}
+
+// {dark, log(flat - dark)} of the chunk's slices (NaN where flat - dark is not
+// positive, which makes raw_log return 0 as the per-sample form does).
+__global__ void dark_log_kernel(const float* flat, const float* dark, long flat_stride,
+                                int slice_base, int n_det, float2* out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  const int s = blockIdx.y;
+  if (k >= n_det) return;
+  const long fo = (long)(slice_base + s) * flat_stride;
+  const float d = __ldg(&dark[fo + k]);
+  const float fd = __ldg(&flat[fo + k]) - d;
+  out[(size_t)s * n_det + k] = make_float2(d, fd > 0.f ? __logf(fd) : __int_as_float(0x7fc00000));
+}
+
+cudaError_t launch_dark_log(const float* flat, const float* dark, long flat_stride, int slice_base,
+                            int n_valid, int n_det, float2* out, cudaStream_t s) {
+  dim3 grid((n_det + 255) / 256, n_valid);
+  dark_log_kernel<<<grid, 256, 0, s>>>(flat, dark, flat_stride, slice_base, n_det, out);
+  return cudaGetLastError();
+}
+
 // Element type of the staged row (the 16-bit types as their bits).
 template <typename T>
 struct StagedType {
@@ -513,6 +543,9 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
   const float* d1 = a.dark ? a.dark + fo : nullptr;
   const float* f2 = f1 ? f1 + a.flat_stride : nullptr;
   const float* d2 = d1 ? d1 + a.flat_stride : nullptr;
+  constexpr bool kRaw = std::is_same<T, uint16_t>::value;
+  const float2* q1 = kRaw && a.dl ? a.dl + (size_t)(2 * pair) * a.n_det : nullptr;
+  const float2* q2 = q1 ? q1 + a.n_det : nullptr;
   float2 v[16];
   // The pair's two rows are contiguous: with an error word and 16-byte-aligned rows,
   // two 1-D bulk copies land them in the exchange buffer (2 n_det elements <= 8 pdim
@@ -541,8 +574,18 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
       const int k = tid + r * nthr;
       float x = 0.f, y = 0.f;
       if (ok && k < a.n_det) {
-        x = from_staged<T>(st1, k, f1, d1);
-        if (r2) y = from_staged<T>(st2, k, f2, d2);
+        if constexpr (kRaw) {
+          if (q1) {
+            x = raw_log(st1[k], q1, k);
+            if (r2) y = raw_log(st2[k], q2, k);
+          } else {
+            x = from_staged<T>(st1, k, f1, d1);
+            if (r2) y = from_staged<T>(st2, k, f2, d2);
+          }
+        } else {
+          x = from_staged<T>(st1, k, f1, d1);
+          if (r2) y = from_staged<T>(st2, k, f2, d2);
+        }
       }
       v[r] = make_float2(x, y);
     }
@@ -553,8 +596,18 @@ __global__ void __launch_bounds__(MAXT, 1024 / MAXT) spectra_kernel(SpectraArgs 
       const int k = tid + r * nthr;
       float x = 0.f, y = 0.f;
       if (k < a.n_det) {
-        x = load_sino<T>(r1, k, f1, d1);
-        if (r2) y = load_sino<T>(r2, k, f2, d2);
+        if constexpr (kRaw) {
+          if (q1) {
+            x = raw_log(ldg_u16(r1, k), q1, k);
+            if (r2) y = raw_log(ldg_u16(r2, k), q2, k);
+          } else {
+            x = load_sino<T>(r1, k, f1, d1);
+            if (r2) y = load_sino<T>(r2, k, f2, d2);
+          }
+        } else {
+          x = load_sino<T>(r1, k, f1, d1);
+          if (r2) y = load_sino<T>(r2, k, f2, d2);
+        }
       }
       v[r] = make_float2(x, y);
     }

@@ -164,6 +164,7 @@ struct Plan {
   int tuned_kernel = -1;
   std::vector<gr_graph*> graphs;    // live CUDA graphs replaying this plan's buffers
   float4* d_pq = nullptr;
+  float2* d_dl = nullptr;  // raw u16 chunks: {dark, log(flat - dark)} per slice and detector
   // pair slots of d_pq holding the ramps of the plan's own centre (no per-slice
   // centres): such calls skip the phase kernel.  Off for good once a call is
   // captured into a graph, whose replays may rewrite d_pq at any time.
@@ -831,10 +832,18 @@ int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1
     cudaGetLastError();
     p->pq_cache_off = true;
   }
+  int launched = 0;
   if (centers || p->pq_cache_off || p->pq_default < pairs) {
     PhaseArgs ph{centers, p->center, slice_base, n_valid, p->d_filt, p->d_pq, p->J, p->pdim, pairs};
     GR_CUDA(launch_phase(ph, st));
     p->pq_default = (centers || p->pq_cache_off) ? 0 : pairs;
+    ++launched;
+  }
+  // raw counts: the chunk's {dark, log(flat - dark)} rows once, not once per angle
+  const bool dl = dt == GR_DTYPE_U16_RAW && flat && dark;
+  if (dl) {
+    GR_CUDA(launch_dark_log(flat, dark, flat_stride, slice_base, n_valid, p->n_det, p->d_dl, st));
+    ++launched;
   }
   GR_MARK();
   const bool tc = use_tc(p, pairs);
@@ -844,6 +853,7 @@ int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1
                  p->d_spec,
                  p->d_tw_p, p->n_det, p->n_ang, p->pdim, p->J, pairs, p->d_roi_off,
                  w32 ? kW32Pairs : ((wide || tc) ? kWidePairs : 0), p->d_err};
+  if (dl) sa.dl = p->d_dl;
   GR_CUDA(launch_spectra(sa, dt, st));
   GR_MARK();
   const GridArgs ga = tc ? grid_args_tc(p, pairs)
@@ -859,8 +869,9 @@ int launch_chunk(Plan* p, int pairs, int n_valid, int slice_base, const void* s1
              p->M, p->M0, p->M02, pairs};
   GR_CUDA(launch_rows(ra, st));
   GR_MARK();
-  // phase, spectra, grid (+ split reduction when tiles are split), cols, rows
-  p->launches += 5 + (ga.n_items > 0 && ga.n_split_tiles > 0 ? 1 : 0);
+  // (phase unless its ramps are cached, dark/log for raw counts,) spectra, grid (+ split
+  // reduction when tiles are split), cols, rows
+  p->launches += launched + 4 + (ga.n_items > 0 && ga.n_split_tiles > 0 ? 1 : 0);
   return GR_OK;
 }
 
@@ -1259,6 +1270,7 @@ int gr::plan_create_ex(const gr_params* prm, const Pswf* pswf, float (*filter_fn
   if ((rc = dev_alloc(p, &p->d_spec, P_spec * p->n_ang * 2 * p->J)) ||
       (rc = dev_alloc(p, &p->d_H, P * (size_t)M * M)) ||
       (rc = dev_alloc(p, &p->d_pq, P * p->J)) ||
+      (rc = dev_alloc(p, &p->d_dl, 2 * P * (size_t)p->n_det)) ||
       (rc = dev_alloc(p, &p->d_queue, 1)) || (rc = dev_alloc(p, &p->d_err, 1))) {
     gr_plan_destroy(p);
     return rc;

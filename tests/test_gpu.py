@@ -470,6 +470,26 @@ def test_per_slice_flat_dark_rows_bit_exact():
     np.testing.assert_array_equal(host, want.cpu().numpy())
 
 
+def test_repeated_pair_call_reuses_phase_ramps():
+    """A plan's own centre gives the same phase ramps on every pair call: the second
+    call skips the phase kernel (one launch fewer on the plan's count) and gives the
+    first call's images bit for bit."""
+    n, a = 128, 90
+    th = ph.angles_deg(a)
+    s1 = _dev(ph.random_ellipse_sinogram(3, n, a, center=64.0)[0])
+    s2 = _dev(ph.random_ellipse_sinogram(4, n, a, center=64.0)[0])
+    with G.Plan(n, a, th, center=64.0, filter=G.FILTER_HANN) as plan:
+        o = torch.zeros((2, 2, plan.M0, plan.M0), device="cuda")
+        plan.reconstruct_pair(s1, s2, o[0, 0], o[0, 1])
+        l1 = plan.launches()
+        plan.reconstruct_pair(s1, s2, o[1, 0], o[1, 1])
+        l2 = plan.launches() - l1
+        torch.cuda.synchronize()
+        plan.device_status()
+    assert l1 - l2 == 1 and l2 in (4, 5)
+    assert torch.equal(o[0], o[1])
+
+
 def test_autotune_keeps_parity_and_caches():
     th = ph.angles_deg(360)
     s1 = ph.shepp_logan_sinogram(512, 360, center=256.3, noise_seed=1)
