@@ -720,6 +720,45 @@ def test_w32_kernel_mixed_chunks_against_16_pair_kernel_and_oracle():
         assert ph.rel_l2(outs[0][i], refs[i]) < TOL, i
 
 
+@pytest.mark.parametrize("dtype", ["float32", "float16", "u16raw"])
+def test_staged_and_elementwise_spectra_input_agree(dtype):
+    """The spectra kernel lands a pair's rows in shared memory by bulk copy when they
+    are 16-byte aligned, and loads them element by element otherwise: the same
+    sinograms given once aligned and once as a view one element off (rows no longer
+    16-byte aligned) give the same images bit for bit."""
+    n, a, S = 256, 120, 4
+    th = ph.angles_deg(a)
+    raws, flats, darks = [], [], []
+    for i in range(S):
+        r, f, d, _ = ph.random_ellipse_raw(30 + i, n, a, "cuda")
+        raws.append(r)
+        flats.append(f)
+        darks.append(d)
+    raw = torch.stack(raws)
+    flat, dark = torch.stack(flats), torch.stack(darks)
+    if dtype == "u16raw":
+        base, kw = raw, dict(flat=flat, dark=dark, dtype=G.DTYPE_U16_RAW)
+    else:
+        v = raw.to(torch.int32).remainder(65536).to(torch.float32) - dark[:, None, :]
+        rr = (flat - dark)[:, None, :] / v
+        base = torch.where((v > 0) & (rr > 0), torch.log(rr), torch.zeros_like(v))
+        base = base.to(getattr(torch, dtype)).contiguous()
+        kw = {}
+    # the same values one element into a larger buffer: every row starts off 16 bytes
+    buf = torch.zeros(base.numel() + 1, dtype=base.dtype, device="cuda")
+    buf[1:] = base.reshape(-1)
+    shifted = buf[1:].view(base.shape)
+    assert shifted.data_ptr() % 16 != 0 and base.data_ptr() % 16 == 0
+    with G.Plan(n, a, th, filter=G.FILTER_HANN, max_pairs=2) as plan:
+        o = torch.zeros((2, S, plan.M0, plan.M0), device="cuda")
+        plan.reconstruct_batch(base, o[0], **kw)
+        plan.reconstruct_batch(shifted, o[1], **kw)
+        torch.cuda.synchronize()
+        plan.device_status()
+    assert torch.isfinite(o).all() and o[0].abs().max() > 0
+    assert torch.equal(o[0], o[1])
+
+
 @pytest.mark.parametrize("dtype", ["float16", "u16raw"])
 def test_w32_kernel_input_types_and_host_streaming(dtype):
     """Reduced-precision and raw-count inputs through the 32-pair kernel (a chunk of
