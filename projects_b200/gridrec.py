@@ -220,6 +220,19 @@ def _stream_ptr(stream) -> int:
     return int(stream.cuda_stream)
 
 
+def _on_stream(stream):
+    """Context in which a wrapper's own torch work (its outputs, workspaces and
+    small uploads) is queued on the stream its kernels run on, so that the caching
+    allocator hands that memory to later work only in stream order after the
+    kernels.  A raw int handle or None leaves the current stream as it is (the
+    caller then orders its streams itself)."""
+    import contextlib
+    import torch
+    if stream is None or isinstance(stream, int):
+        return contextlib.nullcontext()
+    return torch.cuda.stream(stream)
+
+
 class Plan:
     """A gridrec plan: sizes, tables, work list and workspaces on one GPU."""
 
@@ -556,10 +569,11 @@ def ring_removal(sinos, ring_coeff=1.0, iterations=20, stream=None):
     (tomo_recon.cpp:3905-3972; the reference runs 20 rounds, RING_COEFF 1.0)."""
     import torch
     S, a, n = sinos.shape
-    ws = torch.empty(lib().gr_ring_workspace_bytes(S, n, a), dtype=torch.uint8,
-                     device=sinos.device)
-    _check(lib().gr_ring_removal(_ptr(sinos), S, n, a, float(ring_coeff), int(iterations),
-                                 _ptr(ws), _stream_ptr(stream)), "gr_ring_removal")
+    with _on_stream(stream):
+        ws = torch.empty(lib().gr_ring_workspace_bytes(S, n, a), dtype=torch.uint8,
+                         device=sinos.device)
+        _check(lib().gr_ring_removal(_ptr(sinos), S, n, a, float(ring_coeff), int(iterations),
+                                     _ptr(ws), _stream_ptr(stream)), "gr_ring_removal")
     return sinos
 
 
@@ -569,12 +583,17 @@ def shift_pad(sinos, xoffsets, out_width=None, stream=None):
     import torch
     S, a, n = sinos.shape
     w = 2 * n if out_width is None else int(out_width)
-    xo = torch.as_tensor(xoffsets, dtype=torch.float32).reshape(-1).to(sinos.device)
-    if xo.numel() == 1:
-        xo = xo.expand(S).contiguous()
-    out = torch.empty((S, a, w), dtype=torch.float32, device=sinos.device)
-    _check(lib().gr_shift_pad(_ptr(sinos), _ptr(out), S, n, a, _ptr(xo), w, _stream_ptr(stream)),
-           "gr_shift_pad")
+    with _on_stream(stream):
+        xo = torch.as_tensor(xoffsets, dtype=torch.float32).reshape(-1)
+        if xo.device != sinos.device:
+            # staged from pageable memory by the call itself; non_blocking spares
+            # the stream synchronisation of a blocking copy
+            xo = xo.to(sinos.device, non_blocking=True)
+        if xo.numel() == 1:
+            xo = xo.expand(S).contiguous()
+        out = torch.empty((S, a, w), dtype=torch.float32, device=sinos.device)
+        _check(lib().gr_shift_pad(_ptr(sinos), _ptr(out), S, n, a, _ptr(xo), w,
+                                  _stream_ptr(stream)), "gr_shift_pad")
     return out
 
 
@@ -583,11 +602,12 @@ def crop_center(recs, n, offset, radius=0, stream=None):
     zeroes pixels outside the circle of tomo_recon.cpp:2150-2165."""
     import torch
     S, rows, stride = recs.shape
-    out = torch.empty((S, n, n), dtype=torch.float32, device=recs.device)
     if offset + n > rows:
         raise ValueError("crop window exceeds the image rows")
-    _check(lib().gr_crop_center(_ptr(recs), stride, rows * stride, _ptr(out), n, n * n, S, n,
-                                offset, int(radius), _stream_ptr(stream)), "gr_crop_center")
+    with _on_stream(stream):
+        out = torch.empty((S, n, n), dtype=torch.float32, device=recs.device)
+        _check(lib().gr_crop_center(_ptr(recs), stride, rows * stride, _ptr(out), n, n * n, S, n,
+                                    offset, int(radius), _stream_ptr(stream)), "gr_crop_center")
     return out
 
 
@@ -599,12 +619,14 @@ def threshold_range(images, lower_clamp=-1e30, upper_clamp=1e30, stream=None):
     S, rows, cols = images.shape
     if images.stride(2) != 1:
         raise ValueError("images need unit column stride")
-    ws = torch.empty(lib().gr_threshold_workspace_bytes(), dtype=torch.uint8, device=images.device)
-    lohi = torch.empty(2, dtype=torch.float32, device=images.device)
-    _check(lib().gr_threshold_range(_ptr(images), S, rows, cols, images.stride(1),
-                                    images.stride(0), float(lower_clamp), float(upper_clamp),
-                                    _ptr(lohi), _ptr(ws), _stream_ptr(stream)),
-           "gr_threshold_range")
+    with _on_stream(stream):
+        ws = torch.empty(lib().gr_threshold_workspace_bytes(), dtype=torch.uint8,
+                         device=images.device)
+        lohi = torch.empty(2, dtype=torch.float32, device=images.device)
+        _check(lib().gr_threshold_range(_ptr(images), S, rows, cols, images.stride(1),
+                                        images.stride(0), float(lower_clamp), float(upper_clamp),
+                                        _ptr(lohi), _ptr(ws), _stream_ptr(stream)),
+               "gr_threshold_range")
     return lohi
 
 
@@ -615,11 +637,12 @@ def to_u8(images, lohi, radius=0, out=None, stream=None):
     S, rows, cols = images.shape
     if images.stride(2) != 1:
         raise ValueError("images need unit column stride")
-    if out is None:
-        out = torch.empty((S, rows, cols), dtype=torch.uint8, device=images.device)
-    _check(lib().gr_to_u8(_ptr(images), S, rows, cols, images.stride(1), images.stride(0),
-                          _ptr(lohi), int(radius), _ptr(out), out.stride(1), out.stride(0),
-                          _stream_ptr(stream)), "gr_to_u8")
+    with _on_stream(stream):
+        if out is None:
+            out = torch.empty((S, rows, cols), dtype=torch.uint8, device=images.device)
+        _check(lib().gr_to_u8(_ptr(images), S, rows, cols, images.stride(1), images.stride(0),
+                              _ptr(lohi), int(radius), _ptr(out), out.stride(1), out.stride(0),
+                              _stream_ptr(stream)), "gr_to_u8")
     return out
 
 
@@ -631,13 +654,14 @@ def entropy(images, vmin, vmax, nbins, group=1, stream=None):
     if N % group:
         raise ValueError("image count must be a multiple of group")
     G = N // group
-    ws = torch.empty(lib().gr_entropy_workspace_bytes(G, nbins), dtype=torch.uint8,
-                     device=images.device)
-    out = torch.empty(G, dtype=torch.float32, device=images.device)
     st = images.stride()
-    _check(lib().gr_entropy(_ptr(images), G, group, rows, cols, st[1], st[0], st[0] * group,
-                            float(vmin), float(vmax), int(nbins), _ptr(out), _ptr(ws),
-                            _stream_ptr(stream)), "gr_entropy")
+    with _on_stream(stream):
+        ws = torch.empty(lib().gr_entropy_workspace_bytes(G, nbins), dtype=torch.uint8,
+                         device=images.device)
+        out = torch.empty(G, dtype=torch.float32, device=images.device)
+        _check(lib().gr_entropy(_ptr(images), G, group, rows, cols, st[1], st[0], st[0] * group,
+                                float(vmin), float(vmax), int(nbins), _ptr(out), _ptr(ws),
+                                _stream_ptr(stream)), "gr_entropy")
     return out
 
 
@@ -646,10 +670,11 @@ def reconstruct_padded(plan: "Plan", sinos, xoffset=0.0, stream=None):
     plan's width (2 n_det), reconstruct, crop n_det x n_det.  sinos (S, n_ang, n_det)."""
     import torch
     S, a, n = sinos.shape
-    out = torch.empty((S, n, n), dtype=torch.float32, device=sinos.device)
-    _check(lib().gr_reconstruct_padded(plan.handle, _ptr(sinos), S, n, a, float(xoffset),
-                                       _ptr(out), n, _stream_ptr(stream)),
-           "gr_reconstruct_padded")
+    with _on_stream(stream):
+        out = torch.empty((S, n, n), dtype=torch.float32, device=sinos.device)
+        _check(lib().gr_reconstruct_padded(plan.handle, _ptr(sinos), S, n, a, float(xoffset),
+                                           _ptr(out), n, _stream_ptr(stream)),
+               "gr_reconstruct_padded")
     return out
 
 
@@ -663,13 +688,15 @@ def center_search(plan: "Plan", sino1, sino2, shifts, hist_lo, hist_hi, nbins,
     sh = np.ascontiguousarray(shifts, np.float32)
     scores = np.zeros(sh.size, np.float32)
     best = C.c_int(-1)
-    imgs = torch.empty((2, n, n), dtype=torch.float32, device=sino1.device) if want_images \
-        else None
     fp = C.POINTER(C.c_float)
-    _check(lib().gr_center_search(plan.handle, _ptr(sino1), _ptr(sino2), n, a,
-                                  sh.ctypes.data_as(fp), sh.size, float(hist_lo), float(hist_hi),
-                                  int(nbins), scores.ctypes.data_as(fp), C.byref(best),
-                                  _ptr(imgs), _stream_ptr(stream)), "gr_center_search")
+    with _on_stream(stream):
+        imgs = torch.empty((2, n, n), dtype=torch.float32, device=sino1.device) \
+            if want_images else None
+        _check(lib().gr_center_search(plan.handle, _ptr(sino1), _ptr(sino2), n, a,
+                                      sh.ctypes.data_as(fp), sh.size, float(hist_lo),
+                                      float(hist_hi), int(nbins), scores.ctypes.data_as(fp),
+                                      C.byref(best), _ptr(imgs), _stream_ptr(stream)),
+               "gr_center_search")
     return scores, best.value, imgs
 
 
@@ -726,11 +753,12 @@ class FBP:
         """sinos (S, n_ang, n_det) float32 CUDA tensor -> (S, n_det, n_det)."""
         import torch
         S = sinos.shape[0]
-        if recons is None:
-            recons = torch.empty((S, self.n_det, self.n_det), dtype=torch.float32,
-                                 device=sinos.device)
-        _check(lib().gr_fbp_reconstruct(self._h, _ptr(sinos), S, _ptr(recons),
-                                        _stream_ptr(stream)), "gr_fbp_reconstruct")
+        with _on_stream(stream):
+            if recons is None:
+                recons = torch.empty((S, self.n_det, self.n_det), dtype=torch.float32,
+                                     device=sinos.device)
+            _check(lib().gr_fbp_reconstruct(self._h, _ptr(sinos), S, _ptr(recons),
+                                            _stream_ptr(stream)), "gr_fbp_reconstruct")
         return recons
 
     def close(self):

@@ -76,6 +76,9 @@ class CorrectionNet:
         # the fused inference kernel's error word (zeroed; gr_cnn_infer_status clears it)
         self._iws = torch.zeros(int(_lib().gr_cnn_infer_workspace_bytes()), dtype=torch.uint8,
                                 device=self.params.device)
+        # these buffers are filled on the current stream; later calls may run on
+        # another one, so they are complete before the constructor returns
+        torch.cuda.current_stream(self.params.device).synchronize()
 
     def _workspace(self, n, h, w, train=False):
         """Forward-only workspace (the activations) unless training needs the
@@ -95,11 +98,12 @@ class CorrectionNet:
         """x: (N, H, W) float32 CUDA tensor -> y = x + correction."""
         import torch
         n, h, w = x.shape
-        if y is None:
-            y = torch.empty_like(x)
-        ws = self._workspace(n, h, w, train)
-        G._check(_lib().gr_cnn_forward(G._ptr(self.params), G._ptr(x), G._ptr(y), n, h, w,
-                                       G._ptr(ws), G._stream_ptr(stream)), "gr_cnn_forward")
+        with G._on_stream(stream):
+            if y is None:
+                y = torch.empty_like(x)
+            ws = self._workspace(n, h, w, train)
+            G._check(_lib().gr_cnn_forward(G._ptr(self.params), G._ptr(x), G._ptr(y), n, h, w,
+                                           G._ptr(ws), G._stream_ptr(stream)), "gr_cnn_forward")
         return y
 
     def infer(self, x, y=None, stream=None, scale=None):
@@ -109,16 +113,18 @@ class CorrectionNet:
         y_i = s_i * net(x_i / s_i), the scaling done inside the kernel."""
         import torch
         n, h, w = x.shape
-        if y is None:
-            y = torch.empty_like(x)
-        sp = None
-        if scale is not None:
-            scale = scale.reshape(-1).contiguous()
-            if scale.numel() != n or scale.dtype != torch.float32 or scale.device != x.device:
-                raise ValueError("scale: one float32 per image, on the images' device")
-            sp = G._ptr(scale)
-        G._check(_lib().gr_cnn_infer(G._ptr(self.params), G._ptr(x), G._ptr(y), sp, n, h, w,
-                                     G._ptr(self._iws), G._stream_ptr(stream)), "gr_cnn_infer")
+        with G._on_stream(stream):
+            if y is None:
+                y = torch.empty_like(x)
+            sp = None
+            if scale is not None:
+                scale = scale.reshape(-1).contiguous()
+                if scale.numel() != n or scale.dtype != torch.float32 or scale.device != x.device:
+                    raise ValueError("scale: one float32 per image, on the images' device")
+                sp = G._ptr(scale)
+            G._check(_lib().gr_cnn_infer(G._ptr(self.params), G._ptr(x), G._ptr(y), sp, n, h, w,
+                                         G._ptr(self._iws), G._stream_ptr(stream)),
+                     "gr_cnn_infer")
         return y
 
     def infer_status(self, stream=None):
@@ -183,16 +189,19 @@ class LearnedGridrec:
         return rms.clamp_min(1e-30)
 
     def correct(self, raw, stream=None):
-        """s * net(raw / s) per slice (the fused inference kernel, which applies s)."""
-        return self.net.infer(raw.contiguous(), stream=stream, scale=self.scales(raw))
+        """s * net(raw / s) per slice (the fused inference kernel, which applies s).
+        The scales are computed on `stream`, after the kernels that wrote raw."""
+        with G._on_stream(stream):
+            return self.net.infer(raw.contiguous(), stream=stream, scale=self.scales(raw))
 
     def corrected(self, sinos, centers=None, stream=None):
         """Narrow-kernel images corrected by the network, (S, M0, M0)."""
         import torch
         S = sinos.shape[0]
-        raw = torch.empty((S, self.M0, self.M0), dtype=torch.float32, device=sinos.device)
-        self.narrow.reconstruct_batch(sinos, raw, centers=centers, stream=stream)
-        return self.correct(raw, stream=stream)
+        with G._on_stream(stream):
+            raw = torch.empty((S, self.M0, self.M0), dtype=torch.float32, device=sinos.device)
+            self.narrow.reconstruct_batch(sinos, raw, centers=centers, stream=stream)
+            return self.correct(raw, stream=stream)
 
     def reconstruct_batch(self, sinos, centers=None, stream=None):
         """Returns (images, info): info = {"held_out_rel_l2", "fallback"}.  The first
@@ -201,17 +210,20 @@ class LearnedGridrec:
         import torch
         k = min(2, sinos.shape[0])
         ck = None if centers is None else centers[:k]
-        ref = torch.empty((k, self.M0, self.M0), dtype=torch.float32, device=sinos.device)
-        self.full.reconstruct_batch(sinos[:k], ref, centers=ck, stream=stream)
-        probe = self.corrected(sinos[:k], ck, stream)
-        err = float(torch.linalg.vector_norm(probe - ref) / torch.linalg.vector_norm(ref))
-        fallback = err > self.tol
-        out = torch.empty((sinos.shape[0], self.M0, self.M0), dtype=torch.float32,
-                          device=sinos.device)
-        if fallback:
-            self.full.reconstruct_batch(sinos, out, centers=centers, stream=stream)
-        else:
-            out.copy_(self.corrected(sinos, centers, stream))
+        # the torch work here (norms, copies, allocations) runs on `stream`, in
+        # order with the kernels
+        with G._on_stream(stream):
+            ref = torch.empty((k, self.M0, self.M0), dtype=torch.float32, device=sinos.device)
+            self.full.reconstruct_batch(sinos[:k], ref, centers=ck, stream=stream)
+            probe = self.corrected(sinos[:k], ck, stream)
+            err = float(torch.linalg.vector_norm(probe - ref) / torch.linalg.vector_norm(ref))
+            fallback = err > self.tol
+            out = torch.empty((sinos.shape[0], self.M0, self.M0), dtype=torch.float32,
+                              device=sinos.device)
+            if fallback:
+                self.full.reconstruct_batch(sinos, out, centers=centers, stream=stream)
+            else:
+                out.copy_(self.corrected(sinos, centers, stream))
         return out, {"held_out_rel_l2": err, "fallback": fallback}
 
     def close(self):

@@ -162,4 +162,11 @@ def test_learned_path_gains_over_narrow_kernel_and_falls_back():
     out, info = lg.reconstruct_batch(s)
     assert info["fallback"] and info["held_out_rel_l2"] > lg.tol
     assert torch.equal(out, th_full)
+    # on a side stream: the torch work of the path (scales, norms, copies) follows
+    # the kernels on that stream, so the results are the same bits
+    side = torch.cuda.Stream()
+    yh2 = lg.correct(xh, stream=side)
+    out2, info2 = lg.reconstruct_batch(s, stream=side)
+    side.synchronize()
+    assert torch.equal(yh2, yh) and torch.equal(out2, th_full) and info2 == info
     lg.close()

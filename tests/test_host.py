@@ -397,3 +397,14 @@ def test_no_gpu_means_an_error_not_a_fallback():
     with pytest.raises(G.GrError) as err:
         G.Plan(64, 32, ph.angles_deg(32))
     assert "GR_ERR_CUDA" in str(err.value)
+
+
+def test_on_stream_leaves_the_current_stream_for_none_and_raw_handles():
+    """Raw int stream handles and None keep the caller's current stream (no torch
+    stream context is entered); torch streams are entered (checked on the GPU)."""
+    import contextlib
+
+    from projects_b200 import gridrec as G
+    assert isinstance(G._on_stream(None), contextlib.nullcontext)
+    assert isinstance(G._on_stream(0), contextlib.nullcontext)
+    assert isinstance(G._on_stream(12345), contextlib.nullcontext)
