@@ -42,13 +42,17 @@ def test_shift_pad_bit_exact_against_reference(z):
     assert np.array_equal(out, ref)
 
 
-def test_shift_pad_wide_rows_and_port():
+@pytest.mark.parametrize("n_ang,n_det,width", [(50, 300, 700), (50, 301, 603), (3, 12290, 24581)],
+                         ids=["aligned-rows", "unaligned-rows", "rows-longer-than-staging"])
+def test_shift_pad_wide_rows_and_port(n_ang, n_det, width):
+    """Rows staged in shared memory by 16-byte loads (aligned rows), by 4-byte loads
+    (odd n_det), and rows too long to stage (taps read from global memory)."""
     rng = np.random.default_rng(5)
-    s = rng.standard_normal((3, 50, 300)).astype(np.float32)
+    s = rng.standard_normal((3, n_ang, n_det)).astype(np.float32)
     offs = np.array([-7.25, 0.5, 151.0], np.float32)
-    out = G.shift_pad(_dev(s), offs, out_width=700).cpu().numpy()
+    out = G.shift_pad(_dev(s), offs, out_width=width).cpu().numpy()
     for i in range(3):
-        assert np.array_equal(out[i], O.port_shift_pad(s[i], offs[i], 700))
+        assert np.array_equal(out[i], O.port_shift_pad(s[i], offs[i], width))
 
 
 def test_ring_removal_against_reference():
