@@ -81,6 +81,25 @@ def test_ring_removal_batch_against_oracle():
     assert np.array_equal(y.cpu().numpy(), s)
 
 
+@pytest.mark.parametrize("n_det,offset", [(256, 0), (256, 1), (258, 0), (3000, 0)],
+                         ids=["aligned", "unaligned-base", "odd-width", "wider-than-2048"])
+def test_ring_removal_round_kernel_forms(n_det, offset):
+    """The fused round kernel at 1, 2 and 16 columns per thread, on a sinogram that
+    starts 4 bytes past an allocation and with rows of zeros, against the oracle."""
+    rng = np.random.default_rng(8)
+    S, a = 2, 70
+    s = (rng.random((S, a, n_det)) + 0.3).astype(np.float32)
+    s[:, :, 17] *= 1.2
+    s[0, 5, :] = 0.0
+    base = torch.zeros(S * a * n_det + offset, dtype=torch.float32, device="cuda")
+    x = base[offset:].view(S, a, n_det)
+    x.copy_(torch.as_tensor(s))
+    G.ring_removal(x, 0.9, 20)
+    out = x.cpu().numpy()
+    for i in range(S):
+        assert ph.rel_l2(out[i], O.port_ring_removal(s[i], 0.9, 20)) < 2e-5
+
+
 def test_ring_removal_full_size_and_wide_rows():
     """A batch of 2048 x 1500 slices, and rows wider than the fused round kernel
     takes (separate update and column passes)."""
