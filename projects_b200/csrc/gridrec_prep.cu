@@ -294,19 +294,28 @@ __global__ void __launch_bounds__(kPrepThreads) shift_pad_kernel(
     for (int q = q0 + threadIdx.x; q < n_det; q += blockDim.x) srow[q] = __ldg(&r[q]);
     __syncthreads();
   }
+  // Integer-valued floats below 2^24 are exact, so (float)k is kept as a float
+  // counter clamped in float, and (float)nk, (float)(nk + 1) are floor(kk) and
+  // floor(kk) + 1 (the sum rounds like the int-to-float conversion of nk + 1):
+  // the same bits as the reference's expressions with two conversions per output
+  // instead of five (the conversion pipe bounded this kernel).
+  const int lim = 2 * pad + n_det;
+  const float fmax_k = (float)(n_det - 1), fstep = (float)blockDim.x;
+  float fkm = (float)((int)threadIdx.x - pad);  // (float)(kp - pad)
 #pragma unroll 4
-  for (int kp = threadIdx.x; kp < out_width; kp += blockDim.x) {
-    if (kp >= 2 * pad + n_det) {
+  for (int kp = threadIdx.x; kp < out_width; kp += blockDim.x, fkm += fstep) {
+    if (kp >= lim) {
       o[kp] = 0.f;
       continue;
     }
-    const int k = min(max(kp - pad, 0), n_det - 1);
-    const float kk = __fsub_rn((float)k, x0);
-    const int nk = (int)floorf(kk);
+    const float fk = fminf(fmaxf(fkm, 0.f), fmax_k);  // (float)min(max(kp - pad, 0), n_det - 1)
+    const float kk = __fsub_rn(fk, x0);
+    const float fl = floorf(kk);
+    const int nk = (int)fl;
     const int a = min(max(nk, 0), n_det - 1);
     const int b = min(max(nk + 1, 0), n_det - 1);
-    const float wa = __fsub_rn((float)(nk + 1), kk);
-    const float wb = __fsub_rn(kk, (float)nk);
+    const float wa = __fsub_rn(__fadd_rn(fl, 1.f), kk);
+    const float wb = __fsub_rn(kk, fl);
     const float va = kStaged ? srow[a] : __ldg(&r[a]);
     const float vb = kStaged ? srow[b] : __ldg(&r[b]);
     o[kp] = __fadd_rn(__fmul_rn(va, wa), __fmul_rn(vb, wb));
